@@ -1,0 +1,103 @@
+"""ctypes binding of libamgt_b200.so (the C ABI in include/amgt_b200.h).
+
+Loading fails loudly when the library is missing: there is no CPU or
+pure-PyTorch fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libamgt_b200.so")
+
+AMGT_OK = 0
+STATUS = {0: "AMGT_OK", 1: "AMGT_ERR_INVALID", 2: "AMGT_ERR_ALLOC", 3: "AMGT_ERR_CUDA", 4: "AMGT_ERR_DEVICE",
+          5: "AMGT_ERR_UNSUPPORTED", 6: "AMGT_ERR_NO_DEVICE"}
+DOUBLE, FLOAT, HALF, BF16 = 0, 1, 2, 3
+
+c_int, c_double, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+P = ctypes.POINTER
+
+
+class AmgtCsr(ctypes.Structure):
+    _fields_ = [("num_rows", c_int), ("num_cols", c_int), ("num_nonzeros", c_int),
+                ("i", c_void_p), ("j", c_void_p), ("data", c_void_p)]
+
+
+class AmgtBsr(ctypes.Structure):
+    _fields_ = [("row", c_int), ("col", c_int), ("nnz", c_int), ("blc_row", c_int), ("blc_col", c_int),
+                ("blc_num", c_int), ("stand", c_double), ("avg_nnz", c_double),
+                ("blcPtr", c_void_p), ("blcIdx", c_void_p), ("blcVal", c_void_p), ("blcMap", c_void_p),
+                ("warpnum", c_int), ("rowPtrbyWarp", c_void_p), ("rowIdxbyWarp", c_void_p),
+                ("blcVal_fp32", c_void_p), ("blcVal_fp16", c_void_p), ("blcVal_bf16", c_void_p),
+                ("max_blc_per_row", c_int), ("csr_nnz", c_int)]
+
+
+class AmgtVector(ctypes.Structure):
+    _fields_ = [("data", c_void_p), ("size", c_int), ("num_vectors", c_int), ("vecstride", c_int)]
+
+
+class AmgtCSRMatrix(ctypes.Structure):
+    _fields_ = [("coasen_level", c_int), ("bsr_spmv_balanced_tag", ctypes.c_char), ("bsr_tag", ctypes.c_char),
+                ("mixed_precision_flag", ctypes.c_char), ("owns_data", ctypes.c_char),
+                ("bsr_mat", P(AmgtBsr)), ("bsr_mat_T", P(AmgtBsr)), ("csr", AmgtCsr)]
+
+
+# name -> (restype, argtypes); every symbol include/amgt_b200.h declares
+SIGNATURES = {
+    "amgt_status_string": (ctypes.c_char_p, [c_int]),
+    "amgt_init": (c_int, []),
+    "amgt_kernel_launch_count": (ctypes.c_uint64, []),
+    "amgt_set_allocator": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "amgt_precision_for_level": (c_int, [c_int]),
+    "amgt_set_level_policy": (c_int, [P(c_int), c_int]),
+    "amgt_csr_to_bsr": (c_int, [P(AmgtCsr), P(AmgtBsr), c_void_p]),
+    "amgt_bsr_to_csr": (c_int, [P(AmgtBsr), P(AmgtCsr), c_void_p]),
+    "amgt_bsr_balance": (c_int, [P(AmgtBsr), c_void_p]),
+    "amgt_bsr_make_shadow": (c_int, [P(AmgtBsr), c_int, c_void_p]),
+    "amgt_bsr_transpose": (c_int, [P(AmgtBsr), P(AmgtBsr), c_void_p]),
+    "amgt_bsr_free": (c_int, [P(AmgtBsr), c_void_p]),
+    "amgt_csr_free": (c_int, [P(AmgtCsr), c_void_p]),
+    "amgt_spmv": (c_int, [c_int, c_double, P(AmgtBsr), c_void_p, c_double, c_void_p, c_void_p]),
+    "amgt_spmm": (c_int, [c_int, c_double, P(AmgtBsr), c_int, c_void_p, c_int, c_double, c_void_p, c_int, c_void_p]),
+    "amgt_spgemm": (c_int, [c_int, P(AmgtBsr), P(AmgtBsr), P(AmgtBsr), P(AmgtCsr), c_void_p]),
+    "amgt_CSRMatrixCreate": (P(AmgtCSRMatrix), [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int]),
+    "amgt_CSRMatrixDestroy": (c_int, [P(AmgtCSRMatrix)]),
+    "amgt_set_stream": (c_int, [c_void_p]),
+    "amgt_CSRSpGemm": (c_int, [P(AmgtCSRMatrix), P(AmgtCSRMatrix), P(P(AmgtCSRMatrix))]),
+    "amgt_CSRMatrixMatvec": (c_int, [c_int, c_double, P(AmgtCSRMatrix), P(AmgtVector), c_double, P(AmgtVector),
+                                     c_int]),
+}
+
+_lib = None
+
+
+class AmgtError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = "?"
+        if _lib is not None:
+            msg = _lib.amgt_status_string(status).decode()
+        super().__init__(f"{where} failed: {STATUS.get(status, status)} ({msg})")
+        self.status = status
+
+
+def lib():
+    """The loaded library (raises when libamgt_b200.so is absent)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m amgt_b200.build` "
+                              "(there is no fallback implementation)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int, where: str) -> None:
+    if status != AMGT_OK:
+        raise AmgtError(status, where)

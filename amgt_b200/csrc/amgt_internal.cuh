@@ -1,0 +1,156 @@
+// Internal helpers shared by the mBSR kernels (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "../../include/amgt_b200.h"
+
+namespace amgt {
+
+// ------------------------------------------------------------------ status
+#define AMGT_CUDA_TRY(expr)                                                   \
+    do {                                                                      \
+        cudaError_t _e = (expr);                                              \
+        if (_e != cudaSuccess) {                                              \
+            amgt::set_last_cuda_error(_e, #expr, __FILE__, __LINE__);         \
+            return AMGT_ERR_CUDA;                                             \
+        }                                                                     \
+    } while (0)
+
+#define AMGT_TRY(expr)                                                        \
+    do {                                                                      \
+        int _s = (expr);                                                      \
+        if (_s != AMGT_OK) return _s;                                         \
+    } while (0)
+
+void set_last_cuda_error(cudaError_t e, const char *what, const char *file, int line);
+
+// Every kernel launch of the library goes through this so that the launch
+// counter (amgt_kernel_launch_count) is exact.
+void count_launch();
+#define AMGT_LAUNCH(kernel, grid, block, smem, stream, ...)                   \
+    do {                                                                      \
+        amgt::count_launch();                                                 \
+        kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);           \
+        AMGT_CUDA_TRY(cudaGetLastError());                                    \
+    } while (0)
+
+// ------------------------------------------------------------- allocation
+void *dev_alloc(size_t bytes, cudaStream_t s);
+void dev_free(void *p, cudaStream_t s);
+
+template <typename T>
+int alloc_n(T **out, size_t n, cudaStream_t s)
+{
+    *out = nullptr;
+    if (n == 0) n = 1;  // keep a valid pointer for empty arrays
+    *out = static_cast<T *>(dev_alloc(n * sizeof(T), s));
+    return *out ? AMGT_OK : AMGT_ERR_ALLOC;
+}
+
+template <typename T>
+void free_ptr(T *&p, cudaStream_t s)
+{
+    if (p) dev_free((void *)p, s);
+    p = nullptr;
+}
+
+// Per-device state: a device error word that kernels raise instead of
+// trapping, and a pinned host staging buffer for the few scalars the host
+// must read back.
+struct DeviceState {
+    int *err;            // device: 0 = ok, else first error code raised
+    int64_t *pinned;     // host pinned, 16 slots
+    int sm_count;
+};
+int device_state(DeviceState **st);
+
+// Reads the device error word (synchronising the stream) and clears it.
+int check_device_error(cudaStream_t s);
+
+// Error codes a kernel may raise into DeviceState::err
+enum : int {
+    DEV_ERR_PROBE = 1,   // bounded probe / loop limit exceeded
+    DEV_ERR_INDEX = 2,   // index out of range in the input
+    DEV_ERR_CAPACITY = 3 // a per-row work buffer was too small
+};
+
+__device__ __forceinline__ void raise_error(int *err, int code)
+{
+    atomicCAS(err, 0, code);
+}
+
+// Longest block row and spread of block-row lengths (max_blc_per_row,
+// stand) of an mBSR matrix; one host read-back.
+int block_row_stats(amgt_bsr *A, cudaStream_t s);
+
+// Exclusive scan of n ints (in may equal out), CUB with allocator scratch.
+int exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s);
+// Exclusive scan of n 64-bit ints.
+int exclusive_scan_i64(const int64_t *in, int64_t *out, int n, cudaStream_t s);
+
+// Device-to-host read of `count` int64 slots into DeviceState::pinned and a
+// stream synchronize; returns pointer to the pinned slots.
+int read_back(const int64_t *dev, int count, cudaStream_t s, const int64_t **host);
+
+// ----------------------------------------------------------------- bitmaps
+// Boolean 4x4 product of two block bitmaps (bit r*4+c = entry (r, c)): OR
+// over k of column k of a (bits r*4+k) times row k of b (bits 4k..4k+3).
+__host__ __device__ __forceinline__ uint32_t bitmap_mul(uint32_t a, uint32_t b)
+{
+    uint32_t res = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        uint32_t colk = (a >> k) & 0x1111u;
+        uint32_t rowk = (b >> (4 * k)) & 0xFu;
+        res |= (colk * 0xFu) & (rowk * 0x1111u);
+    }
+    return res & 0xFFFFu;
+}
+
+// Transpose of a 4x4 block bitmap.
+__host__ __device__ __forceinline__ uint32_t bitmap_transpose(uint32_t m)
+{
+    uint32_t t = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            if (m & (1u << (4 * r + c))) t |= 1u << (4 * c + r);
+    return t;
+}
+
+constexpr unsigned FULL = 0xFFFFFFFFu;
+
+__device__ __forceinline__ int warp_excl_scan(int v, int lane, int *total)
+{
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += y;
+    }
+    *total = __shfl_sync(FULL, x, 31);
+    return x - v;
+}
+
+__device__ __forceinline__ int warp_sum(int v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+// Grid sizes: a multiple of the SM count, capped by the work.
+inline int grid_for(int units_per_cta, long long units, int sm_count, int ctas_per_sm = 8)
+{
+    long long need = (units + units_per_cta - 1) / units_per_cta;
+    long long cap = (long long)sm_count * ctas_per_sm;
+    if (need < 1) need = 1;
+    return (int)(need < cap ? need : cap);
+}
+
+}  // namespace amgt

@@ -1,0 +1,761 @@
+// CSR <-> mBSR conversions, block transpose, value shadows and the
+// long-row segment table.
+//
+// CSR -> mBSR (replaces CSR2BSR_GPU and its csr2bsr_* kernels,
+// AmgT_HYPRE/src/seq_mv/csr_matvec_device.c:683-1267).  One warp owns one
+// block row (4 CSR rows).  Its entries become (block column, bit) pairs that
+// are sorted in registers (<= 32 entries) or in the warp's shared-memory
+// slice (<= 512 entries); block rows with more entries go to a CTA that
+// sweeps the block-column range in windows of 8192 with a shared-memory
+// bitmap table.  Two passes: count (sizes the arrays, one host read-back),
+// then fill (block columns, bitmaps, zero-padded values).
+#include <cub/device/device_radix_sort.cuh>
+
+#include "rowunion.cuh"
+
+namespace amgt {
+
+constexpr int kWarpCap = 512;   // entries a warp sorts in shared memory
+constexpr int kCvtWarps = 4;    // warps per CTA in the warp paths
+constexpr int kWin = 8192;      // key window of the large-row path
+constexpr int kLargeThreads = 256;
+
+__device__ __forceinline__ unsigned lanemask_le(int lane) { return (lane == 31) ? FULL : ((2u << lane) - 1u); }
+
+// Entry p of block row b -> packed (block column, local index, bit).
+__device__ __forceinline__ unsigned long long csr_entry_pair(const int *ja, int p, int p0, int q_of_p, int n,
+                                                             int *err)
+{
+    const int col = ja[p];
+    if (col < 0 || col >= n) {
+        raise_error(err, DEV_ERR_INDEX);
+        return kSentinel;
+    }
+    return pack_pair(col >> 2, p - p0, 1u << (q_of_p * 4 + (col & 3)));
+}
+
+// Which of the block row's CSR rows holds entry p (rows r0..r0+3).
+__device__ __forceinline__ int row_in_block(int p, int e1, int e2, int e3)
+{
+    return (p >= e1) + (p >= e2) + (p >= e3);
+}
+
+struct BlockRowRange {
+    int p0, p1, e1, e2, e3;
+};
+
+__device__ __forceinline__ BlockRowRange block_row_range(const int *ia, int m, int b)
+{
+    const int r0 = 4 * b;
+    BlockRowRange r;
+    r.p0 = ia[r0];
+    r.e1 = ia[min(r0 + 1, m)];
+    r.e2 = ia[min(r0 + 2, m)];
+    r.e3 = ia[min(r0 + 3, m)];
+    r.p1 = ia[min(r0 + 4, m)];
+    return r;
+}
+
+// ------------------------------------------------------------ count pass
+__global__ void __launch_bounds__(32 * kCvtWarps)
+csr2bsr_count_kernel(int m, int n, const int *__restrict__ ia, const int *__restrict__ ja, int brow,
+                     int *__restrict__ cnt, int *__restrict__ large, int64_t *__restrict__ stats, int *err)
+{
+    __shared__ unsigned long long sbuf[kCvtWarps][kWarpCap];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned long long *s = sbuf[warp];
+    for (int b = blockIdx.x * kCvtWarps + warp; b < brow; b += gridDim.x * kCvtWarps) {
+        const BlockRowRange R = block_row_range(ia, m, b);
+        const int L = R.p1 - R.p0;
+        if (L > kWarpCap) {
+            if (lane == 0) large[atomicAdd((int *)&stats[3], 1)] = b;
+            continue;
+        }
+        int u = 0;
+        if (L <= 32) {
+            unsigned long long v = kSentinel;
+            if (lane < L) {
+                const int p = R.p0 + lane;
+                v = csr_entry_pair(ja, p, R.p0, row_in_block(p, R.e1, R.e2, R.e3), n, err);
+            }
+            v = warp_sort32(v, lane);
+            uint32_t orv;
+            bool head = warp_runs32(v, lane, &orv);
+            u = __popc(__ballot_sync(FULL, head));
+        } else {
+            const int N = next_pow2_min64(L);
+            for (int i = lane; i < N; i += 32) {
+                unsigned long long v = kSentinel;
+                if (i < L) {
+                    const int p = R.p0 + i;
+                    v = csr_entry_pair(ja, p, R.p0, row_in_block(p, R.e1, R.e2, R.e3), n, err);
+                }
+                s[i] = v;
+            }
+            __syncwarp();
+            warp_sort_smem(s, N, lane);
+            for (int i0 = 0; i0 < L; i0 += 32) {
+                const int i = i0 + lane;
+                bool head = false;
+                if (i < L && s[i] != kSentinel) head = (i == 0) || pair_key(s[i]) != pair_key(s[i - 1]);
+                u += __popc(__ballot_sync(FULL, head));
+            }
+            __syncwarp();
+        }
+        if (lane == 0) {
+            cnt[b] = u;
+            atomicMax((unsigned long long *)&stats[0], (unsigned long long)u);
+            atomicAdd((unsigned long long *)&stats[1], (unsigned long long)u * (unsigned long long)u);
+        }
+    }
+}
+
+// Block-wide min / max of the block columns of a long block row.
+__device__ void large_row_key_range(const int *ja, int p0, int p1, int n, int *smin, int *smax, int *kmin,
+                                    int *kmax)
+{
+    if (threadIdx.x == 0) {
+        *smin = 0x7FFFFFFF;
+        *smax = -1;
+    }
+    __syncthreads();
+    int lo = 0x7FFFFFFF, hi = -1;
+    for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+        int col = ja[p];
+        if (col < 0 || col >= n) continue;
+        lo = min(lo, col >> 2);
+        hi = max(hi, col >> 2);
+    }
+    atomicMin(smin, lo);
+    atomicMax(smax, hi);
+    __syncthreads();
+    *kmin = *smin;
+    *kmax = *smax;
+    __syncthreads();
+}
+
+// Block-wide exclusive scan of one int per thread (blockDim.x == 256).
+__device__ int block_excl_scan256(int v, int *sh, int *total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int wt;
+    int x = warp_excl_scan(v, lane, &wt);
+    if (lane == 0) sh[warp] = wt;
+    __syncthreads();
+    if (warp == 0) {
+        int t = (lane < 8) ? sh[lane] : 0, tt;
+        int e = warp_excl_scan(t, lane, &tt);
+        if (lane < 8) sh[lane] = e;
+        if (lane == 0) sh[8] = tt;
+    }
+    __syncthreads();
+    x += sh[warp];
+    *total = sh[8];
+    __syncthreads();
+    return x;
+}
+
+// Large block rows: window sweep with a shared-memory bitmap table.
+// fill == false: count.  fill == true: write columns, bitmaps and values.
+template <bool FILL>
+__global__ void __launch_bounds__(kLargeThreads)
+csr2bsr_large_kernel(int m, int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                     const double *__restrict__ a, const int *__restrict__ large, const int64_t *stats,
+                     int *__restrict__ cnt, const int *__restrict__ bptr, int *__restrict__ bidx,
+                     uint16_t *__restrict__ bmap, double *__restrict__ bval, int64_t *stats_out)
+{
+    extern __shared__ uint32_t smem[];
+    uint32_t *maps = smem;                      // [kWin]
+    int *pos = (int *)(smem + kWin);            // [kWin] (fill only)
+    __shared__ int sh[16];
+    __shared__ int smin, smax;
+    const int nlarge = (int)stats[3];
+    const int tid = threadIdx.x;
+    for (int t = blockIdx.x; t < nlarge; t += gridDim.x) {
+        const int b = large[t];
+        const BlockRowRange R = block_row_range(ia, m, b);
+        int kmin, kmax;
+        large_row_key_range(ja, R.p0, R.p1, n, &smin, &smax, &kmin, &kmax);
+        int total = 0;
+        const int base = FILL ? bptr[b] : 0;
+        for (long long w0 = kmin; w0 <= kmax; w0 += kWin) {
+            for (int i = tid; i < kWin; i += blockDim.x) maps[i] = 0;
+            __syncthreads();
+            for (int p = R.p0 + tid; p < R.p1; p += blockDim.x) {
+                const int col = ja[p];
+                if (col < 0 || col >= n) continue;
+                const long long k = (col >> 2) - w0;
+                if (k < 0 || k >= kWin) continue;
+                const int q = row_in_block(p, R.e1, R.e2, R.e3);
+                atomicOr(&maps[k], 1u << (q * 4 + (col & 3)));
+            }
+            __syncthreads();
+            // each thread owns 32 consecutive slots
+            const int s0 = tid * (kWin / kLargeThreads);
+            int c = 0;
+            for (int i = 0; i < kWin / kLargeThreads; ++i) c += maps[s0 + i] != 0;
+            int wtotal;
+            int off = block_excl_scan256(c, sh, &wtotal);
+            if (FILL) {
+                int o = base + total + off;
+                for (int i = 0; i < kWin / kLargeThreads; ++i) {
+                    const uint32_t mp = maps[s0 + i];
+                    if (mp) {
+                        pos[s0 + i] = o;
+                        bidx[o] = (int)(w0 + s0 + i);
+                        bmap[o] = (uint16_t)mp;
+                        ++o;
+                    }
+                }
+                // zero this window's blocks, then scatter its entries
+                double2 *z = reinterpret_cast<double2 *>(bval + (size_t)16 * (base + total));
+                for (int i = tid; i < 8 * wtotal; i += blockDim.x) z[i] = make_double2(0.0, 0.0);
+                __syncthreads();
+                for (int p = R.p0 + tid; p < R.p1; p += blockDim.x) {
+                    const int col = ja[p];
+                    if (col < 0 || col >= n) continue;
+                    const long long k = (col >> 2) - w0;
+                    if (k < 0 || k >= kWin) continue;
+                    const int q = row_in_block(p, R.e1, R.e2, R.e3);
+                    bval[(size_t)16 * pos[k] + q * 4 + (col & 3)] = a[p];
+                }
+            }
+            total += wtotal;
+            __syncthreads();
+        }
+        if (!FILL && tid == 0) {
+            cnt[b] = total;
+            atomicMax((unsigned long long *)&stats_out[0], (unsigned long long)total);
+            atomicAdd((unsigned long long *)&stats_out[1], (unsigned long long)total * (unsigned long long)total);
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------- fill pass
+__global__ void __launch_bounds__(32 * kCvtWarps)
+csr2bsr_fill_kernel(int m, int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                    const double *__restrict__ a, int brow, const int *__restrict__ bptr, int *__restrict__ bidx,
+                    uint16_t *__restrict__ bmap, double *__restrict__ bval, int *err)
+{
+    __shared__ unsigned long long sbuf[kCvtWarps][kWarpCap];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned long long *s = sbuf[warp];
+    for (int b = blockIdx.x * kCvtWarps + warp; b < brow; b += gridDim.x * kCvtWarps) {
+        const BlockRowRange R = block_row_range(ia, m, b);
+        const int L = R.p1 - R.p0;
+        if (L > kWarpCap) continue;  // large-row kernel
+        const int base = bptr[b], u = bptr[b + 1] - base;
+        double2 *z = reinterpret_cast<double2 *>(bval + (size_t)16 * base);
+        for (int i = lane; i < 8 * u; i += 32) z[i] = make_double2(0.0, 0.0);
+        __syncwarp();
+        if (L <= 32) {
+            unsigned long long v = kSentinel;
+            if (lane < L) {
+                const int p = R.p0 + lane;
+                v = csr_entry_pair(ja, p, R.p0, row_in_block(p, R.e1, R.e2, R.e3), n, err);
+            }
+            v = warp_sort32(v, lane);
+            uint32_t orv;
+            const bool head = warp_runs32(v, lane, &orv);
+            const unsigned hb = __ballot_sync(FULL, head);
+            const int slot = __popc(hb & lanemask_le(lane)) - 1;
+            if (v != kSentinel) {
+                if (head) {
+                    bidx[base + slot] = pair_key(v);
+                    bmap[base + slot] = (uint16_t)orv;
+                }
+                const int bit = __ffs(pair_map(v)) - 1;
+                bval[(size_t)16 * (base + slot) + bit] = a[R.p0 + pair_tag(v)];
+            }
+        } else {
+            const int N = next_pow2_min64(L);
+            for (int i = lane; i < N; i += 32) {
+                unsigned long long v = kSentinel;
+                if (i < L) {
+                    const int p = R.p0 + i;
+                    v = csr_entry_pair(ja, p, R.p0, row_in_block(p, R.e1, R.e2, R.e3), n, err);
+                }
+                s[i] = v;
+            }
+            __syncwarp();
+            warp_sort_smem(s, N, lane);
+            int running = 0;
+            for (int i0 = 0; i0 < L; i0 += 32) {
+                const int i = i0 + lane;
+                const unsigned long long v = (i < L) ? s[i] : kSentinel;
+                bool head = false;
+                if (v != kSentinel) head = (i == 0) || pair_key(v) != pair_key(s[i - 1]);
+                const unsigned hb = __ballot_sync(FULL, head);
+                const int slot = running + __popc(hb & lanemask_le(lane)) - 1;
+                if (v != kSentinel) {
+                    if (head) {
+                        uint32_t orv = 0;
+                        const int key = pair_key(v);
+                        for (int j = i; j < L && s[j] != kSentinel && pair_key(s[j]) == key; ++j) orv |= pair_map(s[j]);
+                        bidx[base + slot] = key;
+                        bmap[base + slot] = (uint16_t)orv;
+                    }
+                    const int bit = __ffs(pair_map(v)) - 1;
+                    bval[(size_t)16 * (base + slot) + bit] = a[R.p0 + pair_tag(v)];
+                }
+                running += __popc(hb);
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// --------------------------------------------------------- mBSR -> CSR
+// Row counts: popcount of nibble q of every bitmap of block row b.
+__global__ void bsr2csr_count_kernel(int m, int brow, const int *__restrict__ bptr,
+                                     const uint16_t *__restrict__ bmap, int *__restrict__ rowcnt)
+{
+    const int lane = threadIdx.x & 31;
+    const int wpc = blockDim.x >> 5;
+    for (int b = blockIdx.x * wpc + (threadIdx.x >> 5); b < brow; b += gridDim.x * wpc) {
+        int c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+        for (int k = bptr[b] + lane; k < bptr[b + 1]; k += 32) {
+            const uint32_t mp = bmap[k];
+            c0 += __popc(mp & 0xFu);
+            c1 += __popc(mp & 0xF0u);
+            c2 += __popc(mp & 0xF00u);
+            c3 += __popc(mp & 0xF000u);
+        }
+        c0 = warp_sum(c0); c1 = warp_sum(c1); c2 = warp_sum(c2); c3 = warp_sum(c3);
+        if (lane < 4) {
+            const int r = 4 * b + lane;
+            const int c = lane == 0 ? c0 : lane == 1 ? c1 : lane == 2 ? c2 : c3;
+            if (r < m) rowcnt[r] = c;
+        }
+    }
+}
+
+// Emission: for each CSR row of the block row, walk the blocks 32 at a time,
+// one block per lane, and place the nibble's set bits with a warp scan.
+__global__ void bsr2csr_fill_kernel(int m, int brow, const int *__restrict__ bptr, const int *__restrict__ bidx,
+                                    const uint16_t *__restrict__ bmap, const double *__restrict__ bval,
+                                    const int *__restrict__ ia, int *__restrict__ ja, double *__restrict__ a)
+{
+    const int lane = threadIdx.x & 31;
+    const int wpc = blockDim.x >> 5;
+    for (int b = blockIdx.x * wpc + (threadIdx.x >> 5); b < brow; b += gridDim.x * wpc) {
+        const int k0 = bptr[b], k1 = bptr[b + 1];
+        for (int q = 0; q < 4 && 4 * b + q < m; ++q) {
+            int out = ia[4 * b + q];
+            for (int kk = k0; kk < k1; kk += 32) {
+                const int k = kk + lane;
+                uint32_t nib = 0;
+                int col0 = 0;
+                if (k < k1) {
+                    nib = (bmap[k] >> (4 * q)) & 0xFu;
+                    col0 = 4 * bidx[k];
+                }
+                int tot;
+                int off = warp_excl_scan(__popc(nib), lane, &tot);
+                if (nib) {
+                    const double *v = bval + (size_t)16 * k + 4 * q;
+                    int o = out + off;
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        if (nib & (1u << c)) {
+                            ja[o] = col0 + c;
+                            a[o] = v[c];
+                            ++o;
+                        }
+                }
+                out += tot;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------ segment table
+// Long block rows are cut into segments of at most 64 blocks
+// (get_rowPtrbyWarp / get_rowIdxbyWarp, csr_matvec_device.c:615-637).
+constexpr int kSegmentBlocks = 64;
+
+__global__ void seg_count_kernel(int brow, const int *__restrict__ bptr, int *__restrict__ segcnt)
+{
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < brow; b += gridDim.x * blockDim.x) {
+        const int len = bptr[b + 1] - bptr[b];
+        segcnt[b] = (len + kSegmentBlocks - 1) / kSegmentBlocks;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) segcnt[brow] = 0;
+}
+
+__global__ void seg_fill_kernel(int brow, const int *__restrict__ segptr, int *__restrict__ segrow)
+{
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < brow; b += gridDim.x * blockDim.x)
+        for (int s = segptr[b]; s < segptr[b + 1]; ++s) segrow[s] = b;
+}
+
+// ------------------------------------------------------------ shadows
+template <int PREC>
+__global__ void shadow_kernel(long long n, const double *__restrict__ v, void *__restrict__ out)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double d = v[i];
+        if (PREC == AMGT_FLOAT) static_cast<float *>(out)[i] = __double2float_rn(d);
+        else if (PREC == AMGT_HALF) static_cast<__half *>(out)[i] = __double2half(d);
+        else static_cast<__nv_bfloat16 *>(out)[i] = __double2bfloat16(d);
+    }
+}
+
+// ------------------------------------------------- block-row statistics
+// out[0] = longest block row (max), out[1] = sum of squared lengths.
+__global__ void row_stats_kernel(int brow, const int *__restrict__ bptr, int64_t *__restrict__ out)
+{
+    long long mx = 0, s2 = 0;
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < brow; b += gridDim.x * blockDim.x) {
+        const long long len = bptr[b + 1] - bptr[b];
+        mx = len > mx ? len : mx;
+        s2 += len * len;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        long long om = __shfl_xor_sync(FULL, mx, o);
+        mx = om > mx ? om : mx;
+        s2 += __shfl_xor_sync(FULL, s2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax((unsigned long long *)&out[0], (unsigned long long)mx);
+        atomicAdd((unsigned long long *)&out[1], (unsigned long long)s2);
+    }
+}
+
+int block_row_stats(amgt_bsr *A, cudaStream_t s)
+{
+    DeviceState *st;
+    AMGT_TRY(device_state(&st));
+    int64_t *d = nullptr;
+    AMGT_TRY(alloc_n(&d, 2, s));
+    AMGT_CUDA_TRY(cudaMemsetAsync(d, 0, sizeof(int64_t) * 2, s));
+    if (A->blc_row > 0)
+        AMGT_LAUNCH(row_stats_kernel, grid_for(256, A->blc_row, st->sm_count, 4), 256, 0, s, A->blc_row, A->blcPtr, d);
+    const int64_t *h = nullptr;
+    int rc = read_back(d, 2, s, &h);
+    free_ptr(d, s);
+    if (rc) return rc;
+    A->max_blc_per_row = (int)h[0];
+    const double brow = A->blc_row, avg = brow > 0 ? A->blc_num / brow : 0.0;
+    const double var = brow > 0 ? (double)h[1] / brow - avg * avg : 0.0;
+    A->stand = var > 0 ? sqrt(var) : 0.0;
+    return AMGT_OK;
+}
+
+// ---------------------------------------------------------- transpose
+__global__ void row_of_block_kernel(int brow, const int *__restrict__ bptr, int *__restrict__ rowid,
+                                    int *__restrict__ iota)
+{
+    const int lane = threadIdx.x & 31;
+    const int wpc = blockDim.x >> 5;
+    for (int b = blockIdx.x * wpc + (threadIdx.x >> 5); b < brow; b += gridDim.x * wpc)
+        for (int k = bptr[b] + lane; k < bptr[b + 1]; k += 32) {
+            rowid[k] = b;
+            iota[k] = k;
+        }
+}
+
+__global__ void col_hist_kernel(int nblk, const int *__restrict__ bidx, int *__restrict__ hist)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nblk; k += gridDim.x * blockDim.x)
+        atomicAdd(&hist[bidx[k]], 1);
+}
+
+// out block d takes source block src[d]: row -> column, values transposed.
+__global__ void transpose_gather_kernel(int nblk, const int *__restrict__ src, const int *__restrict__ rowid,
+                                        const uint16_t *__restrict__ amap, const double *__restrict__ aval,
+                                        int *__restrict__ tidx, uint16_t *__restrict__ tmap,
+                                        double *__restrict__ tval)
+{
+    // 16 threads per block: thread e writes entry e of the transposed block
+    const long long total = (long long)nblk * 16;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int d = (int)(t >> 4), e = (int)(t & 15);
+        const int sidx = src[d];
+        const int r = e >> 2, c = e & 3;  // entry (r, c) of the transpose = (c, r) of the source
+        tval[t] = aval[(size_t)16 * sidx + 4 * c + r];
+        if (e == 0) {
+            tidx[d] = rowid[sidx];
+            tmap[d] = (uint16_t)bitmap_transpose(amap[sidx]);
+        }
+    }
+}
+
+}  // namespace amgt
+
+using namespace amgt;
+
+static int csr_valid(const amgt_csr *A)
+{
+    if (!A || A->num_rows < 0 || A->num_cols < 0 || A->num_nonzeros < 0) return 0;
+    if (A->num_rows > 0 && !A->i) return 0;
+    if (A->num_nonzeros > 0 && (!A->j || !A->data)) return 0;
+    return 1;
+}
+
+extern "C" {
+
+int amgt_bsr_free(amgt_bsr *A, amgt_stream_t stream)
+{
+    if (!A) return AMGT_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    free_ptr(A->blcPtr, s);
+    free_ptr(A->blcIdx, s);
+    free_ptr(A->blcVal, s);
+    free_ptr(A->blcMap, s);
+    free_ptr(A->rowPtrbyWarp, s);
+    free_ptr(A->rowIdxbyWarp, s);
+    free_ptr(A->blcVal_fp32, s);
+    free_ptr(A->blcVal_fp16, s);
+    free_ptr(A->blcVal_bf16, s);
+    memset(A, 0, sizeof(*A));
+    return AMGT_OK;
+}
+
+int amgt_csr_free(amgt_csr *A, amgt_stream_t stream)
+{
+    if (!A) return AMGT_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    free_ptr(A->i, s);
+    free_ptr(A->j, s);
+    free_ptr(A->data, s);
+    memset(A, 0, sizeof(*A));
+    return AMGT_OK;
+}
+
+int amgt_csr_to_bsr(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream)
+{
+    if (!csr_valid(A) || !out) return AMGT_ERR_INVALID;
+    DeviceState *st;
+    AMGT_TRY(device_state(&st));
+    cudaStream_t s = (cudaStream_t)stream;
+    const int m = A->num_rows, n = A->num_cols;
+    const int brow = (m + 3) / 4;
+    memset(out, 0, sizeof(*out));
+    out->row = m;
+    out->col = n;
+    out->blc_row = brow;
+    out->blc_col = (n + 3) / 4;
+
+    int *cnt = nullptr, *large = nullptr;
+    int64_t *stats = nullptr;
+    int rc = AMGT_OK;
+    const int64_t *h = nullptr;
+    int nb = 0;
+    static bool smem_set = false;
+    if (!smem_set) {
+        AMGT_CUDA_TRY(cudaFuncSetAttribute(csr2bsr_large_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           2 * kWin * (int)sizeof(uint32_t)));
+        AMGT_CUDA_TRY(cudaFuncSetAttribute(csr2bsr_large_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           2 * kWin * (int)sizeof(uint32_t)));
+        smem_set = true;
+    }
+    if ((rc = alloc_n(&out->blcPtr, brow + 1, s)) || (rc = alloc_n(&cnt, brow + 1, s)) ||
+        (rc = alloc_n(&large, brow, s)) || (rc = alloc_n(&stats, 4, s)))
+        goto fail;
+    AMGT_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(int64_t) * 4, s));
+    AMGT_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * (brow + 1), s));
+    if (brow > 0) {
+        AMGT_LAUNCH(csr2bsr_count_kernel, grid_for(kCvtWarps, brow, st->sm_count, 16), 32 * kCvtWarps, 0, s, m, n,
+                    A->i, A->j, brow, cnt, large, stats, st->err);
+        AMGT_LAUNCH(csr2bsr_large_kernel<false>, 2 * st->sm_count, kLargeThreads, 2 * kWin * sizeof(uint32_t), s,
+                    m, n, A->i, A->j, A->data, large, stats, cnt, nullptr, nullptr, nullptr, nullptr, stats);
+    }
+    if ((rc = exclusive_scan_int(cnt, out->blcPtr, brow + 1, s))) goto fail;
+    AMGT_CUDA_TRY(cudaMemcpyAsync(&stats[2], out->blcPtr + brow, sizeof(int), cudaMemcpyDeviceToDevice, s));
+    if ((rc = read_back(stats, 4, s, &h))) goto fail;
+    nb = (int)h[2];
+    out->max_blc_per_row = (int)h[0];
+    {
+        const double S2 = (double)h[1];
+        const double avg = brow ? (double)nb / brow : 0.0;
+        double var = brow ? S2 / brow - avg * avg : 0.0;
+        out->stand = var > 0 ? sqrt(var) : 0.0;
+    }
+    if ((rc = check_device_error(s))) goto fail;
+    out->blc_num = nb;
+    out->nnz = (int)(16LL * nb > 0x7FFFFFFF ? 0x7FFFFFFF : 16LL * nb);  // saturates
+    out->avg_nnz = nb ? (double)A->num_nonzeros / nb : 0.0;
+    out->csr_nnz = A->num_nonzeros;
+    if ((rc = alloc_n(&out->blcIdx, nb, s)) || (rc = alloc_n(&out->blcMap, nb, s)) ||
+        (rc = alloc_n(&out->blcVal, (size_t)16 * nb, s)))
+        goto fail;
+    if (brow > 0) {
+        AMGT_LAUNCH(csr2bsr_fill_kernel, grid_for(kCvtWarps, brow, st->sm_count, 16), 32 * kCvtWarps, 0, s, m, n,
+                    A->i, A->j, A->data, brow, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal, st->err);
+        AMGT_LAUNCH(csr2bsr_large_kernel<true>, 2 * st->sm_count, kLargeThreads, 2 * kWin * sizeof(uint32_t), s, m,
+                    n, A->i, A->j, A->data, large, stats, nullptr, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal,
+                    nullptr);
+    }
+    free_ptr(cnt, s);
+    free_ptr(large, s);
+    free_ptr(stats, s);
+    return AMGT_OK;
+fail:
+    free_ptr(cnt, s);
+    free_ptr(large, s);
+    free_ptr(stats, s);
+    amgt_bsr_free(out, stream);
+    return rc;
+}
+
+int amgt_bsr_to_csr(const amgt_bsr *A, amgt_csr *out, amgt_stream_t stream)
+{
+    if (!A || !out || A->row < 0 || (A->blc_row > 0 && !A->blcPtr)) return AMGT_ERR_INVALID;
+    DeviceState *st;
+    AMGT_TRY(device_state(&st));
+    cudaStream_t s = (cudaStream_t)stream;
+    const int m = A->row, brow = A->blc_row;
+    memset(out, 0, sizeof(*out));
+    out->num_rows = m;
+    out->num_cols = A->col;
+    int *cnt = nullptr;
+    int64_t *tot = nullptr;
+    const int64_t *h = nullptr;
+    int rc = AMGT_OK;
+    if ((rc = alloc_n(&out->i, m + 1, s)) || (rc = alloc_n(&cnt, m + 1, s)) || (rc = alloc_n(&tot, 1, s))) goto fail;
+    AMGT_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * (m + 1), s));
+    AMGT_CUDA_TRY(cudaMemsetAsync(tot, 0, sizeof(int64_t), s));
+    if (brow > 0)
+        AMGT_LAUNCH(bsr2csr_count_kernel, grid_for(8, brow, st->sm_count, 8), 256, 0, s, m, brow, A->blcPtr,
+                    A->blcMap, cnt);
+    if ((rc = exclusive_scan_int(cnt, out->i, m + 1, s))) goto fail;
+    AMGT_CUDA_TRY(cudaMemcpyAsync(tot, out->i + m, sizeof(int), cudaMemcpyDeviceToDevice, s));
+    if ((rc = read_back(tot, 1, s, &h))) goto fail;
+    out->num_nonzeros = (int)h[0];
+    if ((rc = alloc_n(&out->j, out->num_nonzeros, s)) || (rc = alloc_n(&out->data, out->num_nonzeros, s))) goto fail;
+    if (brow > 0)
+        AMGT_LAUNCH(bsr2csr_fill_kernel, grid_for(8, brow, st->sm_count, 8), 256, 0, s, m, brow, A->blcPtr, A->blcIdx,
+                    A->blcMap, A->blcVal, out->i, out->j, out->data);
+    free_ptr(cnt, s);
+    free_ptr(tot, s);
+    return AMGT_OK;
+fail:
+    free_ptr(cnt, s);
+    free_ptr(tot, s);
+    amgt_csr_free(out, stream);
+    return rc;
+}
+
+int amgt_bsr_balance(amgt_bsr *A, amgt_stream_t stream)
+{
+    if (!A || (A->blc_row > 0 && !A->blcPtr)) return AMGT_ERR_INVALID;
+    if (A->rowPtrbyWarp) return AMGT_OK;
+    DeviceState *st;
+    AMGT_TRY(device_state(&st));
+    cudaStream_t s = (cudaStream_t)stream;
+    const int brow = A->blc_row;
+    int *cnt = nullptr;
+    int64_t *tot = nullptr;
+    const int64_t *h = nullptr;
+    int rc = AMGT_OK;
+    if ((rc = alloc_n(&cnt, brow + 1, s)) || (rc = alloc_n(&A->rowPtrbyWarp, brow + 1, s)) ||
+        (rc = alloc_n(&tot, 1, s)))
+        goto fail;
+    AMGT_CUDA_TRY(cudaMemsetAsync(tot, 0, sizeof(int64_t), s));
+    AMGT_LAUNCH(seg_count_kernel, grid_for(256, brow + 1, st->sm_count, 8), 256, 0, s, brow, A->blcPtr, cnt);
+    if ((rc = exclusive_scan_int(cnt, A->rowPtrbyWarp, brow + 1, s))) goto fail;
+    AMGT_CUDA_TRY(cudaMemcpyAsync(tot, A->rowPtrbyWarp + brow, sizeof(int), cudaMemcpyDeviceToDevice, s));
+    if ((rc = read_back(tot, 1, s, &h))) goto fail;
+    A->warpnum = (int)h[0];
+    if ((rc = alloc_n(&A->rowIdxbyWarp, A->warpnum, s))) goto fail;
+    if (brow > 0)
+        AMGT_LAUNCH(seg_fill_kernel, grid_for(256, brow, st->sm_count, 8), 256, 0, s, brow, A->rowPtrbyWarp,
+                    A->rowIdxbyWarp);
+    free_ptr(cnt, s);
+    free_ptr(tot, s);
+    return AMGT_OK;
+fail:
+    free_ptr(cnt, s);
+    free_ptr(tot, s);
+    free_ptr(A->rowPtrbyWarp, s);
+    free_ptr(A->rowIdxbyWarp, s);
+    A->warpnum = 0;
+    return rc;
+}
+
+int amgt_bsr_make_shadow(amgt_bsr *A, int prec, amgt_stream_t stream)
+{
+    if (!A || (A->blc_num > 0 && !A->blcVal)) return AMGT_ERR_INVALID;
+    if (prec == AMGT_DOUBLE) return AMGT_OK;
+    DeviceState *st;
+    AMGT_TRY(device_state(&st));
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long n = 16LL * A->blc_num;
+    const int grid = grid_for(256 * 4, n, st->sm_count, 8);
+    switch (prec) {
+    case AMGT_FLOAT:
+        if (A->blcVal_fp32) return AMGT_OK;
+        AMGT_TRY(alloc_n(&A->blcVal_fp32, (size_t)n, s));
+        AMGT_LAUNCH(shadow_kernel<AMGT_FLOAT>, grid, 256, 0, s, n, A->blcVal, (void *)A->blcVal_fp32);
+        return AMGT_OK;
+    case AMGT_HALF:
+        if (A->blcVal_fp16) return AMGT_OK;
+        AMGT_TRY(alloc_n(&A->blcVal_fp16, (size_t)n, s));
+        AMGT_LAUNCH(shadow_kernel<AMGT_HALF>, grid, 256, 0, s, n, A->blcVal, (void *)A->blcVal_fp16);
+        return AMGT_OK;
+    case AMGT_BF16:
+        if (A->blcVal_bf16) return AMGT_OK;
+        AMGT_TRY(alloc_n(&A->blcVal_bf16, (size_t)n, s));
+        AMGT_LAUNCH(shadow_kernel<AMGT_BF16>, grid, 256, 0, s, n, A->blcVal, (void *)A->blcVal_bf16);
+        return AMGT_OK;
+    default:
+        return AMGT_ERR_INVALID;
+    }
+}
+
+int amgt_bsr_transpose(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream)
+{
+    if (!A || !out || (A->blc_row > 0 && !A->blcPtr)) return AMGT_ERR_INVALID;
+    DeviceState *st;
+    AMGT_TRY(device_state(&st));
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nb = A->blc_num, brow = A->blc_row, bcol = A->blc_col;
+    memset(out, 0, sizeof(*out));
+    out->row = A->col;
+    out->col = A->row;
+    out->blc_row = bcol;
+    out->blc_col = brow;
+    out->blc_num = nb;
+    out->nnz = (int)(16LL * nb > 0x7FFFFFFF ? 0x7FFFFFFF : 16LL * nb);  // saturates
+    out->csr_nnz = A->csr_nnz;
+    out->avg_nnz = A->avg_nnz;
+    int *rowid = nullptr, *iota = nullptr, *keys_in = nullptr, *keys_out = nullptr, *src = nullptr, *hist = nullptr;
+    void *tmp = nullptr;
+    size_t tmp_bytes = 0;
+    int rc = AMGT_OK;
+    int bits = 1;
+    while ((1 << bits) <= bcol) ++bits;
+    if ((rc = alloc_n(&out->blcPtr, bcol + 1, s)) || (rc = alloc_n(&out->blcIdx, nb, s)) ||
+        (rc = alloc_n(&out->blcMap, nb, s)) || (rc = alloc_n(&out->blcVal, (size_t)16 * nb, s)) ||
+        (rc = alloc_n(&rowid, nb, s)) || (rc = alloc_n(&iota, nb, s)) || (rc = alloc_n(&keys_out, nb, s)) ||
+        (rc = alloc_n(&src, nb, s)) || (rc = alloc_n(&hist, bcol + 1, s)))
+        goto fail;
+    keys_in = A->blcIdx;
+    AMGT_CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(int) * (bcol + 1), s));
+    if (nb > 0) {
+        AMGT_LAUNCH(row_of_block_kernel, grid_for(8, brow, st->sm_count, 8), 256, 0, s, brow, A->blcPtr, rowid, iota);
+        AMGT_LAUNCH(col_hist_kernel, grid_for(256, nb, st->sm_count, 8), 256, 0, s, nb, A->blcIdx, hist);
+        // stable radix sort by block column keeps block rows ascending inside each column
+        AMGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys_in, keys_out, iota, src, nb, 0, bits, s));
+        tmp = dev_alloc(tmp_bytes ? tmp_bytes : 16, s);
+        if (!tmp) { rc = AMGT_ERR_ALLOC; goto fail; }
+        count_launch();
+        AMGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys_in, keys_out, iota, src, nb, 0, bits, s));
+        AMGT_LAUNCH(transpose_gather_kernel, grid_for(256, 16LL * nb, st->sm_count, 8), 256, 0, s, nb, src, rowid,
+                    A->blcMap, A->blcVal, out->blcIdx, out->blcMap, out->blcVal);
+    }
+    if ((rc = exclusive_scan_int(hist, out->blcPtr, bcol + 1, s))) goto fail;
+    free_ptr(rowid, s); free_ptr(iota, s); free_ptr(keys_out, s); free_ptr(src, s); free_ptr(hist, s);
+    if (tmp) dev_free(tmp, s);
+    return block_row_stats(out, s);
+fail:
+    free_ptr(rowid, s); free_ptr(iota, s); free_ptr(keys_out, s); free_ptr(src, s); free_ptr(hist, s);
+    if (tmp) dev_free(tmp, s);
+    amgt_bsr_free(out, stream);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,607 @@
+// mBSR SpGEMM: C = A * B.
+//
+// Replaces spgemm_amgT_fp64 / _fp32 / _fp16 and the kernels compute_Cub_bin,
+// set_bin, symbolic_spgemm_step1/2 (+_large, _gl), numeric_spgemm_hybrid
+// (+_tf32, _f16) and bsr2csr_* (AmgT_HYPRE/src/seq_mv/csr_spgemm_device.c:
+// 82-1440, 1527-2578).
+//
+// Symbolic.  One warp owns one block row of A.  For each A block (row
+// order) the lanes walk the B row it selects; every B block whose bitmap
+// product with the A block is non-zero (bitMatrixMul, :189-205) becomes a
+// (B block column, product bitmap) pair, appended to the warp's shared
+// memory list.  The list is sorted (registers when <= 32 pairs, shared
+// memory bitonic sort when <= 1024) and equal columns are merged with an OR
+// of their bitmaps: that is C's block pattern and C's bitmap, bit for bit.
+// Rows with more than 1024 pairs go to a CTA that sweeps the column range
+// in windows of 8192 with a shared-memory bitmap table.  Pass 1 counts
+// blocks and CSR nonzeros per row (one host read-back sizes C), pass 2
+// writes C's block columns and bitmaps in place.
+//
+// Numeric.  One warp per C block row accumulates the row's C blocks in
+// shared memory (global memory for rows of more than 64 blocks).  A blocks
+// are taken in row order; per A block the two half-warps take two B blocks
+// at a time, lane e of a half computing entry e = (r, c) of the 4x4 product
+// as the sum over k ascending of a[r][k] * b[k][c] over terms whose A and B
+// bits are set, started from zero, with separate multiply and add (no FMA),
+// and adding it to C(r, c) where the product bitmap has the bit - the
+// arithmetic of the reference's scalar branch (:1289-1339), so the fp64
+// result equals the CPU oracle bit for bit.  C's position is a binary
+// search of the sorted C row.  FP64 arithmetic on the CUDA cores: the 4x4
+// products are too small for tcgen05 (M >= 64), and on B200 the fp64 MMA
+// rate equals the fp64 FMA rate.  The CSR form of C is written by the same
+// kernel (no separate BSR2CSR pass).
+#include "rowunion.cuh"
+
+namespace amgt {
+
+constexpr int kSymWarps = 4;
+constexpr int kSymCap = 1024;     // pairs a warp sorts in shared memory
+constexpr int kSymWin = 8192;     // key window of the large-row path
+constexpr int kSymLargeThreads = 256;
+constexpr int kNumWarps = 4;
+constexpr int kNumCap = 64;       // C blocks a warp accumulates in shared memory
+
+__device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
+
+// Appends the row's non-zero-product pairs to the warp's list s[]; returns
+// the count (> cap only on overflow, which the caller prevents via ub).
+__device__ __forceinline__ int sym_collect(int lane, int a0, int a1, const int *__restrict__ aidx,
+                                           const uint16_t *__restrict__ amap, const int *__restrict__ bptr,
+                                           const int *__restrict__ bidx, const uint16_t *__restrict__ bmap,
+                                           unsigned long long *s)
+{
+    int cnt = 0;
+    for (int i = a0; i < a1; ++i) {
+        const int k = aidx[i];
+        const uint32_t ma = amap[i];
+        const int j0 = bptr[k], j1 = bptr[k + 1];
+        for (int jj = j0; jj < j1; jj += 32) {
+            const int j = jj + lane;
+            uint32_t mc = 0;
+            int key = 0;
+            if (j < j1) {
+                mc = bitmap_mul(ma, bmap[j]);
+                key = bidx[j];
+            }
+            const unsigned bal = __ballot_sync(FULL, mc != 0);
+            if (mc) s[cnt + __popc(bal & lanemask_lt(lane))] = pack_pair(key, 0, mc);
+            cnt += __popc(bal);
+        }
+    }
+    __syncwarp();
+    return cnt;
+}
+
+// Upper bound of the row's pairs: sum of the selected B row lengths.
+__device__ __forceinline__ long long sym_upper_bound(int lane, int a0, int a1, const int *__restrict__ aidx,
+                                                     const int *__restrict__ bptr)
+{
+    long long ub = 0;
+    for (int i = a0 + lane; i < a1; i += 32) {
+        const int k = aidx[i];
+        ub += bptr[k + 1] - bptr[k];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ub += __shfl_xor_sync(FULL, ub, o);
+    return ub;
+}
+
+// Sorted distinct keys with OR-ed bitmaps of the warp's list s[0..cnt).
+// FILL writes them to cidx/cmap; always returns the distinct count and the
+// per-scalar-row CSR counts (popcount of each bitmap nibble).
+template <bool FILL>
+__device__ __forceinline__ int sym_reduce(int lane, int cnt, unsigned long long *s, int *__restrict__ cidx,
+                                          uint16_t *__restrict__ cmap, int csr[4])
+{
+    csr[0] = csr[1] = csr[2] = csr[3] = 0;
+    int u = 0;
+    if (cnt <= 32) {
+        unsigned long long v = (lane < cnt) ? s[lane] : kSentinel;
+        __syncwarp();
+        v = warp_sort32(v, lane);
+        uint32_t orv;
+        const bool head = warp_runs32(v, lane, &orv);
+        const unsigned hb = __ballot_sync(FULL, head);
+        u = __popc(hb);
+        if (head) {
+            const int slot = __popc(hb & lanemask_lt(lane));
+            if (FILL) {
+                cidx[slot] = pair_key(v);
+                cmap[slot] = (uint16_t)orv;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) csr[q] = __popc((orv >> (4 * q)) & 0xFu);
+        }
+    } else {
+        const int N = next_pow2_min64(cnt);
+        for (int i = cnt + lane; i < N; i += 32) s[i] = kSentinel;
+        __syncwarp();
+        warp_sort_smem(s, N, lane);
+        for (int i0 = 0; i0 < cnt; i0 += 32) {
+            const int i = i0 + lane;
+            const unsigned long long v = (i < cnt) ? s[i] : kSentinel;
+            bool head = false;
+            if (v != kSentinel) head = (i == 0) || pair_key(v) != pair_key(s[i - 1]);
+            const unsigned hb = __ballot_sync(FULL, head);
+            if (head) {
+                uint32_t orv = 0;
+                const int key = pair_key(v);
+                for (int j = i; j < cnt && pair_key(s[j]) == key; ++j) orv |= pair_map(s[j]);
+                const int slot = u + __popc(hb & lanemask_lt(lane));
+                if (FILL) {
+                    cidx[slot] = key;
+                    cmap[slot] = (uint16_t)orv;
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) csr[q] += __popc((orv >> (4 * q)) & 0xFu);
+            }
+            u += __popc(hb);
+        }
+        __syncwarp();
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) csr[q] = warp_sum(csr[q]);
+    return u;
+}
+
+// Pass 1 (FILL = false): C blocks per row -> ccnt[b], CSR nonzeros per
+// scalar row -> csrcnt[4b+q]; rows beyond the warp capacity -> large list.
+// Pass 2 (FILL = true): C block columns and bitmaps at cptr[b].
+template <bool FILL>
+__global__ void __launch_bounds__(32 * kSymWarps)
+spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
+                       const uint16_t *__restrict__ amap, const int *__restrict__ bptr,
+                       const int *__restrict__ bidx, const uint16_t *__restrict__ bmap, int *__restrict__ ccnt,
+                       int *__restrict__ csrcnt, int *__restrict__ large, int64_t *__restrict__ stats,
+                       const int *__restrict__ cptr, int *__restrict__ cidx, uint16_t *__restrict__ cmap)
+{
+    __shared__ unsigned long long sbuf[kSymWarps][kSymCap];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned long long *s = sbuf[warp];
+    for (int b = blockIdx.x * kSymWarps + warp; b < brA; b += gridDim.x * kSymWarps) {
+        const int a0 = aptr[b], a1 = aptr[b + 1];
+        const long long ub = sym_upper_bound(lane, a0, a1, aidx, bptr);
+        if (ub > kSymCap) {
+            if (!FILL && lane == 0) large[atomicAdd((int *)&stats[3], 1)] = b;
+            continue;
+        }
+        const int cnt = sym_collect(lane, a0, a1, aidx, amap, bptr, bidx, bmap, s);
+        int csr[4];
+        const int base = FILL ? cptr[b] : 0;
+        const int u = sym_reduce<FILL>(lane, cnt, s, cidx + base, cmap + base, csr);
+        if (!FILL && lane == 0) {
+            ccnt[b] = u;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (4 * b + q < m) csrcnt[4 * b + q] = csr[q];
+            atomicMax((unsigned long long *)&stats[0], (unsigned long long)u);
+            atomicAdd((unsigned long long *)&stats[1], (unsigned long long)u * (unsigned long long)u);
+        }
+    }
+}
+
+// Rows with more than kSymCap pairs: window sweep over the reachable block
+// columns, 8 warps walking the A blocks, lanes the B rows.
+template <bool FILL>
+__global__ void __launch_bounds__(kSymLargeThreads)
+spgemm_symbolic_large_kernel(int m, const int *__restrict__ aptr, const int *__restrict__ aidx,
+                             const uint16_t *__restrict__ amap, const int *__restrict__ bptr,
+                             const int *__restrict__ bidx, const uint16_t *__restrict__ bmap,
+                             const int *__restrict__ large, int64_t *__restrict__ stats, int *__restrict__ ccnt,
+                             int *__restrict__ csrcnt, const int *__restrict__ cptr, int *__restrict__ cidx,
+                             uint16_t *__restrict__ cmap)
+{
+    __shared__ uint32_t maps[kSymWin];
+    __shared__ int sh[16];
+    __shared__ int smin, smax, scsr[4];
+    const int nlarge = (int)stats[3];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    for (int t = blockIdx.x; t < nlarge; t += gridDim.x) {
+        const int b = large[t];
+        const int a0 = aptr[b], a1 = aptr[b + 1];
+        if (tid == 0) {
+            smin = 0x7FFFFFFF;
+            smax = -1;
+            scsr[0] = scsr[1] = scsr[2] = scsr[3] = 0;
+        }
+        __syncthreads();
+        int lo = 0x7FFFFFFF, hi = -1;
+        for (int i = a0 + warp; i < a1; i += nw) {
+            const int k = aidx[i];
+            const uint32_t ma = amap[i];
+            for (int j = bptr[k] + lane; j < bptr[k + 1]; j += 32)
+                if (bitmap_mul(ma, bmap[j])) {
+                    lo = min(lo, bidx[j]);
+                    hi = max(hi, bidx[j]);
+                }
+        }
+        atomicMin(&smin, lo);
+        atomicMax(&smax, hi);
+        __syncthreads();
+        const int kmin = smin, kmax = smax;
+        const int base = FILL ? cptr[b] : 0;
+        int total = 0;
+        int c4[4] = {0, 0, 0, 0};
+        for (long long w0 = kmin; w0 <= kmax; w0 += kSymWin) {
+            for (int i = tid; i < kSymWin; i += blockDim.x) maps[i] = 0;
+            __syncthreads();
+            for (int i = a0 + warp; i < a1; i += nw) {
+                const int k = aidx[i];
+                const uint32_t ma = amap[i];
+                for (int j = bptr[k] + lane; j < bptr[k + 1]; j += 32) {
+                    const long long key = bidx[j] - w0;
+                    if (key < 0 || key >= kSymWin) continue;
+                    const uint32_t mc = bitmap_mul(ma, bmap[j]);
+                    if (mc) atomicOr(&maps[key], mc);
+                }
+            }
+            __syncthreads();
+            const int s0 = tid * (kSymWin / kSymLargeThreads);
+            int c = 0;
+            for (int i = 0; i < kSymWin / kSymLargeThreads; ++i) {
+                const uint32_t mp = maps[s0 + i];
+                if (mp) {
+                    ++c;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) c4[q] += __popc((mp >> (4 * q)) & 0xFu);
+                }
+            }
+            // block exclusive scan of c
+            int wt;
+            int off = warp_excl_scan(c, lane, &wt);
+            if (lane == 0) sh[warp] = wt;
+            __syncthreads();
+            if (warp == 0) {
+                int tv = (lane < 8) ? sh[lane] : 0, tt;
+                int e = warp_excl_scan(tv, lane, &tt);
+                if (lane < 8) sh[lane] = e;
+                if (lane == 0) sh[8] = tt;
+            }
+            __syncthreads();
+            off += sh[warp];
+            const int wtotal = sh[8];
+            if (FILL) {
+                int o = base + total + off;
+                for (int i = 0; i < kSymWin / kSymLargeThreads; ++i) {
+                    const uint32_t mp = maps[s0 + i];
+                    if (mp) {
+                        cidx[o] = (int)(w0 + s0 + i);
+                        cmap[o] = (uint16_t)mp;
+                        ++o;
+                    }
+                }
+            }
+            total += wtotal;
+            __syncthreads();
+        }
+        if (!FILL) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) atomicAdd(&scsr[q], c4[q]);
+            __syncthreads();
+            if (tid == 0) {
+                ccnt[b] = total;
+                for (int q = 0; q < 4; ++q)
+                    if (4 * b + q < m) csrcnt[4 * b + q] = scsr[q];
+                atomicMax((unsigned long long *)&stats[0], (unsigned long long)total);
+                atomicAdd((unsigned long long *)&stats[1], (unsigned long long)total * (unsigned long long)total);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- numeric
+template <int PREC>
+struct NumT;
+template <>
+struct NumT<AMGT_DOUBLE> {
+    using val_t = double;
+    using acc_t = double;
+    __device__ static double ld(const double *p, long long i) { return p[i]; }
+    __device__ static double mul(double a, double b) { return __dmul_rn(a, b); }
+    __device__ static double add(double a, double b) { return __dadd_rn(a, b); }
+};
+template <>
+struct NumT<AMGT_FLOAT> {
+    using val_t = float;
+    using acc_t = float;
+    __device__ static float ld(const float *p, long long i) { return p[i]; }
+    __device__ static float mul(float a, float b) { return __fmul_rn(a, b); }
+    __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
+};
+template <>
+struct NumT<AMGT_HALF> {
+    using val_t = __half;
+    using acc_t = float;
+    __device__ static float ld(const __half *p, long long i) { return __half2float(p[i]); }
+    __device__ static float mul(float a, float b) { return __fmul_rn(a, b); }
+    __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
+};
+template <>
+struct NumT<AMGT_BF16> {
+    using val_t = __nv_bfloat16;
+    using acc_t = float;
+    __device__ static float ld(const __nv_bfloat16 *p, long long i) { return __bfloat162float(p[i]); }
+    __device__ static float mul(float a, float b) { return __fmul_rn(a, b); }
+    __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
+};
+
+template <int PREC>
+__device__ __forceinline__ void store_shadow(void *sh, long long i, typename NumT<PREC>::acc_t v)
+{
+    if constexpr (PREC == AMGT_FLOAT) static_cast<float *>(sh)[i] = v;
+    else if constexpr (PREC == AMGT_HALF) static_cast<__half *>(sh)[i] = __float2half_rn(v);
+    else if constexpr (PREC == AMGT_BF16) static_cast<__nv_bfloat16 *>(sh)[i] = __float2bfloat16_rn(v);
+}
+
+__device__ __forceinline__ int search_sorted(const int *keys, int n, int key)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (keys[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(32 * kNumWarps)
+spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
+                      const uint16_t *__restrict__ amap, const typename NumT<PREC>::val_t *__restrict__ aval,
+                      const int *__restrict__ bptr, const int *__restrict__ bidx,
+                      const uint16_t *__restrict__ bmap, const typename NumT<PREC>::val_t *__restrict__ bval,
+                      const int *__restrict__ cptr, const int *__restrict__ cidx, const uint16_t *__restrict__ cmap,
+                      double *__restrict__ cval, void *__restrict__ cshadow, const int *__restrict__ csr_i,
+                      int *__restrict__ csr_j, double *__restrict__ csr_a)
+{
+    using T = NumT<PREC>;
+    using acc_t = typename T::acc_t;
+    __shared__ int skeys[kNumWarps][kNumCap];
+    __shared__ acc_t sacc[kNumWarps][kNumCap * 16];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int e = lane & 15, r = e >> 2, c = e & 3, half = lane & 16;
+    for (int b = blockIdx.x * kNumWarps + warp; b < brA; b += gridDim.x * kNumWarps) {
+        const int c0 = cptr[b], cn = cptr[b + 1] - c0;
+        const bool in_smem = cn <= kNumCap;
+        const int *keys = in_smem ? skeys[warp] : cidx + c0;
+        acc_t *sa = sacc[warp];
+        double *ga = cval + 16LL * c0;
+        if (in_smem) {
+            for (int t = lane; t < cn; t += 32) skeys[warp][t] = cidx[c0 + t];
+            for (int t = lane; t < 16 * cn; t += 32) sa[t] = (acc_t)0;
+        } else {
+            for (int t = lane; t < 16 * cn; t += 32) ga[t] = 0.0;
+        }
+        __syncwarp();
+        for (int i = aptr[b]; i < aptr[b + 1]; ++i) {
+            const int k = aidx[i];
+            const uint32_t ma = amap[i];
+            const acc_t al = T::ld(aval, 16LL * i + e);
+            const int j0 = bptr[k], j1 = bptr[k + 1];
+            for (int jj = j0; jj < j1; jj += 2) {
+                const int j = jj + (half >> 4);
+                const bool valid = j < j1;
+                const uint32_t mb = valid ? bmap[j] : 0u;
+                const uint32_t mc = bitmap_mul(ma, mb);
+                const acc_t bl = valid ? T::ld(bval, 16LL * j + e) : (acc_t)0;
+                acc_t s = (acc_t)0;
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk) {
+                    const acc_t av = __shfl_sync(FULL, al, half | (r * 4 + kk));
+                    const acc_t bv = __shfl_sync(FULL, bl, half | (kk * 4 + c));
+                    if (((ma >> (r * 4 + kk)) & 1u) && ((mb >> (kk * 4 + c)) & 1u)) s = T::add(s, T::mul(av, bv));
+                }
+                if (valid && ((mc >> e) & 1u)) {
+                    const int t = search_sorted(keys, cn, bidx[j]);
+                    if (in_smem) {
+                        sa[16 * t + e] = T::add(sa[16 * t + e], s);
+                    } else {
+                        const acc_t cur = (acc_t)ga[16 * t + e];
+                        ga[16 * t + e] = (double)T::add(cur, s);
+                    }
+                }
+            }
+            __syncwarp();
+        }
+        // C values (+ shadow)
+        for (int t = lane; t < 16 * cn; t += 32) {
+            const acc_t v = in_smem ? sa[t] : (acc_t)ga[t];
+            ga[t] = (double)v;
+            if (PREC != AMGT_DOUBLE && cshadow) store_shadow<PREC>(cshadow, 16LL * c0 + t, v);
+        }
+        __syncwarp();
+        // CSR rows 4b..4b+3 (BSR2CSR fused)
+        if (csr_i) {
+            for (int q = 0; q < 4 && 4 * b + q < m; ++q) {
+                int out = csr_i[4 * b + q];
+                for (int tt = 0; tt < cn; tt += 32) {
+                    const int t = tt + lane;
+                    uint32_t nib = 0;
+                    int col0 = 0;
+                    if (t < cn) {
+                        nib = (cmap[c0 + t] >> (4 * q)) & 0xFu;
+                        col0 = 4 * cidx[c0 + t];
+                    }
+                    int tot;
+                    const int off = warp_excl_scan(__popc(nib), lane, &tot);
+                    if (nib) {
+                        int o = out + off;
+#pragma unroll
+                        for (int cc = 0; cc < 4; ++cc)
+                            if (nib & (1u << cc)) {
+                                csr_j[o] = col0 + cc;
+                                csr_a[o] = ga[16 * t + 4 * q + cc];
+                                ++o;
+                            }
+                    }
+                    out += tot;
+                }
+            }
+        }
+    }
+}
+
+template <int PREC>
+static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B, const void *bval, amgt_bsr *C,
+                          void *cshadow, amgt_csr *Ccsr, cudaStream_t s, int sm_count)
+{
+    using V = typename NumT<PREC>::val_t;
+    if (A->blc_row == 0) return AMGT_OK;
+    AMGT_LAUNCH(spgemm_numeric_kernel<PREC>, grid_for(kNumWarps, A->blc_row, sm_count, 8), 32 * kNumWarps, 0, s,
+                A->row, A->blc_row, A->blcPtr, A->blcIdx, A->blcMap, (const V *)aval, B->blcPtr, B->blcIdx,
+                B->blcMap, (const V *)bval, C->blcPtr, C->blcIdx, C->blcMap, C->blcVal, cshadow,
+                Ccsr ? Ccsr->i : nullptr, Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr);
+    return AMGT_OK;
+}
+
+static void *shadow_of(const amgt_bsr *A, int prec)
+{
+    switch (prec) {
+    case AMGT_FLOAT: return A->blcVal_fp32;
+    case AMGT_HALF: return A->blcVal_fp16;
+    case AMGT_BF16: return A->blcVal_bf16;
+    default: return A->blcVal;
+    }
+}
+
+}  // namespace amgt
+
+using namespace amgt;
+
+extern "C" {
+
+int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amgt_csr *Ccsr, amgt_stream_t stream)
+{
+    if (!A || !B || !C || prec < AMGT_DOUBLE || prec > AMGT_BF16) return AMGT_ERR_INVALID;
+    if (A->col != B->row) return AMGT_ERR_INVALID;
+    DeviceState *st;
+    AMGT_TRY(device_state(&st));
+    cudaStream_t s = (cudaStream_t)stream;
+    const int m = A->row, brA = A->blc_row;
+    memset(C, 0, sizeof(*C));
+    if (Ccsr) memset(Ccsr, 0, sizeof(*Ccsr));
+    C->row = m;
+    C->col = B->col;
+    C->blc_row = brA;
+    C->blc_col = B->blc_col;
+
+    // reduced precisions read A / B shadows; build temporaries when absent
+    amgt_bsr Atmp = *A, Btmp = *B;
+    bool ownA = false, ownB = false;
+    int rc = AMGT_OK;
+    int *ccnt = nullptr, *csrcnt = nullptr, *large = nullptr, *csr_i = nullptr, *csr_tmp = nullptr;
+    int64_t *stats = nullptr;
+    const int64_t *h = nullptr;
+    int nbC = 0, nnzC = 0;
+    void *cshadow = nullptr;
+    if (prec != AMGT_DOUBLE) {
+        if (!shadow_of(A, prec)) {
+            Atmp.blcVal_fp32 = nullptr; Atmp.blcVal_fp16 = nullptr; Atmp.blcVal_bf16 = nullptr;
+            if ((rc = amgt_bsr_make_shadow(&Atmp, prec, stream))) return rc;
+            ownA = true;
+        }
+        if (!shadow_of(B, prec)) {
+            Btmp.blcVal_fp32 = nullptr; Btmp.blcVal_fp16 = nullptr; Btmp.blcVal_bf16 = nullptr;
+            if ((rc = amgt_bsr_make_shadow(&Btmp, prec, stream))) goto fail;
+            ownB = true;
+        }
+    }
+    if ((rc = alloc_n(&C->blcPtr, brA + 1, s)) || (rc = alloc_n(&ccnt, brA + 1, s)) ||
+        (rc = alloc_n(&csrcnt, m + 1, s)) || (rc = alloc_n(&large, brA, s)) || (rc = alloc_n(&stats, 4, s)))
+        goto fail;
+    AMGT_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(int64_t) * 4, s));
+    AMGT_CUDA_TRY(cudaMemsetAsync(ccnt, 0, sizeof(int) * (brA + 1), s));
+    AMGT_CUDA_TRY(cudaMemsetAsync(csrcnt, 0, sizeof(int) * (m + 1), s));
+    if (brA > 0) {
+        AMGT_LAUNCH(spgemm_symbolic_kernel<false>, grid_for(kSymWarps, brA, st->sm_count, 8), 32 * kSymWarps, 0, s,
+                    m, brA, A->blcPtr, A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, ccnt, csrcnt, large,
+                    stats, nullptr, nullptr, nullptr);
+        AMGT_LAUNCH(spgemm_symbolic_large_kernel<false>, 2 * st->sm_count, kSymLargeThreads, 0, s, m, A->blcPtr,
+                    A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, large, stats, ccnt, csrcnt, nullptr,
+                    nullptr, nullptr);
+    }
+    if ((rc = exclusive_scan_int(ccnt, C->blcPtr, brA + 1, s))) goto fail;
+    AMGT_CUDA_TRY(cudaMemcpyAsync(&stats[2], C->blcPtr + brA, sizeof(int), cudaMemcpyDeviceToDevice, s));
+    // CSR row pointer of C (into Ccsr->i, or a temporary when only the
+    // nonzero count is wanted)
+    if (Ccsr) {
+        Ccsr->num_rows = m;
+        Ccsr->num_cols = B->col;
+        if ((rc = alloc_n(&Ccsr->i, m + 1, s))) goto fail;
+        csr_i = Ccsr->i;
+    } else if ((rc = alloc_n(&csr_tmp, m + 1, s))) {
+        goto fail;
+    } else {
+        csr_i = csr_tmp;
+    }
+    if ((rc = exclusive_scan_int(csrcnt, csr_i, m + 1, s))) goto fail;
+    AMGT_CUDA_TRY(cudaMemcpyAsync((int *)&stats[2] + 1, csr_i + m, sizeof(int), cudaMemcpyDeviceToDevice, s));
+    if ((rc = read_back(stats, 4, s, &h))) goto fail;
+    nbC = (int)(h[2] & 0xFFFFFFFF);
+    nnzC = (int)(h[2] >> 32);
+    C->max_blc_per_row = (int)h[0];
+    {
+        const double avg = brA ? (double)nbC / brA : 0.0;
+        const double var = brA ? (double)h[1] / brA - avg * avg : 0.0;
+        C->stand = var > 0 ? sqrt(var) : 0.0;
+    }
+    C->blc_num = nbC;
+    C->nnz = (int)(16LL * nbC > 0x7FFFFFFF ? 0x7FFFFFFF : 16LL * nbC);  // saturates
+    if ((rc = check_device_error(s))) goto fail;
+    if ((rc = alloc_n(&C->blcIdx, nbC, s)) || (rc = alloc_n(&C->blcMap, nbC, s)) ||
+        (rc = alloc_n(&C->blcVal, 16LL * nbC, s)))
+        goto fail;
+    if (prec == AMGT_FLOAT) {
+        if ((rc = alloc_n(&C->blcVal_fp32, 16LL * nbC, s))) goto fail;
+        cshadow = C->blcVal_fp32;
+    } else if (prec == AMGT_HALF) {
+        if ((rc = alloc_n(&C->blcVal_fp16, 16LL * nbC, s))) goto fail;
+        cshadow = C->blcVal_fp16;
+    } else if (prec == AMGT_BF16) {
+        if ((rc = alloc_n(&C->blcVal_bf16, 16LL * nbC, s))) goto fail;
+        cshadow = C->blcVal_bf16;
+    }
+    if (Ccsr) {
+        Ccsr->num_nonzeros = nnzC;
+        if ((rc = alloc_n(&Ccsr->j, nnzC, s)) || (rc = alloc_n(&Ccsr->data, nnzC, s))) goto fail;
+    }
+    if (brA > 0) {
+        AMGT_LAUNCH(spgemm_symbolic_kernel<true>, grid_for(kSymWarps, brA, st->sm_count, 8), 32 * kSymWarps, 0, s,
+                    m, brA, A->blcPtr, A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, nullptr, nullptr,
+                    nullptr, stats, C->blcPtr, C->blcIdx, C->blcMap);
+        AMGT_LAUNCH(spgemm_symbolic_large_kernel<true>, 2 * st->sm_count, kSymLargeThreads, 0, s, m, A->blcPtr,
+                    A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, large, stats, nullptr, nullptr,
+                    C->blcPtr, C->blcIdx, C->blcMap);
+    }
+    switch (prec) {
+    case AMGT_DOUBLE:
+        rc = launch_numeric<AMGT_DOUBLE>(A, A->blcVal, B, B->blcVal, C, nullptr, Ccsr, s, st->sm_count);
+        break;
+    case AMGT_FLOAT:
+        rc = launch_numeric<AMGT_FLOAT>(A, Atmp.blcVal_fp32, B, Btmp.blcVal_fp32, C, cshadow, Ccsr, s, st->sm_count);
+        break;
+    case AMGT_HALF:
+        rc = launch_numeric<AMGT_HALF>(A, Atmp.blcVal_fp16, B, Btmp.blcVal_fp16, C, cshadow, Ccsr, s, st->sm_count);
+        break;
+    default:
+        rc = launch_numeric<AMGT_BF16>(A, Atmp.blcVal_bf16, B, Btmp.blcVal_bf16, C, cshadow, Ccsr, s, st->sm_count);
+        break;
+    }
+    if (rc) goto fail;
+    C->csr_nnz = nnzC;
+    C->avg_nnz = nbC ? (double)nnzC / nbC : 0.0;
+    free_ptr(ccnt, s); free_ptr(csrcnt, s); free_ptr(large, s); free_ptr(stats, s); free_ptr(csr_tmp, s);
+    if (ownA) { free_ptr(Atmp.blcVal_fp32, s); free_ptr(Atmp.blcVal_fp16, s); free_ptr(Atmp.blcVal_bf16, s); }
+    if (ownB) { free_ptr(Btmp.blcVal_fp32, s); free_ptr(Btmp.blcVal_fp16, s); free_ptr(Btmp.blcVal_bf16, s); }
+    return AMGT_OK;
+fail:
+    free_ptr(ccnt, s); free_ptr(csrcnt, s); free_ptr(large, s); free_ptr(stats, s); free_ptr(csr_tmp, s);
+    if (ownA) { free_ptr(Atmp.blcVal_fp32, s); free_ptr(Atmp.blcVal_fp16, s); free_ptr(Atmp.blcVal_bf16, s); }
+    if (ownB) { free_ptr(Btmp.blcVal_fp32, s); free_ptr(Btmp.blcVal_fp16, s); free_ptr(Btmp.blcVal_bf16, s); }
+    amgt_bsr_free(C, stream);
+    if (Ccsr) amgt_csr_free(Ccsr, stream);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,429 @@
+// mBSR SpMV / SpMM: y <- alpha * A * x + beta * y.
+//
+// Replaces spmv_amgT_fp64 / _fp32 / _fp16 and the bsr_spmv_* kernels
+// (AmgT_HYPRE/src/seq_mv/csr_matvec_device.c:319-613, 1302-1542,
+// 1654-2309).  The reference puts two 4x4 blocks in one m8n8k4 fp64 MMA and
+// keeps the diagonal of the 8x8 result (1/8 of the MMA work is useful);
+// SpMV is bound by HBM bytes, so here the tensor cores are not used at all
+// and the kernel is shaped for bandwidth instead:
+//   - 4 lanes per block, lane q owns block row q: its 4 values are 32
+//     contiguous bytes (two 16-byte loads for fp64, one for fp32, one
+//     8-byte load for fp16/bf16), so a warp streams whole 128-byte blocks;
+//   - LPR lanes per block row (4, 8, 16 or 32) so that short rows do not
+//     leave lanes idle; the LPR/4 groups of a row take every (LPR/4)-th
+//     block and are combined with shuffles (fixed order: deterministic);
+//   - values and block columns are read with evict-first hints so that x
+//     stays in L2;
+//   - beta * y is fused (no separate beta pass), beta == 0 does not read y;
+//   - reduced precisions read the value shadow, convert x in registers and
+//     accumulate in fp32; the result is combined with beta * y in fp64.
+// Very long rows (longest row > 256 blocks and a segment table present) are
+// cut into <= 64-block segments; partial sums go to scratch and a second
+// kernel adds them in segment order (the reference uses fp64 atomicAdd,
+// :593, which is not deterministic).
+#include <cstdlib>
+
+#include "amgt_internal.cuh"
+
+namespace amgt {
+
+template <int PREC>
+struct ValTraits;
+template <>
+struct ValTraits<AMGT_DOUBLE> {
+    using acc_t = double;
+};
+template <>
+struct ValTraits<AMGT_FLOAT> {
+    using acc_t = float;
+};
+template <>
+struct ValTraits<AMGT_HALF> {
+    using acc_t = float;
+};
+template <>
+struct ValTraits<AMGT_BF16> {
+    using acc_t = float;
+};
+
+// Row q of block k as 4 values in the accumulation type.
+template <int PREC>
+__device__ __forceinline__ void load_block_row(const void *__restrict__ val, long long k, int q,
+                                               typename ValTraits<PREC>::acc_t v[4])
+{
+    if constexpr (PREC == AMGT_DOUBLE) {
+        const double2 *p = reinterpret_cast<const double2 *>(val) + (k * 8 + q * 2);
+        const double2 a = __ldcs(p), b = __ldcs(p + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    } else if constexpr (PREC == AMGT_FLOAT) {
+        const float4 a = __ldcs(reinterpret_cast<const float4 *>(val) + (k * 4 + q));
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    } else {
+        const uint2 a = __ldcs(reinterpret_cast<const uint2 *>(val) + (k * 4 + q));
+        if constexpr (PREC == AMGT_HALF) {
+            const float2 f0 = __half22float2(*reinterpret_cast<const __half2 *>(&a.x));
+            const float2 f1 = __half22float2(*reinterpret_cast<const __half2 *>(&a.y));
+            v[0] = f0.x; v[1] = f0.y; v[2] = f1.x; v[3] = f1.y;
+        } else {
+            const float2 f0 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&a.x));
+            const float2 f1 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&a.y));
+            v[0] = f0.x; v[1] = f0.y; v[2] = f1.x; v[3] = f1.y;
+        }
+    }
+}
+
+// x[4*col .. 4*col+3]; SAFE: scalar loads with the n bound (last block
+// column when n % 4 != 0, or x not 16-byte aligned).
+template <bool SAFE>
+__device__ __forceinline__ void load_x4(const double *__restrict__ x, int col, int n, double xv[4])
+{
+    if constexpr (!SAFE) {
+        const double2 *p = reinterpret_cast<const double2 *>(x + 4LL * col);
+        const double2 a = __ldg(p), b = __ldg(p + 1);
+        xv[0] = a.x; xv[1] = a.y; xv[2] = b.x; xv[3] = b.y;
+    } else {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const long long j = 4LL * col + c;
+            xv[c] = (j < n) ? __ldg(x + j) : 0.0;
+        }
+    }
+}
+
+template <int PREC, bool SAFE>
+__device__ __forceinline__ typename ValTraits<PREC>::acc_t block_row_dot(const void *__restrict__ val,
+                                                                         const double *__restrict__ x, int n,
+                                                                         long long k, int q, int col,
+                                                                         typename ValTraits<PREC>::acc_t acc)
+{
+    using acc_t = typename ValTraits<PREC>::acc_t;
+    acc_t v[4];
+    double xv[4];
+    load_block_row<PREC>(val, k, q, v);
+    load_x4<SAFE>(x, col, n, xv);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc = fma(v[c], (acc_t)xv[c], acc);
+    return acc;
+}
+
+template <int PREC, int LPR, bool SAFE>
+__global__ void __launch_bounds__(256)
+spmv_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__restrict__ idx,
+            const void *__restrict__ val, double alpha, const double *__restrict__ x, double beta,
+            double *__restrict__ y)
+{
+    using acc_t = typename ValTraits<PREC>::acc_t;
+    constexpr int RPW = 32 / LPR;  // block rows per warp
+    constexpr int G = LPR / 4;     // blocks in flight per row
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / LPR, l = lane % LPR, g = l >> 2, q = l & 3;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int b0 = warp * RPW; b0 < brow; b0 += nwarps * RPW) {
+        const int b = b0 + sub;
+        acc_t acc = 0;
+        if (b < brow) {
+            const int start = ptr[b], end = ptr[b + 1];
+            int k = start + g;
+            // two blocks per group per step: both loads in flight before the FMAs
+            for (; k + G < end; k += 2 * G) {
+                const int c0 = __ldcs(idx + k), c1 = __ldcs(idx + k + G);
+                acc = block_row_dot<PREC, SAFE>(val, x, n, k, q, c0, acc);
+                acc = block_row_dot<PREC, SAFE>(val, x, n, k + G, q, c1, acc);
+            }
+            if (k < end) acc = block_row_dot<PREC, SAFE>(val, x, n, k, q, __ldcs(idx + k), acc);
+        }
+#pragma unroll
+        for (int o = 4; o < LPR; o <<= 1) acc += __shfl_xor_sync(FULL, acc, o);
+        if (b < brow && g == 0) {
+            const int row = 4 * b + q;
+            if (row < m) {
+                const double t = alpha * (double)acc;
+                y[row] = (beta == 0.0) ? t : t + beta * y[row];
+            }
+        }
+    }
+}
+
+// Long rows: one warp per <= 64-block segment, partial row sums to scratch.
+template <int PREC, bool SAFE>
+__global__ void __launch_bounds__(256)
+spmv_segment_kernel(int n, int nseg, const int *__restrict__ segrow, const int *__restrict__ segptr,
+                    const int *__restrict__ ptr, const int *__restrict__ idx, const void *__restrict__ val,
+                    const double *__restrict__ x, double *__restrict__ part)
+{
+    using acc_t = typename ValTraits<PREC>::acc_t;
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int sgi = warp; sgi < nseg; sgi += nwarps) {
+        const int b = segrow[sgi];
+        const int j = sgi - segptr[b];
+        const int start = ptr[b] + 64 * j, end = min(ptr[b + 1], start + 64);
+        acc_t acc = 0;
+        for (int k = start + g; k < end; k += 8) acc = block_row_dot<PREC, SAFE>(val, x, n, k, q, __ldcs(idx + k), acc);
+#pragma unroll
+        for (int o = 4; o < 32; o <<= 1) acc += __shfl_xor_sync(FULL, acc, o);
+        if (g == 0) part[4LL * sgi + q] = (double)acc;
+    }
+}
+
+__global__ void spmv_segment_combine(int m, int brow, const int *__restrict__ segptr,
+                                     const double *__restrict__ part, double alpha, double beta,
+                                     double *__restrict__ y, int lowp)
+{
+    for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < m; row += gridDim.x * blockDim.x) {
+        const int b = row >> 2, q = row & 3;
+        double t = 0.0;
+        float tf = 0.0f;
+        for (int sgi = segptr[b]; sgi < segptr[b + 1]; ++sgi) {
+            if (lowp) tf += (float)part[4LL * sgi + q];
+            else t += part[4LL * sgi + q];
+        }
+        if (lowp) t = (double)tf;
+        const double r = alpha * t;
+        y[row] = (beta == 0.0) ? r : r + beta * y[row];
+    }
+}
+
+// SpMM: NV vectors per pass, the block row values loaded once for all.
+template <int PREC, int LPR, int NV>
+__global__ void __launch_bounds__(256)
+spmm_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__restrict__ idx,
+            const void *__restrict__ val, double alpha, const double *__restrict__ x, int ldx, double beta,
+            double *__restrict__ y, int ldy)
+{
+    using acc_t = typename ValTraits<PREC>::acc_t;
+    constexpr int RPW = 32 / LPR;
+    constexpr int G = LPR / 4;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / LPR, l = lane % LPR, g = l >> 2, q = l & 3;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int b0 = warp * RPW; b0 < brow; b0 += nwarps * RPW) {
+        const int b = b0 + sub;
+        acc_t acc[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) acc[v] = 0;
+        if (b < brow) {
+            for (int k = ptr[b] + g; k < ptr[b + 1]; k += G) {
+                const int col = __ldcs(idx + k);
+                acc_t a[4];
+                load_block_row<PREC>(val, k, q, a);
+#pragma unroll
+                for (int v = 0; v < NV; ++v)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const long long j = 4LL * col + c;
+                        const double xv = (j < n) ? __ldg(x + (long long)v * ldx + j) : 0.0;
+                        acc[v] = fma(a[c], (acc_t)xv, acc[v]);
+                    }
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+#pragma unroll
+            for (int o = 4; o < LPR; o <<= 1) acc[v] += __shfl_xor_sync(FULL, acc[v], o);
+        if (b < brow && g == 0) {
+            const int row = 4 * b + q;
+            if (row < m) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    double *yy = y + (long long)v * ldy + row;
+                    const double t = alpha * (double)acc[v];
+                    *yy = (beta == 0.0) ? t : t + beta * *yy;
+                }
+            }
+        }
+    }
+}
+
+__global__ void scale_kernel(long long n, double beta, double *__restrict__ y)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] = (beta == 0.0) ? 0.0 : beta * y[i];
+}
+
+static const void *value_array(const amgt_bsr *A, int prec)
+{
+    switch (prec) {
+    case AMGT_DOUBLE: return A->blcVal;
+    case AMGT_FLOAT: return A->blcVal_fp32;
+    case AMGT_HALF: return A->blcVal_fp16;
+    case AMGT_BF16: return A->blcVal_bf16;
+    default: return nullptr;
+    }
+}
+
+// Lanes per block row from the mean block-row length (overridable with
+// AMGT_SPMV_LPR for tuning runs).
+static int pick_lpr(const amgt_bsr *A)
+{
+    static int env = -1;
+    if (env < 0) {
+        const char *e = getenv("AMGT_SPMV_LPR");
+        env = e ? atoi(e) : 0;
+    }
+    if (env == 4 || env == 8 || env == 16 || env == 32) return env;
+    const double avg = A->blc_row ? (double)A->blc_num / A->blc_row : 0.0;
+    if (avg <= 1.5) return 4;
+    if (avg <= 3.0) return 8;
+    if (avg <= 10.0) return 16;
+    return 32;
+}
+
+template <int PREC>
+static int launch_spmv(const amgt_bsr *A, const void *val, double alpha, const double *x, double beta, double *y,
+                       cudaStream_t s, int sm_count)
+{
+    const int brow = A->blc_row;
+    const bool safe = (A->col % 4 != 0) || ((uintptr_t)x % 16 != 0);
+    const int lpr = pick_lpr(A);
+    const int rows_per_cta = 8 * (32 / lpr);
+    const int grid = grid_for(rows_per_cta, brow, sm_count, 8);
+#define AMGT_SPMV_CASE(L)                                                                                   \
+    if (lpr == L) {                                                                                         \
+        if (safe)                                                                                           \
+            AMGT_LAUNCH((spmv_kernel<PREC, L, true>), grid, 256, 0, s, A->row, A->col, brow, A->blcPtr,     \
+                        A->blcIdx, val, alpha, x, beta, y);                                                 \
+        else                                                                                                \
+            AMGT_LAUNCH((spmv_kernel<PREC, L, false>), grid, 256, 0, s, A->row, A->col, brow, A->blcPtr,    \
+                        A->blcIdx, val, alpha, x, beta, y);                                                 \
+        return AMGT_OK;                                                                                     \
+    }
+    AMGT_SPMV_CASE(4)
+    AMGT_SPMV_CASE(8)
+    AMGT_SPMV_CASE(16)
+    AMGT_SPMV_CASE(32)
+#undef AMGT_SPMV_CASE
+    return AMGT_ERR_INVALID;
+}
+
+template <int PREC>
+static int launch_spmv_segmented(const amgt_bsr *A, const void *val, double alpha, const double *x, double beta,
+                                 double *y, cudaStream_t s, int sm_count)
+{
+    const bool safe = (A->col % 4 != 0) || ((uintptr_t)x % 16 != 0);
+    double *part = nullptr;
+    AMGT_TRY(alloc_n(&part, 4LL * A->warpnum, s));
+    const int grid = grid_for(8, A->warpnum, sm_count, 8);
+    if (safe)
+        AMGT_LAUNCH((spmv_segment_kernel<PREC, true>), grid, 256, 0, s, A->col, A->warpnum, A->rowIdxbyWarp,
+                    A->rowPtrbyWarp, A->blcPtr, A->blcIdx, val, x, part);
+    else
+        AMGT_LAUNCH((spmv_segment_kernel<PREC, false>), grid, 256, 0, s, A->col, A->warpnum, A->rowIdxbyWarp,
+                    A->rowPtrbyWarp, A->blcPtr, A->blcIdx, val, x, part);
+    AMGT_LAUNCH(spmv_segment_combine, grid_for(256, A->row, sm_count, 8), 256, 0, s, A->row, A->blc_row,
+                A->rowPtrbyWarp, part, alpha, beta, y, PREC != AMGT_DOUBLE);
+    free_ptr(part, s);
+    return AMGT_OK;
+}
+
+template <int PREC, int LPR>
+static int launch_spmm_lpr(const amgt_bsr *A, const void *val, double alpha, int nvec, const double *x, int ldx,
+                           double beta, double *y, int ldy, cudaStream_t s, int grid)
+{
+    int v0 = 0;
+    while (v0 < nvec) {
+        const int left = nvec - v0;
+        const double *xx = x + (long long)v0 * ldx;
+        double *yy = y + (long long)v0 * ldy;
+        if (left >= 8) {
+            AMGT_LAUNCH((spmm_kernel<PREC, LPR, 8>), grid, 256, 0, s, A->row, A->col, A->blc_row, A->blcPtr,
+                        A->blcIdx, val, alpha, xx, ldx, beta, yy, ldy);
+            v0 += 8;
+        } else if (left >= 4) {
+            AMGT_LAUNCH((spmm_kernel<PREC, LPR, 4>), grid, 256, 0, s, A->row, A->col, A->blc_row, A->blcPtr,
+                        A->blcIdx, val, alpha, xx, ldx, beta, yy, ldy);
+            v0 += 4;
+        } else if (left >= 2) {
+            AMGT_LAUNCH((spmm_kernel<PREC, LPR, 2>), grid, 256, 0, s, A->row, A->col, A->blc_row, A->blcPtr,
+                        A->blcIdx, val, alpha, xx, ldx, beta, yy, ldy);
+            v0 += 2;
+        } else {
+            AMGT_LAUNCH((spmm_kernel<PREC, LPR, 1>), grid, 256, 0, s, A->row, A->col, A->blc_row, A->blcPtr,
+                        A->blcIdx, val, alpha, xx, ldx, beta, yy, ldy);
+            v0 += 1;
+        }
+    }
+    return AMGT_OK;
+}
+
+template <int PREC>
+static int launch_spmm(const amgt_bsr *A, const void *val, double alpha, int nvec, const double *x, int ldx,
+                       double beta, double *y, int ldy, cudaStream_t s, int sm_count)
+{
+    const int lpr = pick_lpr(A);
+    const int grid = grid_for(8 * (32 / lpr), A->blc_row, sm_count, 8);
+    switch (lpr) {
+    case 4: return launch_spmm_lpr<PREC, 4>(A, val, alpha, nvec, x, ldx, beta, y, ldy, s, grid);
+    case 8: return launch_spmm_lpr<PREC, 8>(A, val, alpha, nvec, x, ldx, beta, y, ldy, s, grid);
+    case 16: return launch_spmm_lpr<PREC, 16>(A, val, alpha, nvec, x, ldx, beta, y, ldy, s, grid);
+    default: return launch_spmm_lpr<PREC, 32>(A, val, alpha, nvec, x, ldx, beta, y, ldy, s, grid);
+    }
+}
+
+}  // namespace amgt
+
+using namespace amgt;
+
+extern "C" {
+
+int amgt_spmv(int prec, double alpha, const amgt_bsr *A, const double *x, double beta, double *y,
+              amgt_stream_t stream)
+{
+    if (!A || prec < AMGT_DOUBLE || prec > AMGT_BF16) return AMGT_ERR_INVALID;
+    if (A->row > 0 && !y) return AMGT_ERR_INVALID;
+    if (A->row == 0) return AMGT_OK;
+    DeviceState *st;
+    AMGT_TRY(device_state(&st));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (A->blc_num == 0 || A->col == 0) {
+        AMGT_LAUNCH(scale_kernel, grid_for(256, A->row, st->sm_count, 8), 256, 0, s, (long long)A->row, beta, y);
+        return AMGT_OK;
+    }
+    const void *val = value_array(A, prec);
+    if (!val || !x || !A->blcPtr || !A->blcIdx) return AMGT_ERR_INVALID;
+    const bool seg = A->rowPtrbyWarp && A->rowIdxbyWarp && A->warpnum > 0 && A->max_blc_per_row > 256;
+    switch (prec) {
+    case AMGT_DOUBLE:
+        return seg ? launch_spmv_segmented<AMGT_DOUBLE>(A, val, alpha, x, beta, y, s, st->sm_count)
+                   : launch_spmv<AMGT_DOUBLE>(A, val, alpha, x, beta, y, s, st->sm_count);
+    case AMGT_FLOAT:
+        return seg ? launch_spmv_segmented<AMGT_FLOAT>(A, val, alpha, x, beta, y, s, st->sm_count)
+                   : launch_spmv<AMGT_FLOAT>(A, val, alpha, x, beta, y, s, st->sm_count);
+    case AMGT_HALF:
+        return seg ? launch_spmv_segmented<AMGT_HALF>(A, val, alpha, x, beta, y, s, st->sm_count)
+                   : launch_spmv<AMGT_HALF>(A, val, alpha, x, beta, y, s, st->sm_count);
+    default:
+        return seg ? launch_spmv_segmented<AMGT_BF16>(A, val, alpha, x, beta, y, s, st->sm_count)
+                   : launch_spmv<AMGT_BF16>(A, val, alpha, x, beta, y, s, st->sm_count);
+    }
+}
+
+int amgt_spmm(int prec, double alpha, const amgt_bsr *A, int nvec, const double *x, int ldx, double beta, double *y,
+              int ldy, amgt_stream_t stream)
+{
+    if (!A || prec < AMGT_DOUBLE || prec > AMGT_BF16 || nvec < 0) return AMGT_ERR_INVALID;
+    if (nvec == 0 || A->row == 0) return AMGT_OK;
+    if (!y || ldy < A->row || (A->col > 0 && ldx < A->col)) return AMGT_ERR_INVALID;
+    DeviceState *st;
+    AMGT_TRY(device_state(&st));
+    cudaStream_t s = (cudaStream_t)stream;
+    if (A->blc_num == 0 || A->col == 0) {
+        for (int v = 0; v < nvec; ++v)
+            AMGT_LAUNCH(scale_kernel, grid_for(256, A->row, st->sm_count, 8), 256, 0, s, (long long)A->row, beta,
+                        y + (long long)v * ldy);
+        return AMGT_OK;
+    }
+    const void *val = value_array(A, prec);
+    if (!val || !x) return AMGT_ERR_INVALID;
+    switch (prec) {
+    case AMGT_DOUBLE: return launch_spmm<AMGT_DOUBLE>(A, val, alpha, nvec, x, ldx, beta, y, ldy, s, st->sm_count);
+    case AMGT_FLOAT: return launch_spmm<AMGT_FLOAT>(A, val, alpha, nvec, x, ldx, beta, y, ldy, s, st->sm_count);
+    case AMGT_HALF: return launch_spmm<AMGT_HALF>(A, val, alpha, nvec, x, ldx, beta, y, ldy, s, st->sm_count);
+    default: return launch_spmm<AMGT_BF16>(A, val, alpha, nvec, x, ldx, beta, y, ldy, s, st->sm_count);
+    }
+}
+
+}  // extern "C"

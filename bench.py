@@ -1,0 +1,344 @@
+"""Benchmark of the AmgT hot path on B200.
+
+Workload (the GPU-scale configuration): 3D 7-point Poisson on 128^3
+(2,097,152 rows, 14,581,760 nonzeros), mBSR 4x4 fp64 (3,620,864 blocks),
+seeded uniform x.  One step = one SpMV y = A*x on the finest level, the
+operation that drives smoothing and residuals in solve.  The run also
+builds the Galerkin hierarchy (A_{l+1} = P^T (A_l P), linear interpolation
+P, mBSR SpGEMM) and reports RAP time and SpMV GB/s per level.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--impl amgt|reference]
+Under torchrun (N > 1) every rank runs the same workload on its own GPU
+(replicas: the path does not shard on one node here); rank 0 prints one
+JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "setup+solve s to rtol 1e-8, mixed/learned vs FP64 on 1 B200; SpMV HBM GB/s"
+GRID = (128, 128, 128)
+PROFILE_MD = os.path.join(ROOT, "profiles", "spmv_fp64_7pt128.md")
+
+
+def spmv_bytes(nblk: int, brow: int, m: int, n: int, val_bytes: int = 8, beta: bool = False) -> int:
+    """Algorithmic bytes of one mBSR SpMV: block values + block columns +
+    block-row pointers + x + y (+ y read when beta != 0).  The kernel does
+    not read the bitmaps (values are zero-padded)."""
+    return nblk * (16 * val_bytes + 4) + 4 * (brow + 1) + 8 * n + 8 * m * (2 if beta else 1)
+
+
+def csr_bytes(nnz: int, m: int, n: int) -> int:
+    """Useful bytes of the same product in CSR (values + columns + rowptr + x + y)."""
+    return nnz * 12 + 4 * (m + 1) + 8 * n + 8 * m
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def read_traffic():
+    """traffic_bytes_per_launch recorded from the ncu capture of the SpMV."""
+    if not os.path.exists(PROFILE_MD):
+        return None
+    for line in open(PROFILE_MD):
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return int(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not self.out:
+            return None
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- reference
+def cpu_spmv_rate(steps: int | None, budget_s: float):
+    """CPU SpMV on the same workload, the oracle (C, OpenMP, all host
+    threads).  Runs `steps` products, or as many as fit in budget_s."""
+    from oracle import oracle as orc
+
+    A = orc.laplacian(*GRID)
+    B = orc.csr2bsr(A)
+    x = orc.rand_uniform(0, A.n)
+    y = np.zeros(A.m)
+    orc.lib().orc_bsr_spmv(0, B.m, B.n, B.bptr, B.bidx, B.bval, 1.0, x, 0.0, y)  # warm
+    nbytes = spmv_bytes(B.nblk, B.brow, A.m, A.n)
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        orc.lib().orc_bsr_spmv(0, B.m, B.n, B.bptr, B.bidx, B.bval, 1.0, x, 0.0, y)
+        k += 1
+        el = time.perf_counter() - t0
+        if (steps is not None and k >= steps) or (steps is None and el >= budget_s):
+            break
+    return nbytes * k / el / 1e9, k, el, orc.num_threads()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = max(1, args.steps)
+    for _ in range(max(0, args.warmup)):
+        cpu_spmv_rate(1, 0)
+    gbs, k, el, cores = cpu_spmv_rate(steps, 0)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": k, "warmup": args.warmup, "ms_per_step": round(1e3 * el / k, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "mBSR SpMV y=A*x, 3D 7-point Poisson 128^3 fp64", "parallelism": "host threads"},
+        "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": "port",
+                         "sample": f"{k} full SpMVs of the 128^3 operator (C oracle, OpenMP)"},
+        "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------------- GPU
+def build_hierarchy(amgt, torch, A, grid, max_levels=8, min_rows=512):
+    """Galerkin hierarchy A_{l+1} = P^T (A_l P) with linear interpolation P;
+    returns (per-level info, [A_0, A_1, ...])."""
+    from amgt_b200 import problems
+
+    levels, mats = [], [A]
+    dims = grid
+    for lvl in range(max_levels):
+        Ab = mats[-1]
+        m = Ab.s.row
+        info = {"level": lvl, "rows": m, "blocks": Ab.nblk, "nnz": Ab.s.csr_nnz}
+        levels.append(info)
+        if m <= min_rows or lvl == max_levels - 1:
+            break
+        (pm, pn, pia, pja, pa), cdims = problems.interp(*dims)
+        P = amgt.Bsr.from_csr(pm, pn, torch.from_numpy(pia).cuda(), torch.from_numpy(pja).cuda(),
+                              torch.from_numpy(pa).cuda())
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        AP, _ = amgt.spgemm(Ab, P, want_csr=False)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        R = P.transpose()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        RAP, _ = amgt.spgemm(R, AP, want_csr=True)
+        torch.cuda.synchronize()
+        t3 = time.perf_counter()
+        info.update({"AP_ms": round(1e3 * (t1 - t0), 3), "PT_ms": round(1e3 * (t2 - t1), 3),
+                     "RAP_ms": round(1e3 * (t3 - t2), 3), "P_blocks": P.nblk, "AP_blocks": AP.nblk})
+        mats.append(RAP)
+        dims = cdims
+    return levels, mats
+
+
+def run_amgt(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    import amgt_b200 as amgt
+    from amgt_b200 import problems
+
+    amgt.init()
+    m, n, ia, ja, a = problems.laplacian(*GRID)
+    x_host = problems.rand_uniform(0, n)
+    ia_d, ja_d, a_d = (torch.from_numpy(v).cuda() for v in (ia, ja, a))
+    A = amgt.Bsr.from_csr(m, n, ia_d, ja_d, a_d)
+    x = torch.from_numpy(x_host).cuda()
+    y = torch.zeros(m, dtype=torch.float64, device="cuda")
+    nbytes = spmv_bytes(A.nblk, A.s.blc_row, m, n)
+    ubytes = csr_bytes(int(ja.size), m, n)
+
+    # warm-up (untimed)
+    for _ in range(max(3, args.warmup)):
+        A.spmv(x, y)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = amgt.kernel_launch_count()
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            A.spmv(x, y)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    launches = amgt.kernel_launch_count() - launches0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max = float(t.item())
+    value = world * nbytes / (ms_max * 1e-3) / 1e9
+    per_gpu = nbytes / (ms * 1e-3) / 1e9
+
+    # e2e: host x in, host y out, through the C ABI, every step
+    xh = torch.from_numpy(x_host).pin_memory()
+    yh = torch.empty(m, dtype=torch.float64).pin_memory()
+    for _ in range(2):
+        x.copy_(xh, non_blocking=True)
+        A.spmv(x, y)
+        yh.copy_(y, non_blocking=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        x.copy_(xh, non_blocking=True)
+        A.spmv(x, y)
+        yh.copy_(y, non_blocking=True)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = ev0.elapsed_time(ev1) / args.steps
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * nbytes / (float(t.item()) * 1e-3) / 1e9
+
+    # hierarchy: RAP per level and SpMV GB/s per level (not part of `value`)
+    levels, mats = build_hierarchy(amgt, torch, A, GRID)
+    for lvl, Ab in enumerate(mats):
+        xx = torch.zeros(Ab.s.col, dtype=torch.float64, device="cuda").uniform_(-1, 1)
+        yy = torch.zeros(Ab.s.row, dtype=torch.float64, device="cuda")
+        for _ in range(3):
+            Ab.spmv(xx, yy)
+        reps = 20
+        ev0.record(stream)
+        for _ in range(reps):
+            Ab.spmv(xx, yy)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        lms = ev0.elapsed_time(ev1) / reps
+        b = spmv_bytes(Ab.nblk, Ab.s.blc_row, Ab.s.row, Ab.s.col)
+        levels[lvl]["spmv_ms"] = round(lms, 4)
+        levels[lvl]["spmv_gbs"] = round(b / (lms * 1e-3) / 1e9, 1)
+    del mats
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    peak, peak_kind = read_peaks()
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        gbs, k, el, cores = cpu_spmv_rate(None, args.cpu_seconds)
+        cpu = {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": "port",
+               "sample": f"{k} full SpMVs of the 128^3 operator in {el:.1f} s (C oracle, OpenMP)"}
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": round(ms_max, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "mBSR SpMV y=A*x (fp64), 3D 7-point Poisson 128^3: 2,097,152 rows, "
+                               "14,581,760 nnz, 3,620,864 4x4 blocks", "global_batch": world,
+                   "bytes_per_step": nbytes, "l2": "inputs larger than L2 (matrix 478 MB > 126 MB)",
+                   "parallelism": f"replicas{world}"},
+        "spmv_useful_gbs": round(world * ubytes / (ms_max * 1e-3) / 1e9, 2),
+        "roofline": {"bound": "hbm", "achieved": round(per_gpu, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(per_gpu / peak, 4), "traffic": read_traffic(),
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                     else "fallback"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": 8 * n,
+                "d2h_bytes_per_step": 8 * m},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "levels": levels,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["amgt", "reference"], default="amgt")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_amgt(args)
+
+
+if __name__ == "__main__":
+    main()

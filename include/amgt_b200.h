@@ -1,0 +1,251 @@
+/*
+ * amgt_b200.h - C ABI of the B200 (sm_100a) mBSR kernels behind HYPRE's
+ * device SpGEMM and SpMV hooks.
+ *
+ * Plain C: no CUDA, C++ or torch types cross this boundary.  Every pointer
+ * inside amgt_csr / amgt_bsr / amgt_vector is DEVICE memory unless stated
+ * otherwise.  Every entry point returns an amgt_status (0 = success) and is
+ * stream-ordered on the stream it is given (NULL = the legacy default
+ * stream); an entry point only blocks the host where it must learn a size
+ * that decides an allocation (noted per function).
+ *
+ * Reference interfaces replaced (paths inside the AmgT repository,
+ * R = AmgT_HYPRE/src):
+ *   hypreDevice_CSRSpGemm                 R/seq_mv/csr_spgemm_device.c:2579-2608
+ *   hypre_CSRMatrixMatvecCusparseNewAPI   R/seq_mv/csr_matvec_device.c:2397-2437
+ *   bsrMAT                                R/seq_mv/seq_mv.h:105-129
+ *   AmgT fields of hypre_CSRMatrix        R/seq_mv/seq_mv.h:154-199
+ */
+#ifndef AMGT_B200_H
+#define AMGT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define AMGT_API __attribute__((visibility("default")))
+#else
+#define AMGT_API
+#endif
+
+/* Opaque CUDA stream handle (binary-identical to cudaStream_t). */
+typedef struct CUstream_st *amgt_stream_t;
+
+/* ---------------------------------------------------------------- status */
+typedef enum {
+    AMGT_OK = 0,
+    AMGT_ERR_INVALID = 1,     /* bad argument (NULL, negative size, mismatch) */
+    AMGT_ERR_ALLOC = 2,       /* the allocator returned NULL */
+    AMGT_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+    AMGT_ERR_DEVICE = 4,      /* a kernel raised its device error word
+                                 (bounded hash probe exhausted, bad index) */
+    AMGT_ERR_UNSUPPORTED = 5, /* precision / shape not built */
+    AMGT_ERR_NO_DEVICE = 6    /* no CUDA device visible to the library */
+} amgt_status;
+
+AMGT_API const char *amgt_status_string(int status);
+
+/* Library + device sanity: returns AMGT_OK when an sm_100 device is current
+ * and the kernels of this library can launch on it. */
+AMGT_API int amgt_init(void);
+
+/* Number of kernels this library has launched since load (all entry points,
+ * all streams).  Used to prove that a measured region ran native kernels. */
+AMGT_API uint64_t amgt_kernel_launch_count(void);
+
+/* ---------------------------------------------------------- allocation */
+/* Every array the library returns or uses as scratch comes from this
+ * allocator.  Default: cudaMallocAsync / cudaFreeAsync on the call's stream
+ * (stream-ordered pool).  HYPRE plugs hypre_TAlloc/hypre_TFree here so that
+ * hypre_CSRMatrixDestroy can free an SpGEMM result (the reference allocates C
+ * with hypre_TAlloc, R/seq_mv/csr_spgemm_device.c:1808-1839). */
+typedef void *(*amgt_alloc_fn)(size_t bytes, amgt_stream_t stream, void *ctx);
+typedef void (*amgt_free_fn)(void *ptr, amgt_stream_t stream, void *ctx);
+AMGT_API int amgt_set_allocator(amgt_alloc_fn alloc_fn, amgt_free_fn free_fn, void *ctx);
+
+/* ----------------------------------------------------------- precision */
+/* AMGT_PRECISION of R/seq_mv/seq_mv.h:139-144, plus BF16. */
+typedef enum {
+    AMGT_DOUBLE = 0, /* fp64 values, fp64 arithmetic                      */
+    AMGT_FLOAT = 1,  /* fp32 value shadow, fp32 arithmetic                */
+    AMGT_HALF = 2,   /* fp16 value shadow, fp32 arithmetic (accumulate)   */
+    AMGT_BF16 = 3    /* bf16 value shadow, fp32 arithmetic (accumulate)   */
+} amgt_precision;
+
+/* get_calculationPrecison, R/seq_mv/csr_spgemm_device.c:1847-1862:
+ * level 0 -> DOUBLE, 1 -> FLOAT, >=2 -> HALF under the default policy.
+ * amgt_set_level_policy replaces the table: prec[l] for level l < n, and
+ * prec[n-1] for every deeper level.  n = 0 restores the default. */
+AMGT_API int amgt_precision_for_level(int level);
+AMGT_API int amgt_set_level_policy(const int *prec, int n);
+
+/* ------------------------------------------------------------- formats */
+/* CSR, 0-based, HYPRE_Int = int32 indices, HYPRE_Complex = double values.
+ * Column order inside a row is free (HYPRE stores the diagonal first,
+ * R/parcsr_mv/par_csr_triplemat_device.c:896); duplicates are not allowed. */
+typedef struct {
+    int num_rows;
+    int num_cols;
+    int num_nonzeros;
+    int *i;       /* [num_rows + 1] */
+    int *j;       /* [num_nonzeros] */
+    double *data; /* [num_nonzeros] */
+} amgt_csr;
+
+/* mBSR: 4x4 blocks, bitmap per block.  Mirrors bsrMAT
+ * (R/seq_mv/seq_mv.h:105-129) field for field; the fp16 shadow is stored as
+ * uint16 halves instead of uint32-packed half2, and a bf16 shadow and the
+ * longest block-row length are added.  Block values are row-major, 16 per
+ * block, zero-padded; bit (r*4 + c) of blcMap is set iff the CSR source had
+ * an entry at (4*brow + r, 4*bcol + c).  Block columns ascend within a
+ * block row. */
+typedef struct {
+    int row, col;        /* scalar dimensions                       */
+    int nnz;             /* 16 * blc_num (stored values), saturates at INT_MAX */
+    int blc_row, blc_col;/* ceil(row/4), ceil(col/4)                */
+    int blc_num;         /* number of stored 4x4 blocks             */
+    double stand;        /* std-dev of blocks per block row          */
+    double avg_nnz;      /* CSR nonzeros per stored block            */
+    int *blcPtr;         /* [blc_row + 1]                           */
+    int *blcIdx;         /* [blc_num] block column                  */
+    double *blcVal;      /* [16 * blc_num]                          */
+    uint16_t *blcMap;    /* [blc_num]                               */
+    int warpnum;         /* load-balanced segments (see amgt_bsr_balance) */
+    int *rowPtrbyWarp;   /* [blc_row + 1] segments per block row, scanned */
+    int *rowIdxbyWarp;   /* [warpnum] block row of each segment      */
+    float *blcVal_fp32;  /* [16 * blc_num] or NULL                  */
+    uint16_t *blcVal_fp16; /* [16 * blc_num] IEEE half bits or NULL  */
+    uint16_t *blcVal_bf16; /* [16 * blc_num] bfloat16 bits or NULL   */
+    int max_blc_per_row; /* longest block row                        */
+    int csr_nnz;         /* number of set bitmap bits (CSR nonzeros) */
+} amgt_bsr;
+
+/* Dense vector / column-major multivector, mirrors the fields of
+ * hypre_Vector the matvec hook reads (data, size, num_vectors, vecstride). */
+typedef struct {
+    double *data;
+    int size;
+    int num_vectors;
+    int vecstride;       /* distance between vectors, >= size */
+} amgt_vector;
+
+/* -------------------------------------------------------- conversions */
+/* CSR -> mBSR.  Replaces CSR2BSR_GPU (R/seq_mv/csr_matvec_device.c:1201-1267)
+ * with its kernels csr2bsr_get_ptr / _compute_bin / _set_bin / _getidx /
+ * _getidx_large / getStand (:638-1092).  Fills every field of *out except the
+ * shadows and the balanced-segment arrays (NULL / 0).  Host-blocking once (to
+ * size the block arrays). */
+AMGT_API int amgt_csr_to_bsr(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream);
+
+/* mBSR -> CSR (set bitmap bits, ascending columns per row).  Replaces
+ * BSR2CSR_step1-3 / bsr2csr_get_ptr / bsr2csr_get_idx_val
+ * (R/seq_mv/csr_spgemm_device.c:1344-1440, 1501-1525).  Host-blocking once. */
+AMGT_API int amgt_bsr_to_csr(const amgt_bsr *A, amgt_csr *out, amgt_stream_t stream);
+
+/* Segments of <= 64 blocks for long block rows.  Replaces
+ * BSR_BALANCED_PREPROCESS_GPU + get_rowPtrbyWarp / get_rowIdxbyWarp
+ * (R/seq_mv/csr_matvec_device.c:615-637, 1269-1300); fills warpnum,
+ * rowPtrbyWarp, rowIdxbyWarp.  Host-blocking once. */
+AMGT_API int amgt_bsr_balance(amgt_bsr *A, amgt_stream_t stream);
+
+/* Builds the value shadow for prec (FLOAT / HALF / BF16) from blcVal,
+ * round-to-nearest-even.  Replaces bsr_val_fp64_to_32 / _to_16
+ * (R/seq_mv/csr_spgemm_device.c:1467-1499).  No-op for DOUBLE or when the
+ * shadow exists. */
+AMGT_API int amgt_bsr_make_shadow(amgt_bsr *A, int prec, amgt_stream_t stream);
+
+/* Block transpose: out = A^T in mBSR (values and bitmaps transposed per
+ * block, block columns ascending).  No reference counterpart inside AmgT:
+ * HYPRE builds R = P^T in CSR (keepT, R/parcsr_ls/par_amg.c:307-315); this
+ * keeps it in mBSR.  Host-blocking once. */
+AMGT_API int amgt_bsr_transpose(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream);
+
+/* Frees every array of *A (through the allocator) and zeroes the struct. */
+AMGT_API int amgt_bsr_free(amgt_bsr *A, amgt_stream_t stream);
+AMGT_API int amgt_csr_free(amgt_csr *A, amgt_stream_t stream);
+
+/* ---------------------------------------------------------------- SpMV */
+/* y <- alpha * A * x + beta * y, A in mBSR, x and y fp64.  Replaces
+ * spmv_amgT_fp64 / _fp32 / _fp16 and their bsr_spmv_* kernels
+ * (R/seq_mv/csr_matvec_device.c:319-613, 1302-1542, 1654-2309).
+ * prec selects the value array (DOUBLE: blcVal, FLOAT: blcVal_fp32, HALF:
+ * blcVal_fp16, BF16: blcVal_bf16; the shadow must exist).  Reduced
+ * precisions convert x to fp32 in registers, accumulate in fp32 and combine
+ * with beta*y in fp64.  beta == 0 does not read y.  Deterministic: no
+ * atomics; the sum order depends only on the block-row length.
+ * Never blocks the host. */
+AMGT_API int amgt_spmv(int prec, double alpha, const amgt_bsr *A, const double *x,
+              double beta, double *y, amgt_stream_t stream);
+
+/* Same for nvec column-major vectors (x[v*ldx + i], y[v*ldy + i]); the block
+ * values are read once for all vectors (mBSR SpMM). */
+AMGT_API int amgt_spmm(int prec, double alpha, const amgt_bsr *A, int nvec,
+              const double *x, int ldx, double beta, double *y, int ldy,
+              amgt_stream_t stream);
+
+/* -------------------------------------------------------------- SpGEMM */
+/* C = A * B on mBSR.  Replaces spgemm_amgT_fp64 / _fp32 / _fp16
+ * (R/seq_mv/csr_spgemm_device.c:1527-2578) and its kernels compute_Cub_bin,
+ * set_bin, symbolic_spgemm_step1/2(+_large, _gl), numeric_spgemm_hybrid
+ * (_tf32, _f16) (:82-1342).  The C block pattern is exactly the set of block
+ * columns with a non-zero bitmap product OR-ed over A's row; C's bitmap is
+ * that OR.  prec DOUBLE: fp64 products, each 4x4 product summed in k order
+ * and added to C in A-row order.  FLOAT / HALF / BF16: A and B shadows
+ * (built on demand), fp32 arithmetic, C values rounded to fp64 and a C
+ * shadow of the same precision.  If Ccsr != NULL the CSR form of C
+ * (BSR2CSR) is also written, fused into the numeric pass.
+ * Host-blocking twice (upper bound and C size). */
+AMGT_API int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C,
+                amgt_csr *Ccsr, amgt_stream_t stream);
+
+/* ------------------------------------------ HYPRE-facing mirror layer */
+/* The fields of hypre_CSRMatrix that the AmgT path reads and writes
+ * (R/seq_mv/seq_mv.h:154-199): the CSR arrays, the AmgT level tag and the
+ * lazily built mBSR cache.  bsr_mat_T caches A^T for trans = 1 (the
+ * reference ignores trans). */
+typedef struct {
+    int coasen_level;            /* hypre_Level(A)            */
+    char bsr_spmv_balanced_tag;  /* hypre_BSRBALANCEDTAG(A)   */
+    char bsr_tag;                /* hypre_BSRTAG(A)           */
+    char mixed_precision_flag;   /* hypre_MixedPrecisionTag(A)*/
+    char owns_data;              /* CSR arrays freed by Destroy */
+    amgt_bsr *bsr_mat;           /* hypre_BSR(A)              */
+    amgt_bsr *bsr_mat_T;         /* cached transpose (trans = 1) */
+    amgt_csr csr;                /* i / j / data / sizes      */
+} amgt_CSRMatrix;
+
+/* Wraps caller-owned device CSR arrays (owns_data = 0). */
+AMGT_API amgt_CSRMatrix *amgt_CSRMatrixCreate(int num_rows, int num_cols,
+                                     int num_nonzeros, int *i, int *j,
+                                     double *data, int level);
+/* Frees the mBSR caches, and the CSR arrays when owns_data is set. */
+AMGT_API int amgt_CSRMatrixDestroy(amgt_CSRMatrix *A);
+
+/* Stream used by the mirror layer (HYPRE's hypre_HandleComputeStream). */
+AMGT_API int amgt_set_stream(amgt_stream_t stream);
+
+/* hypreDevice_CSRSpGemm (R/seq_mv/csr_spgemm_device.c:2579-2608): converts
+ * A and B to mBSR on first use (cached), picks the precision from
+ * hypre_Level(A) through amgt_precision_for_level, multiplies, and returns a
+ * new matrix that owns its CSR arrays (from the allocator), carries C's mBSR
+ * with bsr_tag = 1, and has C's level = A's level. */
+AMGT_API int amgt_CSRSpGemm(amgt_CSRMatrix *A, amgt_CSRMatrix *B, amgt_CSRMatrix **C_ptr);
+
+/* hypre_CSRMatrixMatvecCusparseNewAPI
+ * (R/seq_mv/csr_matvec_device.c:2397-2437): y[offset:] = alpha * op(A) * x
+ * + beta * y[offset:], op(A) = A^T when trans != 0 (built once and cached).
+ * offset must be 0 (asserted by the caller in HYPRE, :142).  Multivectors
+ * (num_vectors > 1) go through amgt_spmm.  Precision from hypre_Level(A). */
+AMGT_API int amgt_CSRMatrixMatvec(int trans, double alpha, amgt_CSRMatrix *A,
+                         const amgt_vector *x, double beta, amgt_vector *y,
+                         int offset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AMGT_B200_H */
