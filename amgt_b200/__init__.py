@@ -1,7 +1,7 @@
 """amgt_b200: B200 (sm_100a) mBSR SpGEMM / SpMV behind HYPRE's AmgT hooks.
 
 The kernels live in libamgt_b200.so (CUDA, built in-tree by
-``python -m amgt_b200.build``); this package is the Python face of its C ABI
+``python amgt_b200/build.py``); this package is the Python face of its C ABI
 (include/amgt_b200.h).  Importing it loads the library and fails loudly
 when it is missing.
 """

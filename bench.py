@@ -28,7 +28,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "setup+solve s to rtol 1e-8, mixed/learned vs FP64 on 1 B200; SpMV HBM GB/s"
-GRID = (128, 128, 128)
+GRID = (128, 128, 128)  # the workload; --grid changes it only for profiling captures
 PROFILE_MD = os.path.join(ROOT, "profiles", "spmv_fp64_7pt128.md")
 
 
@@ -271,8 +271,12 @@ def run_amgt(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_value = world * nbytes / (float(t.item()) * 1e-3) / 1e9
 
-    # hierarchy: RAP per level and SpMV GB/s per level (not part of `value`)
-    levels, mats = build_hierarchy(amgt, torch, A, GRID)
+    # hierarchy: RAP per level and SpMV GB/s per level (not part of `value`);
+    # built twice, the first pass loading the kernels' modules
+    levels, mats = [], []
+    if not args.no_levels:
+        build_hierarchy(amgt, torch, A, GRID)  # warm-up pass, result dropped
+        levels, mats = build_hierarchy(amgt, torch, A, GRID)
     for lvl, Ab in enumerate(mats):
         xx = torch.zeros(Ab.s.col, dtype=torch.float64, device="cuda").uniform_(-1, 1)
         yy = torch.zeros(Ab.s.row, dtype=torch.float64, device="cuda")
@@ -306,8 +310,8 @@ def run_amgt(args):
         "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": round(ms_max, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "mBSR SpMV y=A*x (fp64), 3D 7-point Poisson 128^3: 2,097,152 rows, "
-                               "14,581,760 nnz, 3,620,864 4x4 blocks", "global_batch": world,
+        "config": {"workload": f"mBSR SpMV y=A*x (fp64), 3D 7-point Poisson {GRID[0]}^3: {m:,} rows, "
+                               f"{int(ja.size):,} nnz, {A.nblk:,} 4x4 blocks", "global_batch": world,
                    "bytes_per_step": nbytes, "l2": "inputs larger than L2 (matrix 478 MB > 126 MB)",
                    "parallelism": f"replicas{world}"},
         "spmv_useful_gbs": round(world * ubytes / (ms_max * 1e-3) / 1e9, 2),
@@ -332,8 +336,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["amgt", "reference"], default="amgt")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-levels", action="store_true", help="skip the hierarchy / per-level report")
+    ap.add_argument("--grid", type=int, default=128, help="cube side (profiling captures only)")
     args = ap.parse_args()
+    global GRID
+    GRID = (args.grid, args.grid, args.grid)
     if args.impl == "reference":
         run_reference(args)
     else:
