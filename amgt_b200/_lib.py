@@ -87,7 +87,7 @@ def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
-            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m amgt_b200.build` "
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python amgt_b200/build.py` "
                               "(there is no fallback implementation)")
         L = ctypes.CDLL(LIB_PATH)
         for name, (res, args) in SIGNATURES.items():

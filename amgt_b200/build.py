@@ -1,6 +1,7 @@
 """Builds libamgt_b200.so in-tree with nvcc for sm_100a (B200).
 
-python -m amgt_b200.build  (or amgt_b200.build.build())
+python amgt_b200/build.py [-v]   (run as a file: importing the package
+                                 loads the library this script builds)
 """
 from __future__ import annotations
 
