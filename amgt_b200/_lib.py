@@ -13,7 +13,8 @@ LIB_PATH = os.path.join(HERE, "libamgt_b200.so")
 
 AMGT_OK = 0
 STATUS = {0: "AMGT_OK", 1: "AMGT_ERR_INVALID", 2: "AMGT_ERR_ALLOC", 3: "AMGT_ERR_CUDA", 4: "AMGT_ERR_DEVICE",
-          5: "AMGT_ERR_UNSUPPORTED", 6: "AMGT_ERR_NO_DEVICE"}
+          5: "AMGT_ERR_UNSUPPORTED", 6: "AMGT_ERR_NO_DEVICE", 7: "AMGT_ERR_TOO_LARGE"}
+NOALLOC_MAX_SEGMENTS = 1 << 18  # AMGT_NOALLOC_MAX_SEGMENTS
 DOUBLE, FLOAT, HALF, BF16 = 0, 1, 2, 3
 
 c_int, c_double, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
@@ -61,6 +62,7 @@ SIGNATURES = {
     "amgt_csr_free": (c_int, [P(AmgtCsr), c_void_p]),
     "amgt_spmv": (c_int, [c_int, c_double, P(AmgtBsr), c_void_p, c_double, c_void_p, c_void_p]),
     "amgt_spmm": (c_int, [c_int, c_double, P(AmgtBsr), c_int, c_void_p, c_int, c_double, c_void_p, c_int, c_void_p]),
+    "amgt_spmv_segmented_noalloc": (c_int, [c_int, c_double, P(AmgtBsr), c_void_p, c_double, c_void_p, c_void_p]),
     "amgt_spgemm": (c_int, [c_int, P(AmgtBsr), P(AmgtBsr), P(AmgtBsr), P(AmgtCsr), c_void_p]),
     "amgt_CSRMatrixCreate": (P(AmgtCSRMatrix), [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int]),
     "amgt_CSRMatrixDestroy": (c_int, [P(AmgtCSRMatrix)]),

@@ -87,6 +87,11 @@ __device__ __forceinline__ void raise_error(int *err, int code)
 // stand) of an mBSR matrix; one host read-back.
 int block_row_stats(amgt_bsr *A, cudaStream_t s);
 
+// Segmented SpMV (long-row path) with caller-provided partial-sum scratch
+// of 4 * A->warpnum doubles; allocates nothing (spmv.cu).
+int spmv_segmented_with_scratch(int prec, double alpha, const amgt_bsr *A, const double *x, double beta, double *y,
+                                double *part, int sm_count, cudaStream_t s);
+
 // Exclusive scan of n ints (in may equal out), CUB with allocator scratch.
 int exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s);
 // Exclusive scan of n 64-bit ints.

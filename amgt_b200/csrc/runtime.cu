@@ -146,6 +146,7 @@ const char *amgt_status_string(int status)
     case AMGT_ERR_DEVICE: return g_cuda_msg[0] ? g_cuda_msg : "device error word raised";
     case AMGT_ERR_UNSUPPORTED: return "unsupported precision or shape";
     case AMGT_ERR_NO_DEVICE: return "no CUDA device";
+    case AMGT_ERR_TOO_LARGE: return "size exceeds the fixed maximum of this entry point";
     default: return "unknown status";
     }
 }

@@ -363,6 +363,40 @@ static int launch_spmm(const amgt_bsr *A, const void *val, double alpha, int nve
     }
 }
 
+template <int PREC>
+static int launch_segmented_scratch(const amgt_bsr *A, const void *val, double alpha, const double *x,
+                                    double beta, double *y, double *part, int sm_count, cudaStream_t s)
+{
+    const bool safe = (A->col % 4 != 0) || ((uintptr_t)x % 16 != 0);
+    const int grid = grid_for(8, A->warpnum, sm_count, 8);
+    if (safe)
+        AMGT_LAUNCH((spmv_segment_kernel<PREC, true>), grid, 256, 0, s, A->col, A->warpnum, A->rowIdxbyWarp,
+                    A->rowPtrbyWarp, A->blcPtr, A->blcIdx, val, x, part);
+    else
+        AMGT_LAUNCH((spmv_segment_kernel<PREC, false>), grid, 256, 0, s, A->col, A->warpnum, A->rowIdxbyWarp,
+                    A->rowPtrbyWarp, A->blcPtr, A->blcIdx, val, x, part);
+    AMGT_LAUNCH(spmv_segment_combine, grid_for(256, A->row, sm_count, 8), 256, 0, s, A->row, A->blc_row,
+                A->rowPtrbyWarp, part, alpha, beta, y, PREC != AMGT_DOUBLE);
+    return AMGT_OK;
+}
+
+// The segmented SpMV (same two kernels and summation order as the
+// allocating path) writing its partial sums into caller-provided scratch of
+// 4 * A->warpnum doubles.  Performs no allocation and no device query.
+int spmv_segmented_with_scratch(int prec, double alpha, const amgt_bsr *A, const double *x, double beta, double *y,
+                                double *part, int sm_count, cudaStream_t s)
+{
+    const void *val = value_array(A, prec);
+    if (!val) return AMGT_ERR_INVALID;
+    switch (prec) {
+    case AMGT_DOUBLE: return launch_segmented_scratch<AMGT_DOUBLE>(A, val, alpha, x, beta, y, part, sm_count, s);
+    case AMGT_FLOAT: return launch_segmented_scratch<AMGT_FLOAT>(A, val, alpha, x, beta, y, part, sm_count, s);
+    case AMGT_HALF: return launch_segmented_scratch<AMGT_HALF>(A, val, alpha, x, beta, y, part, sm_count, s);
+    case AMGT_BF16: return launch_segmented_scratch<AMGT_BF16>(A, val, alpha, x, beta, y, part, sm_count, s);
+    default: return AMGT_ERR_INVALID;
+    }
+}
+
 }  // namespace amgt
 
 using namespace amgt;

@@ -44,7 +44,8 @@ typedef enum {
     AMGT_ERR_DEVICE = 4,      /* a kernel raised its device error word
                                  (bounded hash probe exhausted, bad index) */
     AMGT_ERR_UNSUPPORTED = 5, /* precision / shape not built */
-    AMGT_ERR_NO_DEVICE = 6    /* no CUDA device visible to the library */
+    AMGT_ERR_NO_DEVICE = 6,   /* no CUDA device visible to the library */
+    AMGT_ERR_TOO_LARGE = 7    /* a size exceeds a fixed maximum of the call */
 } amgt_status;
 
 AMGT_API const char *amgt_status_string(int status);
@@ -186,6 +187,29 @@ AMGT_API int amgt_spmv(int prec, double alpha, const amgt_bsr *A, const double *
 AMGT_API int amgt_spmm(int prec, double alpha, const amgt_bsr *A, int nvec,
               const double *x, int ldx, double beta, double *y, int ldy,
               amgt_stream_t stream);
+
+/* Segmented SpMV that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory while they run a matvec:
+ * a solver whose device memory went, whole, to a pool sized at set-up and
+ * not allowed to grow; a caller whose allocator hook may not be called from
+ * the thread issuing the solve; a caller that cannot pay for cudaMalloc /
+ * cudaFree, which can synchronise the whole device.  Computes y <- alpha*A*x
+ * + beta*y exactly as amgt_spmv does on its long-row (segmented) path, same
+ * kernels and summation order, but takes the partial-sum scratch from a
+ * fixed device array of AMGT_NOALLOC_MAX_SEGMENTS * 4 doubles (8 MiB, held
+ * by every GPU that loads the library until the process exits) instead of
+ * the allocator.  A must carry the segment table (amgt_bsr_balance, called
+ * during set-up); A->warpnum > AMGT_NOALLOC_MAX_SEGMENTS returns
+ * AMGT_ERR_TOO_LARGE.  The first call on a device, with that device
+ * current, looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  All calls share the array:
+ * calls whose kernels overlap on the GPU race and must be ordered by the
+ * caller.  Never blocks the host. */
+#define AMGT_NOALLOC_MAX_SEGMENTS (1 << 18)
+AMGT_API int amgt_spmv_segmented_noalloc(int prec, double alpha, const amgt_bsr *A,
+                                         const double *x, double beta, double *y,
+                                         amgt_stream_t stream);
 
 /* -------------------------------------------------------------- SpGEMM */
 /* C = A * B on mBSR.  Replaces spgemm_amgT_fp64 / _fp32 / _fp16
