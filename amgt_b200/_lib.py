@@ -45,6 +45,12 @@ class AmgtCSRMatrix(ctypes.Structure):
                 ("bsr_mat", P(AmgtBsr)), ("bsr_mat_T", P(AmgtBsr)), ("csr", AmgtCsr)]
 
 
+class AmgtAmgParams(ctypes.Structure):
+    _fields_ = [("max_levels", c_int), ("max_coarse_rows", c_int), ("tol", c_double), ("max_iter", c_int),
+                ("relax_weight", c_double), ("flexible", c_int), ("use_graph", c_int),
+                ("galerkin_by_level", c_int), ("smooth_prec0", c_int)]
+
+
 # name -> (restype, argtypes); every symbol include/amgt_b200.h declares
 SIGNATURES = {
     "amgt_status_string": (ctypes.c_char_p, [c_int]),
@@ -62,8 +68,19 @@ SIGNATURES = {
     "amgt_csr_free": (c_int, [P(AmgtCsr), c_void_p]),
     "amgt_spmv": (c_int, [c_int, c_double, P(AmgtBsr), c_void_p, c_double, c_void_p, c_void_p]),
     "amgt_spmm": (c_int, [c_int, c_double, P(AmgtBsr), c_int, c_void_p, c_int, c_double, c_void_p, c_int, c_void_p]),
+    "amgt_bsr_l1_norms": (c_int, [P(AmgtBsr), c_void_p, c_void_p]),
+    "amgt_bsr_residual": (c_int, [c_int, P(AmgtBsr), c_void_p, c_void_p, c_void_p, c_void_p]),
+    "amgt_bsr_jacobi": (c_int, [c_int, P(AmgtBsr), c_void_p, c_double, c_void_p, c_void_p, c_void_p, c_void_p]),
     "amgt_spmv_segmented_noalloc": (c_int, [c_int, c_double, P(AmgtBsr), c_void_p, c_double, c_void_p, c_void_p]),
     "amgt_spgemm": (c_int, [c_int, P(AmgtBsr), P(AmgtBsr), P(AmgtBsr), P(AmgtCsr), c_void_p]),
+    "amgt_amg_default_params": (None, [P(AmgtAmgParams)]),
+    "amgt_amg_setup": (c_int, [P(AmgtCsr), c_int, P(AmgtCsr), P(AmgtAmgParams), P(c_void_p), c_void_p]),
+    "amgt_amg_solve": (c_int, [c_void_p, c_void_p, c_void_p, P(c_int), P(c_double), c_void_p]),
+    "amgt_amg_num_levels": (c_int, [c_void_p]),
+    "amgt_amg_level": (c_int, [c_void_p, c_int, P(AmgtBsr), P(c_int)]),
+    "amgt_amg_setup_times": (c_int, [c_void_p, P(c_double)]),
+    "amgt_amg_residual_history": (c_int, [c_void_p, P(c_double), c_int]),
+    "amgt_amg_destroy": (c_int, [c_void_p, c_void_p]),
     "amgt_CSRMatrixCreate": (P(AmgtCSRMatrix), [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int]),
     "amgt_CSRMatrixDestroy": (c_int, [P(AmgtCSRMatrix)]),
     "amgt_set_stream": (c_int, [c_void_p]),

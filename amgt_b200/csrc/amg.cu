@@ -1,0 +1,563 @@
+// Galerkin AMG hierarchy on mBSR and a PCG solve preconditioned by one
+// V(1,1) cycle with l1-Jacobi smoothing, for the setup + solve measurement.
+//
+// The coarsening and interpolation stay the caller's (in HYPRE they are
+// BoomerAMG's, outside the AmgT path): the caller passes P_0 .. P_{L-2}.
+// Everything else runs here, on the GPU, through the mBSR kernels:
+//   setup  A_0 = CSR->mBSR; per level P_l -> mBSR, R_l = P_l^T (block
+//          transpose), A_{l+1} = R_l (A_l P_l) (two SpGEMMs, the
+//          Galerkin product of hypre_ParCSRMatrixRAPKT,
+//          par_csr_triplemat_device.c:630-905), inverse l1 row norms
+//          (relax 18, ams.c:627-636), value shadows, and the dense inverse
+//          of the coarsest operator (HYPRE's coarse GE, relax 9);
+//   cycle  pre-smooth from zero u = w f ./ l1; r = f - A u (fused);
+//          f_c = R r; recurse; u += P e; post-smooth u + w (f - A u) ./ l1
+//          (fused), as hypre_BoomerAMGCycle does with relax 18
+//          (par_cycle.c:678-751, par_relax.c:1178-1260);
+//   solve  PCG (krylov/pcg.c:405-580), optionally flexible (Polak-Ribiere
+//          beta), with the scalars kept on the device and every iteration
+//          one CUDA graph launch plus one 8-byte read of ||r||^2.
+// Dots are deterministic: fixed grids, per-CTA partials reduced in a fixed
+// order by one CTA.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "amgt_internal.cuh"
+
+namespace amgt {
+
+constexpr int kDotGrid = 296;  // 2 x 148 SMs
+constexpr int kDotThreads = 256;
+
+enum { S_BB = 0, S_RR = 1, S_RZ = 2, S_PQ = 3, S_ALPHA = 4, S_BETA = 5, S_ZRPREV = 6, S_NSCAL = 8 };
+enum { OP_STORE = 0, OP_ALPHA = 1, OP_BETA = 2, OP_BETA_FLEX = 3 };
+
+__global__ void __launch_bounds__(kDotThreads) dot_kernel(long long n, const double *__restrict__ a,
+                                                         const double *__restrict__ b, double *__restrict__ part)
+{
+    __shared__ double sred[kDotThreads / 32];
+    double s = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        s += a[i] * b[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+    if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kDotThreads / 32; ++w) t += sred[w];
+        part[blockIdx.x] = t;
+    }
+}
+
+// Sums np partials in a fixed order into scal[slot] and applies op.
+__global__ void __launch_bounds__(kDotThreads) reduce_kernel(const double *__restrict__ part, int np,
+                                                            double *__restrict__ scal, int slot, int op)
+{
+    __shared__ double sred[kDotThreads / 32];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) s += part[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+    if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kDotThreads / 32; ++w) t += sred[w];
+        if (op == OP_ALPHA) {
+            scal[S_PQ] = t;
+            scal[S_ALPHA] = (t != 0.0) ? scal[S_RZ] / t : 0.0;
+        } else if (op == OP_BETA || op == OP_BETA_FLEX) {
+            const double rz_old = scal[S_RZ];
+            const double num = (op == OP_BETA_FLEX) ? t - scal[S_ZRPREV] : t;
+            scal[S_BETA] = (rz_old != 0.0) ? num / rz_old : 0.0;
+            scal[S_RZ] = t;
+        } else {
+            scal[slot] = t;
+        }
+    }
+}
+
+// x += alpha p; r -= alpha q; partials of r . r
+__global__ void __launch_bounds__(kDotThreads) axpy2_dot_kernel(long long n, const double *__restrict__ scal,
+                                                               const double *__restrict__ p,
+                                                               const double *__restrict__ q, double *__restrict__ x,
+                                                               double *__restrict__ r, double *__restrict__ part)
+{
+    __shared__ double sred[kDotThreads / 32];
+    const double alpha = scal[S_ALPHA];
+    double s = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        x[i] += alpha * p[i];
+        const double ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        s += ri * ri;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+    if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kDotThreads / 32; ++w) t += sred[w];
+        part[blockIdx.x] = t;
+    }
+}
+
+// p = z + beta p
+__global__ void xpby_kernel(long long n, const double *__restrict__ z, const double *__restrict__ scal,
+                            double *__restrict__ p)
+{
+    const double beta = scal[S_BETA];
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = z[i] + beta * p[i];
+}
+
+// u = w f ./ l1 (l1-Jacobi sweep from a zero guess)
+__global__ void jacobi_zero_kernel(long long n, const double *__restrict__ f, const double *__restrict__ inv_l1,
+                                   double w, double *__restrict__ u)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        u[i] = w * f[i] * inv_l1[i];
+}
+
+// u = M f with M dense (row-major, nc x nc), one warp per row
+__global__ void dense_mv_kernel(int nc, const double *__restrict__ M, const double *__restrict__ f,
+                                double *__restrict__ u)
+{
+    const int lane = threadIdx.x & 31;
+    for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nc; row += (gridDim.x * blockDim.x) >> 5) {
+        double s = 0.0;
+        for (int j = lane; j < nc; j += 32) s += M[(long long)row * nc + j] * f[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+        if (lane == 0) u[row] = s;
+    }
+}
+
+// mBSR -> dense (row-major), for the coarsest operator
+__global__ void bsr_to_dense_kernel(int m, int n, const int *__restrict__ ptr, const int *__restrict__ idx,
+                                    const double *__restrict__ val, double *__restrict__ D)
+{
+    for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < m; row += gridDim.x * blockDim.x) {
+        const int b = row >> 2, q = row & 3;
+        for (int k = ptr[b]; k < ptr[b + 1]; ++k)
+            for (int c = 0; c < 4; ++c) {
+                const int col = 4 * idx[k] + c;
+                if (col < n) D[(long long)row * n + col] = val[16LL * k + 4 * q + c];
+            }
+    }
+}
+
+// Inverse of an SPD matrix by Cholesky (A = L L^T), then L^-T L^-1; falls
+// back to Gauss-Jordan with partial pivoting when a pivot is not positive.
+static bool host_invert(int n, std::vector<double> &A)
+{
+    std::vector<double> L(A);
+    bool spd = true;
+    for (int j = 0; j < n && spd; ++j) {
+        double d = L[(size_t)j * n + j];
+        for (int k = 0; k < j; ++k) d -= L[(size_t)j * n + k] * L[(size_t)j * n + k];
+        if (!(d > 0.0)) { spd = false; break; }
+        d = std::sqrt(d);
+        L[(size_t)j * n + j] = d;
+        for (int i = j + 1; i < n; ++i) {
+            double s = L[(size_t)i * n + j];
+            for (int k = 0; k < j; ++k) s -= L[(size_t)i * n + k] * L[(size_t)j * n + k];
+            L[(size_t)i * n + j] = s / d;
+        }
+    }
+    if (spd) {
+        // Linv (lower), then Ainv = Linv^T Linv
+        std::vector<double> Li((size_t)n * n, 0.0);
+        for (int j = 0; j < n; ++j) {
+            Li[(size_t)j * n + j] = 1.0 / L[(size_t)j * n + j];
+            for (int i = j + 1; i < n; ++i) {
+                double s = 0.0;
+                for (int k = j; k < i; ++k) s -= L[(size_t)i * n + k] * Li[(size_t)k * n + j];
+                Li[(size_t)i * n + j] = s / L[(size_t)i * n + i];
+            }
+        }
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                double s = 0.0;
+                for (int k = std::max(i, j); k < n; ++k) s += Li[(size_t)k * n + i] * Li[(size_t)k * n + j];
+                A[(size_t)i * n + j] = s;
+            }
+        return true;
+    }
+    std::vector<double> M(A), I((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i) I[(size_t)i * n + i] = 1.0;
+    for (int c = 0; c < n; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < n; ++r)
+            if (std::fabs(M[(size_t)r * n + c]) > std::fabs(M[(size_t)piv * n + c])) piv = r;
+        if (M[(size_t)piv * n + c] == 0.0) return false;
+        if (piv != c)
+            for (int k = 0; k < n; ++k) {
+                std::swap(M[(size_t)c * n + k], M[(size_t)piv * n + k]);
+                std::swap(I[(size_t)c * n + k], I[(size_t)piv * n + k]);
+            }
+        const double inv = 1.0 / M[(size_t)c * n + c];
+        for (int k = 0; k < n; ++k) { M[(size_t)c * n + k] *= inv; I[(size_t)c * n + k] *= inv; }
+        for (int r = 0; r < n; ++r) {
+            if (r == c) continue;
+            const double fct = M[(size_t)r * n + c];
+            if (fct == 0.0) continue;
+            for (int k = 0; k < n; ++k) {
+                M[(size_t)r * n + k] -= fct * M[(size_t)c * n + k];
+                I[(size_t)r * n + k] -= fct * I[(size_t)c * n + k];
+            }
+        }
+    }
+    A.swap(I);
+    return true;
+}
+
+struct Level {
+    amgt_bsr A{}, P{}, R{};
+    double *inv_l1 = nullptr;
+    double *f = nullptr, *u = nullptr, *t = nullptr, *s = nullptr;
+    int n = 0;
+    int prec = AMGT_DOUBLE;           // smoother SpMVs on A_l
+    int prec_transfer = AMGT_DOUBLE;  // R_l / P_l SpMVs
+};
+
+}  // namespace amgt
+
+// Opaque handle of the C ABI.
+struct amgt_amg {
+    std::vector<amgt::Level> lv;
+    amgt_amg_params prm;
+    double *coarse_inv = nullptr;
+    int nc = 0;
+    long long n0 = 0;
+    double *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
+    double *scal = nullptr, *part = nullptr;
+    double *pinned = nullptr;  // host: ||r||^2 read-back
+    int sm_count = 0, grid0 = 0;
+    cudaGraphExec_t graph = nullptr;
+    cudaStream_t graph_stream = nullptr;
+    const double *graph_b = nullptr;
+    double *graph_xout = nullptr;
+    double setup_ms[5] = {0, 0, 0, 0, 0};
+    std::vector<double> hist;
+};
+
+using namespace amgt;
+
+namespace {
+
+void free_level(Level &v, cudaStream_t s)
+{
+    amgt_bsr_free(&v.A, (amgt_stream_t)s);
+    amgt_bsr_free(&v.P, (amgt_stream_t)s);
+    amgt_bsr_free(&v.R, (amgt_stream_t)s);
+    free_ptr(v.inv_l1, s);
+    free_ptr(v.f, s);
+    free_ptr(v.u, s);
+    free_ptr(v.t, s);
+    free_ptr(v.s, s);
+}
+
+void destroy_handle(amgt_amg *h, cudaStream_t s)
+{
+    if (!h) return;
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    if (h->graph_stream) cudaStreamDestroy(h->graph_stream);
+    for (auto &v : h->lv) free_level(v, s);
+    free_ptr(h->coarse_inv, s);
+    free_ptr(h->r, s);
+    free_ptr(h->z, s);
+    free_ptr(h->p, s);
+    free_ptr(h->q, s);
+    free_ptr(h->scal, s);
+    free_ptr(h->part, s);
+    if (h->pinned) cudaFreeHost(h->pinned);
+    delete h;
+}
+
+double now_ms()
+{
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+int grid_n(amgt_amg *h, long long n) { return grid_for(256, n, h->sm_count, 8); }
+
+// z = M f: one V(1,1) cycle
+int cycle(amgt_amg *h, const double *rhs0, double *out0, cudaStream_t s)
+{
+    auto &lv = h->lv;
+    const int L = (int)lv.size();
+    const double w = h->prm.relax_weight;
+    for (int l = 0; l < L - 1; ++l) {
+        Level &v = lv[l];
+        const double *f = (l == 0) ? rhs0 : v.f;
+        AMGT_LAUNCH(jacobi_zero_kernel, grid_n(h, v.n), 256, 0, s, (long long)v.n, f, v.inv_l1, w, v.u);
+        AMGT_TRY(spmv_residual(l == 0 ? AMGT_DOUBLE : v.prec, &v.A, f, v.u, v.t, s, h->sm_count));
+        AMGT_TRY(amgt_spmv(v.prec_transfer, 1.0, &v.R, v.t, 0.0, lv[l + 1].f, (amgt_stream_t)s));
+    }
+    Level &c = lv[L - 1];
+    const double *fc = (L == 1) ? rhs0 : c.f;
+    double *uc = (L == 1) ? out0 : c.s;
+    AMGT_LAUNCH(dense_mv_kernel, grid_for(8, c.n, h->sm_count, 8), 256, 0, s, c.n, h->coarse_inv, fc, uc);
+    for (int l = L - 2; l >= 0; --l) {
+        Level &v = lv[l];
+        const double *f = (l == 0) ? rhs0 : v.f;
+        double *out = (l == 0) ? out0 : v.s;
+        AMGT_TRY(amgt_spmv(v.prec_transfer, 1.0, &v.P, lv[l + 1].s, 1.0, v.u, (amgt_stream_t)s));
+        AMGT_TRY(spmv_jacobi(l == 0 ? h->prm.smooth_prec0 : v.prec, &v.A, v.inv_l1, w, f, v.u, out, s, h->sm_count));
+    }
+    return AMGT_OK;
+}
+
+int dot(amgt_amg *h, const double *a, const double *b, int slot, int op, cudaStream_t s)
+{
+    AMGT_LAUNCH(dot_kernel, kDotGrid, kDotThreads, 0, s, h->n0, a, b, h->part);
+    AMGT_LAUNCH(reduce_kernel, 1, kDotThreads, 0, s, h->part, kDotGrid, h->scal, slot, op);
+    return AMGT_OK;
+}
+
+// One PCG iteration after the first (q = A p ... p = z + beta p).
+int pcg_iteration(amgt_amg *h, double *x, cudaStream_t s)
+{
+    Level &v0 = h->lv[0];
+    AMGT_TRY(spmv_dot(AMGT_DOUBLE, &v0.A, h->p, h->q, h->part, h->grid0, s));
+    AMGT_LAUNCH(reduce_kernel, 1, kDotThreads, 0, s, h->part, h->grid0, h->scal, (int)S_PQ, (int)OP_ALPHA);
+    AMGT_LAUNCH(axpy2_dot_kernel, kDotGrid, kDotThreads, 0, s, h->n0, h->scal, h->p, h->q, x, h->r, h->part);
+    AMGT_LAUNCH(reduce_kernel, 1, kDotThreads, 0, s, h->part, kDotGrid, h->scal, (int)S_RR, (int)OP_STORE);
+    AMGT_CUDA_TRY(cudaMemcpyAsync(h->pinned, h->scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (h->prm.flexible) AMGT_TRY(dot(h, h->z, h->r, S_ZRPREV, OP_STORE, s));
+    AMGT_TRY(cycle(h, h->r, h->z, s));
+    AMGT_TRY(dot(h, h->r, h->z, S_RZ, h->prm.flexible ? OP_BETA_FLEX : OP_BETA, s));
+    AMGT_LAUNCH(xpby_kernel, grid_n(h, h->n0), 256, 0, s, h->n0, h->z, h->scal, h->p);
+    return AMGT_OK;
+}
+
+int build_graph(amgt_amg *h, double *x)
+{
+    if (h->graph && h->graph_xout == x) return AMGT_OK;
+    if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+    }
+    if (!h->graph_stream) AMGT_CUDA_TRY(cudaStreamCreateWithFlags(&h->graph_stream, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    AMGT_CUDA_TRY(cudaStreamBeginCapture(h->graph_stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = pcg_iteration(h, x, h->graph_stream);
+    const cudaError_t e = cudaStreamEndCapture(h->graph_stream, &g);
+    if (rc != AMGT_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    AMGT_CUDA_TRY(e);
+    const cudaError_t ei = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    AMGT_CUDA_TRY(ei);
+    h->graph_xout = x;
+    return AMGT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void amgt_amg_default_params(amgt_amg_params *p)
+{
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->max_levels = 25;
+    p->max_coarse_rows = 4096;
+    p->tol = 1e-8;
+    p->max_iter = 200;
+    p->relax_weight = 1.0;
+    p->flexible = 0;
+    p->use_graph = 1;
+    p->galerkin_by_level = 0;
+    p->smooth_prec0 = AMGT_DOUBLE;
+}
+
+int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const amgt_amg_params *params,
+                   amgt_amg **out, amgt_stream_t stream)
+{
+    if (!A || !out || num_interp < 0 || (num_interp > 0 && !P) || A->num_rows != A->num_cols || A->num_rows <= 0)
+        return AMGT_ERR_INVALID;
+    *out = nullptr;
+    DeviceState *st;
+    AMGT_TRY(device_state(&st));
+    cudaStream_t s = (cudaStream_t)stream;
+    amgt_amg *h = new amgt_amg();
+    if (params) h->prm = *params;
+    else amgt_amg_default_params(&h->prm);
+    if (h->prm.smooth_prec0 < AMGT_DOUBLE || h->prm.smooth_prec0 > AMGT_BF16) h->prm.smooth_prec0 = AMGT_DOUBLE;
+    h->sm_count = st->sm_count;
+    int L = num_interp + 1;
+    if (h->prm.max_levels > 0 && L > h->prm.max_levels) L = h->prm.max_levels;
+    int rc = AMGT_OK;
+    double t0 = now_ms(), t1;
+    h->lv.resize(L);
+    // hierarchy
+    if ((rc = amgt_csr_to_bsr(A, &h->lv[0].A, stream))) goto fail;
+    h->lv[0].n = A->num_rows;
+    AMGT_CUDA_TRY(cudaStreamSynchronize(s));
+    t1 = now_ms();
+    h->setup_ms[0] += t1 - t0;
+    for (int l = 0; l < L - 1; ++l) {
+        Level &v = h->lv[l];
+        if (P[l].num_rows != v.n || P[l].num_cols <= 0) { rc = AMGT_ERR_INVALID; goto fail; }
+        v.prec = amgt_precision_for_level(l);
+        v.prec_transfer = amgt_precision_for_level(l + 1);
+        t0 = now_ms();
+        if ((rc = amgt_csr_to_bsr(&P[l], &v.P, stream))) goto fail;
+        if ((rc = amgt_bsr_transpose(&v.P, &v.R, stream))) goto fail;
+        AMGT_CUDA_TRY(cudaStreamSynchronize(s));
+        t1 = now_ms();
+        h->setup_ms[1] += t1 - t0;
+        const int gp = h->prm.galerkin_by_level ? v.prec : AMGT_DOUBLE;
+        amgt_bsr AP{};
+        if ((rc = amgt_spgemm(gp, &v.A, &v.P, &AP, nullptr, stream))) goto fail;
+        rc = amgt_spgemm(gp, &v.R, &AP, &h->lv[l + 1].A, nullptr, stream);
+        amgt_bsr_free(&AP, stream);
+        if (rc) goto fail;
+        h->lv[l + 1].n = h->lv[l + 1].A.row;
+        AMGT_CUDA_TRY(cudaStreamSynchronize(s));
+        t0 = now_ms();
+        h->setup_ms[2] += t0 - t1;
+    }
+    h->lv[L - 1].prec = amgt_precision_for_level(L - 1);
+    t0 = now_ms();
+    // smoother data, shadows, work vectors
+    for (int l = 0; l < L; ++l) {
+        Level &v = h->lv[l];
+        if ((rc = alloc_n(&v.inv_l1, v.n, s))) goto fail;
+        if ((rc = bsr_l1_norms(&v.A, v.inv_l1, 1, s, h->sm_count))) goto fail;
+        if ((rc = amgt_bsr_make_shadow(&v.A, v.prec, stream))) goto fail;
+        if (l == 0 && (rc = amgt_bsr_make_shadow(&v.A, h->prm.smooth_prec0, stream))) goto fail;
+        if (l < L - 1) {
+            if ((rc = amgt_bsr_make_shadow(&v.P, v.prec_transfer, stream))) goto fail;
+            if ((rc = amgt_bsr_make_shadow(&v.R, v.prec_transfer, stream))) goto fail;
+        }
+        if ((rc = alloc_n(&v.u, v.n, s)) || (rc = alloc_n(&v.t, v.n, s))) goto fail;
+        if (l > 0 && ((rc = alloc_n(&v.f, v.n, s)) || (rc = alloc_n(&v.s, v.n, s)))) goto fail;
+    }
+    // coarsest: dense inverse
+    {
+        Level &c = h->lv[L - 1];
+        h->nc = c.n;
+        if (c.n > h->prm.max_coarse_rows) { rc = AMGT_ERR_TOO_LARGE; goto fail; }
+        double *D = nullptr;
+        if ((rc = alloc_n(&D, (size_t)c.n * c.n, s))) goto fail;
+        AMGT_CUDA_TRY(cudaMemsetAsync(D, 0, sizeof(double) * c.n * c.n, s));
+        AMGT_LAUNCH(bsr_to_dense_kernel, grid_for(256, c.n, h->sm_count, 8), 256, 0, s, c.n, c.n, c.A.blcPtr,
+                    c.A.blcIdx, c.A.blcVal, D);
+        std::vector<double> hd((size_t)c.n * c.n);
+        AMGT_CUDA_TRY(cudaMemcpyAsync(hd.data(), D, sizeof(double) * hd.size(), cudaMemcpyDeviceToHost, s));
+        AMGT_CUDA_TRY(cudaStreamSynchronize(s));
+        if (!host_invert(c.n, hd)) {
+            free_ptr(D, s);
+            rc = AMGT_ERR_INVALID;
+            goto fail;
+        }
+        AMGT_CUDA_TRY(cudaMemcpyAsync(D, hd.data(), sizeof(double) * hd.size(), cudaMemcpyHostToDevice, s));
+        h->coarse_inv = D;
+        if (L == 1) c.s = nullptr;
+    }
+    // Krylov vectors and scalars
+    h->n0 = h->lv[0].n;
+    h->grid0 = epi_grid(&h->lv[0].A, h->sm_count);
+    if ((rc = alloc_n(&h->r, h->n0, s)) || (rc = alloc_n(&h->z, h->n0, s)) || (rc = alloc_n(&h->p, h->n0, s)) ||
+        (rc = alloc_n(&h->q, h->n0, s)) || (rc = alloc_n(&h->scal, S_NSCAL, s)) ||
+        (rc = alloc_n(&h->part, std::max(h->grid0, kDotGrid), s)))
+        goto fail;
+    AMGT_CUDA_TRY(cudaMemsetAsync(h->scal, 0, sizeof(double) * S_NSCAL, s));
+    AMGT_CUDA_TRY(cudaMallocHost(&h->pinned, sizeof(double) * 4));
+    AMGT_CUDA_TRY(cudaStreamSynchronize(s));
+    h->setup_ms[3] += now_ms() - t0;
+    *out = h;
+    return AMGT_OK;
+fail:
+    destroy_handle(h, s);
+    return rc;
+}
+
+int amgt_amg_solve(amgt_amg *h, const double *b, double *x, int *iterations, double *rel_res, amgt_stream_t stream)
+{
+    if (!h || !b || !x) return AMGT_ERR_INVALID;
+    cudaStream_t s = (cudaStream_t)stream;
+    Level &v0 = h->lv[0];
+    h->hist.clear();
+    // r = b - A x, ||b||^2, ||r||^2
+    AMGT_TRY(spmv_residual(AMGT_DOUBLE, &v0.A, b, x, h->r, s, h->sm_count));
+    AMGT_TRY(dot(h, b, b, S_BB, OP_STORE, s));
+    AMGT_TRY(dot(h, h->r, h->r, S_RR, OP_STORE, s));
+    AMGT_CUDA_TRY(cudaMemcpyAsync(h->pinned, h->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    AMGT_CUDA_TRY(cudaStreamSynchronize(s));
+    const double bb = h->pinned[S_BB];
+    double rel = bb > 0 ? std::sqrt(h->pinned[S_RR] / bb) : 0.0;
+    h->hist.push_back(rel);
+    int it = 0;
+    if (rel > h->prm.tol) {
+        AMGT_TRY(cycle(h, h->r, h->z, s));
+        AMGT_TRY(dot(h, h->r, h->z, S_RZ, OP_STORE, s));
+        AMGT_CUDA_TRY(cudaMemcpyAsync(h->p, h->z, sizeof(double) * h->n0, cudaMemcpyDeviceToDevice, s));
+        uint64_t per_iter = 0;
+        if (h->prm.use_graph) {
+            const uint64_t c0 = amgt_kernel_launch_count();
+            AMGT_TRY(build_graph(h, x));
+            per_iter = amgt_kernel_launch_count() - c0;
+        }
+        for (it = 1; it <= h->prm.max_iter; ++it) {
+            if (h->prm.use_graph) {
+                AMGT_CUDA_TRY(cudaGraphLaunch(h->graph, s));
+                for (uint64_t k = 0; k < per_iter; ++k) count_launch();
+            } else {
+                AMGT_TRY(pcg_iteration(h, x, s));
+            }
+            AMGT_CUDA_TRY(cudaStreamSynchronize(s));
+            rel = std::sqrt(std::max(0.0, h->pinned[0]) / bb);
+            h->hist.push_back(rel);
+            if (rel <= h->prm.tol) break;
+        }
+        if (it > h->prm.max_iter) it = h->prm.max_iter;
+    }
+    if (iterations) *iterations = it;
+    if (rel_res) *rel_res = rel;
+    return AMGT_OK;
+}
+
+int amgt_amg_num_levels(const amgt_amg *h) { return h ? (int)h->lv.size() : 0; }
+
+int amgt_amg_level(const amgt_amg *h, int level, amgt_bsr *A_view, int *prec)
+{
+    if (!h || level < 0 || level >= (int)h->lv.size()) return AMGT_ERR_INVALID;
+    if (A_view) *A_view = h->lv[level].A;
+    if (prec) *prec = h->lv[level].prec;
+    return AMGT_OK;
+}
+
+int amgt_amg_setup_times(const amgt_amg *h, double *ms)
+{
+    if (!h || !ms) return AMGT_ERR_INVALID;
+    for (int i = 0; i < 4; ++i) ms[i] = h->setup_ms[i];
+    return AMGT_OK;
+}
+
+int amgt_amg_residual_history(const amgt_amg *h, double *hist, int cap)
+{
+    if (!h) return -1;
+    const int n = (int)h->hist.size();
+    for (int i = 0; i < n && i < cap && hist; ++i) hist[i] = h->hist[i];
+    return n;
+}
+
+int amgt_amg_destroy(amgt_amg *h, amgt_stream_t stream)
+{
+    destroy_handle(h, (cudaStream_t)stream);
+    return AMGT_OK;
+}
+
+}  // extern "C"

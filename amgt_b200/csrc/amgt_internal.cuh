@@ -92,6 +92,17 @@ int block_row_stats(amgt_bsr *A, cudaStream_t s);
 int spmv_segmented_with_scratch(int prec, double alpha, const amgt_bsr *A, const double *x, double beta, double *y,
                                 double *part, int sm_count, cudaStream_t s);
 
+// Fused SpMV forms (spmv.cu): r = f - A u; u_out = u + w (f - A u) .* inv_l1;
+// out = A u with per-CTA partials of u . out (grid CTAs, from epi_grid);
+// l1 row norms (or their inverses).
+int epi_grid(const amgt_bsr *A, int sm_count);
+int spmv_residual(int prec, const amgt_bsr *A, const double *f, const double *u, double *r, cudaStream_t s,
+                  int sm_count);
+int spmv_jacobi(int prec, const amgt_bsr *A, const double *inv_l1, double w, const double *f, const double *u,
+                double *u_out, cudaStream_t s, int sm_count);
+int spmv_dot(int prec, const amgt_bsr *A, const double *u, double *out, double *partial, int grid, cudaStream_t s);
+int bsr_l1_norms(const amgt_bsr *A, double *l1, int invert, cudaStream_t s, int sm_count);
+
 // Exclusive scan of n ints (in may equal out), CUB with allocator scratch.
 int exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s);
 // Exclusive scan of n 64-bit ints.

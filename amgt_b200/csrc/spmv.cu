@@ -238,6 +238,95 @@ spmm_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__re
     }
 }
 
+// SpMV with a fused row epilogue (the smoother / residual / Krylov forms).
+//   EPI_RESID : out = f - A u                          (residual, par_cycle.c:678)
+//   EPI_JACOBI: out = u + w (f - A u) / l1             (Relax 18, par_relax.c:1178-1260)
+//   EPI_DOT   : out = A u, and dot partials of u . out (PCG's p.q), one per CTA
+// x is u.  Same load pattern and per-row summation order as spmv_kernel.
+enum { EPI_RESID = 0, EPI_JACOBI = 1, EPI_DOT = 2 };
+
+struct EpiArgs {
+    const double *f;       // RESID, JACOBI
+    const double *inv_l1;  // JACOBI
+    double w;              // JACOBI
+    double *out;
+    double *partial;       // DOT: [gridDim.x]
+};
+
+template <int PREC, int LPR, bool SAFE, int EPI>
+__global__ void __launch_bounds__(256)
+spmv_epi_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__restrict__ idx,
+                const void *__restrict__ val, const double *__restrict__ x, EpiArgs e)
+{
+    using acc_t = typename ValTraits<PREC>::acc_t;
+    constexpr int RPW = 32 / LPR;
+    constexpr int G = LPR / 4;
+    __shared__ double sred[8];
+    const int lane = threadIdx.x & 31;
+    const int sub = lane / LPR, l = lane % LPR, g = l >> 2, q = l & 3;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    double dot = 0.0;
+    for (int b0 = warp * RPW; b0 < brow; b0 += nwarps * RPW) {
+        const int b = b0 + sub;
+        acc_t acc = 0;
+        if (b < brow) {
+            const int start = ptr[b], end = ptr[b + 1];
+            int k = start + g;
+            for (; k + G < end; k += 2 * G) {
+                const int c0 = __ldcs(idx + k), c1 = __ldcs(idx + k + G);
+                acc = block_row_dot<PREC, SAFE>(val, x, n, k, q, c0, acc);
+                acc = block_row_dot<PREC, SAFE>(val, x, n, k + G, q, c1, acc);
+            }
+            if (k < end) acc = block_row_dot<PREC, SAFE>(val, x, n, k, q, __ldcs(idx + k), acc);
+        }
+#pragma unroll
+        for (int o = 4; o < LPR; o <<= 1) acc += __shfl_xor_sync(FULL, acc, o);
+        if (b < brow && g == 0) {
+            const int row = 4 * b + q;
+            if (row < m) {
+                const double ax = (double)acc;
+                if constexpr (EPI == EPI_RESID) {
+                    e.out[row] = e.f[row] - ax;
+                } else if constexpr (EPI == EPI_JACOBI) {
+                    e.out[row] = x[row] + e.w * (e.f[row] - ax) * e.inv_l1[row];
+                } else {
+                    e.out[row] = ax;
+                    dot += x[row] * ax;
+                }
+            }
+        }
+    }
+    if constexpr (EPI == EPI_DOT) {
+        // fixed-order reduction: lanes, then warps (deterministic for a fixed grid)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(FULL, dot, o);
+        if (lane == 0) sred[threadIdx.x >> 5] = dot;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0.0;
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += sred[i];
+            e.partial[blockIdx.x] = s;
+        }
+    }
+}
+
+// l1 row norms sum_j |a_ij| (hypre_ParCSRComputeL1Norms option 1,
+// AmgT_HYPRE/src/parcsr_ls/ams.c:627-636), one thread per scalar row.
+__global__ void l1_norm_kernel(int m, const int *__restrict__ ptr, const double *__restrict__ val,
+                               double *__restrict__ l1, int invert)
+{
+    for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < m; row += gridDim.x * blockDim.x) {
+        const int b = row >> 2, q = row & 3;
+        double s = 0.0;
+        for (int k = ptr[b]; k < ptr[b + 1]; ++k) {
+            const double *v = val + 16LL * k + 4 * q;
+            s += fabs(v[0]) + fabs(v[1]) + fabs(v[2]) + fabs(v[3]);
+        }
+        l1[row] = invert ? (s != 0.0 ? 1.0 / s : 0.0) : s;
+    }
+}
+
 __global__ void scale_kernel(long long n, double beta, double *__restrict__ y)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -397,6 +486,78 @@ int spmv_segmented_with_scratch(int prec, double alpha, const amgt_bsr *A, const
     }
 }
 
+template <int PREC, int EPI>
+static int launch_epi(const amgt_bsr *A, const void *val, const double *x, const EpiArgs &e, int grid,
+                      cudaStream_t s)
+{
+    const bool safe = (A->col % 4 != 0) || ((uintptr_t)x % 16 != 0);
+    const int lpr = pick_lpr(A);
+#define AMGT_EPI_CASE(L)                                                                                     \
+    if (lpr == L) {                                                                                          \
+        if (safe)                                                                                            \
+            AMGT_LAUNCH((spmv_epi_kernel<PREC, L, true, EPI>), grid, 256, 0, s, A->row, A->col, A->blc_row,  \
+                        A->blcPtr, A->blcIdx, val, x, e);                                                    \
+        else                                                                                                 \
+            AMGT_LAUNCH((spmv_epi_kernel<PREC, L, false, EPI>), grid, 256, 0, s, A->row, A->col, A->blc_row, \
+                        A->blcPtr, A->blcIdx, val, x, e);                                                    \
+        return AMGT_OK;                                                                                      \
+    }
+    AMGT_EPI_CASE(4)
+    AMGT_EPI_CASE(8)
+    AMGT_EPI_CASE(16)
+    AMGT_EPI_CASE(32)
+#undef AMGT_EPI_CASE
+    return AMGT_ERR_INVALID;
+}
+
+template <int EPI>
+static int launch_epi_prec(int prec, const amgt_bsr *A, const double *x, const EpiArgs &e, int grid,
+                           cudaStream_t s)
+{
+    const void *val = value_array(A, prec);
+    if (!val) return AMGT_ERR_INVALID;
+    switch (prec) {
+    case AMGT_DOUBLE: return launch_epi<AMGT_DOUBLE, EPI>(A, val, x, e, grid, s);
+    case AMGT_FLOAT: return launch_epi<AMGT_FLOAT, EPI>(A, val, x, e, grid, s);
+    case AMGT_HALF: return launch_epi<AMGT_HALF, EPI>(A, val, x, e, grid, s);
+    case AMGT_BF16: return launch_epi<AMGT_BF16, EPI>(A, val, x, e, grid, s);
+    default: return AMGT_ERR_INVALID;
+    }
+}
+
+int epi_grid(const amgt_bsr *A, int sm_count)
+{
+    const int lpr = pick_lpr(A);
+    return grid_for(8 * (32 / lpr), A->blc_row, sm_count, 8);
+}
+
+int spmv_residual(int prec, const amgt_bsr *A, const double *f, const double *u, double *r, cudaStream_t s,
+                  int sm_count)
+{
+    EpiArgs e{f, nullptr, 0.0, r, nullptr};
+    return launch_epi_prec<EPI_RESID>(prec, A, u, e, epi_grid(A, sm_count), s);
+}
+
+int spmv_jacobi(int prec, const amgt_bsr *A, const double *inv_l1, double w, const double *f, const double *u,
+                double *u_out, cudaStream_t s, int sm_count)
+{
+    EpiArgs e{f, inv_l1, w, u_out, nullptr};
+    return launch_epi_prec<EPI_JACOBI>(prec, A, u, e, epi_grid(A, sm_count), s);
+}
+
+int spmv_dot(int prec, const amgt_bsr *A, const double *u, double *out, double *partial, int grid, cudaStream_t s)
+{
+    EpiArgs e{nullptr, nullptr, 0.0, out, partial};
+    return launch_epi_prec<EPI_DOT>(prec, A, u, e, grid, s);
+}
+
+int bsr_l1_norms(const amgt_bsr *A, double *l1, int invert, cudaStream_t s, int sm_count)
+{
+    AMGT_LAUNCH(l1_norm_kernel, grid_for(256, A->row, sm_count, 8), 256, 0, s, A->row, A->blcPtr, A->blcVal, l1,
+                invert);
+    return AMGT_OK;
+}
+
 }  // namespace amgt
 
 using namespace amgt;
@@ -458,6 +619,41 @@ int amgt_spmm(int prec, double alpha, const amgt_bsr *A, int nvec, const double 
     case AMGT_HALF: return launch_spmm<AMGT_HALF>(A, val, alpha, nvec, x, ldx, beta, y, ldy, s, st->sm_count);
     default: return launch_spmm<AMGT_BF16>(A, val, alpha, nvec, x, ldx, beta, y, ldy, s, st->sm_count);
     }
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int amgt_bsr_l1_norms(const amgt_bsr *A, double *l1, amgt_stream_t stream)
+{
+    if (!A || (A->row > 0 && (!l1 || !A->blcPtr))) return AMGT_ERR_INVALID;
+    if (A->row == 0) return AMGT_OK;
+    DeviceState *st;
+    AMGT_TRY(device_state(&st));
+    return bsr_l1_norms(A, l1, 0, (cudaStream_t)stream, st->sm_count);
+}
+
+int amgt_bsr_residual(int prec, const amgt_bsr *A, const double *f, const double *u, double *r,
+                      amgt_stream_t stream)
+{
+    if (!A || prec < AMGT_DOUBLE || prec > AMGT_BF16) return AMGT_ERR_INVALID;
+    if (A->row == 0) return AMGT_OK;
+    if (!f || !u || !r || !A->blcPtr || !value_array(A, prec)) return AMGT_ERR_INVALID;
+    DeviceState *st;
+    AMGT_TRY(device_state(&st));
+    return spmv_residual(prec, A, f, u, r, (cudaStream_t)stream, st->sm_count);
+}
+
+int amgt_bsr_jacobi(int prec, const amgt_bsr *A, const double *inv_l1, double weight, const double *f,
+                    const double *u, double *u_out, amgt_stream_t stream)
+{
+    if (!A || prec < AMGT_DOUBLE || prec > AMGT_BF16 || A->row != A->col) return AMGT_ERR_INVALID;
+    if (A->row == 0) return AMGT_OK;
+    if (!inv_l1 || !f || !u || !u_out || u == u_out || !A->blcPtr || !value_array(A, prec)) return AMGT_ERR_INVALID;
+    DeviceState *st;
+    AMGT_TRY(device_state(&st));
+    return spmv_jacobi(prec, A, inv_l1, weight, f, u, u_out, (cudaStream_t)stream, st->sm_count);
 }
 
 }  // extern "C"

@@ -197,6 +197,94 @@ def build_hierarchy(amgt, torch, A, grid, max_levels=8, min_rows=512):
     return levels, mats
 
 
+def geometric_interps(problems, dims, coarse_rows=64):
+    """Linear interpolation operators (host CSR) down to <= coarse_rows."""
+    Ps = []
+    while dims[0] * dims[1] * dims[2] > coarse_rows:
+        P, cd = problems.interp(*dims)
+        if cd == dims:
+            break
+        Ps.append(P)
+        dims = cd
+    return Ps
+
+
+MIXED_POLICY = [0, 1, 1, 2]  # level 0 fp64, 1-2 fp32, >= 3 fp16 (values); fp32 accumulation
+
+
+def amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, policy, smooth0, flexible, reps=2):
+    """Setup + solve to ||b - A x|| / ||b|| <= 1e-8 through the library;
+    device-resident inputs.  Returns timings, iterations and the residual
+    recomputed in fp64 from the returned x."""
+    from amgt_b200.amg import AmgSolver, default_params
+
+    amgt.set_level_policy(policy)
+    dev = lambda M: (M[0], M[1]) + tuple(torch.from_numpy(v).cuda() for v in M[2:])  # noqa: E731
+    dA, dPs = dev(A_host), [dev(P) for P in Ps_host]
+    b = torch.from_numpy(b_host).cuda()
+    prm = default_params(flexible=flexible, smooth_prec0=smooth0)
+    S = AmgSolver(dA, dPs, prm)  # warm-up: module loads, pools
+    S.solve(b)
+    S.free()
+    torch.cuda.synchronize()
+    best = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        S = AmgSolver(dA, dPs, prm)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        x, it, rel = S.solve(b)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        run = {"setup_s": t1 - t0, "solve_s": t2 - t1, "iters": it, "relres": rel}
+        if best is None or run["setup_s"] + run["solve_s"] < best["setup_s"] + best["solve_s"]:
+            best = dict(run, x=x.clone(), levels=[S.level(l) for l in range(S.num_levels())],
+                        setup_ms=S.setup_times())
+        S.free()
+    # fp64 verification of the returned solution (library fp64 SpMV)
+    Ab = amgt.Bsr.from_csr(*dA)
+    r = b.clone()
+    Ab.spmv(best["x"], r, alpha=-1.0, beta=1.0)
+    best["relres_fp64_verified"] = float(torch.linalg.vector_norm(r) / torch.linalg.vector_norm(b))
+    amgt.set_level_policy([])
+    return best
+
+
+def amg_e2e(amgt, torch, A_host, Ps_host, b_host, policy, smooth0, flexible):
+    """Same, end to end from host buffers: CSR + interpolation + b copied to
+    the device, setup, solve, x copied back, all inside the timed region."""
+    from amgt_b200.amg import AmgSolver, default_params
+
+    amgt.set_level_policy(policy)
+    prm = default_params(flexible=flexible, smooth_prec0=smooth0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    dev = lambda M: (M[0], M[1]) + tuple(torch.from_numpy(v).cuda() for v in M[2:])  # noqa: E731
+    S = AmgSolver(dev(A_host), [dev(P) for P in Ps_host], prm)
+    x, it, rel = S.solve(torch.from_numpy(b_host).cuda())
+    xh = x.cpu()
+    t1 = time.perf_counter()
+    S.free()
+    amgt.set_level_policy([])
+    h2d = sum(v.nbytes for M in [A_host] + list(Ps_host) for v in M[2:]) + b_host.nbytes
+    return {"value": round(t1 - t0, 4), "unit": "s", "iters": it, "h2d_bytes": int(h2d), "d2h_bytes": int(xh.numel() * 8)}
+
+
+def cpu_amg(grid, b_host):
+    """The oracle's AMG-PCG (C, OpenMP, all host threads) on the same problem."""
+    from oracle import oracle as orc
+
+    A = orc.laplacian(*grid)
+    Ps = orc.geometric_hierarchy(*grid)
+    t0 = time.perf_counter()
+    h = orc.Amg(A, Ps)
+    t1 = time.perf_counter()
+    x, it, rel, _ = h.solve(b_host)
+    t2 = time.perf_counter()
+    return {"setup_s": round(t1 - t0, 3), "solve_s": round(t2 - t1, 3), "total_s": round(t2 - t0, 3), "iters": it,
+            "relres": rel, "cores": orc.num_threads(), "kind": "port"}, x
+
+
 def run_amgt(args):
     import torch
     import torch.distributed as dist
@@ -294,6 +382,33 @@ def run_amgt(args):
         levels[lvl]["spmv_gbs"] = round(b / (lms * 1e-3) / 1e9, 1)
     del mats
 
+    # setup + solve to 1e-8: plain fp64 and mixed precision (the metric's first part)
+    setup_solve = None
+    if not args.no_solve:
+        Ps_host = geometric_interps(problems, GRID)
+        A_host = (m, n, ia, ja, a)
+        b_host = problems.rand_uniform(0, n)
+        f64 = amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, [0], 0, 0)
+        mix = amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, MIXED_POLICY, 1, 1)
+        err = float(torch.linalg.vector_norm(mix["x"] - f64["x"]) / torch.linalg.vector_norm(f64["x"]))
+        setup_solve = {}
+        for name, rres in (("fp64", f64), ("mixed", mix)):
+            setup_solve[name] = {k: (round(v, 5) if isinstance(v, float) else v) for k, v in rres.items()
+                                 if k not in ("x", "levels", "setup_ms")}
+            setup_solve[name]["total_s"] = round(rres["setup_s"] + rres["solve_s"], 5)
+            setup_solve[name]["setup_ms"] = {k: round(v, 3) for k, v in rres["setup_ms"].items()}
+            setup_solve[name]["levels"] = rres["levels"]
+        setup_solve["mixed"]["policy"] = "levels 0 fp64 (residual) / fp32 smoother, 1-2 fp32, >=3 fp16; flexible CG"
+        setup_solve["mixed"]["rel_err_vs_fp64_solution"] = err
+        setup_solve["mixed"]["speedup_vs_fp64"] = round(setup_solve["fp64"]["total_s"] / setup_solve["mixed"]["total_s"], 3)
+        setup_solve["e2e_fp64"] = amg_e2e(amgt, torch, A_host, Ps_host, b_host, [0], 0, 0)
+        setup_solve["problem"] = (f"3D 7-point Poisson {GRID[0]}^3, b uniform[-1,1] seed 0, linear-interpolation "
+                                  f"hierarchy ({len(Ps_host) + 1} levels), PCG + V(1,1) l1-Jacobi, tol 1e-8")
+        if world == 1 and rank == 0 and not args.no_cpu:
+            setup_solve["cpu_oracle"], xo = cpu_amg(GRID, b_host)
+            setup_solve["fp64"]["rel_err_vs_cpu_oracle"] = float(
+                np.linalg.norm(f64["x"].cpu().numpy() - xo) / np.linalg.norm(xo))
+
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -325,6 +440,7 @@ def run_amgt(args):
         "gpu_launches": int(launches),
         "clocks": clocks,
         "levels": levels,
+        "setup_solve": setup_solve,
     }
     print(json.dumps(line), flush=True)
 
@@ -338,6 +454,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-levels", action="store_true", help="skip the hierarchy / per-level report")
+    ap.add_argument("--no-solve", action="store_true", help="skip the AMG setup + solve report")
     ap.add_argument("--grid", type=int, default=128, help="cube side (profiling captures only)")
     args = ap.parse_args()
     global GRID

@@ -188,6 +188,25 @@ AMGT_API int amgt_spmm(int prec, double alpha, const amgt_bsr *A, int nvec,
               const double *x, int ldx, double beta, double *y, int ldy,
               amgt_stream_t stream);
 
+/* ------------------------------------------------ smoother / residual */
+/* l1 row norms l1[i] = sum_j |a_ij| of the fp64 values: the norms HYPRE's
+ * l1-Jacobi (relax 18) divides by, hypre_ParCSRComputeL1Norms option 1
+ * (R/parcsr_ls/ams.c:627-636). */
+AMGT_API int amgt_bsr_l1_norms(const amgt_bsr *A, double *l1, amgt_stream_t stream);
+
+/* r = f - A u in one pass (the residual of hypre_BoomerAMGCycle,
+ * R/parcsr_ls/par_cycle.c:678, MatvecOutOfPlace(-1, A, u, 1, f, r)). */
+AMGT_API int amgt_bsr_residual(int prec, const amgt_bsr *A, const double *f,
+                               const double *u, double *r, amgt_stream_t stream);
+
+/* One l1-Jacobi sweep in one pass: u_out = u + weight * (f - A u) ./ l1,
+ * inv_l1 = 1 ./ l1 (relax 18, hypre_BoomerAMGRelax18WeightedL1Jacobi /
+ * Relax7Jacobi, R/parcsr_ls/par_relax.c:1178-1260, which needs a copy of f,
+ * a matvec and a vector update).  u_out must not alias u. */
+AMGT_API int amgt_bsr_jacobi(int prec, const amgt_bsr *A, const double *inv_l1,
+                             double weight, const double *f, const double *u,
+                             double *u_out, amgt_stream_t stream);
+
 /* Segmented SpMV that allocates nothing.  No counterpart in the reference.
  *
  * For callers that cannot allocate device memory while they run a matvec:
@@ -225,6 +244,49 @@ AMGT_API int amgt_spmv_segmented_noalloc(int prec, double alpha, const amgt_bsr 
  * Host-blocking twice (upper bound and C size). */
 AMGT_API int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C,
                 amgt_csr *Ccsr, amgt_stream_t stream);
+
+/* ------------------------------------------------ AMG setup + solve */
+/* Galerkin hierarchy on mBSR and a PCG solve preconditioned by one V(1,1)
+ * cycle with l1-Jacobi smoothing: the setup + solve that the two hooks
+ * drive inside BoomerAMG-PCG (hypre_ParCSRMatrixRAPKT for the products,
+ * hypre_BoomerAMGCycle with relax 18, krylov/pcg.c).  Coarsening and
+ * interpolation are the caller's (they are BoomerAMG's, outside the AmgT
+ * path): P[l] maps level l+1 to level l.  Level precisions follow
+ * amgt_precision_for_level; the finest residual, the Krylov vectors and
+ * dots, and the coarsest (dense, inverted) solve are always fp64. */
+typedef struct {
+    int max_levels;        /* cap on levels (default 25)                    */
+    int max_coarse_rows;   /* largest coarsest level (dense inverse), 4096  */
+    double tol;            /* ||b - A x|| / ||b|| target (default 1e-8)     */
+    int max_iter;          /* default 200                                   */
+    double relax_weight;   /* l1-Jacobi weight (default 1)                  */
+    int flexible;          /* flexible CG (Polak-Ribiere beta), default 0   */
+    int use_graph;         /* one CUDA graph per iteration (default 1)      */
+    int galerkin_by_level; /* Galerkin products at each level's precision,
+                              as AmgT's hypreDevice_CSRSpGemm does (0: fp64) */
+    int smooth_prec0;      /* precision of the finest-level smoother SpMV   */
+} amgt_amg_params;
+
+typedef struct amgt_amg amgt_amg;
+
+AMGT_API void amgt_amg_default_params(amgt_amg_params *p);
+/* Host-blocking (sizes of every level; coarsest inverse on the host). */
+AMGT_API int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P,
+                            const amgt_amg_params *params, amgt_amg **out,
+                            amgt_stream_t stream);
+/* x: initial guess in, solution out (device).  Reads ||r||^2 (8 bytes) once
+ * per iteration; each iteration after the first is one CUDA graph launch. */
+AMGT_API int amgt_amg_solve(amgt_amg *amg, const double *b, double *x,
+                            int *iterations, double *rel_res, amgt_stream_t stream);
+AMGT_API int amgt_amg_num_levels(const amgt_amg *amg);
+/* Borrowed view of level `level`'s operator and its cycle precision. */
+AMGT_API int amgt_amg_level(const amgt_amg *amg, int level, amgt_bsr *A_view, int *prec);
+/* ms[0..3]: conversion of A, P conversion + transpose, Galerkin SpGEMMs,
+ * smoother data + shadows + coarse inverse + vectors. */
+AMGT_API int amgt_amg_setup_times(const amgt_amg *amg, double *ms);
+/* Relative residual per iteration (entry 0 = initial); returns the count. */
+AMGT_API int amgt_amg_residual_history(const amgt_amg *amg, double *hist, int cap);
+AMGT_API int amgt_amg_destroy(amgt_amg *amg, amgt_stream_t stream);
 
 /* ------------------------------------------ HYPRE-facing mirror layer */
 /* The fields of hypre_CSRMatrix that the AmgT path reads and writes

@@ -769,3 +769,301 @@ ORC_EXPORT void orc_bsr_transpose(int brA, int bcA, const int *aptr, const int *
         }
     free(fill);
 }
+
+/* ------------------------------------------------------------------ AMG */
+/* CPU restatement of the setup + solve that drives the two hooks
+ * (BoomerAMG-PCG with a V(1,1) l1-Jacobi cycle): Galerkin products
+ * A_{l+1} = P_l^T (A_l P_l) on mBSR (hypre_ParCSRMatrixRAPKT,
+ * R/parcsr_mv/par_csr_triplemat_device.c:630-905), l1 norms (option 1,
+ * R/parcsr_ls/ams.c:627-636), the cycle of R/parcsr_ls/par_cycle.c:678-751
+ * with relax 18 (R/parcsr_ls/par_relax.c:1178-1260), a dense inverse on the
+ * coarsest level, and PCG with ||r||/||b|| stopping (R/krylov/pcg.c).  All
+ * fp64.  Interpolation operators are inputs. */
+typedef struct {
+    int n;
+    int *bptr, *bidx;
+    uint16_t *bmap;
+    double *bval;
+    int nblk;
+    /* transfer to the next level */
+    int pn;                               /* coarse size */
+    int *pptr, *pidx, *rptr, *ridx;
+    uint16_t *pmap, *rmap;
+    double *pval, *rval;
+    double *inv_l1, *f, *u, *t, *s;
+} orc_level;
+
+typedef struct {
+    int L;
+    orc_level *lv;
+    double *cinv; /* dense inverse of the coarsest operator */
+    double w;
+    double *r, *z, *p, *q;
+} orc_amg;
+
+static void orc_csr_to_level(int m, int n, const int *ia, const int *ja, const double *a, int **bptr, int **bidx,
+                             uint16_t **bmap, double **bval, int *nblk)
+{
+    const int brow = (m + 3) / 4;
+    *bptr = (int *)calloc((size_t)brow + 1, sizeof(int));
+    int mx;
+    int64_t nb = orc_csr2bsr_count(m, n, ia, ja, *bptr, &mx);
+    *bidx = (int *)malloc(sizeof(int) * (size_t)(nb ? nb : 1));
+    *bmap = (uint16_t *)malloc(sizeof(uint16_t) * (size_t)(nb ? nb : 1));
+    *bval = (double *)malloc(sizeof(double) * 16 * (size_t)(nb ? nb : 1));
+    double st, av;
+    orc_csr2bsr_fill(m, n, ia, ja, a, *bptr, *bidx, *bmap, *bval, &st, &av);
+    *nblk = (int)nb;
+}
+
+/* dense inverse (Cholesky, then Gauss-Jordan fallback) */
+static int orc_invert(int n, double *A)
+{
+    double *L = (double *)malloc(sizeof(double) * (size_t)n * n);
+    memcpy(L, A, sizeof(double) * (size_t)n * n);
+    int spd = 1;
+    for (int j = 0; j < n && spd; ++j) {
+        double d = L[(size_t)j * n + j];
+        for (int k = 0; k < j; ++k) d -= L[(size_t)j * n + k] * L[(size_t)j * n + k];
+        if (!(d > 0.0)) { spd = 0; break; }
+        d = sqrt(d);
+        L[(size_t)j * n + j] = d;
+        for (int i = j + 1; i < n; ++i) {
+            double s = L[(size_t)i * n + j];
+            for (int k = 0; k < j; ++k) s -= L[(size_t)i * n + k] * L[(size_t)j * n + k];
+            L[(size_t)i * n + j] = s / d;
+        }
+    }
+    if (spd) {
+        double *Li = (double *)calloc((size_t)n * n, sizeof(double));
+        for (int j = 0; j < n; ++j) {
+            Li[(size_t)j * n + j] = 1.0 / L[(size_t)j * n + j];
+            for (int i = j + 1; i < n; ++i) {
+                double s = 0.0;
+                for (int k = j; k < i; ++k) s -= L[(size_t)i * n + k] * Li[(size_t)k * n + j];
+                Li[(size_t)i * n + j] = s / L[(size_t)i * n + i];
+            }
+        }
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) {
+                double s = 0.0;
+                for (int k = (i > j ? i : j); k < n; ++k) s += Li[(size_t)k * n + i] * Li[(size_t)k * n + j];
+                A[(size_t)i * n + j] = s;
+            }
+        free(Li);
+        free(L);
+        return 0;
+    }
+    free(L);
+    return -1;
+}
+
+ORC_EXPORT void *orc_amg_setup(int n, const int *ia, const int *ja, const double *a, int nP, const int *pm,
+                               const int *pn, const int *const *pia, const int *const *pja,
+                               const double *const *pa, double w)
+{
+    orc_amg *h = (orc_amg *)calloc(1, sizeof(orc_amg));
+    h->L = nP + 1;
+    h->w = w;
+    h->lv = (orc_level *)calloc((size_t)h->L, sizeof(orc_level));
+    orc_level *lv = h->lv;
+    lv[0].n = n;
+    orc_csr_to_level(n, n, ia, ja, a, &lv[0].bptr, &lv[0].bidx, &lv[0].bmap, &lv[0].bval, &lv[0].nblk);
+    for (int l = 0; l < h->L - 1; ++l) {
+        orc_level *v = &lv[l], *c = &lv[l + 1];
+        (void)pm;
+        v->pn = pn[l];
+        int pnb;
+        orc_csr_to_level(v->n, pn[l], pia[l], pja[l], pa[l], &v->pptr, &v->pidx, &v->pmap, &v->pval, &pnb);
+        const int pbc = (pn[l] + 3) / 4, pbr = (v->n + 3) / 4;
+        v->rptr = (int *)calloc((size_t)pbc + 1, sizeof(int));
+        v->ridx = (int *)malloc(sizeof(int) * (size_t)(pnb ? pnb : 1));
+        v->rmap = (uint16_t *)malloc(sizeof(uint16_t) * (size_t)(pnb ? pnb : 1));
+        v->rval = (double *)malloc(sizeof(double) * 16 * (size_t)(pnb ? pnb : 1));
+        orc_bsr_transpose(pbr, pbc, v->pptr, v->pidx, v->pmap, v->pval, v->rptr, v->ridx, v->rmap, v->rval);
+        /* AP = A P */
+        const int abr = (v->n + 3) / 4;
+        int *apptr = (int *)calloc((size_t)abr + 1, sizeof(int));
+        int64_t bits;
+        int64_t apn = orc_spgemm_count(abr, v->bptr, v->bidx, v->bmap, pbc, v->pptr, v->pidx, v->pmap, apptr, &bits);
+        int *apidx = (int *)malloc(sizeof(int) * (size_t)(apn ? apn : 1));
+        uint16_t *apmap = (uint16_t *)malloc(sizeof(uint16_t) * (size_t)(apn ? apn : 1));
+        double *apval = (double *)malloc(sizeof(double) * 16 * (size_t)(apn ? apn : 1));
+        orc_spgemm_fill(ORC_DOUBLE, abr, v->bptr, v->bidx, v->bmap, v->bval, pbc, v->pptr, v->pidx, v->pmap, v->pval,
+                        apptr, apidx, apmap, apval, NULL);
+        /* RAP = R AP */
+        c->n = pn[l];
+        c->bptr = (int *)calloc((size_t)pbc + 1, sizeof(int));
+        int64_t cn = orc_spgemm_count(pbc, v->rptr, v->ridx, v->rmap, pbc, apptr, apidx, apmap, c->bptr, &bits);
+        c->nblk = (int)cn;
+        c->bidx = (int *)malloc(sizeof(int) * (size_t)(cn ? cn : 1));
+        c->bmap = (uint16_t *)malloc(sizeof(uint16_t) * (size_t)(cn ? cn : 1));
+        c->bval = (double *)malloc(sizeof(double) * 16 * (size_t)(cn ? cn : 1));
+        orc_spgemm_fill(ORC_DOUBLE, pbc, v->rptr, v->ridx, v->rmap, v->rval, pbc, apptr, apidx, apmap, apval, c->bptr,
+                        c->bidx, c->bmap, c->bval, NULL);
+        free(apptr); free(apidx); free(apmap); free(apval);
+    }
+    for (int l = 0; l < h->L; ++l) {
+        orc_level *v = &lv[l];
+        v->inv_l1 = (double *)malloc(sizeof(double) * (size_t)v->n);
+        for (int r = 0; r < v->n; ++r) {
+            const int b = r >> 2, q = r & 3;
+            double s = 0.0;
+            for (int k = v->bptr[b]; k < v->bptr[b + 1]; ++k)
+                for (int c = 0; c < 4; ++c) s += fabs(v->bval[(size_t)16 * k + 4 * q + c]);
+            v->inv_l1[r] = s != 0.0 ? 1.0 / s : 0.0;
+        }
+        v->f = (double *)calloc((size_t)v->n, sizeof(double));
+        v->u = (double *)calloc((size_t)v->n, sizeof(double));
+        v->t = (double *)calloc((size_t)v->n, sizeof(double));
+        v->s = (double *)calloc((size_t)v->n, sizeof(double));
+    }
+    orc_level *c = &lv[h->L - 1];
+    h->cinv = (double *)calloc((size_t)c->n * c->n, sizeof(double));
+    for (int r = 0; r < c->n; ++r) {
+        const int b = r >> 2, q = r & 3;
+        for (int k = c->bptr[b]; k < c->bptr[b + 1]; ++k)
+            for (int cc = 0; cc < 4; ++cc) {
+                const int col = 4 * c->bidx[k] + cc;
+                if (col < c->n) h->cinv[(size_t)r * c->n + col] = c->bval[(size_t)16 * k + 4 * q + cc];
+            }
+    }
+    orc_invert(c->n, h->cinv);
+    h->r = (double *)calloc((size_t)n, sizeof(double));
+    h->z = (double *)calloc((size_t)n, sizeof(double));
+    h->p = (double *)calloc((size_t)n, sizeof(double));
+    h->q = (double *)calloc((size_t)n, sizeof(double));
+    return h;
+}
+
+ORC_EXPORT int orc_amg_num_levels(void *hv) { return ((orc_amg *)hv)->L; }
+
+ORC_EXPORT int orc_amg_level_size(void *hv, int l, int *nblk)
+{
+    orc_amg *h = (orc_amg *)hv;
+    if (nblk) *nblk = h->lv[l].nblk;
+    return h->lv[l].n;
+}
+
+/* out = f - A u (resid) or u + w (f - A u) ./ l1 (jacobi) */
+static void orc_level_apply(const orc_level *v, const double *f, const double *u, double *out, int jacobi, double w)
+{
+#pragma omp parallel for schedule(static)
+    for (int r = 0; r < v->n; ++r) {
+        const int b = r >> 2, q = r & 3;
+        double t = 0.0;
+        for (int k = v->bptr[b]; k < v->bptr[b + 1]; ++k) {
+            const double *val = v->bval + (size_t)16 * k + 4 * q;
+            for (int c = 0; c < 4; ++c) {
+                const int col = 4 * v->bidx[k] + c;
+                if (col < v->n) t += val[c] * u[col];
+            }
+        }
+        out[r] = jacobi ? u[r] + w * (f[r] - t) * v->inv_l1[r] : f[r] - t;
+    }
+}
+
+static void orc_cycle(orc_amg *h, const double *rhs, double *out)
+{
+    orc_level *lv = h->lv;
+    const int L = h->L;
+    for (int l = 0; l < L - 1; ++l) {
+        orc_level *v = &lv[l];
+        const double *f = l == 0 ? rhs : v->f;
+        for (int r = 0; r < v->n; ++r) v->u[r] = h->w * f[r] * v->inv_l1[r];
+        orc_level_apply(v, f, v->u, v->t, 0, h->w);
+        orc_bsr_spmv(ORC_DOUBLE, v->pn, v->n, v->rptr, v->ridx, v->rval, 1.0, v->t, 0.0, lv[l + 1].f);
+    }
+    orc_level *c = &lv[L - 1];
+    const double *fc = L == 1 ? rhs : c->f;
+    double *uc = L == 1 ? out : c->s;
+#pragma omp parallel for schedule(static)
+    for (int r = 0; r < c->n; ++r) {
+        double s = 0.0;
+        for (int j = 0; j < c->n; ++j) s += h->cinv[(size_t)r * c->n + j] * fc[j];
+        uc[r] = s;
+    }
+    for (int l = L - 2; l >= 0; --l) {
+        orc_level *v = &lv[l];
+        const double *f = l == 0 ? rhs : v->f;
+        double *o = l == 0 ? out : v->s;
+        orc_bsr_spmv(ORC_DOUBLE, v->n, v->pn, v->pptr, v->pidx, v->pval, 1.0, lv[l + 1].s, 1.0, v->u);
+        orc_level_apply(v, f, v->u, o, 1, h->w);
+    }
+}
+
+static double orc_dot(int n, const double *a, const double *b)
+{
+    double s = 0.0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+    for (int i = 0; i < n; ++i) s += a[i] * b[i];
+    return s;
+}
+
+/* PCG; hist receives ||r||/||b|| per iteration (entry 0 = initial), cap
+ * maxit + 1 entries.  Returns the iteration count. */
+ORC_EXPORT int orc_amg_solve(void *hv, const double *b, double *x, double tol, int maxit, double *hist,
+                             double *relres)
+{
+    orc_amg *h = (orc_amg *)hv;
+    orc_level *v0 = &h->lv[0];
+    const int n = v0->n;
+    orc_level_apply(v0, b, x, h->r, 0, 0.0);
+    const double bb = orc_dot(n, b, b);
+    double rr = orc_dot(n, h->r, h->r);
+    double rel = bb > 0 ? sqrt(rr / bb) : 0.0;
+    if (hist) hist[0] = rel;
+    int it = 0;
+    if (rel > tol) {
+        orc_cycle(h, h->r, h->z);
+        double rz = orc_dot(n, h->r, h->z);
+        memcpy(h->p, h->z, sizeof(double) * (size_t)n);
+        for (it = 1; it <= maxit; ++it) {
+            /* q = A p */
+#pragma omp parallel for schedule(static)
+            for (int r = 0; r < n; ++r) {
+                const int bb4 = r >> 2, q = r & 3;
+                double t = 0.0;
+                for (int k = v0->bptr[bb4]; k < v0->bptr[bb4 + 1]; ++k)
+                    for (int c = 0; c < 4; ++c) {
+                        const int col = 4 * v0->bidx[k] + c;
+                        if (col < n) t += v0->bval[(size_t)16 * k + 4 * q + c] * h->p[col];
+                    }
+                h->q[r] = t;
+            }
+            const double pq = orc_dot(n, h->p, h->q);
+            const double alpha = pq != 0.0 ? rz / pq : 0.0;
+            for (int i = 0; i < n; ++i) {
+                x[i] += alpha * h->p[i];
+                h->r[i] -= alpha * h->q[i];
+            }
+            rr = orc_dot(n, h->r, h->r);
+            rel = sqrt(rr / bb);
+            if (hist) hist[it] = rel;
+            if (rel <= tol) break;
+            orc_cycle(h, h->r, h->z);
+            const double rz_new = orc_dot(n, h->r, h->z);
+            const double beta = rz != 0.0 ? rz_new / rz : 0.0;
+            rz = rz_new;
+            for (int i = 0; i < n; ++i) h->p[i] = h->z[i] + beta * h->p[i];
+        }
+        if (it > maxit) it = maxit;
+    }
+    if (relres) *relres = rel;
+    return it;
+}
+
+ORC_EXPORT void orc_amg_free(void *hv)
+{
+    orc_amg *h = (orc_amg *)hv;
+    if (!h) return;
+    for (int l = 0; l < h->L; ++l) {
+        orc_level *v = &h->lv[l];
+        free(v->bptr); free(v->bidx); free(v->bmap); free(v->bval);
+        free(v->pptr); free(v->pidx); free(v->pmap); free(v->pval);
+        free(v->rptr); free(v->ridx); free(v->rmap); free(v->rval);
+        free(v->inv_l1); free(v->f); free(v->u); free(v->t); free(v->s);
+    }
+    free(h->lv); free(h->cinv); free(h->r); free(h->z); free(h->p); free(h->q);
+    free(h);
+}

@@ -74,6 +74,15 @@ def lib():
                                        ctypes.POINTER(_i64)]
         L.orc_spgemm_fill.argtypes = [c_int, c_int, _i32p, _i32p, _u16p, _f64p, c_int, _i32p, _i32p, _u16p,
                                       _f64p, _i32p, _i32p, _u16p, _f64p, _vp]
+        L.orc_amg_setup.restype = _vp
+        L.orc_amg_setup.argtypes = [c_int, _i32p, _i32p, _f64p, c_int, _vp, _vp, _vp, _vp, _vp, c_double]
+        L.orc_amg_solve.restype = c_int
+        L.orc_amg_solve.argtypes = [_vp, _f64p, _f64p, c_double, c_int, _f64p, ctypes.POINTER(c_double)]
+        L.orc_amg_num_levels.restype = c_int
+        L.orc_amg_num_levels.argtypes = [_vp]
+        L.orc_amg_level_size.restype = c_int
+        L.orc_amg_level_size.argtypes = [_vp, c_int, ctypes.POINTER(c_int)]
+        L.orc_amg_free.argtypes = [_vp]
         L.orc_bsr_transpose.argtypes = [c_int, c_int, _i32p, _i32p, _u16p, _vp, _i32p, _i32p, _u16p, _vp]
         _lib = L
     return _lib
@@ -282,3 +291,59 @@ def transpose(B: BSR) -> BSR:
     L.orc_bsr_transpose(B.brow, B.bcol, B.bptr, np.ascontiguousarray(B.bidx), np.ascontiguousarray(B.bmap),
                         None if B.bval is None else B.bval.ctypes.data, tptr, tidx, tmap, tval.ctypes.data)
     return BSR(B.n, B.m, tptr, tidx[:nb], tmap[:nb], tval[: nb * 16])
+
+
+# --------------------------------------------------------------------- AMG
+class Amg:
+    """The oracle's AMG-PCG (fp64): Galerkin hierarchy on mBSR from given
+    interpolation operators, V(1,1) l1-Jacobi, dense coarsest inverse."""
+
+    def __init__(self, A: CSR, Ps, w: float = 1.0):
+        L = lib()
+        nP = len(Ps)
+        self._keep = [A] + list(Ps)
+        pm = np.array([P.m for P in Ps] or [0], np.int32)
+        pn = np.array([P.n for P in Ps] or [0], np.int32)
+        pia = (ctypes.c_void_p * max(nP, 1))(*[P.ia.ctypes.data for P in Ps])
+        pja = (ctypes.c_void_p * max(nP, 1))(*[P.ja.ctypes.data for P in Ps])
+        pa = (ctypes.c_void_p * max(nP, 1))(*[P.a.ctypes.data for P in Ps])
+        self._arrs = (pm, pn, pia, pja, pa)
+        self.h = L.orc_amg_setup(A.m, A.ia, A.ja, A.a, nP, pm.ctypes.data, pn.ctypes.data,
+                                 ctypes.cast(pia, ctypes.c_void_p), ctypes.cast(pja, ctypes.c_void_p),
+                                 ctypes.cast(pa, ctypes.c_void_p), w)
+        self.n = A.m
+
+    def solve(self, b, x0=None, tol=1e-8, maxit=200):
+        x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        hist = np.zeros(maxit + 1)
+        rel = ctypes.c_double()
+        it = lib().orc_amg_solve(self.h, np.ascontiguousarray(b, np.float64), x, tol, maxit, hist, ctypes.byref(rel))
+        return x, it, rel.value, hist[: it + 1]
+
+    def levels(self):
+        out = []
+        for l in range(lib().orc_amg_num_levels(self.h)):
+            nb = ctypes.c_int()
+            n = lib().orc_amg_level_size(self.h, l, ctypes.byref(nb))
+            out.append((n, nb.value))
+        return out
+
+    def __del__(self):
+        try:
+            lib().orc_amg_free(self.h)
+        except Exception:
+            pass
+
+
+def geometric_hierarchy(nx, ny, nz, coarse_rows=64):
+    """Linear interpolation operators from (nx, ny, nz) down to a grid of at
+    most coarse_rows points."""
+    Ps = []
+    dims = (nx, ny, nz)
+    while dims[0] * dims[1] * dims[2] > coarse_rows:
+        P, cd = interp(*dims)
+        if cd == dims:
+            break
+        Ps.append(P)
+        dims = cd
+    return Ps

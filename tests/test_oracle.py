@@ -209,3 +209,22 @@ def test_galerkin_product_is_symmetric(orc):
     RAP, _ = orc.spgemm(orc.transpose(BP), AP)
     C = orc.bsr2csr(RAP).to_scipy()
     assert abs(C - C.T).max() < 1e-13
+
+
+def test_oracle_amg_pcg_converges(orc):
+    """The oracle's AMG-PCG (Galerkin hierarchy on mBSR, V(1,1) l1-Jacobi)
+    reaches 1e-8 on 2D and 3D Poisson with b = A x*, x* uniform seed 0."""
+    for dims, max_it in (((64, 64, 1), 16), ((20, 18, 16), 18)):
+        A = orc.laplacian(*dims)
+        Ps = orc.geometric_hierarchy(*dims)
+        xs = orc.rand_uniform(0, A.n)
+        b = A.to_scipy() @ xs
+        h = orc.Amg(A, Ps)
+        x, it, rel, hist = h.solve(b)
+        assert rel <= 1e-8 and it <= max_it
+        assert np.linalg.norm(b - A.to_scipy() @ x) <= 1.0000001e-8 * np.linalg.norm(b)
+        assert hist[0] == pytest.approx(1.0)
+        # Galerkin levels equal P^T A P computed by scipy
+        n1, nb1 = h.levels()[1]
+        C = (Ps[0].to_scipy().T @ A.to_scipy() @ Ps[0].to_scipy()).tocsr()
+        assert n1 == C.shape[0]
