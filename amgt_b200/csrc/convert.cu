@@ -64,6 +64,7 @@ csr2bsr_count_kernel(int m, int n, const int *__restrict__ ia, const int *__rest
     __shared__ unsigned long long sbuf[kCvtWarps][kWarpCap];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long *s = sbuf[warp];
+    unsigned long long wmax = 0, wsq = 0;  // per-warp statistics, one atomic each at the end
     for (int b = blockIdx.x * kCvtWarps + warp; b < brow; b += gridDim.x * kCvtWarps) {
         const BlockRowRange R = block_row_range(ia, m, b);
         const int L = R.p1 - R.p0;
@@ -104,9 +105,13 @@ csr2bsr_count_kernel(int m, int n, const int *__restrict__ ia, const int *__rest
         }
         if (lane == 0) {
             cnt[b] = u;
-            atomicMax((unsigned long long *)&stats[0], (unsigned long long)u);
-            atomicAdd((unsigned long long *)&stats[1], (unsigned long long)u * (unsigned long long)u);
+            wmax = wmax > (unsigned long long)u ? wmax : (unsigned long long)u;
+            wsq += (unsigned long long)u * (unsigned long long)u;
         }
+    }
+    if (lane == 0 && wsq) {
+        atomicMax((unsigned long long *)&stats[0], wmax);
+        atomicAdd((unsigned long long *)&stats[1], wsq);
     }
 }
 

@@ -22,10 +22,44 @@ void set_last_cuda_error(cudaError_t e, const char *what, const char *file, int 
 }
 
 // ------------------------------------------------------------- allocator
+// Default allocator: a stream-ordered pool owned by the library, one per
+// device, that keeps freed memory for reuse (release threshold = max).  The
+// device's default pool returns memory to the driver at every synchronize,
+// which made each SpGEMM / conversion pay for fresh page mappings.
+static cudaMemPool_t g_pools[64];
+static std::mutex g_pool_mu;
+
+static cudaMemPool_t library_pool()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    if (g_pools[dev]) return g_pools[dev];
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        g_pools[dev] = pool;
+    }
+    return g_pools[dev];
+}
+
 static void *default_alloc(size_t bytes, amgt_stream_t s, void *)
 {
     void *p = nullptr;
-    if (cudaMallocAsync(&p, bytes, (cudaStream_t)s) != cudaSuccess) {
+    cudaMemPool_t pool = library_pool();
+    cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, (cudaStream_t)s)
+                         : cudaMallocAsync(&p, bytes, (cudaStream_t)s);
+    if (e != cudaSuccess) {
         cudaGetLastError();
         return nullptr;
     }
@@ -163,6 +197,15 @@ int amgt_init(void)
 }
 
 uint64_t amgt_kernel_launch_count(void) { return g_launches.load(); }
+
+int amgt_trim_pool(size_t keep_bytes)
+{
+    cudaMemPool_t pool = library_pool();
+    if (!pool) return AMGT_ERR_NO_DEVICE;
+    AMGT_CUDA_TRY(cudaDeviceSynchronize());
+    AMGT_CUDA_TRY(cudaMemPoolTrimTo(pool, keep_bytes));
+    return AMGT_OK;
+}
 
 int amgt_set_allocator(amgt_alloc_fn alloc_fn, amgt_free_fn free_fn, void *ctx)
 {

@@ -18,15 +18,15 @@
 // writes C's block columns and bitmaps in place.
 //
 // Numeric.  One warp per C block row accumulates the row's C blocks in
-// shared memory (global memory for rows of more than 64 blocks).  A blocks
-// are taken in row order; per A block the two half-warps take two B blocks
-// at a time, lane e of a half computing entry e = (r, c) of the 4x4 product
+// shared memory (global memory for rows of more than 32 blocks); lane t
+// holds C block column t, so a product finds its C block with one ballot.
+// A blocks are taken in row order; per A block the two half-warps take two
+// B blocks at a time, lane e of a half computing entry e = (r, c) of the 4x4 product
 // as the sum over k ascending of a[r][k] * b[k][c] over terms whose A and B
 // bits are set, started from zero, with separate multiply and add (no FMA),
 // and adding it to C(r, c) where the product bitmap has the bit - the
 // arithmetic of the reference's scalar branch (:1289-1339), so the fp64
-// result equals the CPU oracle bit for bit.  C's position is a binary
-// search of the sorted C row.  FP64 arithmetic on the CUDA cores: the 4x4
+// result equals the CPU oracle bit for bit.  FP64 arithmetic on the CUDA cores: the 4x4
 // products are too small for tcgen05 (M >= 64), and on B200 the fp64 MMA
 // rate equals the fp64 FMA rate.  The CSR form of C is written by the same
 // kernel (no separate BSR2CSR pass).
@@ -39,28 +39,57 @@ constexpr int kSymCap = 1024;     // pairs a warp sorts in shared memory
 constexpr int kSymWin = 8192;     // key window of the large-row path
 constexpr int kSymLargeThreads = 256;
 constexpr int kNumWarps = 4;
-constexpr int kNumCap = 64;       // C blocks a warp accumulates in shared memory
+constexpr int kNumCap = 32;       // C blocks a warp accumulates in shared memory (one per lane)
 
 __device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
 
 // Appends the row's non-zero-product pairs to the warp's list s[]; returns
-// the count (> cap only on overflow, which the caller prevents via ub).
+// the count (the caller bounds it via the upper bound).  Up to 32 A blocks
+// at a time: lane i fetches A block i's B row range, a warp scan of the
+// range lengths flattens the (A block, B block) pairs, and lane t takes
+// pair t, finding its A block by a five-step shuffle search; so every load
+// of a chunk is in flight at once.  Pairs come out in (A block, B block)
+// order.
 __device__ __forceinline__ int sym_collect(int lane, int a0, int a1, const int *__restrict__ aidx,
                                            const uint16_t *__restrict__ amap, const int *__restrict__ bptr,
                                            const int *__restrict__ bidx, const uint16_t *__restrict__ bmap,
                                            unsigned long long *s)
 {
     int cnt = 0;
-    for (int i = a0; i < a1; ++i) {
-        const int k = aidx[i];
-        const uint32_t ma = amap[i];
-        const int j0 = bptr[k], j1 = bptr[k + 1];
-        for (int jj = j0; jj < j1; jj += 32) {
-            const int j = jj + lane;
+    for (int ib = a0; ib < a1; ib += 32) {
+        const int i = ib + lane;
+        int j0 = 0, len = 0;
+        uint32_t ma = 0;
+        if (i < a1) {
+            const int k = aidx[i];
+            ma = amap[i];
+            j0 = bptr[k];
+            len = bptr[k + 1] - j0;
+        }
+        int incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        const int excl = incl - len;
+        for (int t0 = 0; t0 < total; t0 += 32) {
+            const int t = t0 + lane;
+            int src = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int v = __shfl_sync(FULL, incl, min(src + step - 1, 31));
+                if (v <= t) src += step;
+            }
+            src = min(src, 31);
+            const int sj0 = __shfl_sync(FULL, j0, src), sex = __shfl_sync(FULL, excl, src);
+            const uint32_t sma = __shfl_sync(FULL, ma, src);
             uint32_t mc = 0;
             int key = 0;
-            if (j < j1) {
-                mc = bitmap_mul(ma, bmap[j]);
+            if (t < total) {
+                const int j = sj0 + (t - sex);
+                mc = bitmap_mul(sma, bmap[j]);
                 key = bidx[j];
             }
             const unsigned bal = __ballot_sync(FULL, mc != 0);
@@ -158,6 +187,7 @@ spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *
     __shared__ unsigned long long sbuf[kSymWarps][kSymCap];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long *s = sbuf[warp];
+    unsigned long long wmax = 0, wsq = 0;  // per-warp statistics, one atomic each at the end
     for (int b = blockIdx.x * kSymWarps + warp; b < brA; b += gridDim.x * kSymWarps) {
         const int a0 = aptr[b], a1 = aptr[b + 1];
         const long long ub = sym_upper_bound(lane, a0, a1, aidx, bptr);
@@ -174,9 +204,13 @@ spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *
 #pragma unroll
             for (int q = 0; q < 4; ++q)
                 if (4 * b + q < m) csrcnt[4 * b + q] = csr[q];
-            atomicMax((unsigned long long *)&stats[0], (unsigned long long)u);
-            atomicAdd((unsigned long long *)&stats[1], (unsigned long long)u * (unsigned long long)u);
+            wmax = wmax > (unsigned long long)u ? wmax : (unsigned long long)u;
+            wsq += (unsigned long long)u * (unsigned long long)u;
         }
+    }
+    if (!FILL && lane == 0 && wsq) {
+        atomicMax((unsigned long long *)&stats[0], wmax);
+        atomicAdd((unsigned long long *)&stats[1], wsq);
     }
 }
 
@@ -357,44 +391,65 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
 {
     using T = NumT<PREC>;
     using acc_t = typename T::acc_t;
-    __shared__ int skeys[kNumWarps][kNumCap];
     __shared__ acc_t sacc[kNumWarps][kNumCap * 16];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int e = lane & 15, r = e >> 2, c = e & 3, half = lane & 16;
     for (int b = blockIdx.x * kNumWarps + warp; b < brA; b += gridDim.x * kNumWarps) {
         const int c0 = cptr[b], cn = cptr[b + 1] - c0;
-        const bool in_smem = cn <= kNumCap;
-        const int *keys = in_smem ? skeys[warp] : cidx + c0;
+        // rows of up to 32 C blocks: lane t holds C column t and the row
+        // accumulates in shared memory; longer rows accumulate in place
+        const bool small = cn <= kNumCap;
+        const int mykey = (small && lane < cn) ? cidx[c0 + lane] : -1;
         acc_t *sa = sacc[warp];
         double *ga = cval + 16LL * c0;
-        if (in_smem) {
-            for (int t = lane; t < cn; t += 32) skeys[warp][t] = cidx[c0 + t];
+        if (small) {
             for (int t = lane; t < 16 * cn; t += 32) sa[t] = (acc_t)0;
         } else {
             for (int t = lane; t < 16 * cn; t += 32) ga[t] = 0.0;
         }
         __syncwarp();
-        for (int i = aptr[b]; i < aptr[b + 1]; ++i) {
-            const int k = aidx[i];
-            const uint32_t ma = amap[i];
-            const acc_t al = T::ld(aval, 16LL * i + e);
-            const int j0 = bptr[k], j1 = bptr[k + 1];
+        const int a0 = aptr[b], a1 = aptr[b + 1];
+        for (int ib = a0; ib < a1; ib += 32) {
+          // lane i fetches A block ib+i's bitmap and B row range up front
+          int pj0 = 0, pj1 = 0;
+          uint32_t pma = 0;
+          if (ib + lane < a1) {
+              const int k = aidx[ib + lane];
+              pma = amap[ib + lane];
+              pj0 = bptr[k];
+              pj1 = bptr[k + 1];
+          }
+          const int na = min(32, a1 - ib);
+          for (int ii = 0; ii < na; ++ii) {
+            const int i = ib + ii;
+            const uint32_t ma = __shfl_sync(FULL, pma, ii);
+            const int j0 = __shfl_sync(FULL, pj0, ii), j1 = __shfl_sync(FULL, pj1, ii);
+            acc_t ar[4];  // row r of the A block
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) ar[kk] = T::ld(aval, 16LL * i + 4 * r + kk);
             for (int jj = j0; jj < j1; jj += 2) {
                 const int j = jj + (half >> 4);
                 const bool valid = j < j1;
                 const uint32_t mb = valid ? bmap[j] : 0u;
                 const uint32_t mc = bitmap_mul(ma, mb);
                 const acc_t bl = valid ? T::ld(bval, 16LL * j + e) : (acc_t)0;
+                const int key = valid ? bidx[j] : -2;
                 acc_t s = (acc_t)0;
 #pragma unroll
                 for (int kk = 0; kk < 4; ++kk) {
-                    const acc_t av = __shfl_sync(FULL, al, half | (r * 4 + kk));
                     const acc_t bv = __shfl_sync(FULL, bl, half | (kk * 4 + c));
-                    if (((ma >> (r * 4 + kk)) & 1u) && ((mb >> (kk * 4 + c)) & 1u)) s = T::add(s, T::mul(av, bv));
+                    if (((ma >> (r * 4 + kk)) & 1u) && ((mb >> (kk * 4 + c)) & 1u)) s = T::add(s, T::mul(ar[kk], bv));
+                }
+                int t;
+                if (small) {
+                    const int k0 = __shfl_sync(FULL, key, 0), k1 = __shfl_sync(FULL, key, 16);
+                    const unsigned m0 = __ballot_sync(FULL, mykey == k0), m1 = __ballot_sync(FULL, mykey == k1);
+                    t = __ffs(half ? m1 : m0) - 1;
+                } else {
+                    t = valid ? search_sorted(cidx + c0, cn, key) : 0;
                 }
                 if (valid && ((mc >> e) & 1u)) {
-                    const int t = search_sorted(keys, cn, bidx[j]);
-                    if (in_smem) {
+                    if (small) {
                         sa[16 * t + e] = T::add(sa[16 * t + e], s);
                     } else {
                         const acc_t cur = (acc_t)ga[16 * t + e];
@@ -403,10 +458,11 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                 }
             }
             __syncwarp();
+          }
         }
         // C values (+ shadow)
         for (int t = lane; t < 16 * cn; t += 32) {
-            const acc_t v = in_smem ? sa[t] : (acc_t)ga[t];
+            const acc_t v = small ? sa[t] : (acc_t)ga[t];
             ga[t] = (double)v;
             if (PREC != AMGT_DOUBLE && cshadow) store_shadow<PREC>(cshadow, 16LL * c0 + t, v);
         }

@@ -393,7 +393,7 @@ def run_amgt(args):
         err = float(torch.linalg.vector_norm(mix["x"] - f64["x"]) / torch.linalg.vector_norm(f64["x"]))
         setup_solve = {}
         for name, rres in (("fp64", f64), ("mixed", mix)):
-            setup_solve[name] = {k: (round(v, 5) if isinstance(v, float) else v) for k, v in rres.items()
+            setup_solve[name] = {k: (float(f"{v:.5g}") if isinstance(v, float) else v) for k, v in rres.items()
                                  if k not in ("x", "levels", "setup_ms")}
             setup_solve[name]["total_s"] = round(rres["setup_s"] + rres["solve_s"], 5)
             setup_solve[name]["setup_ms"] = {k: round(v, 3) for k, v in rres["setup_ms"].items()}

@@ -60,10 +60,13 @@ AMGT_API uint64_t amgt_kernel_launch_count(void);
 
 /* ---------------------------------------------------------- allocation */
 /* Every array the library returns or uses as scratch comes from this
- * allocator.  Default: cudaMallocAsync / cudaFreeAsync on the call's stream
- * (stream-ordered pool).  HYPRE plugs hypre_TAlloc/hypre_TFree here so that
+ * allocator.  HYPRE plugs hypre_TAlloc/hypre_TFree here so that
  * hypre_CSRMatrixDestroy can free an SpGEMM result (the reference allocates C
  * with hypre_TAlloc, R/seq_mv/csr_spgemm_device.c:1808-1839). */
+/* Default: a stream-ordered memory pool owned by the library (one per
+ * device) that keeps freed memory for reuse; amgt_trim_pool(keep) returns
+ * all but `keep` bytes of it to the driver (synchronises the device). */
+AMGT_API int amgt_trim_pool(size_t keep_bytes);
 typedef void *(*amgt_alloc_fn)(size_t bytes, amgt_stream_t stream, void *ctx);
 typedef void (*amgt_free_fn)(void *ptr, amgt_stream_t stream, void *ctx);
 AMGT_API int amgt_set_allocator(amgt_alloc_fn alloc_fn, amgt_free_fn free_fn, void *ctx);
