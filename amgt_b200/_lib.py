@@ -48,7 +48,13 @@ class AmgtCSRMatrix(ctypes.Structure):
 class AmgtAmgParams(ctypes.Structure):
     _fields_ = [("max_levels", c_int), ("max_coarse_rows", c_int), ("tol", c_double), ("max_iter", c_int),
                 ("relax_weight", c_double), ("flexible", c_int), ("use_graph", c_int),
-                ("galerkin_by_level", c_int), ("smooth_prec0", c_int)]
+                ("galerkin_by_level", c_int), ("smooth_prec0", c_int), ("packed", c_int)]
+
+
+class AmgtPbsr(ctypes.Structure):
+    _fields_ = [("row", c_int), ("col", c_int), ("blc_row", c_int), ("blc_col", c_int), ("blc_num", c_int),
+                ("nnz", c_int), ("prec", c_int), ("blcPtr", c_void_p), ("blcIdx", c_void_p), ("blcMap", c_void_p),
+                ("blcVoff", c_void_p), ("val", c_void_p), ("max_blc_per_row", c_int)]
 
 
 # name -> (restype, argtypes); every symbol include/amgt_b200.h declares
@@ -72,6 +78,11 @@ SIGNATURES = {
     "amgt_bsr_l1_norms": (c_int, [P(AmgtBsr), c_void_p, c_void_p]),
     "amgt_bsr_residual": (c_int, [c_int, P(AmgtBsr), c_void_p, c_void_p, c_void_p, c_void_p]),
     "amgt_bsr_jacobi": (c_int, [c_int, P(AmgtBsr), c_void_p, c_double, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "amgt_bsr_pack": (c_int, [P(AmgtBsr), c_int, P(AmgtPbsr), c_void_p]),
+    "amgt_pbsr_free": (c_int, [P(AmgtPbsr), c_void_p]),
+    "amgt_pbsr_spmv": (c_int, [c_double, P(AmgtPbsr), c_void_p, c_double, c_void_p, c_void_p]),
+    "amgt_pbsr_residual": (c_int, [P(AmgtPbsr), c_void_p, c_void_p, c_void_p, c_void_p]),
+    "amgt_pbsr_jacobi": (c_int, [P(AmgtPbsr), c_void_p, c_double, c_void_p, c_void_p, c_void_p, c_void_p]),
     "amgt_spmv_segmented_noalloc": (c_int, [c_int, c_double, P(AmgtBsr), c_void_p, c_double, c_void_p, c_void_p]),
     "amgt_spgemm": (c_int, [c_int, P(AmgtBsr), P(AmgtBsr), P(AmgtBsr), P(AmgtCsr), c_void_p]),
     "amgt_amg_default_params": (None, [P(AmgtAmgParams)]),

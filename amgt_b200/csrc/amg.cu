@@ -220,6 +220,7 @@ static bool host_invert(int n, std::vector<double> &A)
 
 struct Level {
     amgt_bsr A{}, P{}, R{};
+    amgt_pbsr pA{}, pAs{}, pP{}, pR{};  // packed: cycle operator, level-0 smoother, transfers
     double *inv_l1 = nullptr;
     double *f = nullptr, *u = nullptr, *t = nullptr, *s = nullptr;
     int n = 0;
@@ -257,6 +258,10 @@ void free_level(Level &v, cudaStream_t s)
     amgt_bsr_free(&v.A, (amgt_stream_t)s);
     amgt_bsr_free(&v.P, (amgt_stream_t)s);
     amgt_bsr_free(&v.R, (amgt_stream_t)s);
+    amgt_pbsr_free(&v.pA, (amgt_stream_t)s);
+    amgt_pbsr_free(&v.pAs, (amgt_stream_t)s);
+    amgt_pbsr_free(&v.pP, (amgt_stream_t)s);
+    amgt_pbsr_free(&v.pR, (amgt_stream_t)s);
     free_ptr(v.inv_l1, s);
     free_ptr(v.f, s);
     free_ptr(v.u, s);
@@ -294,12 +299,18 @@ int cycle(amgt_amg *h, const double *rhs0, double *out0, cudaStream_t s)
     auto &lv = h->lv;
     const int L = (int)lv.size();
     const double w = h->prm.relax_weight;
+    const bool pk = h->prm.packed != 0;
     for (int l = 0; l < L - 1; ++l) {
         Level &v = lv[l];
         const double *f = (l == 0) ? rhs0 : v.f;
         AMGT_LAUNCH(jacobi_zero_kernel, grid_n(h, v.n), 256, 0, s, (long long)v.n, f, v.inv_l1, w, v.u);
-        AMGT_TRY(spmv_residual(l == 0 ? AMGT_DOUBLE : v.prec, &v.A, f, v.u, v.t, s, h->sm_count));
-        AMGT_TRY(amgt_spmv(v.prec_transfer, 1.0, &v.R, v.t, 0.0, lv[l + 1].f, (amgt_stream_t)s));
+        if (pk) {
+            AMGT_TRY(pbsr_residual(&v.pA, f, v.u, v.t, s, h->sm_count));
+            AMGT_TRY(pbsr_spmv(&v.pR, 1.0, v.t, 0.0, lv[l + 1].f, s, h->sm_count));
+        } else {
+            AMGT_TRY(spmv_residual(l == 0 ? AMGT_DOUBLE : v.prec, &v.A, f, v.u, v.t, s, h->sm_count));
+            AMGT_TRY(amgt_spmv(v.prec_transfer, 1.0, &v.R, v.t, 0.0, lv[l + 1].f, (amgt_stream_t)s));
+        }
     }
     Level &c = lv[L - 1];
     const double *fc = (L == 1) ? rhs0 : c.f;
@@ -309,8 +320,14 @@ int cycle(amgt_amg *h, const double *rhs0, double *out0, cudaStream_t s)
         Level &v = lv[l];
         const double *f = (l == 0) ? rhs0 : v.f;
         double *out = (l == 0) ? out0 : v.s;
-        AMGT_TRY(amgt_spmv(v.prec_transfer, 1.0, &v.P, lv[l + 1].s, 1.0, v.u, (amgt_stream_t)s));
-        AMGT_TRY(spmv_jacobi(l == 0 ? h->prm.smooth_prec0 : v.prec, &v.A, v.inv_l1, w, f, v.u, out, s, h->sm_count));
+        if (pk) {
+            AMGT_TRY(pbsr_spmv(&v.pP, 1.0, lv[l + 1].s, 1.0, v.u, s, h->sm_count));
+            AMGT_TRY(pbsr_jacobi(l == 0 ? &v.pAs : &v.pA, v.inv_l1, w, f, v.u, out, s, h->sm_count));
+        } else {
+            AMGT_TRY(amgt_spmv(v.prec_transfer, 1.0, &v.P, lv[l + 1].s, 1.0, v.u, (amgt_stream_t)s));
+            AMGT_TRY(spmv_jacobi(l == 0 ? h->prm.smooth_prec0 : v.prec, &v.A, v.inv_l1, w, f, v.u, out, s,
+                                 h->sm_count));
+        }
     }
     return AMGT_OK;
 }
@@ -326,7 +343,8 @@ int dot(amgt_amg *h, const double *a, const double *b, int slot, int op, cudaStr
 int pcg_iteration(amgt_amg *h, double *x, cudaStream_t s)
 {
     Level &v0 = h->lv[0];
-    AMGT_TRY(spmv_dot(AMGT_DOUBLE, &v0.A, h->p, h->q, h->part, h->grid0, s));
+    if (h->prm.packed) AMGT_TRY(pbsr_dot(&v0.pA, h->p, h->q, h->part, h->grid0, s));
+    else AMGT_TRY(spmv_dot(AMGT_DOUBLE, &v0.A, h->p, h->q, h->part, h->grid0, s));
     AMGT_LAUNCH(reduce_kernel, 1, kDotThreads, 0, s, h->part, h->grid0, h->scal, (int)S_PQ, (int)OP_ALPHA);
     AMGT_LAUNCH(axpy2_dot_kernel, kDotGrid, kDotThreads, 0, s, h->n0, h->scal, h->p, h->q, x, h->r, h->part);
     AMGT_LAUNCH(reduce_kernel, 1, kDotThreads, 0, s, h->part, kDotGrid, h->scal, (int)S_RR, (int)OP_STORE);
@@ -379,6 +397,7 @@ void amgt_amg_default_params(amgt_amg_params *p)
     p->use_graph = 1;
     p->galerkin_by_level = 0;
     p->smooth_prec0 = AMGT_DOUBLE;
+    p->packed = 0;
 }
 
 int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const amgt_amg_params *params,
@@ -441,6 +460,15 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
             if ((rc = amgt_bsr_make_shadow(&v.P, v.prec_transfer, stream))) goto fail;
             if ((rc = amgt_bsr_make_shadow(&v.R, v.prec_transfer, stream))) goto fail;
         }
+        if (h->prm.packed) {
+            // level 0: fp64 for the residual and the Krylov product, the
+            // smoother at smooth_prec0; coarser levels at their precision
+            if ((rc = amgt_bsr_pack(&v.A, l == 0 ? AMGT_DOUBLE : v.prec, &v.pA, stream))) goto fail;
+            if (l == 0 && (rc = amgt_bsr_pack(&v.A, h->prm.smooth_prec0, &v.pAs, stream))) goto fail;
+            if (l < L - 1 && ((rc = amgt_bsr_pack(&v.P, v.prec_transfer, &v.pP, stream)) ||
+                              (rc = amgt_bsr_pack(&v.R, v.prec_transfer, &v.pR, stream))))
+                goto fail;
+        }
         if ((rc = alloc_n(&v.u, v.n, s)) || (rc = alloc_n(&v.t, v.n, s))) goto fail;
         if (l > 0 && ((rc = alloc_n(&v.f, v.n, s)) || (rc = alloc_n(&v.s, v.n, s)))) goto fail;
     }
@@ -468,7 +496,7 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     }
     // Krylov vectors and scalars
     h->n0 = h->lv[0].n;
-    h->grid0 = epi_grid(&h->lv[0].A, h->sm_count);
+    h->grid0 = h->prm.packed ? pbsr_grid(&h->lv[0].pA, h->sm_count) : epi_grid(&h->lv[0].A, h->sm_count);
     if ((rc = alloc_n(&h->r, h->n0, s)) || (rc = alloc_n(&h->z, h->n0, s)) || (rc = alloc_n(&h->p, h->n0, s)) ||
         (rc = alloc_n(&h->q, h->n0, s)) || (rc = alloc_n(&h->scal, S_NSCAL, s)) ||
         (rc = alloc_n(&h->part, std::max(h->grid0, kDotGrid), s)))

@@ -103,6 +103,15 @@ int spmv_jacobi(int prec, const amgt_bsr *A, const double *inv_l1, double w, con
 int spmv_dot(int prec, const amgt_bsr *A, const double *u, double *out, double *partial, int grid, cudaStream_t s);
 int bsr_l1_norms(const amgt_bsr *A, double *l1, int invert, cudaStream_t s, int sm_count);
 
+// Packed-value forms (packed.cu), same contracts as the dense ones.
+int pbsr_grid(const amgt_pbsr *A, int sm_count);
+int pbsr_spmv(const amgt_pbsr *A, double alpha, const double *x, double beta, double *y, cudaStream_t s,
+              int sm_count);
+int pbsr_residual(const amgt_pbsr *A, const double *f, const double *u, double *r, cudaStream_t s, int sm_count);
+int pbsr_jacobi(const amgt_pbsr *A, const double *inv_l1, double w, const double *f, const double *u, double *u_out,
+                cudaStream_t s, int sm_count);
+int pbsr_dot(const amgt_pbsr *A, const double *u, double *out, double *partial, int grid, cudaStream_t s);
+
 // Exclusive scan of n ints (in may equal out), CUB with allocator scratch.
 int exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s);
 // Exclusive scan of n 64-bit ints.

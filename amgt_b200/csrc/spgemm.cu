@@ -13,9 +13,10 @@
 // memory bitonic sort when <= 1024) and equal columns are merged with an OR
 // of their bitmaps: that is C's block pattern and C's bitmap, bit for bit.
 // Rows with more than 1024 pairs go to a CTA that sweeps the column range
-// in windows of 8192 with a shared-memory bitmap table.  Pass 1 counts
-// blocks and CSR nonzeros per row (one host read-back sizes C), pass 2
-// writes C's block columns and bitmaps in place.
+// in windows of 8192 with a shared-memory bitmap table.  One pass: each
+// row's sorted pattern goes to its slice of a scratch array (offsets from a
+// scan of the per-row pair bounds) with its block and CSR counts; one host
+// read-back then sizes C, and the numeric kernel moves the pattern into C.
 //
 // Numeric.  One warp per C block row accumulates the row's C blocks in
 // shared memory (global memory for rows of more than 32 blocks); lane t
@@ -173,16 +174,32 @@ __device__ __forceinline__ int sym_reduce(int lane, int cnt, unsigned long long 
     return u;
 }
 
-// Pass 1 (FILL = false): C blocks per row -> ccnt[b], CSR nonzeros per
-// scalar row -> csrcnt[4b+q]; rows beyond the warp capacity -> large list.
-// Pass 2 (FILL = true): C block columns and bitmaps at cptr[b].
-template <bool FILL>
+// Upper bound of pairs per A block row (sum of the selected B row
+// lengths); ub[brA] = 0 so that an exclusive scan gives scratch offsets.
+__global__ void spgemm_ub_kernel(int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
+                                 const int *__restrict__ bptr, int64_t *__restrict__ ub)
+{
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= brA; b += gridDim.x * blockDim.x) {
+        long long t = 0;
+        if (b < brA)
+            for (int i = aptr[b]; i < aptr[b + 1]; ++i) {
+                const int k = aidx[i];
+                t += bptr[k + 1] - bptr[k];
+            }
+        ub[b] = t;
+    }
+}
+
+// One pass: per A block row, the sorted C block columns and bitmaps go to
+// the row's scratch slice (offset ub_off[b], capacity ub[b]); C blocks per
+// row -> ccnt[b], CSR nonzeros per scalar row -> csrcnt[4b+q]; rows beyond
+// the warp capacity -> large list.
 __global__ void __launch_bounds__(32 * kSymWarps)
 spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
                        const uint16_t *__restrict__ amap, const int *__restrict__ bptr,
                        const int *__restrict__ bidx, const uint16_t *__restrict__ bmap, int *__restrict__ ccnt,
                        int *__restrict__ csrcnt, int *__restrict__ large, int64_t *__restrict__ stats,
-                       const int *__restrict__ cptr, int *__restrict__ cidx, uint16_t *__restrict__ cmap)
+                       const int64_t *__restrict__ ub_off, int *__restrict__ skey, uint16_t *__restrict__ smap)
 {
     __shared__ unsigned long long sbuf[kSymWarps][kSymCap];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -190,16 +207,16 @@ spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *
     unsigned long long wmax = 0, wsq = 0;  // per-warp statistics, one atomic each at the end
     for (int b = blockIdx.x * kSymWarps + warp; b < brA; b += gridDim.x * kSymWarps) {
         const int a0 = aptr[b], a1 = aptr[b + 1];
-        const long long ub = sym_upper_bound(lane, a0, a1, aidx, bptr);
+        const long long ub = ub_off[b + 1] - ub_off[b];
         if (ub > kSymCap) {
-            if (!FILL && lane == 0) large[atomicAdd((int *)&stats[3], 1)] = b;
+            if (lane == 0) large[atomicAdd((int *)&stats[3], 1)] = b;
             continue;
         }
         const int cnt = sym_collect(lane, a0, a1, aidx, amap, bptr, bidx, bmap, s);
         int csr[4];
-        const int base = FILL ? cptr[b] : 0;
-        const int u = sym_reduce<FILL>(lane, cnt, s, cidx + base, cmap + base, csr);
-        if (!FILL && lane == 0) {
+        const long long base = ub_off[b];
+        const int u = sym_reduce<true>(lane, cnt, s, skey + base, smap + base, csr);
+        if (lane == 0) {
             ccnt[b] = u;
 #pragma unroll
             for (int q = 0; q < 4; ++q)
@@ -208,7 +225,7 @@ spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *
             wsq += (unsigned long long)u * (unsigned long long)u;
         }
     }
-    if (!FILL && lane == 0 && wsq) {
+    if (lane == 0 && wsq) {
         atomicMax((unsigned long long *)&stats[0], wmax);
         atomicAdd((unsigned long long *)&stats[1], wsq);
     }
@@ -216,14 +233,13 @@ spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *
 
 // Rows with more than kSymCap pairs: window sweep over the reachable block
 // columns, 8 warps walking the A blocks, lanes the B rows.
-template <bool FILL>
 __global__ void __launch_bounds__(kSymLargeThreads)
 spgemm_symbolic_large_kernel(int m, const int *__restrict__ aptr, const int *__restrict__ aidx,
                              const uint16_t *__restrict__ amap, const int *__restrict__ bptr,
                              const int *__restrict__ bidx, const uint16_t *__restrict__ bmap,
                              const int *__restrict__ large, int64_t *__restrict__ stats, int *__restrict__ ccnt,
-                             int *__restrict__ csrcnt, const int *__restrict__ cptr, int *__restrict__ cidx,
-                             uint16_t *__restrict__ cmap)
+                             int *__restrict__ csrcnt, const int64_t *__restrict__ ub_off, int *__restrict__ skey,
+                             uint16_t *__restrict__ smap)
 {
     __shared__ uint32_t maps[kSymWin];
     __shared__ int sh[16];
@@ -253,7 +269,7 @@ spgemm_symbolic_large_kernel(int m, const int *__restrict__ aptr, const int *__r
         atomicMax(&smax, hi);
         __syncthreads();
         const int kmin = smin, kmax = smax;
-        const int base = FILL ? cptr[b] : 0;
+        const long long base = ub_off[b];
         int total = 0;
         int c4[4] = {0, 0, 0, 0};
         for (long long w0 = kmin; w0 <= kmax; w0 += kSymWin) {
@@ -294,13 +310,13 @@ spgemm_symbolic_large_kernel(int m, const int *__restrict__ aptr, const int *__r
             __syncthreads();
             off += sh[warp];
             const int wtotal = sh[8];
-            if (FILL) {
-                int o = base + total + off;
+            {
+                long long o = base + total + off;
                 for (int i = 0; i < kSymWin / kSymLargeThreads; ++i) {
                     const uint32_t mp = maps[s0 + i];
                     if (mp) {
-                        cidx[o] = (int)(w0 + s0 + i);
-                        cmap[o] = (uint16_t)mp;
+                        skey[o] = (int)(w0 + s0 + i);
+                        smap[o] = (uint16_t)mp;
                         ++o;
                     }
                 }
@@ -308,7 +324,7 @@ spgemm_symbolic_large_kernel(int m, const int *__restrict__ aptr, const int *__r
             total += wtotal;
             __syncthreads();
         }
-        if (!FILL) {
+        {
 #pragma unroll
             for (int q = 0; q < 4; ++q) atomicAdd(&scsr[q], c4[q]);
             __syncthreads();
@@ -385,9 +401,10 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                       const uint16_t *__restrict__ amap, const typename NumT<PREC>::val_t *__restrict__ aval,
                       const int *__restrict__ bptr, const int *__restrict__ bidx,
                       const uint16_t *__restrict__ bmap, const typename NumT<PREC>::val_t *__restrict__ bval,
-                      const int *__restrict__ cptr, const int *__restrict__ cidx, const uint16_t *__restrict__ cmap,
+                      const int *__restrict__ cptr, int *__restrict__ cidx, uint16_t *__restrict__ cmap,
                       double *__restrict__ cval, void *__restrict__ cshadow, const int *__restrict__ csr_i,
-                      int *__restrict__ csr_j, double *__restrict__ csr_a)
+                      int *__restrict__ csr_j, double *__restrict__ csr_a, const int64_t *__restrict__ ub_off,
+                      const int *__restrict__ skey, const uint16_t *__restrict__ smap)
 {
     using T = NumT<PREC>;
     using acc_t = typename T::acc_t;
@@ -396,12 +413,19 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
     const int e = lane & 15, r = e >> 2, c = e & 3, half = lane & 16;
     for (int b = blockIdx.x * kNumWarps + warp; b < brA; b += gridDim.x * kNumWarps) {
         const int c0 = cptr[b], cn = cptr[b + 1] - c0;
+        // the row's pattern, sorted by the symbolic pass, moves from scratch to C
+        const long long sb = ub_off[b];
+        for (int t = lane; t < cn; t += 32) {
+            cidx[c0 + t] = skey[sb + t];
+            cmap[c0 + t] = smap[sb + t];
+        }
         // rows of up to 32 C blocks: lane t holds C column t and the row
         // accumulates in shared memory; longer rows accumulate in place
         const bool small = cn <= kNumCap;
-        const int mykey = (small && lane < cn) ? cidx[c0 + lane] : -1;
+        const int mykey = (small && lane < cn) ? skey[sb + lane] : -1;
         acc_t *sa = sacc[warp];
         double *ga = cval + 16LL * c0;
+        __syncwarp();
         if (small) {
             for (int t = lane; t < 16 * cn; t += 32) sa[t] = (acc_t)0;
         } else {
@@ -427,18 +451,21 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
             acc_t ar[4];  // row r of the A block
 #pragma unroll
             for (int kk = 0; kk < 4; ++kk) ar[kk] = T::ld(aval, 16LL * i + 4 * r + kk);
+            const uint32_t arow = (ma >> (4 * r)) & 0xFu;  // bit kk: A(r, kk) stored
             for (int jj = j0; jj < j1; jj += 2) {
                 const int j = jj + (half >> 4);
                 const bool valid = j < j1;
                 const uint32_t mb = valid ? bmap[j] : 0u;
-                const uint32_t mc = bitmap_mul(ma, mb);
                 const acc_t bl = valid ? T::ld(bval, 16LL * j + e) : (acc_t)0;
                 const int key = valid ? bidx[j] : -2;
+                // bit kk of terms: A(r, kk) and B(kk, c) both stored
+                const uint32_t bcol = (mb >> c) & 0x1111u;
+                const uint32_t terms = arow & ((bcol | (bcol >> 3) | (bcol >> 6) | (bcol >> 9)) & 0xFu);
                 acc_t s = (acc_t)0;
 #pragma unroll
                 for (int kk = 0; kk < 4; ++kk) {
                     const acc_t bv = __shfl_sync(FULL, bl, half | (kk * 4 + c));
-                    if (((ma >> (r * 4 + kk)) & 1u) && ((mb >> (kk * 4 + c)) & 1u)) s = T::add(s, T::mul(ar[kk], bv));
+                    if ((terms >> kk) & 1u) s = T::add(s, T::mul(ar[kk], bv));
                 }
                 int t;
                 if (small) {
@@ -448,7 +475,7 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                 } else {
                     t = valid ? search_sorted(cidx + c0, cn, key) : 0;
                 }
-                if (valid && ((mc >> e) & 1u)) {
+                if (valid && terms) {
                     if (small) {
                         sa[16 * t + e] = T::add(sa[16 * t + e], s);
                     } else {
@@ -500,14 +527,16 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
 
 template <int PREC>
 static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B, const void *bval, amgt_bsr *C,
-                          void *cshadow, amgt_csr *Ccsr, cudaStream_t s, int sm_count)
+                          void *cshadow, amgt_csr *Ccsr, const int64_t *ub_off, const int *skey,
+                          const uint16_t *smap, cudaStream_t s, int sm_count)
 {
     using V = typename NumT<PREC>::val_t;
     if (A->blc_row == 0) return AMGT_OK;
     AMGT_LAUNCH(spgemm_numeric_kernel<PREC>, grid_for(kNumWarps, A->blc_row, sm_count, 8), 32 * kNumWarps, 0, s,
                 A->row, A->blc_row, A->blcPtr, A->blcIdx, A->blcMap, (const V *)aval, B->blcPtr, B->blcIdx,
                 B->blcMap, (const V *)bval, C->blcPtr, C->blcIdx, C->blcMap, C->blcVal, cshadow,
-                Ccsr ? Ccsr->i : nullptr, Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr);
+                Ccsr ? Ccsr->i : nullptr, Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr, ub_off, skey,
+                smap);
     return AMGT_OK;
 }
 
@@ -547,7 +576,9 @@ int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     bool ownA = false, ownB = false;
     int rc = AMGT_OK;
     int *ccnt = nullptr, *csrcnt = nullptr, *large = nullptr, *csr_i = nullptr, *csr_tmp = nullptr;
-    int64_t *stats = nullptr;
+    int64_t *stats = nullptr, *ub = nullptr, *ub_off = nullptr;
+    int *skey = nullptr;
+    uint16_t *smap = nullptr;
     const int64_t *h = nullptr;
     int nbC = 0, nnzC = 0;
     void *cshadow = nullptr;
@@ -564,18 +595,36 @@ int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
         }
     }
     if ((rc = alloc_n(&C->blcPtr, brA + 1, s)) || (rc = alloc_n(&ccnt, brA + 1, s)) ||
-        (rc = alloc_n(&csrcnt, m + 1, s)) || (rc = alloc_n(&large, brA, s)) || (rc = alloc_n(&stats, 4, s)))
+        (rc = alloc_n(&csrcnt, m + 1, s)) || (rc = alloc_n(&large, brA, s)) || (rc = alloc_n(&stats, 4, s)) ||
+        (rc = alloc_n(&ub, (size_t)brA + 1, s)) || (rc = alloc_n(&ub_off, (size_t)brA + 1, s)))
         goto fail;
     AMGT_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(int64_t) * 4, s));
     AMGT_CUDA_TRY(cudaMemsetAsync(ccnt, 0, sizeof(int) * (brA + 1), s));
     AMGT_CUDA_TRY(cudaMemsetAsync(csrcnt, 0, sizeof(int) * (m + 1), s));
+    // per-row pair bounds -> scratch offsets for the rows' sorted patterns
+    AMGT_LAUNCH(spgemm_ub_kernel, grid_for(256, brA + 1LL, st->sm_count, 8), 256, 0, s, brA, A->blcPtr, A->blcIdx,
+                B->blcPtr, ub);
+    if ((rc = exclusive_scan_i64(ub, ub_off, brA + 1, s))) goto fail;
+    {
+        // scratch size: the host-side bound nblk(A) * longest B row when it is
+        // modest, else the exact total (one read-back)
+        long long cap = (B->max_blc_per_row > 0 || B->blc_num == 0)
+                            ? (long long)A->blc_num * (long long)B->max_blc_per_row
+                            : -1;
+        if (cap < 0 || cap > (256LL << 20)) {
+            AMGT_CUDA_TRY(cudaMemcpyAsync(&stats[2], ub_off + brA, sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
+            if ((rc = read_back(stats, 4, s, &h))) goto fail;
+            cap = h[2];
+            AMGT_CUDA_TRY(cudaMemsetAsync(&stats[2], 0, sizeof(int64_t), s));
+        }
+        if ((rc = alloc_n(&skey, (size_t)cap, s)) || (rc = alloc_n(&smap, (size_t)cap, s))) goto fail;
+    }
     if (brA > 0) {
-        AMGT_LAUNCH(spgemm_symbolic_kernel<false>, grid_for(kSymWarps, brA, st->sm_count, 8), 32 * kSymWarps, 0, s,
-                    m, brA, A->blcPtr, A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, ccnt, csrcnt, large,
-                    stats, nullptr, nullptr, nullptr);
-        AMGT_LAUNCH(spgemm_symbolic_large_kernel<false>, 2 * st->sm_count, kSymLargeThreads, 0, s, m, A->blcPtr,
-                    A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, large, stats, ccnt, csrcnt, nullptr,
-                    nullptr, nullptr);
+        AMGT_LAUNCH(spgemm_symbolic_kernel, grid_for(kSymWarps, brA, st->sm_count, 8), 32 * kSymWarps, 0, s, m, brA,
+                    A->blcPtr, A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, ccnt, csrcnt, large, stats,
+                    ub_off, skey, smap);
+        AMGT_LAUNCH(spgemm_symbolic_large_kernel, 2 * st->sm_count, kSymLargeThreads, 0, s, m, A->blcPtr, A->blcIdx,
+                    A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, large, stats, ccnt, csrcnt, ub_off, skey, smap);
     }
     if ((rc = exclusive_scan_int(ccnt, C->blcPtr, brA + 1, s))) goto fail;
     AMGT_CUDA_TRY(cudaMemcpyAsync(&stats[2], C->blcPtr + brA, sizeof(int), cudaMemcpyDeviceToDevice, s));
@@ -622,37 +671,35 @@ int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
         Ccsr->num_nonzeros = nnzC;
         if ((rc = alloc_n(&Ccsr->j, nnzC, s)) || (rc = alloc_n(&Ccsr->data, nnzC, s))) goto fail;
     }
-    if (brA > 0) {
-        AMGT_LAUNCH(spgemm_symbolic_kernel<true>, grid_for(kSymWarps, brA, st->sm_count, 8), 32 * kSymWarps, 0, s,
-                    m, brA, A->blcPtr, A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, nullptr, nullptr,
-                    nullptr, stats, C->blcPtr, C->blcIdx, C->blcMap);
-        AMGT_LAUNCH(spgemm_symbolic_large_kernel<true>, 2 * st->sm_count, kSymLargeThreads, 0, s, m, A->blcPtr,
-                    A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, large, stats, nullptr, nullptr,
-                    C->blcPtr, C->blcIdx, C->blcMap);
-    }
     switch (prec) {
     case AMGT_DOUBLE:
-        rc = launch_numeric<AMGT_DOUBLE>(A, A->blcVal, B, B->blcVal, C, nullptr, Ccsr, s, st->sm_count);
+        rc = launch_numeric<AMGT_DOUBLE>(A, A->blcVal, B, B->blcVal, C, nullptr, Ccsr, ub_off, skey, smap, s,
+                                         st->sm_count);
         break;
     case AMGT_FLOAT:
-        rc = launch_numeric<AMGT_FLOAT>(A, Atmp.blcVal_fp32, B, Btmp.blcVal_fp32, C, cshadow, Ccsr, s, st->sm_count);
+        rc = launch_numeric<AMGT_FLOAT>(A, Atmp.blcVal_fp32, B, Btmp.blcVal_fp32, C, cshadow, Ccsr, ub_off, skey,
+                                        smap, s, st->sm_count);
         break;
     case AMGT_HALF:
-        rc = launch_numeric<AMGT_HALF>(A, Atmp.blcVal_fp16, B, Btmp.blcVal_fp16, C, cshadow, Ccsr, s, st->sm_count);
+        rc = launch_numeric<AMGT_HALF>(A, Atmp.blcVal_fp16, B, Btmp.blcVal_fp16, C, cshadow, Ccsr, ub_off, skey,
+                                       smap, s, st->sm_count);
         break;
     default:
-        rc = launch_numeric<AMGT_BF16>(A, Atmp.blcVal_bf16, B, Btmp.blcVal_bf16, C, cshadow, Ccsr, s, st->sm_count);
+        rc = launch_numeric<AMGT_BF16>(A, Atmp.blcVal_bf16, B, Btmp.blcVal_bf16, C, cshadow, Ccsr, ub_off, skey,
+                                       smap, s, st->sm_count);
         break;
     }
     if (rc) goto fail;
     C->csr_nnz = nnzC;
     C->avg_nnz = nbC ? (double)nnzC / nbC : 0.0;
     free_ptr(ccnt, s); free_ptr(csrcnt, s); free_ptr(large, s); free_ptr(stats, s); free_ptr(csr_tmp, s);
+    free_ptr(ub, s); free_ptr(ub_off, s); free_ptr(skey, s); free_ptr(smap, s);
     if (ownA) { free_ptr(Atmp.blcVal_fp32, s); free_ptr(Atmp.blcVal_fp16, s); free_ptr(Atmp.blcVal_bf16, s); }
     if (ownB) { free_ptr(Btmp.blcVal_fp32, s); free_ptr(Btmp.blcVal_fp16, s); free_ptr(Btmp.blcVal_bf16, s); }
     return AMGT_OK;
 fail:
     free_ptr(ccnt, s); free_ptr(csrcnt, s); free_ptr(large, s); free_ptr(stats, s); free_ptr(csr_tmp, s);
+    free_ptr(ub, s); free_ptr(ub_off, s); free_ptr(skey, s); free_ptr(smap, s);
     if (ownA) { free_ptr(Atmp.blcVal_fp32, s); free_ptr(Atmp.blcVal_fp16, s); free_ptr(Atmp.blcVal_bf16, s); }
     if (ownB) { free_ptr(Btmp.blcVal_fp32, s); free_ptr(Btmp.blcVal_fp16, s); free_ptr(Btmp.blcVal_bf16, s); }
     amgt_bsr_free(C, stream);

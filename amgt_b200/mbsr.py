@@ -11,7 +11,7 @@ import ctypes
 import torch
 
 from . import _lib as L
-from ._lib import AmgtBsr, AmgtCsr, check
+from ._lib import AmgtBsr, AmgtCsr, AmgtPbsr, check
 
 DOUBLE, FLOAT, HALF, BF16 = L.DOUBLE, L.FLOAT, L.HALF, L.BF16
 PREC_NAMES = {DOUBLE: "fp64", FLOAT: "fp32", HALF: "fp16", BF16: "bf16"}
@@ -134,6 +134,15 @@ class Bsr:
             L.lib().amgt_csr_free(ctypes.byref(c), _stream(stream))
         return out
 
+    def pack(self, prec: int = DOUBLE, stream=None) -> "PackedBsr":
+        """Bitmap-packed copy of the values (the block structure stays
+        borrowed from this matrix, which must outlive it)."""
+        P_ = PackedBsr(self)
+        check(L.lib().amgt_bsr_pack(ctypes.byref(self.s), prec, ctypes.byref(P_.s), _stream(stream)),
+              "amgt_bsr_pack")
+        P_._live = True
+        return P_
+
     def spmv(self, x: torch.Tensor, y: torch.Tensor | None = None, alpha: float = 1.0, beta: float = 0.0,
              prec: int = DOUBLE, stream=None) -> torch.Tensor:
         if y is None:
@@ -159,6 +168,48 @@ class Bsr:
         check(L.lib().amgt_spmm(prec, alpha, ctypes.byref(self.s), nvec, X.data_ptr(), X.stride(0), beta,
                                 Y.data_ptr(), Y.stride(0), _stream(stream)), "amgt_spmm")
         return Y
+
+
+class PackedBsr:
+    """amgt_pbsr: mBSR with only the set bits' values stored."""
+
+    def __init__(self, owner: Bsr):
+        self.s = AmgtPbsr()
+        self._owner = owner
+        self._live = False
+
+    def free(self, stream=None) -> None:
+        if self._live:
+            L.lib().amgt_pbsr_free(ctypes.byref(self.s), _stream(stream))
+            self._live = False
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def spmv(self, x, y=None, alpha=1.0, beta=0.0, stream=None):
+        if y is None:
+            y = torch.zeros(self.s.row, dtype=torch.float64, device="cuda")
+            beta = 0.0
+        _vec_check(x, self.s.col)
+        _vec_check(y, self.s.row)
+        check(L.lib().amgt_pbsr_spmv(alpha, ctypes.byref(self.s), x.data_ptr(), beta, y.data_ptr(),
+                                     _stream(stream)), "amgt_pbsr_spmv")
+        return y
+
+    def residual(self, f, u, r=None, stream=None):
+        r = torch.empty_like(f) if r is None else r
+        check(L.lib().amgt_pbsr_residual(ctypes.byref(self.s), f.data_ptr(), u.data_ptr(), r.data_ptr(),
+                                         _stream(stream)), "amgt_pbsr_residual")
+        return r
+
+    def jacobi(self, inv_l1, weight, f, u, out=None, stream=None):
+        out = torch.empty_like(u) if out is None else out
+        check(L.lib().amgt_pbsr_jacobi(ctypes.byref(self.s), inv_l1.data_ptr(), weight, f.data_ptr(),
+                                       u.data_ptr(), out.data_ptr(), _stream(stream)), "amgt_pbsr_jacobi")
+        return out
 
 
 def _vec_check(v: torch.Tensor, n: int) -> None:

@@ -210,6 +210,38 @@ AMGT_API int amgt_bsr_jacobi(int prec, const amgt_bsr *A, const double *inv_l1,
                              double weight, const double *f, const double *u,
                              double *u_out, amgt_stream_t stream);
 
+/* ------------------------------------------------- bitmap-packed values */
+/* mBSR with only the values of set bitmap bits stored, block after block in
+ * bitmap (row-major) order, plus each block's offset into them.  The block
+ * structure (blcPtr, blcIdx, blcMap) is borrowed from the amgt_bsr it was
+ * packed from, which must outlive it.  At the fill of AMG operators (about
+ * 4 of 16) an SpMV reads ~3x fewer bytes than on the 16-value blocks.  No
+ * counterpart in the reference (it keeps 16 values per block). */
+typedef struct {
+    int row, col, blc_row, blc_col, blc_num;
+    int nnz;                  /* stored values (= set bits)            */
+    int prec;                 /* amgt_precision of val                 */
+    const int *blcPtr;        /* borrowed                              */
+    const int *blcIdx;        /* borrowed                              */
+    const uint16_t *blcMap;   /* borrowed                              */
+    int *blcVoff;             /* [blc_num + 1] value offset per block  */
+    void *val;                /* [nnz] double / float / half / bf16    */
+    int max_blc_per_row;
+} amgt_pbsr;
+
+AMGT_API int amgt_bsr_pack(const amgt_bsr *A, int prec, amgt_pbsr *out, amgt_stream_t stream);
+AMGT_API int amgt_pbsr_free(amgt_pbsr *A, amgt_stream_t stream);
+/* y <- alpha A x + beta y; r = f - A u; u_out = u + w (f - A u) ./ l1: the
+ * same forms as amgt_spmv / amgt_bsr_residual / amgt_bsr_jacobi, in the
+ * packed matrix's precision (fp32 accumulation below fp64). */
+AMGT_API int amgt_pbsr_spmv(double alpha, const amgt_pbsr *A, const double *x, double beta,
+                            double *y, amgt_stream_t stream);
+AMGT_API int amgt_pbsr_residual(const amgt_pbsr *A, const double *f, const double *u,
+                                double *r, amgt_stream_t stream);
+AMGT_API int amgt_pbsr_jacobi(const amgt_pbsr *A, const double *inv_l1, double weight,
+                              const double *f, const double *u, double *u_out,
+                              amgt_stream_t stream);
+
 /* Segmented SpMV that allocates nothing.  No counterpart in the reference.
  *
  * For callers that cannot allocate device memory while they run a matvec:
@@ -268,6 +300,8 @@ typedef struct {
     int galerkin_by_level; /* Galerkin products at each level's precision,
                               as AmgT's hypreDevice_CSRSpGemm does (0: fp64) */
     int smooth_prec0;      /* precision of the finest-level smoother SpMV   */
+    int packed;            /* cycle / Krylov SpMVs on bitmap-packed values
+                              (amgt_pbsr), default 0                        */
 } amgt_amg_params;
 
 typedef struct amgt_amg amgt_amg;
