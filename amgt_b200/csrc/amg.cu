@@ -30,7 +30,7 @@
 
 namespace amgt {
 
-constexpr int kDotGrid = 296;  // 2 x 148 SMs
+constexpr int kDotGrid = 1184;  // 8 x 148 SMs
 constexpr int kDotThreads = 256;
 
 enum { S_BB = 0, S_RR = 1, S_RZ = 2, S_PQ = 3, S_ALPHA = 4, S_BETA = 5, S_ZRPREV = 6, S_NSCAL = 8 };

@@ -7,8 +7,9 @@
 // are sorted in registers (<= 32 entries) or in the warp's shared-memory
 // slice (<= 512 entries); block rows with more entries go to a CTA that
 // sweeps the block-column range in windows of 8192 with a shared-memory
-// bitmap table.  Two passes: count (sizes the arrays, one host read-back),
-// then fill (block columns, bitmaps, zero-padded values).
+// bitmap table.  Two passes: count (sorts, keeps the sorted pairs in
+// scratch, sizes the arrays with one host read-back), then fill (block
+// columns, bitmaps, zero-padded values from the kept pairs).
 #include <cub/device/device_radix_sort.cuh>
 
 #include "rowunion.cuh"
@@ -59,7 +60,8 @@ __device__ __forceinline__ BlockRowRange block_row_range(const int *ia, int m, i
 // ------------------------------------------------------------ count pass
 __global__ void __launch_bounds__(32 * kCvtWarps)
 csr2bsr_count_kernel(int m, int n, const int *__restrict__ ia, const int *__restrict__ ja, int brow,
-                     int *__restrict__ cnt, int *__restrict__ large, int64_t *__restrict__ stats, int *err)
+                     int *__restrict__ cnt, int *__restrict__ large, int64_t *__restrict__ stats, int *err,
+                     unsigned long long *__restrict__ sorted)
 {
     __shared__ unsigned long long sbuf[kCvtWarps][kWarpCap];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -80,6 +82,7 @@ csr2bsr_count_kernel(int m, int n, const int *__restrict__ ia, const int *__rest
                 v = csr_entry_pair(ja, p, R.p0, row_in_block(p, R.e1, R.e2, R.e3), n, err);
             }
             v = warp_sort32(v, lane);
+            if (lane < L) sorted[R.p0 + lane] = v;  // reused by the fill pass
             uint32_t orv;
             bool head = warp_runs32(v, lane, &orv);
             u = __popc(__ballot_sync(FULL, head));
@@ -98,6 +101,7 @@ csr2bsr_count_kernel(int m, int n, const int *__restrict__ ia, const int *__rest
             for (int i0 = 0; i0 < L; i0 += 32) {
                 const int i = i0 + lane;
                 bool head = false;
+                if (i < L) sorted[R.p0 + i] = s[i];  // reused by the fill pass
                 if (i < L && s[i] != kSentinel) head = (i == 0) || pair_key(s[i]) != pair_key(s[i - 1]);
                 u += __popc(__ballot_sync(FULL, head));
             }
@@ -238,14 +242,15 @@ csr2bsr_large_kernel(int m, int n, const int *__restrict__ ia, const int *__rest
 }
 
 // ------------------------------------------------------------- fill pass
+// Takes each block row's pairs as the count pass sorted them (scratch at the
+// block row's CSR offset) and writes block columns, OR-ed bitmaps and the
+// zero-padded values.
 __global__ void __launch_bounds__(32 * kCvtWarps)
-csr2bsr_fill_kernel(int m, int n, const int *__restrict__ ia, const int *__restrict__ ja,
-                    const double *__restrict__ a, int brow, const int *__restrict__ bptr, int *__restrict__ bidx,
-                    uint16_t *__restrict__ bmap, double *__restrict__ bval, int *err)
+csr2bsr_fill_kernel(int m, int n, const int *__restrict__ ia, const double *__restrict__ a, int brow,
+                    const int *__restrict__ bptr, int *__restrict__ bidx, uint16_t *__restrict__ bmap,
+                    double *__restrict__ bval, const unsigned long long *__restrict__ sorted)
 {
-    __shared__ unsigned long long sbuf[kCvtWarps][kWarpCap];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned long long *s = sbuf[warp];
     for (int b = blockIdx.x * kCvtWarps + warp; b < brow; b += gridDim.x * kCvtWarps) {
         const BlockRowRange R = block_row_range(ia, m, b);
         const int L = R.p1 - R.p0;
@@ -254,13 +259,9 @@ csr2bsr_fill_kernel(int m, int n, const int *__restrict__ ia, const int *__restr
         double2 *z = reinterpret_cast<double2 *>(bval + (size_t)16 * base);
         for (int i = lane; i < 8 * u; i += 32) z[i] = make_double2(0.0, 0.0);
         __syncwarp();
+        const unsigned long long *sp = sorted + R.p0;
         if (L <= 32) {
-            unsigned long long v = kSentinel;
-            if (lane < L) {
-                const int p = R.p0 + lane;
-                v = csr_entry_pair(ja, p, R.p0, row_in_block(p, R.e1, R.e2, R.e3), n, err);
-            }
-            v = warp_sort32(v, lane);
+            const unsigned long long v = (lane < L) ? sp[lane] : kSentinel;
             uint32_t orv;
             const bool head = warp_runs32(v, lane, &orv);
             const unsigned hb = __ballot_sync(FULL, head);
@@ -274,30 +275,20 @@ csr2bsr_fill_kernel(int m, int n, const int *__restrict__ ia, const int *__restr
                 bval[(size_t)16 * (base + slot) + bit] = a[R.p0 + pair_tag(v)];
             }
         } else {
-            const int N = next_pow2_min64(L);
-            for (int i = lane; i < N; i += 32) {
-                unsigned long long v = kSentinel;
-                if (i < L) {
-                    const int p = R.p0 + i;
-                    v = csr_entry_pair(ja, p, R.p0, row_in_block(p, R.e1, R.e2, R.e3), n, err);
-                }
-                s[i] = v;
-            }
-            __syncwarp();
-            warp_sort_smem(s, N, lane);
             int running = 0;
             for (int i0 = 0; i0 < L; i0 += 32) {
                 const int i = i0 + lane;
-                const unsigned long long v = (i < L) ? s[i] : kSentinel;
+                const unsigned long long v = (i < L) ? sp[i] : kSentinel;
                 bool head = false;
-                if (v != kSentinel) head = (i == 0) || pair_key(v) != pair_key(s[i - 1]);
+                if (v != kSentinel) head = (i == 0) || pair_key(v) != pair_key(sp[i - 1]);
                 const unsigned hb = __ballot_sync(FULL, head);
                 const int slot = running + __popc(hb & lanemask_le(lane)) - 1;
                 if (v != kSentinel) {
                     if (head) {
                         uint32_t orv = 0;
                         const int key = pair_key(v);
-                        for (int j = i; j < L && s[j] != kSentinel && pair_key(s[j]) == key; ++j) orv |= pair_map(s[j]);
+                        for (int jj = i; jj < L && sp[jj] != kSentinel && pair_key(sp[jj]) == key; ++jj)
+                            orv |= pair_map(sp[jj]);
                         bidx[base + slot] = key;
                         bmap[base + slot] = (uint16_t)orv;
                     }
@@ -306,7 +297,6 @@ csr2bsr_fill_kernel(int m, int n, const int *__restrict__ ia, const int *__restr
                 }
                 running += __popc(hb);
             }
-            __syncwarp();
         }
     }
 }
@@ -546,6 +536,7 @@ int amgt_csr_to_bsr(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream)
 
     int *cnt = nullptr, *large = nullptr;
     int64_t *stats = nullptr;
+    unsigned long long *sorted = nullptr;
     int rc = AMGT_OK;
     const int64_t *h = nullptr;
     int nb = 0;
@@ -558,13 +549,14 @@ int amgt_csr_to_bsr(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream)
         smem_set = true;
     }
     if ((rc = alloc_n(&out->blcPtr, brow + 1, s)) || (rc = alloc_n(&cnt, brow + 1, s)) ||
-        (rc = alloc_n(&large, brow, s)) || (rc = alloc_n(&stats, 4, s)))
+        (rc = alloc_n(&large, brow, s)) || (rc = alloc_n(&stats, 4, s)) ||
+        (rc = alloc_n(&sorted, (size_t)A->num_nonzeros, s)))
         goto fail;
     AMGT_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(int64_t) * 4, s));
     AMGT_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * (brow + 1), s));
     if (brow > 0) {
         AMGT_LAUNCH(csr2bsr_count_kernel, grid_for(kCvtWarps, brow, st->sm_count, 16), 32 * kCvtWarps, 0, s, m, n,
-                    A->i, A->j, brow, cnt, large, stats, st->err);
+                    A->i, A->j, brow, cnt, large, stats, st->err, sorted);
         AMGT_LAUNCH(csr2bsr_large_kernel<false>, 2 * st->sm_count, kLargeThreads, 2 * kWin * sizeof(uint32_t), s,
                     m, n, A->i, A->j, A->data, large, stats, cnt, nullptr, nullptr, nullptr, nullptr, stats);
     }
@@ -589,7 +581,7 @@ int amgt_csr_to_bsr(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream)
         goto fail;
     if (brow > 0) {
         AMGT_LAUNCH(csr2bsr_fill_kernel, grid_for(kCvtWarps, brow, st->sm_count, 16), 32 * kCvtWarps, 0, s, m, n,
-                    A->i, A->j, A->data, brow, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal, st->err);
+                    A->i, A->data, brow, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal, sorted);
         AMGT_LAUNCH(csr2bsr_large_kernel<true>, 2 * st->sm_count, kLargeThreads, 2 * kWin * sizeof(uint32_t), s, m,
                     n, A->i, A->j, A->data, large, stats, nullptr, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal,
                     nullptr);
@@ -597,11 +589,13 @@ int amgt_csr_to_bsr(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream)
     free_ptr(cnt, s);
     free_ptr(large, s);
     free_ptr(stats, s);
+    free_ptr(sorted, s);
     return AMGT_OK;
 fail:
     free_ptr(cnt, s);
     free_ptr(large, s);
     free_ptr(stats, s);
+    free_ptr(sorted, s);
     amgt_bsr_free(out, stream);
     return rc;
 }

@@ -6,11 +6,9 @@
 // packed form keeps the block structure (block-row pointers, block columns
 // and bitmaps, borrowed from the mBSR matrix) and stores only the values of
 // set bits, block after block, in bitmap order (row-major inside the
-// block), plus each block's offset into that array.  Lane q of a block's
-// 4-lane group reads nibble q of the bitmap, skips to its row's first value
-// with a popcount, and multiplies the set entries of its row: the same
-// per-row sum, in the same order, as the dense kernel minus its zero terms.
-// Bytes per block: 4 (column) + 4 (offset) + 2 (bitmap) + s * set bits.
+// block), plus each block row's offset into that array.
+// Bytes per block: 4 (column) + 2 (bitmap) + s * set bits, plus 4 per
+// block row.
 #include <cstdlib>
 
 #include "spmv_common.cuh"
@@ -42,55 +40,116 @@ __device__ __forceinline__ typename ValTraits<PREC>::acc_t packed_value(const vo
     }
 }
 
-template <int PREC, bool SAFE>
-__device__ __forceinline__ typename ValTraits<PREC>::acc_t packed_row_dot(
-    const void *__restrict__ val, const uint16_t *__restrict__ map, const int *__restrict__ voff,
-    const double *__restrict__ x, int n, int k, int q, int col, typename ValTraits<PREC>::acc_t acc)
+template <int PREC>
+struct PackedT {
+    using val_t = double;
+};
+template <>
+struct PackedT<AMGT_FLOAT> {
+    using val_t = float;
+};
+template <>
+struct PackedT<AMGT_HALF> {
+    using val_t = unsigned short;
+};
+template <>
+struct PackedT<AMGT_BF16> {
+    using val_t = unsigned short;
+};
+
+template <int PREC>
+__device__ __forceinline__ typename ValTraits<PREC>::acc_t widen(typename PackedT<PREC>::val_t v)
 {
-    using acc_t = typename ValTraits<PREC>::acc_t;
-    const uint32_t mp = __ldcs(map + k);
-    const uint32_t nib = (mp >> (4 * q)) & 0xFu;
-    if (nib) {
-        long long off = __ldcs(voff + k) + __popc(mp & ((1u << (4 * q)) - 1u));
-        double xv[4];
-        load_x4<SAFE>(x, col, n, xv);
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-            if ((nib >> c) & 1u) {
-                acc = fma(packed_value<PREC>(val, off), (acc_t)xv[c], acc);
-                ++off;
-            }
-    }
-    return acc;
+    if constexpr (PREC == AMGT_HALF) return __half2float(__ushort_as_half(v));
+    else if constexpr (PREC == AMGT_BF16) return __bfloat162float(__ushort_as_bfloat16(v));
+    else return v;
 }
 
+// One warp, 32 / LPR segments of LPR lanes, one block row per segment.
+// The row's packed values are contiguous (row offset rvoff[b]), so the
+// segment loads them into shared memory with consecutive loads in the same
+// round trip as the row's block columns and bitmaps (lane j of the segment
+// takes block j of a chunk of LPR blocks); a popcount scan over the chunk
+// gives each block's first value.  Then 4 lanes per block, lane q taking
+// block row q, multiply with x like the 16-value kernel (an FMA for every
+// column, zero where the bit is clear).  Segments step in lockstep so the
+// warp can synchronise; rows whose values do not fit the staging slice are
+// taken in chunks of LPR blocks.
 template <int PREC, int LPR, bool SAFE, int EPI>
 __global__ void __launch_bounds__(256)
 pspmv_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__restrict__ idx,
-             const uint16_t *__restrict__ map, const int *__restrict__ voff, const void *__restrict__ val,
+             const uint16_t *__restrict__ map, const int *__restrict__ rvoff, const void *__restrict__ valv,
              const double *__restrict__ x, PEpiArgs e)
 {
     using acc_t = typename ValTraits<PREC>::acc_t;
+    using val_t = typename PackedT<PREC>::val_t;
     constexpr int RPW = 32 / LPR;
     constexpr int G = LPR / 4;
+    constexpr int CAP = 16 * LPR;  // staged values per segment (a chunk of LPR full blocks)
+    __shared__ val_t stage[8][RPW][CAP];
     __shared__ double sred[8];
-    const int lane = threadIdx.x & 31;
+    const val_t *__restrict__ val = static_cast<const val_t *>(valv);
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int sub = lane / LPR, l = lane % LPR, g = l >> 2, q = l & 3;
+    const int seg0 = sub * LPR;  // first lane of this segment
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    val_t *st = stage[wib][sub];
     double dot = 0.0;
     for (int b0 = warp * RPW; b0 < brow; b0 += nwarps * RPW) {
         const int b = b0 + sub;
-        acc_t acc = 0;
+        int start = 0, end = 0, v0 = 0;
         if (b < brow) {
-            const int start = ptr[b], end = ptr[b + 1];
-            int k = start + g;
-            for (; k + G < end; k += 2 * G) {
-                const int c0 = __ldcs(idx + k), c1 = __ldcs(idx + k + G);
-                acc = packed_row_dot<PREC, SAFE>(val, map, voff, x, n, k, q, c0, acc);
-                acc = packed_row_dot<PREC, SAFE>(val, map, voff, x, n, k + G, q, c1, acc);
+            start = ptr[b];
+            end = ptr[b + 1];
+            v0 = rvoff[b];
+        }
+        int chunks = (end - start + LPR - 1) / LPR;
+#pragma unroll
+        for (int o = LPR; o < 32; o <<= 1) chunks = max(chunks, __shfl_xor_sync(FULL, chunks, o));
+        acc_t acc = 0;
+        for (int ch = 0; ch < chunks; ++ch) {
+            const int cb = start + ch * LPR;
+            const int j = cb + l;  // this lane's block of the chunk
+            uint32_t mp = 0;
+            int col = 0;
+            if (j < end) {
+                mp = __ldcs(map + j);
+                col = __ldcs(idx + j);
             }
-            if (k < end) acc = packed_row_dot<PREC, SAFE>(val, map, voff, x, n, k, q, __ldcs(idx + k), acc);
+            const int cnt = __popc(mp);
+            // values of the chunk: [v0, v0 + chunk total); a single-chunk row
+            // knows its range from rvoff alone
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < LPR; o <<= 1) {
+                const int y = __shfl_up_sync(FULL, incl, o, LPR);
+                if (l >= o) incl += y;
+            }
+            const int total = __shfl_sync(FULL, incl, LPR - 1, LPR);
+            for (int v = l; v < total; v += LPR) st[v] = __ldcs(val + v0 + v);
+            const int excl = incl - cnt;
+            __syncwarp();
+            for (int it = 0; it < LPR / G; ++it) {
+                const int jj = it * G + g;  // block of the chunk this 4-lane group takes
+                const uint32_t bm = __shfl_sync(FULL, mp, seg0 + jj);
+                const int bc = __shfl_sync(FULL, col, seg0 + jj);
+                const int bo = __shfl_sync(FULL, excl, seg0 + jj);
+                if (cb + jj < end) {
+                    double xv[4];
+                    load_x4<SAFE>(x, bc, n, xv);
+                    const uint32_t nib = (bm >> (4 * q)) & 0xFu;
+                    int o = bo + __popc(bm & ((1u << (4 * q)) - 1u));
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        acc_t w = (acc_t)0;
+                        if ((nib >> c) & 1u) w = widen<PREC>(st[o++]);
+                        acc = fma(w, (acc_t)xv[c], acc);
+                    }
+                }
+            }
+            v0 += total;
+            __syncwarp();
         }
 #pragma unroll
         for (int o = 4; o < LPR; o <<= 1) acc += __shfl_xor_sync(FULL, acc, o);
@@ -132,6 +191,14 @@ __global__ void popc_kernel(int nblk, const uint16_t *__restrict__ map, int *__r
         cnt[k] = __popc((uint32_t)map[k]);
 }
 
+// row offset = value offset of the row's first block
+__global__ void row_offset_kernel(int brow, const int *__restrict__ ptr, const int *__restrict__ voff,
+                                  int *__restrict__ rvoff)
+{
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= brow; b += gridDim.x * blockDim.x)
+        rvoff[b] = voff[ptr[b]];
+}
+
 template <int PREC>
 __global__ void pack_kernel(long long nblk, const uint16_t *__restrict__ map, const int *__restrict__ voff,
                             const double *__restrict__ val, void *__restrict__ out)
@@ -153,10 +220,15 @@ __global__ void pack_kernel(long long nblk, const uint16_t *__restrict__ map, co
 
 static int packed_lpr(const amgt_pbsr *A)
 {
+    static int env = -1;
+    if (env < 0) {
+        const char *ev = getenv("AMGT_PSPMV_LPR");
+        env = ev ? atoi(ev) : 0;
+    }
+    if (env == 8 || env == 16 || env == 32) return env;
     const double avg = A->blc_row ? (double)A->blc_num / A->blc_row : 0.0;
-    if (avg <= 1.5) return 4;
     if (avg <= 3.0) return 8;
-    if (avg <= 10.0) return 16;
+    if (avg <= 12.0) return 16;
     return 32;
 }
 
@@ -174,13 +246,12 @@ static int launch_packed(const amgt_pbsr *A, const double *x, const PEpiArgs &e,
     if (lpr == L) {                                                                                          \
         if (safe)                                                                                            \
             AMGT_LAUNCH((pspmv_kernel<PREC, L, true, EPI>), grid, 256, 0, s, A->row, A->col, A->blc_row,     \
-                        A->blcPtr, A->blcIdx, A->blcMap, A->blcVoff, A->val, x, e);                          \
+                        A->blcPtr, A->blcIdx, A->blcMap, A->rowVoff, A->val, x, e);                          \
         else                                                                                                 \
             AMGT_LAUNCH((pspmv_kernel<PREC, L, false, EPI>), grid, 256, 0, s, A->row, A->col, A->blc_row,    \
-                        A->blcPtr, A->blcIdx, A->blcMap, A->blcVoff, A->val, x, e);                          \
+                        A->blcPtr, A->blcIdx, A->blcMap, A->rowVoff, A->val, x, e);                          \
         return AMGT_OK;                                                                                      \
     }
-    AMGT_P_CASE(4)
     AMGT_P_CASE(8)
     AMGT_P_CASE(16)
     AMGT_P_CASE(32)
@@ -236,7 +307,7 @@ int amgt_pbsr_free(amgt_pbsr *A, amgt_stream_t stream)
 {
     if (!A) return AMGT_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
-    free_ptr(A->blcVoff, s);
+    free_ptr(A->rowVoff, s);
     free_ptr(A->val, s);
     memset(A, 0, sizeof(*A));
     return AMGT_OK;
@@ -261,42 +332,48 @@ int amgt_bsr_pack(const amgt_bsr *A, int prec, amgt_pbsr *out, amgt_stream_t str
     out->blcMap = A->blcMap;
     out->max_blc_per_row = A->max_blc_per_row;
     const int nb = A->blc_num;
-    int *cnt = nullptr;
+    int *cnt = nullptr, *voff = nullptr;
     int64_t *tot = nullptr;
     const int64_t *h = nullptr;
     int rc = AMGT_OK;
     const size_t vs = prec == AMGT_DOUBLE ? 8 : (prec == AMGT_FLOAT ? 4 : 2);
-    if ((rc = alloc_n(&out->blcVoff, (size_t)nb + 1, s)) || (rc = alloc_n(&cnt, (size_t)nb + 1, s)) ||
-        (rc = alloc_n(&tot, 1, s)))
+    if ((rc = alloc_n(&voff, (size_t)nb + 1, s)) || (rc = alloc_n(&out->rowVoff, (size_t)A->blc_row + 1, s)) ||
+        (rc = alloc_n(&cnt, (size_t)nb + 1, s)) || (rc = alloc_n(&tot, 1, s)))
         goto fail;
     AMGT_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * ((size_t)nb + 1), s));
     AMGT_CUDA_TRY(cudaMemsetAsync(tot, 0, sizeof(int64_t), s));
     if (nb > 0) AMGT_LAUNCH(popc_kernel, grid_for(256, nb, st->sm_count, 8), 256, 0, s, nb, A->blcMap, cnt);
-    if ((rc = exclusive_scan_int(cnt, out->blcVoff, nb + 1, s))) goto fail;
+    if ((rc = exclusive_scan_int(cnt, voff, nb + 1, s))) goto fail;
+    AMGT_LAUNCH(row_offset_kernel, grid_for(256, A->blc_row + 1LL, st->sm_count, 8), 256, 0, s, A->blc_row,
+                A->blcPtr, voff, out->rowVoff);
     if (A->csr_nnz > 0 || nb == 0) {
         out->nnz = A->csr_nnz;  // number of set bits, known: no read-back
     } else {
-        AMGT_CUDA_TRY(cudaMemcpyAsync(tot, out->blcVoff + nb, sizeof(int), cudaMemcpyDeviceToDevice, s));
+        AMGT_CUDA_TRY(cudaMemcpyAsync(tot, voff + nb, sizeof(int), cudaMemcpyDeviceToDevice, s));
         if ((rc = read_back(tot, 1, s, &h))) goto fail;
         out->nnz = (int)h[0];
     }
-    out->val = dev_alloc((size_t)(out->nnz > 0 ? out->nnz : 1) * vs, s);
+    // 4 values of padding: the kernels read a row's 4 candidates unconditionally
+    out->val = dev_alloc(((size_t)out->nnz + 4) * vs, s);
     if (!out->val) { rc = AMGT_ERR_ALLOC; goto fail; }
+    AMGT_CUDA_TRY(cudaMemsetAsync((char *)out->val + (size_t)out->nnz * vs, 0, 4 * vs, s));
     if (nb > 0) {
         const int grid = grid_for(256, 16LL * nb, st->sm_count, 8);
         switch (prec) {
-        case AMGT_DOUBLE: AMGT_LAUNCH(pack_kernel<AMGT_DOUBLE>, grid, 256, 0, s, (long long)nb, A->blcMap, out->blcVoff, A->blcVal, out->val); break;
-        case AMGT_FLOAT: AMGT_LAUNCH(pack_kernel<AMGT_FLOAT>, grid, 256, 0, s, (long long)nb, A->blcMap, out->blcVoff, A->blcVal, out->val); break;
-        case AMGT_HALF: AMGT_LAUNCH(pack_kernel<AMGT_HALF>, grid, 256, 0, s, (long long)nb, A->blcMap, out->blcVoff, A->blcVal, out->val); break;
-        default: AMGT_LAUNCH(pack_kernel<AMGT_BF16>, grid, 256, 0, s, (long long)nb, A->blcMap, out->blcVoff, A->blcVal, out->val); break;
+        case AMGT_DOUBLE: AMGT_LAUNCH(pack_kernel<AMGT_DOUBLE>, grid, 256, 0, s, (long long)nb, A->blcMap, voff, A->blcVal, out->val); break;
+        case AMGT_FLOAT: AMGT_LAUNCH(pack_kernel<AMGT_FLOAT>, grid, 256, 0, s, (long long)nb, A->blcMap, voff, A->blcVal, out->val); break;
+        case AMGT_HALF: AMGT_LAUNCH(pack_kernel<AMGT_HALF>, grid, 256, 0, s, (long long)nb, A->blcMap, voff, A->blcVal, out->val); break;
+        default: AMGT_LAUNCH(pack_kernel<AMGT_BF16>, grid, 256, 0, s, (long long)nb, A->blcMap, voff, A->blcVal, out->val); break;
         }
     }
     free_ptr(cnt, s);
     free_ptr(tot, s);
+    free_ptr(voff, s);
     return AMGT_OK;
 fail:
     free_ptr(cnt, s);
     free_ptr(tot, s);
+    free_ptr(voff, s);
     amgt_pbsr_free(out, stream);
     return rc;
 }
@@ -305,7 +382,7 @@ int amgt_pbsr_spmv(double alpha, const amgt_pbsr *A, const double *x, double bet
 {
     if (!A || (A->row > 0 && !y)) return AMGT_ERR_INVALID;
     if (A->row == 0) return AMGT_OK;
-    if (A->blc_num > 0 && (!x || !A->val || !A->blcVoff)) return AMGT_ERR_INVALID;
+    if (A->blc_num > 0 && (!x || !A->val || !A->rowVoff)) return AMGT_ERR_INVALID;
     DeviceState *st;
     AMGT_TRY(device_state(&st));
     return pbsr_spmv(A, alpha, x, beta, y, (cudaStream_t)stream, st->sm_count);

@@ -216,7 +216,8 @@ AMGT_API int amgt_bsr_jacobi(int prec, const amgt_bsr *A, const double *inv_l1,
  * structure (blcPtr, blcIdx, blcMap) is borrowed from the amgt_bsr it was
  * packed from, which must outlive it.  At the fill of AMG operators (about
  * 4 of 16) an SpMV reads ~3x fewer bytes than on the 16-value blocks.  No
- * counterpart in the reference (it keeps 16 values per block). */
+ * counterpart in the reference (it keeps 16 values per block).  Each block
+ * row's values are contiguous, starting at rowVoff[b]. */
 typedef struct {
     int row, col, blc_row, blc_col, blc_num;
     int nnz;                  /* stored values (= set bits)            */
@@ -224,7 +225,8 @@ typedef struct {
     const int *blcPtr;        /* borrowed                              */
     const int *blcIdx;        /* borrowed                              */
     const uint16_t *blcMap;   /* borrowed                              */
-    int *blcVoff;             /* [blc_num + 1] value offset per block  */
+    int *rowVoff;             /* [blc_row + 1] offset of each block
+                                 row's first value                      */
     void *val;                /* [nnz] double / float / half / bf16    */
     int max_blc_per_row;
 } amgt_pbsr;
