@@ -44,6 +44,25 @@ def csr_bytes(nnz: int, m: int, n: int) -> int:
     return nnz * 12 + 4 * (m + 1) + 8 * n + 8 * m
 
 
+def max_over_ranks(x: float, device="cpu") -> float:
+    """The largest x over all ranks (timings are reported as the max over
+    ranks); identity without an initialised process group."""
+    import torch
+    import torch.distributed as dist
+
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_gbs(bytes_per_rank: int, ms_max: float, world: int) -> float:
+    """Aggregate GB/s of `world` replicas that each moved bytes_per_rank in
+    ms_max milliseconds (the slowest rank's time)."""
+    return world * bytes_per_rank / (ms_max * 1e-3) / 1e9
+
+
 def read_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -153,9 +172,9 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "n_gpus": args.gpus,
         "steps": k, "warmup": args.warmup, "ms_per_step": round(1e3 * el / k, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "mBSR SpMV y=A*x, 3D 7-point Poisson 128^3 fp64", "parallelism": "host threads"},
+        "config": {"workload": f"mBSR SpMV y=A*x (fp64), 3D 7-point Poisson {GRID[0]}^3", "parallelism": "host threads"},
         "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": cores, "kind": "port",
-                         "sample": f"{k} full SpMVs of the 128^3 operator (C oracle, OpenMP)"},
+                         "sample": f"{k} full SpMVs of the {GRID[0]}^3 operator (C oracle, OpenMP)"},
         "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -328,12 +347,10 @@ def run_amgt(args):
         torch.cuda.synchronize()
     launches = amgt.kernel_launch_count() - launches0
     ms = ev0.elapsed_time(ev1) / args.steps
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    ms_max = max_over_ranks(ms, device="cuda")
     if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    ms_max = float(t.item())
-    value = world * nbytes / (ms_max * 1e-3) / 1e9
+    value = whole_job_gbs(nbytes, ms_max, world)
     per_gpu = nbytes / (ms * 1e-3) / 1e9
 
     # the same product on the bitmap-packed values (what the solver runs)
@@ -371,10 +388,7 @@ def run_amgt(args):
     ev1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = ev0.elapsed_time(ev1) / args.steps
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * nbytes / (float(t.item()) * 1e-3) / 1e9
+    e2e_value = whole_job_gbs(nbytes, max_over_ranks(e2e_ms, device="cuda"), world)
 
     # hierarchy: RAP per level and SpMV GB/s per level (not part of `value`);
     # built twice, the first pass loading the kernels' modules
