@@ -192,24 +192,32 @@ __global__ void spgemm_ub_kernel(int brA, const int *__restrict__ aptr, const in
 
 // One pass: per A block row, the sorted C block columns and bitmaps go to
 // the row's scratch slice (offset ub_off[b], capacity ub[b]); C blocks per
-// row -> ccnt[b], CSR nonzeros per scalar row -> csrcnt[4b+q]; rows beyond
-// the warp capacity -> large list.
+// row -> ccnt[b], CSR nonzeros per scalar row -> csrcnt[4b+q].  Two
+// instances: CAP = 256 over all rows (small shared buffer, high occupancy),
+// passing rows with more pairs to the CAP = 1024 instance through a list
+// (rows[], count in *nrows), which passes rows beyond that to the window
+// kernel's list.
+template <int CAP>
 __global__ void __launch_bounds__(32 * kSymWarps)
 spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
                        const uint16_t *__restrict__ amap, const int *__restrict__ bptr,
                        const int *__restrict__ bidx, const uint16_t *__restrict__ bmap, int *__restrict__ ccnt,
                        int *__restrict__ csrcnt, int *__restrict__ large, int64_t *__restrict__ stats,
-                       const int64_t *__restrict__ ub_off, int *__restrict__ skey, uint16_t *__restrict__ smap)
+                       const int64_t *__restrict__ ub_off, int *__restrict__ skey, uint16_t *__restrict__ smap,
+                       const int *__restrict__ rows, const int *__restrict__ nrows, int *__restrict__ over,
+                       int *__restrict__ nover)
 {
-    __shared__ unsigned long long sbuf[kSymWarps][kSymCap];
+    __shared__ unsigned long long sbuf[kSymWarps][CAP];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long *s = sbuf[warp];
     unsigned long long wmax = 0, wsq = 0;  // per-warp statistics, one atomic each at the end
-    for (int b = blockIdx.x * kSymWarps + warp; b < brA; b += gridDim.x * kSymWarps) {
+    const int nr = rows ? *nrows : brA;
+    for (int t = blockIdx.x * kSymWarps + warp; t < nr; t += gridDim.x * kSymWarps) {
+        const int b = rows ? rows[t] : t;
         const int a0 = aptr[b], a1 = aptr[b + 1];
         const long long ub = ub_off[b + 1] - ub_off[b];
-        if (ub > kSymCap) {
-            if (lane == 0) large[atomicAdd((int *)&stats[3], 1)] = b;
+        if (ub > CAP) {
+            if (lane == 0) over[atomicAdd(nover, 1)] = b;
             continue;
         }
         const int cnt = sym_collect(lane, a0, a1, aidx, amap, bptr, bidx, bmap, s);
@@ -396,7 +404,7 @@ __device__ __forceinline__ int search_sorted(const int *keys, int n, int key)
 }
 
 template <int PREC>
-__global__ void __launch_bounds__(32 * kNumWarps)
+__global__ void __launch_bounds__(32 * kNumWarps, 12)
 spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
                       const uint16_t *__restrict__ amap, const typename NumT<PREC>::val_t *__restrict__ aval,
                       const int *__restrict__ bptr, const int *__restrict__ bidx,
@@ -532,7 +540,7 @@ static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B
 {
     using V = typename NumT<PREC>::val_t;
     if (A->blc_row == 0) return AMGT_OK;
-    AMGT_LAUNCH(spgemm_numeric_kernel<PREC>, grid_for(kNumWarps, A->blc_row, sm_count, 8), 32 * kNumWarps, 0, s,
+    AMGT_LAUNCH(spgemm_numeric_kernel<PREC>, grid_for(kNumWarps, A->blc_row, sm_count, 12), 32 * kNumWarps, 0, s,
                 A->row, A->blc_row, A->blcPtr, A->blcIdx, A->blcMap, (const V *)aval, B->blcPtr, B->blcIdx,
                 B->blcMap, (const V *)bval, C->blcPtr, C->blcIdx, C->blcMap, C->blcVal, cshadow,
                 Ccsr ? Ccsr->i : nullptr, Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr, ub_off, skey,
@@ -595,8 +603,9 @@ int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
         }
     }
     if ((rc = alloc_n(&C->blcPtr, brA + 1, s)) || (rc = alloc_n(&ccnt, brA + 1, s)) ||
-        (rc = alloc_n(&csrcnt, m + 1, s)) || (rc = alloc_n(&large, brA, s)) || (rc = alloc_n(&stats, 4, s)) ||
-        (rc = alloc_n(&ub, (size_t)brA + 1, s)) || (rc = alloc_n(&ub_off, (size_t)brA + 1, s)))
+        (rc = alloc_n(&csrcnt, m + 1, s)) || (rc = alloc_n(&large, 2 * (size_t)brA + 1, s)) ||
+        (rc = alloc_n(&stats, 4, s)) || (rc = alloc_n(&ub, (size_t)brA + 1, s)) ||
+        (rc = alloc_n(&ub_off, (size_t)brA + 1, s)))
         goto fail;
     AMGT_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(int64_t) * 4, s));
     AMGT_CUDA_TRY(cudaMemsetAsync(ccnt, 0, sizeof(int) * (brA + 1), s));
@@ -620,9 +629,15 @@ int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
         if ((rc = alloc_n(&skey, (size_t)cap, s)) || (rc = alloc_n(&smap, (size_t)cap, s))) goto fail;
     }
     if (brA > 0) {
-        AMGT_LAUNCH(spgemm_symbolic_kernel, grid_for(kSymWarps, brA, st->sm_count, 8), 32 * kSymWarps, 0, s, m, brA,
-                    A->blcPtr, A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, ccnt, csrcnt, large, stats,
-                    ub_off, skey, smap);
+        // medium-row list and count live behind the large list (2 * brA + 1 ints)
+        int *medium = large + brA, *nmedium = large + 2 * brA;
+        AMGT_CUDA_TRY(cudaMemsetAsync(nmedium, 0, sizeof(int), s));
+        AMGT_LAUNCH(spgemm_symbolic_kernel<256>, grid_for(kSymWarps, brA, st->sm_count, 16), 32 * kSymWarps, 0, s, m,
+                    brA, A->blcPtr, A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, ccnt, csrcnt, large,
+                    stats, ub_off, skey, smap, nullptr, nullptr, medium, nmedium);
+        AMGT_LAUNCH(spgemm_symbolic_kernel<kSymCap>, 2 * st->sm_count, 32 * kSymWarps, 0, s, m, brA, A->blcPtr,
+                    A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, ccnt, csrcnt, large, stats, ub_off, skey,
+                    smap, medium, nmedium, large, (int *)&stats[3]);
         AMGT_LAUNCH(spgemm_symbolic_large_kernel, 2 * st->sm_count, kSymLargeThreads, 0, s, m, A->blcPtr, A->blcIdx,
                     A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, large, stats, ccnt, csrcnt, ub_off, skey, smap);
     }
