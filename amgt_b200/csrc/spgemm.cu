@@ -18,19 +18,19 @@
 // scan of the per-row pair bounds) with its block and CSR counts; one host
 // read-back then sizes C, and the numeric kernel moves the pattern into C.
 //
-// Numeric.  One warp per C block row accumulates the row's C blocks in
-// shared memory (global memory for rows of more than 32 blocks); lane t
-// holds C block column t, so a product finds its C block with one ballot.
-// A blocks are taken in row order; per A block the two half-warps take two
-// B blocks at a time, lane e of a half computing entry e = (r, c) of the 4x4 product
-// as the sum over k ascending of a[r][k] * b[k][c] over terms whose A and B
-// bits are set, started from zero, with separate multiply and add (no FMA),
-// and adding it to C(r, c) where the product bitmap has the bit - the
+// Numeric.  One warp per A block row; the row's (A block, B block) pairs
+// are flattened and taken 8 at a time, 4 lanes per pair (lane r: row r of
+// the 4x4 product), B blocks staged through shared memory, so that every
+// load of a step is in flight at once.  Entry (r, c) of a product is the
+// sum over k ascending of a[r][k] * b[k][c] with separate multiply and add
+// (no FMA); products are added to their C block in A block order, the
 // arithmetic of the reference's scalar branch (:1289-1339), so the fp64
-// result equals the CPU oracle bit for bit.  FP64 arithmetic on the CUDA cores: the 4x4
-// products are too small for tcgen05 (M >= 64), and on B200 the fp64 MMA
-// rate equals the fp64 FMA rate.  The CSR form of C is written by the same
-// kernel (no separate BSR2CSR pass).
+// result equals the CPU oracle bit for bit (for finite values: unstored
+// entries are zero and their products change no sum).  C rows of up to 32
+// blocks accumulate in shared memory, longer rows in place.  FP64
+// arithmetic on the CUDA cores: the 4x4 products are too small for tcgen05
+// (M >= 64), and on B200 the fp64 MMA rate equals the fp64 FMA rate.  The
+// CSR form of C is written by the same kernel (no separate BSR2CSR pass).
 #include "rowunion.cuh"
 
 namespace amgt {
@@ -403,115 +403,217 @@ __device__ __forceinline__ int search_sorted(const int *keys, int n, int key)
     return lo;
 }
 
+// Accumulator and B-stage strides (elements) per C block: 16 values plus a
+// 16-byte pad, so that the 16-byte row accesses of the 8 pairs of one step
+// fall in distinct banks.
+template <typename acc_t>
+struct NumStride {
+    static constexpr int v = 16 + 16 / (int)sizeof(acc_t);
+};
+
+// Four consecutive values of a block row, widened to the accumulator type.
 template <int PREC>
-__global__ void __launch_bounds__(32 * kNumWarps, 12)
+__device__ __forceinline__ void load_row4(const typename NumT<PREC>::val_t *p, typename NumT<PREC>::acc_t out[4])
+{
+    if constexpr (PREC == AMGT_DOUBLE) {
+        const double2 u = reinterpret_cast<const double2 *>(p)[0], w = reinterpret_cast<const double2 *>(p)[1];
+        out[0] = u.x; out[1] = u.y; out[2] = w.x; out[3] = w.y;
+    } else if constexpr (PREC == AMGT_FLOAT) {
+        const float4 u = *reinterpret_cast<const float4 *>(p);
+        out[0] = u.x; out[1] = u.y; out[2] = u.z; out[3] = u.w;
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) out[q] = NumT<PREC>::ld(p, q);
+    }
+}
+
+// Widens one 16-byte chunk of stored values and writes it to shared memory.
+template <int PREC>
+__device__ __forceinline__ void stage_chunk(const uint4 raw, typename NumT<PREC>::acc_t *dst)
+{
+    using V = typename NumT<PREC>::val_t;
+    constexpr int VPC = 16 / (int)sizeof(V);
+    const V *v = reinterpret_cast<const V *>(&raw);
+    if constexpr (PREC == AMGT_DOUBLE) {
+        *reinterpret_cast<double2 *>(dst) = make_double2(v[0], v[1]);
+    } else if constexpr (PREC == AMGT_FLOAT) {
+        *reinterpret_cast<float4 *>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < VPC; ++q) dst[q] = NumT<PREC>::ld(v, q);
+    }
+}
+
+// Numeric phase.  One warp per A block row; the row's (A block, B block)
+// pairs are flattened (up to 32 A blocks at a time: lane i holds A block
+// i's B row range, a warp scan of the lengths numbers the pairs) and taken
+// 8 at a time, 4 lanes per pair, lane r computing row r of the 4x4 product.
+// The 8 B blocks are staged through shared memory with 16-byte loads; all
+// loads of a step are independent, so each step costs one memory round
+// trip.  Every term of the product is computed (unstored entries are zero):
+// for finite values this gives the stored-term sums of the reference's
+// scalar branch bit for bit, because adding a zero product leaves a
+// non-zero partial sum unchanged and a partial sum started from +0 never
+// becomes -0.  Products are added to their C block in pair order (= A block
+// order): pairs of one step that hit the same C block row are applied in
+// rounds, lowest lane first (match_any), so the accumulation order is the
+// sequential one.  Rows of up to 32 C blocks accumulate in shared memory
+// (lane t holds C column t; a product finds its slot by a five-step shuffle
+// search), longer rows in place in C (binary search in the sorted pattern).
+template <int PREC>
+__global__ void __launch_bounds__(32 * kNumWarps, 8)
 spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
-                      const uint16_t *__restrict__ amap, const typename NumT<PREC>::val_t *__restrict__ aval,
-                      const int *__restrict__ bptr, const int *__restrict__ bidx,
-                      const uint16_t *__restrict__ bmap, const typename NumT<PREC>::val_t *__restrict__ bval,
+                      const typename NumT<PREC>::val_t *__restrict__ aval, const int *__restrict__ bptr,
+                      const int *__restrict__ bidx, const typename NumT<PREC>::val_t *__restrict__ bval,
                       const int *__restrict__ cptr, int *__restrict__ cidx, uint16_t *__restrict__ cmap,
                       double *__restrict__ cval, void *__restrict__ cshadow, const int *__restrict__ csr_i,
                       int *__restrict__ csr_j, double *__restrict__ csr_a, const int64_t *__restrict__ ub_off,
                       const int *__restrict__ skey, const uint16_t *__restrict__ smap)
 {
     using T = NumT<PREC>;
+    using V = typename T::val_t;
     using acc_t = typename T::acc_t;
-    __shared__ acc_t sacc[kNumWarps][kNumCap * 16];
+    constexpr int SS = NumStride<acc_t>::v;
+    constexpr int CH = (int)sizeof(V);  // 16-byte chunks per block (16 values)
+    constexpr int VPC = 16 / CH;        // values per chunk
+    __shared__ __align__(16) acc_t sacc[kNumWarps][kNumCap * SS];
+    __shared__ __align__(16) acc_t sstage[kNumWarps][8 * SS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int e = lane & 15, r = e >> 2, c = e & 3, half = lane & 16;
+    const int ps = lane >> 2, r = lane & 3;
+    acc_t *sa = sacc[warp];
+    acc_t *sb = sstage[warp];
     for (int b = blockIdx.x * kNumWarps + warp; b < brA; b += gridDim.x * kNumWarps) {
         const int c0 = cptr[b], cn = cptr[b + 1] - c0;
         // the row's pattern, sorted by the symbolic pass, moves from scratch to C
-        const long long sb = ub_off[b];
+        const long long sbase = ub_off[b];
         for (int t = lane; t < cn; t += 32) {
-            cidx[c0 + t] = skey[sb + t];
-            cmap[c0 + t] = smap[sb + t];
+            cidx[c0 + t] = skey[sbase + t];
+            cmap[c0 + t] = smap[sbase + t];
         }
-        // rows of up to 32 C blocks: lane t holds C column t and the row
-        // accumulates in shared memory; longer rows accumulate in place
         const bool small = cn <= kNumCap;
-        const int mykey = (small && lane < cn) ? skey[sb + lane] : -1;
-        acc_t *sa = sacc[warp];
+        const int mykey = (small && lane < cn) ? skey[sbase + lane] : 0x7FFFFFFF;
         double *ga = cval + 16LL * c0;
-        __syncwarp();
         if (small) {
-            for (int t = lane; t < 16 * cn; t += 32) sa[t] = (acc_t)0;
+            for (int t = lane; t < 16 * cn; t += 32) sa[(t >> 4) * SS + (t & 15)] = (acc_t)0;
         } else {
             for (int t = lane; t < 16 * cn; t += 32) ga[t] = 0.0;
         }
         __syncwarp();
         const int a0 = aptr[b], a1 = aptr[b + 1];
         for (int ib = a0; ib < a1; ib += 32) {
-          // lane i fetches A block ib+i's bitmap and B row range up front
-          int pj0 = 0, pj1 = 0;
-          uint32_t pma = 0;
-          if (ib + lane < a1) {
-              const int k = aidx[ib + lane];
-              pma = amap[ib + lane];
-              pj0 = bptr[k];
-              pj1 = bptr[k + 1];
-          }
-          const int na = min(32, a1 - ib);
-          for (int ii = 0; ii < na; ++ii) {
-            const int i = ib + ii;
-            const uint32_t ma = __shfl_sync(FULL, pma, ii);
-            const int j0 = __shfl_sync(FULL, pj0, ii), j1 = __shfl_sync(FULL, pj1, ii);
-            acc_t ar[4];  // row r of the A block
+            int j0 = 0, len = 0;
+            if (ib + lane < a1) {
+                const int k = aidx[ib + lane];
+                j0 = bptr[k];
+                len = bptr[k + 1] - j0;
+            }
+            int incl = len;
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk) ar[kk] = T::ld(aval, 16LL * i + 4 * r + kk);
-            const uint32_t arow = (ma >> (4 * r)) & 0xFu;  // bit kk: A(r, kk) stored
-            for (int jj = j0; jj < j1; jj += 2) {
-                const int j = jj + (half >> 4);
-                const bool valid = j < j1;
-                const uint32_t mb = valid ? bmap[j] : 0u;
-                const acc_t bl = valid ? T::ld(bval, 16LL * j + e) : (acc_t)0;
-                const int key = valid ? bidx[j] : -2;
-                // bit kk of terms: A(r, kk) and B(kk, c) both stored
-                const uint32_t bcol = (mb >> c) & 0x1111u;
-                const uint32_t terms = arow & ((bcol | (bcol >> 3) | (bcol >> 6) | (bcol >> 9)) & 0xFu);
-                acc_t s = (acc_t)0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int total = __shfl_sync(FULL, incl, 31);
+            const int jd = j0 - (incl - len);  // B block of pair q of A block i: q + jd[i]
+            for (int q0 = 0; q0 < total; q0 += 8) {
+                const int q = q0 + ps;
+                const bool valid = q < total;
+                int src = 0;
 #pragma unroll
-                for (int kk = 0; kk < 4; ++kk) {
-                    const acc_t bv = __shfl_sync(FULL, bl, half | (kk * 4 + c));
-                    if ((terms >> kk) & 1u) s = T::add(s, T::mul(ar[kk], bv));
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int v = __shfl_sync(FULL, incl, min(src + step - 1, 31));
+                    if (v <= q) src += step;
                 }
-                int t;
-                if (small) {
-                    const int k0 = __shfl_sync(FULL, key, 0), k1 = __shfl_sync(FULL, key, 16);
-                    const unsigned m0 = __ballot_sync(FULL, mykey == k0), m1 = __ballot_sync(FULL, mykey == k1);
-                    t = __ffs(half ? m1 : m0) - 1;
-                } else {
-                    t = valid ? search_sorted(cidx + c0, cn, key) : 0;
-                }
-                if (valid && terms) {
-                    if (small) {
-                        sa[16 * t + e] = T::add(sa[16 * t + e], s);
-                    } else {
-                        const acc_t cur = (acc_t)ga[16 * t + e];
-                        ga[16 * t + e] = (double)T::add(cur, s);
+                src = min(src, 31);
+                const int j = q + __shfl_sync(FULL, jd, src);
+                const int key = valid ? bidx[j] : -1;
+                acc_t ar[4];
+                if (valid) load_row4<PREC>(aval + 16LL * (ib + src) + 4 * r, ar);
+                // stage the step's B blocks: chunk w of pair p to p * SS + w * VPC
+#pragma unroll
+                for (int h = 0; h < (8 * CH + 31) / 32; ++h) {
+                    const int cq = lane + 32 * h;
+                    const int p = cq / CH, w = cq % CH;
+                    const int pl = min(4 * p, 31);
+                    const int jp = __shfl_sync(FULL, j, pl);
+                    const bool vp = __shfl_sync(FULL, (int)valid, pl) && cq < 8 * CH;
+                    if (vp) {
+                        const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(bval + 16LL * jp) + w);
+                        stage_chunk<PREC>(raw, sb + p * SS + w * VPC);
                     }
                 }
+                // C slot of the product
+                int t;
+                bool found;
+                if (small) {
+                    t = 0;
+#pragma unroll
+                    for (int step = 16; step > 0; step >>= 1)
+                        if (__shfl_sync(FULL, mykey, t + step - 1) < key) t += step;
+                    const int kt = __shfl_sync(FULL, mykey, t);  // every lane takes part
+                    found = valid && kt == key;
+                } else {
+                    t = valid ? search_sorted(skey + sbase, cn, key) : 0;
+                    found = valid && skey[sbase + t] == key;
+                }
+                __syncwarp();
+                acc_t s[4];
+                if (valid) {
+                    const acc_t *bp = sb + ps * SS;
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk) {
+                        acc_t bk[4];
+                        if constexpr (sizeof(acc_t) == 8) {
+                            const double2 u = reinterpret_cast<const double2 *>(bp + 4 * kk)[0];
+                            const double2 w2 = reinterpret_cast<const double2 *>(bp + 4 * kk)[1];
+                            bk[0] = u.x; bk[1] = u.y; bk[2] = w2.x; bk[3] = w2.y;
+                        } else {
+                            const float4 u = *reinterpret_cast<const float4 *>(bp + 4 * kk);
+                            bk[0] = u.x; bk[1] = u.y; bk[2] = u.z; bk[3] = u.w;
+                        }
+#pragma unroll
+                        for (int c = 0; c < 4; ++c)
+                            s[c] = kk == 0 ? T::mul(ar[0], bk[c]) : T::add(s[c], T::mul(ar[kk], bk[c]));
+                    }
+                }
+                // ordered accumulation: same C block row -> rounds in lane order
+                const int tag = found ? 4 * t + r : -1 - lane;
+                const unsigned peers = __match_any_sync(FULL, tag);
+                const int rank = __popc(peers & lanemask_lt(lane));
+                const int rounds = __reduce_max_sync(FULL, found ? rank : 0);
+                for (int rd = 0; rd <= rounds; ++rd) {
+                    if (found && rank == rd) {
+                        if (small) {
+                            acc_t *d = sa + t * SS + 4 * r;
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) d[c] = T::add(d[c], s[c]);
+                        } else {
+                            double *d = ga + 16LL * t + 4 * r;
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) d[c] = (double)T::add((acc_t)d[c], s[c]);
+                        }
+                    }
+                    __syncwarp();
+                }
             }
-            __syncwarp();
-          }
         }
         // C values (+ shadow)
         for (int t = lane; t < 16 * cn; t += 32) {
-            const acc_t v = small ? sa[t] : (acc_t)ga[t];
+            const acc_t v = small ? sa[(t >> 4) * SS + (t & 15)] : (acc_t)ga[t];
             ga[t] = (double)v;
             if (PREC != AMGT_DOUBLE && cshadow) store_shadow<PREC>(cshadow, 16LL * c0 + t, v);
         }
         __syncwarp();
         // CSR rows 4b..4b+3 (BSR2CSR fused)
         if (csr_i) {
-            for (int q = 0; q < 4 && 4 * b + q < m; ++q) {
-                int out = csr_i[4 * b + q];
+            for (int qr = 0; qr < 4 && 4 * b + qr < m; ++qr) {
+                int out = csr_i[4 * b + qr];
                 for (int tt = 0; tt < cn; tt += 32) {
                     const int t = tt + lane;
                     uint32_t nib = 0;
                     int col0 = 0;
                     if (t < cn) {
-                        nib = (cmap[c0 + t] >> (4 * q)) & 0xFu;
+                        nib = (cmap[c0 + t] >> (4 * qr)) & 0xFu;
                         col0 = 4 * cidx[c0 + t];
                     }
                     int tot;
@@ -522,7 +624,7 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                         for (int cc = 0; cc < 4; ++cc)
                             if (nib & (1u << cc)) {
                                 csr_j[o] = col0 + cc;
-                                csr_a[o] = ga[16 * t + 4 * q + cc];
+                                csr_a[o] = ga[16 * t + 4 * qr + cc];
                                 ++o;
                             }
                     }
@@ -530,6 +632,7 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                 }
             }
         }
+        __syncwarp();
     }
 }
 
@@ -540,11 +643,10 @@ static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B
 {
     using V = typename NumT<PREC>::val_t;
     if (A->blc_row == 0) return AMGT_OK;
-    AMGT_LAUNCH(spgemm_numeric_kernel<PREC>, grid_for(kNumWarps, A->blc_row, sm_count, 12), 32 * kNumWarps, 0, s,
-                A->row, A->blc_row, A->blcPtr, A->blcIdx, A->blcMap, (const V *)aval, B->blcPtr, B->blcIdx,
-                B->blcMap, (const V *)bval, C->blcPtr, C->blcIdx, C->blcMap, C->blcVal, cshadow,
-                Ccsr ? Ccsr->i : nullptr, Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr, ub_off, skey,
-                smap);
+    AMGT_LAUNCH(spgemm_numeric_kernel<PREC>, grid_for(kNumWarps, A->blc_row, sm_count, 8), 32 * kNumWarps, 0, s,
+                A->row, A->blc_row, A->blcPtr, A->blcIdx, (const V *)aval, B->blcPtr, B->blcIdx, (const V *)bval,
+                C->blcPtr, C->blcIdx, C->blcMap, C->blcVal, cshadow, Ccsr ? Ccsr->i : nullptr,
+                Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr, ub_off, skey, smap);
     return AMGT_OK;
 }
 
