@@ -40,7 +40,8 @@ constexpr int kSymCap = 1024;     // pairs a warp sorts in shared memory
 constexpr int kSymWin = 8192;     // key window of the large-row path
 constexpr int kSymLargeThreads = 256;
 constexpr int kNumWarps = 4;
-constexpr int kNumCap = 32;       // C blocks a warp accumulates in shared memory (one per lane)
+constexpr int kNumCap = 32;       // C blocks a warp accumulates in shared memory
+constexpr int kNumWin = 256;      // pairs per window of the numeric pair -> A block table
 
 __device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
 
@@ -50,13 +51,15 @@ __device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) 
 // range lengths flattens the (A block, B block) pairs, and lane t takes
 // pair t, finding its A block by a five-step shuffle search; so every load
 // of a chunk is in flight at once.  Pairs come out in (A block, B block)
-// order.
+// order, tagged with their ordinal in the row (< 65536: rows here have at
+// most kSymCap pairs); pslot[ordinal] = 0xFFFF marks the pairs whose
+// bitmap product is zero (they add nothing to C).
 __device__ __forceinline__ int sym_collect(int lane, int a0, int a1, const int *__restrict__ aidx,
                                            const uint16_t *__restrict__ amap, const int *__restrict__ bptr,
                                            const int *__restrict__ bidx, const uint16_t *__restrict__ bmap,
-                                           unsigned long long *s)
+                                           unsigned long long *s, uint16_t *__restrict__ pslot)
 {
-    int cnt = 0;
+    int cnt = 0, qbase = 0;
     for (int ib = a0; ib < a1; ib += 32) {
         const int i = ib + lane;
         int j0 = 0, len = 0;
@@ -92,11 +95,13 @@ __device__ __forceinline__ int sym_collect(int lane, int a0, int a1, const int *
                 const int j = sj0 + (t - sex);
                 mc = bitmap_mul(sma, bmap[j]);
                 key = bidx[j];
+                if (!mc) pslot[qbase + t] = 0xFFFF;
             }
             const unsigned bal = __ballot_sync(FULL, mc != 0);
-            if (mc) s[cnt + __popc(bal & lanemask_lt(lane))] = pack_pair(key, 0, mc);
+            if (mc) s[cnt + __popc(bal & lanemask_lt(lane))] = pack_pair(key, qbase + t, mc);
             cnt += __popc(bal);
         }
+        qbase += total;
     }
     __syncwarp();
     return cnt;
@@ -118,10 +123,11 @@ __device__ __forceinline__ long long sym_upper_bound(int lane, int a0, int a1, c
 
 // Sorted distinct keys with OR-ed bitmaps of the warp's list s[0..cnt).
 // FILL writes them to cidx/cmap; always returns the distinct count and the
-// per-scalar-row CSR counts (popcount of each bitmap nibble).
+// per-scalar-row CSR counts (popcount of each bitmap nibble).  pslot (may
+// be null) receives, per pair ordinal (the tag), the index of its C block.
 template <bool FILL>
 __device__ __forceinline__ int sym_reduce(int lane, int cnt, unsigned long long *s, int *__restrict__ cidx,
-                                          uint16_t *__restrict__ cmap, int csr[4])
+                                          uint16_t *__restrict__ cmap, int csr[4], uint16_t *__restrict__ pslot)
 {
     csr[0] = csr[1] = csr[2] = csr[3] = 0;
     int u = 0;
@@ -133,6 +139,7 @@ __device__ __forceinline__ int sym_reduce(int lane, int cnt, unsigned long long 
         const bool head = warp_runs32(v, lane, &orv);
         const unsigned hb = __ballot_sync(FULL, head);
         u = __popc(hb);
+        if (pslot && v != kSentinel) pslot[pair_tag(v)] = (uint16_t)(__popc(hb & ((2u << lane) - 1u)) - 1);
         if (head) {
             const int slot = __popc(hb & lanemask_lt(lane));
             if (FILL) {
@@ -153,6 +160,7 @@ __device__ __forceinline__ int sym_reduce(int lane, int cnt, unsigned long long 
             bool head = false;
             if (v != kSentinel) head = (i == 0) || pair_key(v) != pair_key(s[i - 1]);
             const unsigned hb = __ballot_sync(FULL, head);
+            if (pslot && v != kSentinel) pslot[pair_tag(v)] = (uint16_t)(u + __popc(hb & ((2u << lane) - 1u)) - 1);
             if (head) {
                 uint32_t orv = 0;
                 const int key = pair_key(v);
@@ -205,7 +213,7 @@ spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *
                        int *__restrict__ csrcnt, int *__restrict__ large, int64_t *__restrict__ stats,
                        const int64_t *__restrict__ ub_off, int *__restrict__ skey, uint16_t *__restrict__ smap,
                        const int *__restrict__ rows, const int *__restrict__ nrows, int *__restrict__ over,
-                       int *__restrict__ nover)
+                       int *__restrict__ nover, uint16_t *__restrict__ pslot)
 {
     __shared__ unsigned long long sbuf[kSymWarps][CAP];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -220,10 +228,10 @@ spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *
             if (lane == 0) over[atomicAdd(nover, 1)] = b;
             continue;
         }
-        const int cnt = sym_collect(lane, a0, a1, aidx, amap, bptr, bidx, bmap, s);
-        int csr[4];
         const long long base = ub_off[b];
-        const int u = sym_reduce<true>(lane, cnt, s, skey + base, smap + base, csr);
+        const int cnt = sym_collect(lane, a0, a1, aidx, amap, bptr, bidx, bmap, s, pslot + base);
+        int csr[4];
+        const int u = sym_reduce<true>(lane, cnt, s, skey + base, smap + base, csr, pslot + base);
         if (lane == 0) {
             ccnt[b] = u;
 #pragma unroll
@@ -446,20 +454,23 @@ __device__ __forceinline__ void stage_chunk(const uint4 raw, typename NumT<PREC>
 
 // Numeric phase.  One warp per A block row; the row's (A block, B block)
 // pairs are flattened (up to 32 A blocks at a time: lane i holds A block
-// i's B row range, a warp scan of the lengths numbers the pairs) and taken
-// 8 at a time, 4 lanes per pair, lane r computing row r of the 4x4 product.
-// The 8 B blocks are staged through shared memory with 16-byte loads; all
-// loads of a step are independent, so each step costs one memory round
-// trip.  Every term of the product is computed (unstored entries are zero):
-// for finite values this gives the stored-term sums of the reference's
-// scalar branch bit for bit, because adding a zero product leaves a
-// non-zero partial sum unchanged and a partial sum started from +0 never
-// becomes -0.  Products are added to their C block in pair order (= A block
-// order): pairs of one step that hit the same C block row are applied in
-// rounds, lowest lane first (match_any), so the accumulation order is the
-// sequential one.  Rows of up to 32 C blocks accumulate in shared memory
-// (lane t holds C column t; a product finds its slot by a five-step shuffle
-// search), longer rows in place in C (binary search in the sorted pattern).
+// i's B row range, a warp scan of the lengths numbers the pairs, and a
+// shared table maps each pair of a 256-pair window to its A block) and
+// taken 8 at a time, 4 lanes per pair, lane r computing row r of the 4x4
+// product.  Lane r stages rows of its own pair's B block through shared
+// memory with 16-byte loads; all loads of a step are independent, so each
+// step costs one memory round trip.  A pair's C block comes from the
+// symbolic pass (pslot, by pair ordinal; 0xFFFF = zero bitmap product) on
+// rows of at most kSymCap pairs, else from a binary search of the row's
+// sorted pattern.  Every term of the product is computed (unstored entries
+// are zero): for finite values this gives the stored-term sums of the
+// reference's scalar branch bit for bit, because adding a zero product
+// leaves a non-zero partial sum unchanged and a partial sum started from +0
+// never becomes -0.  Products are added to their C block in pair order
+// (= A block order): pairs of one step that hit the same C block row are
+// applied in rounds, lowest lane first (match_any), so the accumulation
+// order is the sequential one.  Rows of up to 32 C blocks accumulate in
+// shared memory, longer rows in place in C.
 template <int PREC>
 __global__ void __launch_bounds__(32 * kNumWarps, 8)
 spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
@@ -468,7 +479,8 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                       const int *__restrict__ cptr, int *__restrict__ cidx, uint16_t *__restrict__ cmap,
                       double *__restrict__ cval, void *__restrict__ cshadow, const int *__restrict__ csr_i,
                       int *__restrict__ csr_j, double *__restrict__ csr_a, const int64_t *__restrict__ ub_off,
-                      const int *__restrict__ skey, const uint16_t *__restrict__ smap)
+                      const int *__restrict__ skey, const uint16_t *__restrict__ smap,
+                      const uint16_t *__restrict__ pslot)
 {
     using T = NumT<PREC>;
     using V = typename T::val_t;
@@ -476,22 +488,25 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
     constexpr int SS = NumStride<acc_t>::v;
     constexpr int CH = (int)sizeof(V);  // 16-byte chunks per block (16 values)
     constexpr int VPC = 16 / CH;        // values per chunk
+    constexpr int CPL = (CH + 3) / 4;   // chunks staged per lane
     __shared__ __align__(16) acc_t sacc[kNumWarps][kNumCap * SS];
     __shared__ __align__(16) acc_t sstage[kNumWarps][8 * SS];
+    __shared__ unsigned char spair[kNumWarps][kNumWin];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ps = lane >> 2, r = lane & 3;
     acc_t *sa = sacc[warp];
     acc_t *sb = sstage[warp];
+    unsigned char *sp = spair[warp];
     for (int b = blockIdx.x * kNumWarps + warp; b < brA; b += gridDim.x * kNumWarps) {
         const int c0 = cptr[b], cn = cptr[b + 1] - c0;
         // the row's pattern, sorted by the symbolic pass, moves from scratch to C
         const long long sbase = ub_off[b];
+        const bool direct = ub_off[b + 1] - sbase <= kSymCap;
         for (int t = lane; t < cn; t += 32) {
             cidx[c0 + t] = skey[sbase + t];
             cmap[c0 + t] = smap[sbase + t];
         }
         const bool small = cn <= kNumCap;
-        const int mykey = (small && lane < cn) ? skey[sbase + lane] : 0x7FFFFFFF;
         double *ga = cval + 16LL * c0;
         if (small) {
             for (int t = lane; t < 16 * cn; t += 32) sa[(t >> 4) * SS + (t & 15)] = (acc_t)0;
@@ -500,6 +515,7 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
         }
         __syncwarp();
         const int a0 = aptr[b], a1 = aptr[b + 1];
+        long long qbase = sbase;  // scratch index of the chunk's first pair
         for (int ib = a0; ib < a1; ib += 32) {
             int j0 = 0, len = 0;
             if (ib + lane < a1) {
@@ -514,88 +530,81 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                 if (lane >= o) incl += y;
             }
             const int total = __shfl_sync(FULL, incl, 31);
-            const int jd = j0 - (incl - len);  // B block of pair q of A block i: q + jd[i]
-            for (int q0 = 0; q0 < total; q0 += 8) {
-                const int q = q0 + ps;
-                const bool valid = q < total;
-                int src = 0;
-#pragma unroll
-                for (int step = 16; step > 0; step >>= 1) {
-                    const int v = __shfl_sync(FULL, incl, min(src + step - 1, 31));
-                    if (v <= q) src += step;
-                }
-                src = min(src, 31);
-                const int j = q + __shfl_sync(FULL, jd, src);
-                const int key = valid ? bidx[j] : -1;
-                acc_t ar[4];
-                if (valid) load_row4<PREC>(aval + 16LL * (ib + src) + 4 * r, ar);
-                // stage the step's B blocks: chunk w of pair p to p * SS + w * VPC
-#pragma unroll
-                for (int h = 0; h < (8 * CH + 31) / 32; ++h) {
-                    const int cq = lane + 32 * h;
-                    const int p = cq / CH, w = cq % CH;
-                    const int pl = min(4 * p, 31);
-                    const int jp = __shfl_sync(FULL, j, pl);
-                    const bool vp = __shfl_sync(FULL, (int)valid, pl) && cq < 8 * CH;
-                    if (vp) {
-                        const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(bval + 16LL * jp) + w);
-                        stage_chunk<PREC>(raw, sb + p * SS + w * VPC);
-                    }
-                }
-                // C slot of the product
-                int t;
-                bool found;
-                if (small) {
-                    t = 0;
-#pragma unroll
-                    for (int step = 16; step > 0; step >>= 1)
-                        if (__shfl_sync(FULL, mykey, t + step - 1) < key) t += step;
-                    const int kt = __shfl_sync(FULL, mykey, t);  // every lane takes part
-                    found = valid && kt == key;
-                } else {
-                    t = valid ? search_sorted(skey + sbase, cn, key) : 0;
-                    found = valid && skey[sbase + t] == key;
-                }
+            const int excl = incl - len;
+            const int jd = j0 - excl;  // B block of pair q of A block i: q + jd[i]
+            for (int w0 = 0; w0 < total; w0 += kNumWin) {
+                const int wend = min(total, w0 + kNumWin);
+                for (int q = max(excl, w0); q < min(incl, wend); ++q) sp[q - w0] = (unsigned char)lane;
                 __syncwarp();
-                acc_t s[4];
-                if (valid) {
-                    const acc_t *bp = sb + ps * SS;
-#pragma unroll
-                    for (int kk = 0; kk < 4; ++kk) {
-                        acc_t bk[4];
-                        if constexpr (sizeof(acc_t) == 8) {
-                            const double2 u = reinterpret_cast<const double2 *>(bp + 4 * kk)[0];
-                            const double2 w2 = reinterpret_cast<const double2 *>(bp + 4 * kk)[1];
-                            bk[0] = u.x; bk[1] = u.y; bk[2] = w2.x; bk[3] = w2.y;
+                for (int q0 = w0; q0 < wend; q0 += 8) {
+                    const int q = q0 + ps;
+                    const bool valid = q < wend;
+                    const int src = valid ? sp[q - w0] : 0;
+                    const int j = q + __shfl_sync(FULL, jd, src);
+                    int t = -1;
+                    if (valid) {
+                        if (direct) {
+                            t = pslot[qbase + q];
                         } else {
-                            const float4 u = *reinterpret_cast<const float4 *>(bp + 4 * kk);
-                            bk[0] = u.x; bk[1] = u.y; bk[2] = u.z; bk[3] = u.w;
+                            const int key = bidx[j];
+                            const int tt = cn > 0 ? search_sorted(skey + sbase, cn, key) : 0;
+                            t = (tt < cn && skey[sbase + tt] == key) ? tt : -1;
                         }
-#pragma unroll
-                        for (int c = 0; c < 4; ++c)
-                            s[c] = kk == 0 ? T::mul(ar[0], bk[c]) : T::add(s[c], T::mul(ar[kk], bk[c]));
                     }
-                }
-                // ordered accumulation: same C block row -> rounds in lane order
-                const int tag = found ? 4 * t + r : -1 - lane;
-                const unsigned peers = __match_any_sync(FULL, tag);
-                const int rank = __popc(peers & lanemask_lt(lane));
-                const int rounds = __reduce_max_sync(FULL, found ? rank : 0);
-                for (int rd = 0; rd <= rounds; ++rd) {
-                    if (found && rank == rd) {
-                        if (small) {
-                            acc_t *d = sa + t * SS + 4 * r;
+                    const bool found = (unsigned)t < (unsigned)cn;  // pslot 0xFFFF: no product
+                    acc_t ar[4];
+                    if (valid) load_row4<PREC>(aval + 16LL * (ib + src) + 4 * r, ar);
+                    // lane r stages chunks r * CPL .. of its own pair's B block
 #pragma unroll
-                            for (int c = 0; c < 4; ++c) d[c] = T::add(d[c], s[c]);
-                        } else {
-                            double *d = ga + 16LL * t + 4 * r;
-#pragma unroll
-                            for (int c = 0; c < 4; ++c) d[c] = (double)T::add((acc_t)d[c], s[c]);
+                    for (int h = 0; h < CPL; ++h) {
+                        const int w = r * CPL + h;
+                        if (valid && w < CH) {
+                            const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(bval + 16LL * j) + w);
+                            stage_chunk<PREC>(raw, sb + ps * SS + w * VPC);
                         }
                     }
                     __syncwarp();
+                    acc_t s[4];
+                    if (found) {
+                        const acc_t *bp = sb + ps * SS;
+#pragma unroll
+                        for (int kk = 0; kk < 4; ++kk) {
+                            acc_t bk[4];
+                            if constexpr (sizeof(acc_t) == 8) {
+                                const double2 u = reinterpret_cast<const double2 *>(bp + 4 * kk)[0];
+                                const double2 w2 = reinterpret_cast<const double2 *>(bp + 4 * kk)[1];
+                                bk[0] = u.x; bk[1] = u.y; bk[2] = w2.x; bk[3] = w2.y;
+                            } else {
+                                const float4 u = *reinterpret_cast<const float4 *>(bp + 4 * kk);
+                                bk[0] = u.x; bk[1] = u.y; bk[2] = u.z; bk[3] = u.w;
+                            }
+#pragma unroll
+                            for (int c = 0; c < 4; ++c)
+                                s[c] = kk == 0 ? T::mul(ar[0], bk[c]) : T::add(s[c], T::mul(ar[kk], bk[c]));
+                        }
+                    }
+                    // ordered accumulation: same C block row -> rounds in lane order
+                    const int tag = found ? 4 * t + r : -1 - lane;
+                    const unsigned peers = __match_any_sync(FULL, tag);
+                    const int rank = __popc(peers & lanemask_lt(lane));
+                    const int rounds = __reduce_max_sync(FULL, found ? rank : 0);
+                    for (int rd = 0; rd <= rounds; ++rd) {
+                        if (found && rank == rd) {
+                            if (small) {
+                                acc_t *d = sa + t * SS + 4 * r;
+#pragma unroll
+                                for (int c = 0; c < 4; ++c) d[c] = T::add(d[c], s[c]);
+                            } else {
+                                double *d = ga + 16LL * t + 4 * r;
+#pragma unroll
+                                for (int c = 0; c < 4; ++c) d[c] = (double)T::add((acc_t)d[c], s[c]);
+                            }
+                        }
+                        __syncwarp();
+                    }
                 }
             }
+            qbase += total;
         }
         // C values (+ shadow)
         for (int t = lane; t < 16 * cn; t += 32) {
@@ -639,14 +648,14 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
 template <int PREC>
 static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B, const void *bval, amgt_bsr *C,
                           void *cshadow, amgt_csr *Ccsr, const int64_t *ub_off, const int *skey,
-                          const uint16_t *smap, cudaStream_t s, int sm_count)
+                          const uint16_t *smap, const uint16_t *pslot, cudaStream_t s, int sm_count)
 {
     using V = typename NumT<PREC>::val_t;
     if (A->blc_row == 0) return AMGT_OK;
     AMGT_LAUNCH(spgemm_numeric_kernel<PREC>, grid_for(kNumWarps, A->blc_row, sm_count, 8), 32 * kNumWarps, 0, s,
                 A->row, A->blc_row, A->blcPtr, A->blcIdx, (const V *)aval, B->blcPtr, B->blcIdx, (const V *)bval,
                 C->blcPtr, C->blcIdx, C->blcMap, C->blcVal, cshadow, Ccsr ? Ccsr->i : nullptr,
-                Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr, ub_off, skey, smap);
+                Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr, ub_off, skey, smap, pslot);
     return AMGT_OK;
 }
 
@@ -688,7 +697,7 @@ int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     int *ccnt = nullptr, *csrcnt = nullptr, *large = nullptr, *csr_i = nullptr, *csr_tmp = nullptr;
     int64_t *stats = nullptr, *ub = nullptr, *ub_off = nullptr;
     int *skey = nullptr;
-    uint16_t *smap = nullptr;
+    uint16_t *smap = nullptr, *pslot = nullptr;  // scratch: pattern, per-pair C block
     const int64_t *h = nullptr;
     int nbC = 0, nnzC = 0;
     void *cshadow = nullptr;
@@ -728,7 +737,9 @@ int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
             cap = h[2];
             AMGT_CUDA_TRY(cudaMemsetAsync(&stats[2], 0, sizeof(int64_t), s));
         }
-        if ((rc = alloc_n(&skey, (size_t)cap, s)) || (rc = alloc_n(&smap, (size_t)cap, s))) goto fail;
+        if ((rc = alloc_n(&skey, (size_t)cap, s)) || (rc = alloc_n(&smap, (size_t)cap, s)) ||
+            (rc = alloc_n(&pslot, (size_t)cap, s)))
+            goto fail;
     }
     if (brA > 0) {
         // medium-row list and count live behind the large list (2 * brA + 1 ints)
@@ -736,10 +747,10 @@ int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
         AMGT_CUDA_TRY(cudaMemsetAsync(nmedium, 0, sizeof(int), s));
         AMGT_LAUNCH(spgemm_symbolic_kernel<256>, grid_for(kSymWarps, brA, st->sm_count, 16), 32 * kSymWarps, 0, s, m,
                     brA, A->blcPtr, A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, ccnt, csrcnt, large,
-                    stats, ub_off, skey, smap, nullptr, nullptr, medium, nmedium);
+                    stats, ub_off, skey, smap, nullptr, nullptr, medium, nmedium, pslot);
         AMGT_LAUNCH(spgemm_symbolic_kernel<kSymCap>, 2 * st->sm_count, 32 * kSymWarps, 0, s, m, brA, A->blcPtr,
                     A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, ccnt, csrcnt, large, stats, ub_off, skey,
-                    smap, medium, nmedium, large, (int *)&stats[3]);
+                    smap, medium, nmedium, large, (int *)&stats[3], pslot);
         AMGT_LAUNCH(spgemm_symbolic_large_kernel, 2 * st->sm_count, kSymLargeThreads, 0, s, m, A->blcPtr, A->blcIdx,
                     A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, large, stats, ccnt, csrcnt, ub_off, skey, smap);
     }
@@ -790,33 +801,33 @@ int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     }
     switch (prec) {
     case AMGT_DOUBLE:
-        rc = launch_numeric<AMGT_DOUBLE>(A, A->blcVal, B, B->blcVal, C, nullptr, Ccsr, ub_off, skey, smap, s,
+        rc = launch_numeric<AMGT_DOUBLE>(A, A->blcVal, B, B->blcVal, C, nullptr, Ccsr, ub_off, skey, smap, pslot, s,
                                          st->sm_count);
         break;
     case AMGT_FLOAT:
         rc = launch_numeric<AMGT_FLOAT>(A, Atmp.blcVal_fp32, B, Btmp.blcVal_fp32, C, cshadow, Ccsr, ub_off, skey,
-                                        smap, s, st->sm_count);
+                                        smap, pslot, s, st->sm_count);
         break;
     case AMGT_HALF:
         rc = launch_numeric<AMGT_HALF>(A, Atmp.blcVal_fp16, B, Btmp.blcVal_fp16, C, cshadow, Ccsr, ub_off, skey,
-                                       smap, s, st->sm_count);
+                                       smap, pslot, s, st->sm_count);
         break;
     default:
         rc = launch_numeric<AMGT_BF16>(A, Atmp.blcVal_bf16, B, Btmp.blcVal_bf16, C, cshadow, Ccsr, ub_off, skey,
-                                       smap, s, st->sm_count);
+                                       smap, pslot, s, st->sm_count);
         break;
     }
     if (rc) goto fail;
     C->csr_nnz = nnzC;
     C->avg_nnz = nbC ? (double)nnzC / nbC : 0.0;
     free_ptr(ccnt, s); free_ptr(csrcnt, s); free_ptr(large, s); free_ptr(stats, s); free_ptr(csr_tmp, s);
-    free_ptr(ub, s); free_ptr(ub_off, s); free_ptr(skey, s); free_ptr(smap, s);
+    free_ptr(ub, s); free_ptr(ub_off, s); free_ptr(skey, s); free_ptr(smap, s); free_ptr(pslot, s);
     if (ownA) { free_ptr(Atmp.blcVal_fp32, s); free_ptr(Atmp.blcVal_fp16, s); free_ptr(Atmp.blcVal_bf16, s); }
     if (ownB) { free_ptr(Btmp.blcVal_fp32, s); free_ptr(Btmp.blcVal_fp16, s); free_ptr(Btmp.blcVal_bf16, s); }
     return AMGT_OK;
 fail:
     free_ptr(ccnt, s); free_ptr(csrcnt, s); free_ptr(large, s); free_ptr(stats, s); free_ptr(csr_tmp, s);
-    free_ptr(ub, s); free_ptr(ub_off, s); free_ptr(skey, s); free_ptr(smap, s);
+    free_ptr(ub, s); free_ptr(ub_off, s); free_ptr(skey, s); free_ptr(smap, s); free_ptr(pslot, s);
     if (ownA) { free_ptr(Atmp.blcVal_fp32, s); free_ptr(Atmp.blcVal_fp16, s); free_ptr(Atmp.blcVal_bf16, s); }
     if (ownB) { free_ptr(Btmp.blcVal_fp32, s); free_ptr(Btmp.blcVal_fp16, s); free_ptr(Btmp.blcVal_bf16, s); }
     amgt_bsr_free(C, stream);
