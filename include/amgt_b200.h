@@ -212,7 +212,7 @@ AMGT_API int amgt_bsr_jacobi(int prec, const amgt_bsr *A, const double *inv_l1,
 
 /* ------------------------------------------------- bitmap-packed values */
 /* mBSR with only the values of set bitmap bits stored, block after block in
- * bitmap (row-major) order, plus each block's offset into them.  The block
+ * bitmap (row-major) order.  The block
  * structure (blcPtr, blcIdx, blcMap) is borrowed from the amgt_bsr it was
  * packed from, which must outlive it.  At the fill of AMG operators (about
  * 4 of 16) an SpMV reads ~3x fewer bytes than on the 16-value blocks.  No
