@@ -411,17 +411,34 @@ __device__ __forceinline__ int search_sorted(const int *keys, int n, int key)
     return lo;
 }
 
-// Accumulator and B-stage strides (elements) per C block: 16 values plus a
-// 16-byte pad, so that the 16-byte row accesses of the 8 pairs of one step
-// fall in distinct banks.
+// Accumulator stride (elements) per C block: 16 values plus a 16-byte pad,
+// so that the 16-byte row accesses of the 8 pairs of one step fall in
+// distinct banks.
 template <typename acc_t>
 struct NumStride {
     static constexpr int v = 16 + 16 / (int)sizeof(acc_t);
 };
 
-// Four consecutive values of a block row, widened to the accumulator type.
+// Asynchronous global -> shared copies of 16 bytes (8 for half-precision
+// A rows); completion is awaited per step with wait_group.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Four consecutive stored values (one block row) from shared memory,
+// widened to the accumulator type.
 template <int PREC>
-__device__ __forceinline__ void load_row4(const typename NumT<PREC>::val_t *p, typename NumT<PREC>::acc_t out[4])
+__device__ __forceinline__ void row4_smem(const unsigned char *p, typename NumT<PREC>::acc_t out[4])
 {
     if constexpr (PREC == AMGT_DOUBLE) {
         const double2 u = reinterpret_cast<const double2 *>(p)[0], w = reinterpret_cast<const double2 *>(p)[1];
@@ -430,49 +447,49 @@ __device__ __forceinline__ void load_row4(const typename NumT<PREC>::val_t *p, t
         const float4 u = *reinterpret_cast<const float4 *>(p);
         out[0] = u.x; out[1] = u.y; out[2] = u.z; out[3] = u.w;
     } else {
+        const typename NumT<PREC>::val_t *v = reinterpret_cast<const typename NumT<PREC>::val_t *>(p);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) out[q] = NumT<PREC>::ld(p, q);
+        for (int q = 0; q < 4; ++q) out[q] = NumT<PREC>::ld(v, q);
     }
 }
 
-// Widens one 16-byte chunk of stored values and writes it to shared memory.
+// Shared memory of the numeric kernel per warp: C accumulators, two stages
+// of 8 staged B blocks (16 values + 16-byte pad) and 8 x 4 A rows, and the
+// pair -> A block table.
 template <int PREC>
-__device__ __forceinline__ void stage_chunk(const uint4 raw, typename NumT<PREC>::acc_t *dst)
-{
+struct NumSmem {
     using V = typename NumT<PREC>::val_t;
-    constexpr int VPC = 16 / (int)sizeof(V);
-    const V *v = reinterpret_cast<const V *>(&raw);
-    if constexpr (PREC == AMGT_DOUBLE) {
-        *reinterpret_cast<double2 *>(dst) = make_double2(v[0], v[1]);
-    } else if constexpr (PREC == AMGT_FLOAT) {
-        *reinterpret_cast<float4 *>(dst) = make_float4(v[0], v[1], v[2], v[3]);
-    } else {
-#pragma unroll
-        for (int q = 0; q < VPC; ++q) dst[q] = NumT<PREC>::ld(v, q);
-    }
-}
+    using acc_t = typename NumT<PREC>::acc_t;
+    static constexpr int BB = 16 * (int)sizeof(V) + 16;  // staged B block bytes
+    static constexpr int AR = 4 * (int)sizeof(V);        // staged A row bytes
+    static constexpr int b_off = kNumCap * NumStride<acc_t>::v * (int)sizeof(acc_t);
+    static constexpr int a_off = b_off + 2 * 8 * BB;
+    static constexpr int p_off = a_off + 2 * 32 * AR;
+    static constexpr int per_warp = (p_off + kNumWin + 15) / 16 * 16;
+};
 
 // Numeric phase.  One warp per A block row; the row's (A block, B block)
 // pairs are flattened (up to 32 A blocks at a time: lane i holds A block
 // i's B row range, a warp scan of the lengths numbers the pairs, and a
 // shared table maps each pair of a 256-pair window to its A block) and
 // taken 8 at a time, 4 lanes per pair, lane r computing row r of the 4x4
-// product.  Lane r stages rows of its own pair's B block through shared
-// memory with 16-byte loads; all loads of a step are independent, so each
-// step costs one memory round trip.  A pair's C block comes from the
-// symbolic pass (pslot, by pair ordinal; 0xFFFF = zero bitmap product) on
-// rows of at most kSymCap pairs, else from a binary search of the row's
-// sorted pattern.  Every term of the product is computed (unstored entries
-// are zero): for finite values this gives the stored-term sums of the
-// reference's scalar branch bit for bit, because adding a zero product
-// leaves a non-zero partial sum unchanged and a partial sum started from +0
-// never becomes -0.  Products are added to their C block in pair order
-// (= A block order): pairs of one step that hit the same C block row are
-// applied in rounds, lowest lane first (match_any), so the accumulation
-// order is the sequential one.  Rows of up to 32 C blocks accumulate in
-// shared memory, longer rows in place in C.
+// product.  Steps are double-buffered: while step k is computed from
+// shared memory, the asynchronous copies of step k+1's B blocks and A rows
+// (each lane copies its own rows of its own pair) and its pairs' C slots
+// are in flight.  A pair's C block comes from the symbolic pass (pslot, by
+// pair ordinal; 0xFFFF = zero bitmap product) on rows of at most kSymCap
+// pairs, else from a binary search of the row's sorted pattern.  Every term
+// of the product is computed (unstored entries are zero): for finite values
+// this gives the stored-term sums of the reference's scalar branch bit for
+// bit, because adding a zero product leaves a non-zero partial sum
+// unchanged and a partial sum started from +0 never becomes -0.  Products
+// are added to their C block in pair order (= A block order): pairs of one
+// step that hit the same C block row are applied in rounds, lowest lane
+// first (match_any), so the accumulation order is the sequential one.  Rows
+// of up to 32 C blocks accumulate in shared memory, longer rows in place in
+// C.
 template <int PREC>
-__global__ void __launch_bounds__(32 * kNumWarps, 8)
+__global__ void __launch_bounds__(32 * kNumWarps, 6)
 spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
                       const typename NumT<PREC>::val_t *__restrict__ aval, const int *__restrict__ bptr,
                       const int *__restrict__ bidx, const typename NumT<PREC>::val_t *__restrict__ bval,
@@ -485,18 +502,17 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
     using T = NumT<PREC>;
     using V = typename T::val_t;
     using acc_t = typename T::acc_t;
+    using SM = NumSmem<PREC>;
     constexpr int SS = NumStride<acc_t>::v;
     constexpr int CH = (int)sizeof(V);  // 16-byte chunks per block (16 values)
-    constexpr int VPC = 16 / CH;        // values per chunk
-    constexpr int CPL = (CH + 3) / 4;   // chunks staged per lane
-    __shared__ __align__(16) acc_t sacc[kNumWarps][kNumCap * SS];
-    __shared__ __align__(16) acc_t sstage[kNumWarps][8 * SS];
-    __shared__ unsigned char spair[kNumWarps][kNumWin];
+    constexpr int CPL = (CH + 3) / 4;   // B chunks copied per lane
+    constexpr int BB = SM::BB, AR = SM::AR;
+    extern __shared__ __align__(16) unsigned char num_smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int ps = lane >> 2, r = lane & 3;
-    acc_t *sa = sacc[warp];
-    acc_t *sb = sstage[warp];
-    unsigned char *sp = spair[warp];
+    unsigned char *wbase = num_smem + warp * SM::per_warp;
+    acc_t *sa = reinterpret_cast<acc_t *>(wbase);
+    unsigned char *sB = wbase + SM::b_off, *sA = wbase + SM::a_off, *sp = wbase + SM::p_off;
     for (int b = blockIdx.x * kNumWarps + warp; b < brA; b += gridDim.x * kNumWarps) {
         const int c0 = cptr[b], cn = cptr[b + 1] - c0;
         // the row's pattern, sorted by the symbolic pass, moves from scratch to C
@@ -536,13 +552,33 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                 const int wend = min(total, w0 + kNumWin);
                 for (int q = max(excl, w0); q < min(incl, wend); ++q) sp[q - w0] = (unsigned char)lane;
                 __syncwarp();
-                for (int q0 = w0; q0 < wend; q0 += 8) {
+                // issue of one step into stage `st`: copies of the lane's B
+                // rows and A row, and the pair's C slot (-1: no product)
+                auto issue = [&](int q0, int st) -> int {
                     const int q = q0 + ps;
                     const bool valid = q < wend;
                     const int src = valid ? sp[q - w0] : 0;
                     const int j = q + __shfl_sync(FULL, jd, src);
                     int t = -1;
                     if (valid) {
+                        const unsigned char *bsrc = reinterpret_cast<const unsigned char *>(bval + 16LL * j);
+                        unsigned char *bdst = sB + (st * 8 + ps) * BB;
+#pragma unroll
+                        for (int h = 0; h < CPL; ++h) {
+                            const int w = r * CPL + h;
+                            if (w < CH) cp_async16(bdst + 16 * w, bsrc + 16 * w);
+                        }
+                        const unsigned char *asrc =
+                            reinterpret_cast<const unsigned char *>(aval + 16LL * (ib + src) + 4 * r);
+                        unsigned char *adst = sA + (st * 32 + lane) * AR;
+                        if constexpr (AR == 32) {
+                            cp_async16(adst, asrc);
+                            cp_async16(adst + 16, asrc + 16);
+                        } else if constexpr (AR == 16) {
+                            cp_async16(adst, asrc);
+                        } else {
+                            cp_async8(adst, asrc);
+                        }
                         if (direct) {
                             t = pslot[qbase + q];
                         } else {
@@ -551,33 +587,31 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                             t = (tt < cn && skey[sbase + tt] == key) ? tt : -1;
                         }
                     }
-                    const bool found = (unsigned)t < (unsigned)cn;  // pslot 0xFFFF: no product
-                    acc_t ar[4];
-                    if (valid) load_row4<PREC>(aval + 16LL * (ib + src) + 4 * r, ar);
-                    // lane r stages chunks r * CPL .. of its own pair's B block
-#pragma unroll
-                    for (int h = 0; h < CPL; ++h) {
-                        const int w = r * CPL + h;
-                        if (valid && w < CH) {
-                            const uint4 raw = __ldg(reinterpret_cast<const uint4 *>(bval + 16LL * j) + w);
-                            stage_chunk<PREC>(raw, sb + ps * SS + w * VPC);
-                        }
+                    cp_async_commit();
+                    return t;
+                };
+                int tcur = issue(w0, 0);
+                int st = 0;
+                for (int q0 = w0; q0 < wend; q0 += 8, st ^= 1) {
+                    int tnext = -1;
+                    if (q0 + 8 < wend) {
+                        tnext = issue(q0 + 8, st ^ 1);
+                        cp_async_wait<1>();
+                    } else {
+                        cp_async_wait<0>();
                     }
                     __syncwarp();
+                    const int t = tcur;
+                    const bool found = (unsigned)t < (unsigned)cn;  // pslot 0xFFFF: no product
                     acc_t s[4];
                     if (found) {
-                        const acc_t *bp = sb + ps * SS;
+                        acc_t ar[4];
+                        row4_smem<PREC>(sA + (st * 32 + lane) * AR, ar);
+                        const unsigned char *bp = sB + (st * 8 + ps) * BB;
 #pragma unroll
                         for (int kk = 0; kk < 4; ++kk) {
                             acc_t bk[4];
-                            if constexpr (sizeof(acc_t) == 8) {
-                                const double2 u = reinterpret_cast<const double2 *>(bp + 4 * kk)[0];
-                                const double2 w2 = reinterpret_cast<const double2 *>(bp + 4 * kk)[1];
-                                bk[0] = u.x; bk[1] = u.y; bk[2] = w2.x; bk[3] = w2.y;
-                            } else {
-                                const float4 u = *reinterpret_cast<const float4 *>(bp + 4 * kk);
-                                bk[0] = u.x; bk[1] = u.y; bk[2] = u.z; bk[3] = u.w;
-                            }
+                            row4_smem<PREC>(bp + kk * AR, bk);
 #pragma unroll
                             for (int c = 0; c < 4; ++c)
                                 s[c] = kk == 0 ? T::mul(ar[0], bk[c]) : T::add(s[c], T::mul(ar[kk], bk[c]));
@@ -602,6 +636,7 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                         }
                         __syncwarp();
                     }
+                    tcur = tnext;
                 }
             }
             qbase += total;
@@ -652,7 +687,9 @@ static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B
 {
     using V = typename NumT<PREC>::val_t;
     if (A->blc_row == 0) return AMGT_OK;
-    AMGT_LAUNCH(spgemm_numeric_kernel<PREC>, grid_for(kNumWarps, A->blc_row, sm_count, 8), 32 * kNumWarps, 0, s,
+    constexpr int smem = kNumWarps * NumSmem<PREC>::per_warp;
+    AMGT_CUDA_TRY(cudaFuncSetAttribute(spgemm_numeric_kernel<PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    AMGT_LAUNCH(spgemm_numeric_kernel<PREC>, grid_for(kNumWarps, A->blc_row, sm_count, 6), 32 * kNumWarps, smem, s,
                 A->row, A->blc_row, A->blcPtr, A->blcIdx, (const V *)aval, B->blcPtr, B->blcIdx, (const V *)bval,
                 C->blcPtr, C->blcIdx, C->blcMap, C->blcVal, cshadow, Ccsr ? Ccsr->i : nullptr,
                 Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr, ub_off, skey, smap, pslot);
