@@ -518,9 +518,13 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
         // the row's pattern, sorted by the symbolic pass, moves from scratch to C
         const long long sbase = ub_off[b];
         const bool direct = ub_off[b + 1] - sbase <= kSymCap;
-        for (int t = lane; t < cn; t += 32) {
-            cidx[c0 + t] = skey[sbase + t];
-            cmap[c0 + t] = smap[sbase + t];
+        // the first 32 pattern entries are read now and stored at the end,
+        // so that no store waits on its load
+        int pkey = 0;
+        uint32_t pmap = 0;
+        if (lane < cn) {
+            pkey = skey[sbase + lane];
+            pmap = smap[sbase + lane];
         }
         const bool small = cn <= kNumCap;
         double *ga = cval + 16LL * c0;
@@ -641,7 +645,15 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
             }
             qbase += total;
         }
-        // C values (+ shadow)
+        // pattern, C values (+ shadow)
+        if (lane < cn) {
+            cidx[c0 + lane] = pkey;
+            cmap[c0 + lane] = (uint16_t)pmap;
+        }
+        for (int t = 32 + lane; t < cn; t += 32) {
+            cidx[c0 + t] = skey[sbase + t];
+            cmap[c0 + t] = smap[sbase + t];
+        }
         for (int t = lane; t < 16 * cn; t += 32) {
             const acc_t v = small ? sa[(t >> 4) * SS + (t & 15)] : (acc_t)ga[t];
             ga[t] = (double)v;
