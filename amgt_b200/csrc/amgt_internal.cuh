@@ -68,7 +68,9 @@ struct DeviceState {
 };
 int device_state(DeviceState **st);
 
-// Reads the device error word (synchronising the stream) and clears it.
+// Reports the device error word as the last read_back on this device
+// copied it (no further synchronisation) and clears a raised word.  Call
+// right after a read_back.
 int check_device_error(cudaStream_t s);
 
 // Error codes a kernel may raise into DeviceState::err

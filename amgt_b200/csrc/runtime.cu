@@ -4,6 +4,8 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <unordered_map>
+#include <vector>
 
 #include <cub/device/device_scan.cuh>
 
@@ -53,8 +55,78 @@ static cudaMemPool_t library_pool()
     return g_pools[dev];
 }
 
+// Large blocks (>= 32 MiB) are kept when freed and handed to the next
+// request of 75-100 % of their size: the pool serves such a request from
+// freed memory only by re-mapping it into a new contiguous range, which
+// cost 0.3 ms for a 0.5 GB block inside each AMG setup.  A block carries
+// an event recorded on the freeing stream; reuse on another stream waits
+// for it, and eviction (beyond 8 GiB cached, or amgt_trim_pool) waits for
+// it on the host before returning the block to the pool.
+struct CachedBlock {
+    void *p;
+    size_t bytes;
+    int dev;
+    cudaStream_t stream;
+    cudaEvent_t done;
+};
+static constexpr size_t kCacheMin = 32ull << 20, kCacheCap = 8ull << 30;
+static std::mutex g_cache_mu;
+static std::vector<CachedBlock> g_cache;                 // freed, kept
+static std::unordered_map<void *, size_t> g_big_sizes;  // live large blocks
+static size_t g_cache_bytes = 0;
+
+static void release_block(CachedBlock &c)
+{
+    cudaEventSynchronize(c.done);
+    cudaEventDestroy(c.done);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != c.dev) cudaSetDevice(c.dev);
+    cudaFreeAsync(c.p, nullptr);  // no use is pending: the event completed
+    if (cur != c.dev) cudaSetDevice(cur);
+}
+
+// Returns every cached block of `dev` (all devices when dev < 0) to the pool.
+static void flush_cache(int dev)
+{
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (size_t i = 0; i < g_cache.size();) {
+        if (dev < 0 || g_cache[i].dev == dev) {
+            g_cache_bytes -= g_cache[i].bytes;
+            release_block(g_cache[i]);
+            g_cache.erase(g_cache.begin() + (long)i);
+        } else {
+            ++i;
+        }
+    }
+}
+
 static void *default_alloc(size_t bytes, amgt_stream_t s, void *)
 {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (bytes >= kCacheMin) {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        int best = -1;
+        for (int i = 0; i < (int)g_cache.size(); ++i) {
+            const CachedBlock &c = g_cache[i];
+            if (c.dev == dev && c.bytes >= bytes && bytes >= c.bytes - c.bytes / 4 &&
+                (best < 0 || c.bytes < g_cache[best].bytes))
+                best = i;
+        }
+        if (best >= 0) {
+            CachedBlock c = g_cache[best];
+            g_cache.erase(g_cache.begin() + best);
+            g_cache_bytes -= c.bytes;
+            if (c.stream != (cudaStream_t)s) cudaStreamWaitEvent((cudaStream_t)s, c.done, 0);
+            cudaEventDestroy(c.done);
+            g_big_sizes[c.p] = c.bytes;
+            return c.p;
+        }
+    }
     void *p = nullptr;
     cudaMemPool_t pool = library_pool();
     cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, (cudaStream_t)s)
@@ -63,11 +135,38 @@ static void *default_alloc(size_t bytes, amgt_stream_t s, void *)
         cudaGetLastError();
         return nullptr;
     }
+    if (bytes >= kCacheMin) {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        g_big_sizes[p] = bytes;
+    }
     return p;
 }
 
 static void default_free(void *p, amgt_stream_t s, void *)
 {
+    if (!p) return;
+    {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        auto it = g_big_sizes.find(p);
+        if (it != g_big_sizes.end()) {
+            CachedBlock c{p, it->second, 0, (cudaStream_t)s, nullptr};
+            g_big_sizes.erase(it);
+            if (cudaGetDevice(&c.dev) == cudaSuccess &&
+                cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming) == cudaSuccess &&
+                cudaEventRecord(c.done, (cudaStream_t)s) == cudaSuccess) {
+                g_cache.push_back(c);
+                g_cache_bytes += c.bytes;
+                while (g_cache_bytes > kCacheCap && !g_cache.empty()) {  // oldest first
+                    g_cache_bytes -= g_cache.front().bytes;
+                    release_block(g_cache.front());
+                    g_cache.erase(g_cache.begin());
+                }
+                return;
+            }
+            cudaGetLastError();
+            if (c.done) cudaEventDestroy(c.done);
+        }
+    }
     cudaFreeAsync(p, (cudaStream_t)s);
 }
 
@@ -106,14 +205,18 @@ int device_state(DeviceState **st)
     return AMGT_OK;
 }
 
+// The error word as of the last read_back on this device (copied with it
+// into pinned slot kErrSlot, so no second synchronisation is needed); a
+// raised word is cleared on the stream and reported once.
+static constexpr int kErrSlot = 15;
+
 int check_device_error(cudaStream_t s)
 {
     DeviceState *st;
     AMGT_TRY(device_state(&st));
-    int h = 0;
-    AMGT_CUDA_TRY(cudaMemcpyAsync(&h, st->err, sizeof(int), cudaMemcpyDeviceToHost, s));
-    AMGT_CUDA_TRY(cudaStreamSynchronize(s));
+    const int h = (int)st->pinned[kErrSlot];
     if (h != 0) {
+        st->pinned[kErrSlot] = 0;
         AMGT_CUDA_TRY(cudaMemsetAsync(st->err, 0, sizeof(int), s));
         snprintf(g_cuda_msg, sizeof(g_cuda_msg), "device error word raised: %d", h);
         return AMGT_ERR_DEVICE;
@@ -125,7 +228,10 @@ int read_back(const int64_t *dev, int count, cudaStream_t s, const int64_t **hos
 {
     DeviceState *st;
     AMGT_TRY(device_state(&st));
+    if (count > kErrSlot) return AMGT_ERR_INVALID;
+    st->pinned[kErrSlot] = 0;
     AMGT_CUDA_TRY(cudaMemcpyAsync(st->pinned, dev, sizeof(int64_t) * count, cudaMemcpyDeviceToHost, s));
+    AMGT_CUDA_TRY(cudaMemcpyAsync(&st->pinned[kErrSlot], st->err, sizeof(int), cudaMemcpyDeviceToHost, s));
     AMGT_CUDA_TRY(cudaStreamSynchronize(s));
     *host = st->pinned;
     return AMGT_OK;
@@ -202,6 +308,9 @@ int amgt_trim_pool(size_t keep_bytes)
 {
     cudaMemPool_t pool = library_pool();
     if (!pool) return AMGT_ERR_NO_DEVICE;
+    int dev = 0;
+    AMGT_CUDA_TRY(cudaGetDevice(&dev));
+    flush_cache(dev);
     AMGT_CUDA_TRY(cudaDeviceSynchronize());
     AMGT_CUDA_TRY(cudaMemPoolTrimTo(pool, keep_bytes));
     return AMGT_OK;
@@ -210,6 +319,7 @@ int amgt_trim_pool(size_t keep_bytes)
 int amgt_set_allocator(amgt_alloc_fn alloc_fn, amgt_free_fn free_fn, void *ctx)
 {
     if ((alloc_fn == nullptr) != (free_fn == nullptr)) return AMGT_ERR_INVALID;
+    if (alloc_fn) flush_cache(-1);  // the default allocator's kept blocks go back to its pool
     g_alloc = alloc_fn ? alloc_fn : default_alloc;
     g_free = free_fn ? free_fn : default_free;
     g_alloc_ctx = alloc_fn ? ctx : nullptr;
