@@ -121,62 +121,117 @@ __device__ __forceinline__ long long sym_upper_bound(int lane, int a0, int a1, c
     return ub;
 }
 
-// Sorted distinct keys with OR-ed bitmaps of the warp's list s[0..cnt).
-// FILL writes them to cidx/cmap; always returns the distinct count and the
-// per-scalar-row CSR counts (popcount of each bitmap nibble).  pslot (may
-// be null) receives, per pair ordinal (the tag), the index of its C block.
-template <bool FILL>
-__device__ __forceinline__ int sym_reduce(int lane, int cnt, unsigned long long *s, int *__restrict__ cidx,
-                                          uint16_t *__restrict__ cmap, int csr[4], uint16_t *__restrict__ pslot)
+// Sorted distinct keys with OR-ed bitmaps of the warp's list s[0..cnt),
+// cnt <= 32 (one pair per lane, a register sort).  Writes them to
+// cidx/cmap, the index of each pair's C block to pslot (by the pair's tag,
+// its ordinal in the row), and returns the distinct count and the
+// per-scalar-row CSR counts (popcount of each bitmap nibble).
+__device__ __forceinline__ int sym_reduce32(int lane, int cnt, unsigned long long *s, int *__restrict__ cidx,
+                                            uint16_t *__restrict__ cmap, int csr[4], uint16_t *__restrict__ pslot)
 {
     csr[0] = csr[1] = csr[2] = csr[3] = 0;
+    unsigned long long v = (lane < cnt) ? s[lane] : kSentinel;
+    __syncwarp();
+    v = warp_sort32(v, lane);
+    uint32_t orv;
+    const bool head = warp_runs32(v, lane, &orv);
+    const unsigned hb = __ballot_sync(FULL, head);
+    const int u = __popc(hb);
+    if (v != kSentinel) pslot[pair_tag(v)] = (uint16_t)(__popc(hb & ((2u << lane) - 1u)) - 1);
+    if (head) {
+        const int slot = __popc(hb & lanemask_lt(lane));
+        cidx[slot] = pair_key(v);
+        cmap[slot] = (uint16_t)orv;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) csr[q] = __popc((orv >> (4 * q)) & 0xFu);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) csr[q] = warp_sum(csr[q]);
+    return u;
+}
+
+// The same for rows of more than 32 pairs (cnt <= H, H a power of two and
+// a multiple of 32).  The pairs' columns are first made distinct through a
+// shared hash table of H slots (atomicCAS on the column, atomicOr on the
+// bitmap; linear probing, bounded by H), so only the distinct columns are
+// sorted (C rows here hold a tenth of their pairs' count or fewer); each
+// pair's C block is found through its table slot.  The result equals
+// sorting all pairs: C's columns ascending with OR-ed bitmaps, and the rank
+// of each pair's column.  pslot first receives the pairs' table slots and
+// then, in a second pass over the row's npairs ordinals, their ranks.
+template <int H>
+__device__ int sym_reduce_hashed(int lane, int cnt, unsigned long long *s, int *tkey, unsigned *tval,
+                                 int *__restrict__ cidx, uint16_t *__restrict__ cmap, int csr[4],
+                                 uint16_t *__restrict__ pslot, int npairs, int *__restrict__ err)
+{
+    constexpr int LOG2H = __builtin_ctz(H);
+    for (int i = lane; i < H; i += 32) {
+        tkey[i] = -1;
+        tval[i] = 0;
+    }
+    __syncwarp();
+    for (int i = lane; i < cnt; i += 32) {
+        const unsigned long long v = s[i];
+        const int key = pair_key(v);
+        unsigned h = ((unsigned)key * 0x9E3779B1u) >> (32 - LOG2H);
+        int probe = 0;
+        for (; probe < H; ++probe) {
+            const int prev = atomicCAS(&tkey[h], -1, key);
+            if (prev == -1 || prev == key) break;
+            h = (h + 1) & (H - 1);
+        }
+        if (probe == H) {  // cannot happen (cnt <= H); kept as a bound
+            raise_error(err, DEV_ERR_PROBE);
+            continue;
+        }
+        atomicOr(&tval[h], pair_map(v));
+        pslot[pair_tag(v)] = (uint16_t)h;
+    }
+    __syncwarp();
+    // distinct columns -> s[0..u), tagged with their table slot
     int u = 0;
-    if (cnt <= 32) {
-        unsigned long long v = (lane < cnt) ? s[lane] : kSentinel;
+    for (int i0 = 0; i0 < H; i0 += 32) {
+        const int i = i0 + lane;
+        const int key = tkey[i];
+        const unsigned bal = __ballot_sync(FULL, key >= 0);
+        if (key >= 0) s[u + __popc(bal & lanemask_lt(lane))] = pack_pair(key, i, tval[i]);
+        u += __popc(bal);
+    }
+    __syncwarp();
+    csr[0] = csr[1] = csr[2] = csr[3] = 0;
+    if (u <= 32) {
+        unsigned long long v = (lane < u) ? s[lane] : kSentinel;
         __syncwarp();
         v = warp_sort32(v, lane);
-        uint32_t orv;
-        const bool head = warp_runs32(v, lane, &orv);
-        const unsigned hb = __ballot_sync(FULL, head);
-        u = __popc(hb);
-        if (pslot && v != kSentinel) pslot[pair_tag(v)] = (uint16_t)(__popc(hb & ((2u << lane) - 1u)) - 1);
-        if (head) {
-            const int slot = __popc(hb & lanemask_lt(lane));
-            if (FILL) {
-                cidx[slot] = pair_key(v);
-                cmap[slot] = (uint16_t)orv;
-            }
+        if (v != kSentinel) {
+            const uint32_t mp = pair_map(v);
+            cidx[lane] = pair_key(v);
+            cmap[lane] = (uint16_t)mp;
+            tval[pair_tag(v)] = (unsigned)lane;  // rank of the column
 #pragma unroll
-            for (int q = 0; q < 4; ++q) csr[q] = __popc((orv >> (4 * q)) & 0xFu);
+            for (int q = 0; q < 4; ++q) csr[q] = __popc((mp >> (4 * q)) & 0xFu);
         }
     } else {
-        const int N = next_pow2_min64(cnt);
-        for (int i = cnt + lane; i < N; i += 32) s[i] = kSentinel;
+        const int N = next_pow2_min64(u);
+        for (int i = u + lane; i < N; i += 32) s[i] = kSentinel;
         __syncwarp();
         warp_sort_smem(s, N, lane);
-        for (int i0 = 0; i0 < cnt; i0 += 32) {
-            const int i = i0 + lane;
-            const unsigned long long v = (i < cnt) ? s[i] : kSentinel;
-            bool head = false;
-            if (v != kSentinel) head = (i == 0) || pair_key(v) != pair_key(s[i - 1]);
-            const unsigned hb = __ballot_sync(FULL, head);
-            if (pslot && v != kSentinel) pslot[pair_tag(v)] = (uint16_t)(u + __popc(hb & ((2u << lane) - 1u)) - 1);
-            if (head) {
-                uint32_t orv = 0;
-                const int key = pair_key(v);
-                for (int j = i; j < cnt && pair_key(s[j]) == key; ++j) orv |= pair_map(s[j]);
-                const int slot = u + __popc(hb & lanemask_lt(lane));
-                if (FILL) {
-                    cidx[slot] = key;
-                    cmap[slot] = (uint16_t)orv;
-                }
+        for (int i = lane; i < u; i += 32) {
+            const unsigned long long v = s[i];
+            const uint32_t mp = pair_map(v);
+            cidx[i] = pair_key(v);
+            cmap[i] = (uint16_t)mp;
+            tval[pair_tag(v)] = (unsigned)i;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) csr[q] += __popc((orv >> (4 * q)) & 0xFu);
-            }
-            u += __popc(hb);
+            for (int q = 0; q < 4; ++q) csr[q] += __popc((mp >> (4 * q)) & 0xFu);
         }
-        __syncwarp();
     }
+    __syncwarp();
+    for (int q = lane; q < npairs; q += 32) {
+        const uint16_t h = pslot[q];
+        if (h != 0xFFFF) pslot[q] = (uint16_t)tval[h];
+    }
+    __syncwarp();
 #pragma unroll
     for (int q = 0; q < 4; ++q) csr[q] = warp_sum(csr[q]);
     return u;
@@ -205,22 +260,24 @@ __global__ void spgemm_ub_kernel(int brA, const int *__restrict__ aptr, const in
 // passing rows with more pairs to the CAP = 1024 instance through a list
 // (rows[], count in *nrows), which passes rows beyond that to the window
 // kernel's list.
-template <int CAP>
-__global__ void __launch_bounds__(32 * kSymWarps)
+template <int CAP, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS)
 spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
                        const uint16_t *__restrict__ amap, const int *__restrict__ bptr,
                        const int *__restrict__ bidx, const uint16_t *__restrict__ bmap, int *__restrict__ ccnt,
                        int *__restrict__ csrcnt, int *__restrict__ large, int64_t *__restrict__ stats,
                        const int64_t *__restrict__ ub_off, int *__restrict__ skey, uint16_t *__restrict__ smap,
                        const int *__restrict__ rows, const int *__restrict__ nrows, int *__restrict__ over,
-                       int *__restrict__ nover, uint16_t *__restrict__ pslot)
+                       int *__restrict__ nover, uint16_t *__restrict__ pslot, int *__restrict__ err)
 {
-    __shared__ unsigned long long sbuf[kSymWarps][CAP];
+    __shared__ unsigned long long sbuf[WARPS][CAP];
+    __shared__ int stkey[WARPS][CAP];       // hash table of the long rows
+    __shared__ unsigned stval[WARPS][CAP];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long *s = sbuf[warp];
     unsigned long long wmax = 0, wsq = 0;  // per-warp statistics, one atomic each at the end
     const int nr = rows ? *nrows : brA;
-    for (int t = blockIdx.x * kSymWarps + warp; t < nr; t += gridDim.x * kSymWarps) {
+    for (int t = blockIdx.x * WARPS + warp; t < nr; t += gridDim.x * WARPS) {
         const int b = rows ? rows[t] : t;
         const int a0 = aptr[b], a1 = aptr[b + 1];
         const long long ub = ub_off[b + 1] - ub_off[b];
@@ -231,7 +288,9 @@ spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *
         const long long base = ub_off[b];
         const int cnt = sym_collect(lane, a0, a1, aidx, amap, bptr, bidx, bmap, s, pslot + base);
         int csr[4];
-        const int u = sym_reduce<true>(lane, cnt, s, skey + base, smap + base, csr, pslot + base);
+        const int u = cnt <= 32 ? sym_reduce32(lane, cnt, s, skey + base, smap + base, csr, pslot + base)
+                                : sym_reduce_hashed<CAP>(lane, cnt, s, stkey[warp], stval[warp], skey + base,
+                                                         smap + base, csr, pslot + base, (int)ub, err);
         if (lane == 0) {
             ccnt[b] = u;
 #pragma unroll
@@ -794,12 +853,13 @@ int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
         // medium-row list and count live behind the large list (2 * brA + 1 ints)
         int *medium = large + brA, *nmedium = large + 2 * brA;
         AMGT_CUDA_TRY(cudaMemsetAsync(nmedium, 0, sizeof(int), s));
-        AMGT_LAUNCH(spgemm_symbolic_kernel<256>, grid_for(kSymWarps, brA, st->sm_count, 16), 32 * kSymWarps, 0, s, m,
-                    brA, A->blcPtr, A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, ccnt, csrcnt, large,
-                    stats, ub_off, skey, smap, nullptr, nullptr, medium, nmedium, pslot);
-        AMGT_LAUNCH(spgemm_symbolic_kernel<kSymCap>, 2 * st->sm_count, 32 * kSymWarps, 0, s, m, brA, A->blcPtr,
+        AMGT_LAUNCH((spgemm_symbolic_kernel<256, kSymWarps>), grid_for(kSymWarps, brA, st->sm_count, 16),
+                    32 * kSymWarps, 0, s, m, brA, A->blcPtr, A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap,
+                    ccnt, csrcnt, large, stats, ub_off, skey, smap, nullptr, nullptr, medium, nmedium, pslot,
+                    st->err);
+        AMGT_LAUNCH((spgemm_symbolic_kernel<kSymCap, 2>), 6 * st->sm_count, 64, 0, s, m, brA, A->blcPtr,
                     A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, ccnt, csrcnt, large, stats, ub_off, skey,
-                    smap, medium, nmedium, large, (int *)&stats[3], pslot);
+                    smap, medium, nmedium, large, (int *)&stats[3], pslot, st->err);
         AMGT_LAUNCH(spgemm_symbolic_large_kernel, 2 * st->sm_count, kSymLargeThreads, 0, s, m, A->blcPtr, A->blcIdx,
                     A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, large, stats, ccnt, csrcnt, ub_off, skey, smap);
     }
