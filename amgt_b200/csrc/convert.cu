@@ -58,6 +58,14 @@ __device__ __forceinline__ BlockRowRange block_row_range(const int *ia, int m, i
 }
 
 // ------------------------------------------------------------ count pass
+// A warp takes kCvtGroup consecutive block rows at a time: their 4 * G + 1
+// row pointers arrive in one coalesced load and their entries (rows of at
+// most 32) in independent loads, so G block rows cost two memory round
+// trips instead of 2 G.  Each block row is then sorted on its own
+// (registers for <= 32 entries, the warp's shared-memory slice for <= 512);
+// longer ones go to the large list.
+constexpr int kCvtGroup = 4;
+
 __global__ void __launch_bounds__(32 * kCvtWarps)
 csr2bsr_count_kernel(int m, int n, const int *__restrict__ ia, const int *__restrict__ ja, int brow,
                      int *__restrict__ cnt, int *__restrict__ large, int64_t *__restrict__ stats, int *err,
@@ -67,50 +75,76 @@ csr2bsr_count_kernel(int m, int n, const int *__restrict__ ia, const int *__rest
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long *s = sbuf[warp];
     unsigned long long wmax = 0, wsq = 0;  // per-warp statistics, one atomic each at the end
-    for (int b = blockIdx.x * kCvtWarps + warp; b < brow; b += gridDim.x * kCvtWarps) {
-        const BlockRowRange R = block_row_range(ia, m, b);
-        const int L = R.p1 - R.p0;
-        if (L > kWarpCap) {
-            if (lane == 0) large[atomicAdd((int *)&stats[3], 1)] = b;
-            continue;
-        }
-        int u = 0;
-        if (L <= 32) {
-            unsigned long long v = kSentinel;
-            if (lane < L) {
-                const int p = R.p0 + lane;
-                v = csr_entry_pair(ja, p, R.p0, row_in_block(p, R.e1, R.e2, R.e3), n, err);
+    const int ngroups = (brow + kCvtGroup - 1) / kCvtGroup;
+    for (int g = blockIdx.x * kCvtWarps + warp; g < ngroups; g += gridDim.x * kCvtWarps) {
+        const int b0 = g * kCvtGroup;
+        const int nb = min(kCvtGroup, brow - b0);
+        // lane i holds ia[min(4 b0 + i, m)], i <= 4 nb (rows past m are empty)
+        const int iav = (lane <= 4 * nb) ? ia[min(4 * b0 + lane, m)] : 0;
+        auto range = [&](int j) {  // block row b0 + j's entries and row ends
+            BlockRowRange r;
+            r.p0 = __shfl_sync(FULL, iav, 4 * j);
+            r.e1 = __shfl_sync(FULL, iav, 4 * j + 1);
+            r.e2 = __shfl_sync(FULL, iav, 4 * j + 2);
+            r.e3 = __shfl_sync(FULL, iav, 4 * j + 3);
+            r.p1 = __shfl_sync(FULL, iav, 4 * j + 4);
+            return r;
+        };
+        unsigned long long v[kCvtGroup];
+#pragma unroll
+        for (int j = 0; j < kCvtGroup; ++j) {
+            const BlockRowRange r = range(j);
+            v[j] = kSentinel;
+            const int L = r.p1 - r.p0;
+            if (j < nb && L <= 32 && lane < L) {
+                const int p = r.p0 + lane;
+                v[j] = csr_entry_pair(ja, p, r.p0, row_in_block(p, r.e1, r.e2, r.e3), n, err);
             }
-            v = warp_sort32(v, lane);
-            if (lane < L) sorted[R.p0 + lane] = v;  // reused by the fill pass
-            uint32_t orv;
-            bool head = warp_runs32(v, lane, &orv);
-            u = __popc(__ballot_sync(FULL, head));
-        } else {
-            const int N = next_pow2_min64(L);
-            for (int i = lane; i < N; i += 32) {
-                unsigned long long v = kSentinel;
-                if (i < L) {
-                    const int p = R.p0 + i;
-                    v = csr_entry_pair(ja, p, R.p0, row_in_block(p, R.e1, R.e2, R.e3), n, err);
+        }
+#pragma unroll
+        for (int j = 0; j < kCvtGroup; ++j) {
+            const BlockRowRange Rj = range(j);
+            const int b = b0 + j;
+            const int L = Rj.p1 - Rj.p0;
+            if (j >= nb) {
+                // past the last block row (warp-uniform)
+            } else if (L > kWarpCap) {
+                if (lane == 0) large[atomicAdd((int *)&stats[3], 1)] = b;
+            } else {
+            int u = 0;
+            if (L <= 32) {
+                // distinct block columns: lanes with equal columns match,
+                // the lowest lane of each group counts it (no sort needed)
+                const int key = (v[j] != kSentinel) ? pair_key(v[j]) : -1 - lane;
+                const unsigned peers = __match_any_sync(FULL, key);
+                u = __popc(__ballot_sync(FULL, v[j] != kSentinel && (__ffs(peers) - 1) == lane));
+            } else {
+                const int N = next_pow2_min64(L);
+                for (int i = lane; i < N; i += 32) {
+                    unsigned long long x = kSentinel;
+                    if (i < L) {
+                        const int p = Rj.p0 + i;
+                        x = csr_entry_pair(ja, p, Rj.p0, row_in_block(p, Rj.e1, Rj.e2, Rj.e3), n, err);
+                    }
+                    s[i] = x;
                 }
-                s[i] = v;
+                __syncwarp();
+                warp_sort_smem(s, N, lane);
+                for (int i0 = 0; i0 < L; i0 += 32) {
+                    const int i = i0 + lane;
+                    bool head = false;
+                    if (i < L) sorted[Rj.p0 + i] = s[i];  // reused by the fill pass
+                    if (i < L && s[i] != kSentinel) head = (i == 0) || pair_key(s[i]) != pair_key(s[i - 1]);
+                    u += __popc(__ballot_sync(FULL, head));
+                }
+                __syncwarp();
             }
-            __syncwarp();
-            warp_sort_smem(s, N, lane);
-            for (int i0 = 0; i0 < L; i0 += 32) {
-                const int i = i0 + lane;
-                bool head = false;
-                if (i < L) sorted[R.p0 + i] = s[i];  // reused by the fill pass
-                if (i < L && s[i] != kSentinel) head = (i == 0) || pair_key(s[i]) != pair_key(s[i - 1]);
-                u += __popc(__ballot_sync(FULL, head));
+            if (lane == 0) {
+                cnt[b] = u;
+                wmax = wmax > (unsigned long long)u ? wmax : (unsigned long long)u;
+                wsq += (unsigned long long)u * (unsigned long long)u;
             }
-            __syncwarp();
-        }
-        if (lane == 0) {
-            cnt[b] = u;
-            wmax = wmax > (unsigned long long)u ? wmax : (unsigned long long)u;
-            wsq += (unsigned long long)u * (unsigned long long)u;
+            }
         }
     }
     if (lane == 0 && wsq) {
@@ -246,56 +280,100 @@ csr2bsr_large_kernel(int m, int n, const int *__restrict__ ia, const int *__rest
 // block row's CSR offset) and writes block columns, OR-ed bitmaps and the
 // zero-padded values.
 __global__ void __launch_bounds__(32 * kCvtWarps)
-csr2bsr_fill_kernel(int m, int n, const int *__restrict__ ia, const double *__restrict__ a, int brow,
-                    const int *__restrict__ bptr, int *__restrict__ bidx, uint16_t *__restrict__ bmap,
-                    double *__restrict__ bval, const unsigned long long *__restrict__ sorted)
+csr2bsr_fill_kernel(int m, int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                    const double *__restrict__ a, int brow, const int *__restrict__ bptr, int *__restrict__ bidx,
+                    uint16_t *__restrict__ bmap, double *__restrict__ bval,
+                    const unsigned long long *__restrict__ sorted, int *err)
 {
+    __shared__ unsigned sorv[kCvtWarps][32];  // per-slot OR of the bitmaps
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int b = blockIdx.x * kCvtWarps + warp; b < brow; b += gridDim.x * kCvtWarps) {
-        const BlockRowRange R = block_row_range(ia, m, b);
-        const int L = R.p1 - R.p0;
-        if (L > kWarpCap) continue;  // large-row kernel
-        const int base = bptr[b], u = bptr[b + 1] - base;
-        double2 *z = reinterpret_cast<double2 *>(bval + (size_t)16 * base);
-        for (int i = lane; i < 8 * u; i += 32) z[i] = make_double2(0.0, 0.0);
-        __syncwarp();
-        const unsigned long long *sp = sorted + R.p0;
-        if (L <= 32) {
-            const unsigned long long v = (lane < L) ? sp[lane] : kSentinel;
-            uint32_t orv;
-            const bool head = warp_runs32(v, lane, &orv);
-            const unsigned hb = __ballot_sync(FULL, head);
-            const int slot = __popc(hb & lanemask_le(lane)) - 1;
-            if (v != kSentinel) {
-                if (head) {
-                    bidx[base + slot] = pair_key(v);
-                    bmap[base + slot] = (uint16_t)orv;
-                }
-                const int bit = __ffs(pair_map(v)) - 1;
-                bval[(size_t)16 * (base + slot) + bit] = a[R.p0 + pair_tag(v)];
+    unsigned *so = sorv[warp];
+    const int ngroups = (brow + kCvtGroup - 1) / kCvtGroup;
+    for (int g = blockIdx.x * kCvtWarps + warp; g < ngroups; g += gridDim.x * kCvtWarps) {
+        // kCvtGroup block rows at a time, as in the count pass: row pointers
+        // and block offsets in one load each, sorted pairs and values of the
+        // short rows in independent loads
+        const int b0 = g * kCvtGroup;
+        const int nb = min(kCvtGroup, brow - b0);
+        const int iav = (lane <= 4 * nb) ? ia[min(4 * b0 + lane, m)] : 0;
+        const int bpv = (lane <= nb) ? bptr[b0 + lane] : 0;
+        unsigned long long v[kCvtGroup];
+        double av[kCvtGroup];
+#pragma unroll
+        for (int j = 0; j < kCvtGroup; ++j) {
+            const int p0 = __shfl_sync(FULL, iav, 4 * j), e1 = __shfl_sync(FULL, iav, 4 * j + 1),
+                      e2 = __shfl_sync(FULL, iav, 4 * j + 2), e3 = __shfl_sync(FULL, iav, 4 * j + 3),
+                      p1 = __shfl_sync(FULL, iav, 4 * j + 4);
+            const int L = p1 - p0;
+            v[j] = kSentinel;
+            av[j] = 0.0;
+            if (j < nb && L <= 32 && lane < L) {  // short rows: entries straight from ja / a
+                const int p = p0 + lane;
+                v[j] = csr_entry_pair(ja, p, p0, row_in_block(p, e1, e2, e3), n, err);
+                av[j] = a[p];
             }
-        } else {
-            int running = 0;
-            for (int i0 = 0; i0 < L; i0 += 32) {
-                const int i = i0 + lane;
-                const unsigned long long v = (i < L) ? sp[i] : kSentinel;
-                bool head = false;
-                if (v != kSentinel) head = (i == 0) || pair_key(v) != pair_key(sp[i - 1]);
-                const unsigned hb = __ballot_sync(FULL, head);
-                const int slot = running + __popc(hb & lanemask_le(lane)) - 1;
-                if (v != kSentinel) {
-                    if (head) {
-                        uint32_t orv = 0;
-                        const int key = pair_key(v);
-                        for (int jj = i; jj < L && sp[jj] != kSentinel && pair_key(sp[jj]) == key; ++jj)
-                            orv |= pair_map(sp[jj]);
-                        bidx[base + slot] = key;
-                        bmap[base + slot] = (uint16_t)orv;
+        }
+#pragma unroll
+        for (int j = 0; j < kCvtGroup; ++j) {
+            const int p0 = __shfl_sync(FULL, iav, 4 * j), p1 = __shfl_sync(FULL, iav, 4 * j + 4);
+            const int L = p1 - p0;
+            const int base = __shfl_sync(FULL, bpv, j), u = __shfl_sync(FULL, bpv, j + 1) - base;
+            if (j < nb && L <= kWarpCap) {  // warp-uniform; longer rows: large-row kernel
+                double2 *z = reinterpret_cast<double2 *>(bval + (size_t)16 * base);
+                for (int i = lane; i < 8 * u; i += 32) z[i] = make_double2(0.0, 0.0);
+                __syncwarp();
+                if (L <= 32) {
+                    // group the entries by block column (match), OR the
+                    // group's bits, rank the column among the row's distinct
+                    // columns by comparing with each group's leader
+                    const bool valid = v[j] != kSentinel;
+                    const int key = valid ? pair_key(v[j]) : -1 - lane;
+                    const unsigned peers = __match_any_sync(FULL, key);
+                    const bool leader = valid && (__ffs(peers) - 1) == lane;
+                    unsigned lm = __ballot_sync(FULL, leader);
+                    int slot = 0;
+                    while (lm) {  // warp-uniform: the row's distinct columns
+                        const int l = __ffs(lm) - 1;
+                        lm &= lm - 1;
+                        slot += __shfl_sync(FULL, key, l) < key;
                     }
-                    const int bit = __ffs(pair_map(v)) - 1;
-                    bval[(size_t)16 * (base + slot) + bit] = a[R.p0 + pair_tag(v)];
+                    so[lane] = 0;
+                    __syncwarp();
+                    if (valid) atomicOr(&so[slot], pair_map(v[j]));
+                    __syncwarp();
+                    if (valid) {
+                        if (leader) {
+                            bidx[base + slot] = key;
+                            bmap[base + slot] = (uint16_t)so[slot];
+                        }
+                        const int bit = __ffs(pair_map(v[j])) - 1;
+                        bval[(size_t)16 * (base + slot) + bit] = av[j];
+                    }
+                } else {
+                    const unsigned long long *sp = sorted + p0;
+                    int running = 0;
+                    for (int i0 = 0; i0 < L; i0 += 32) {
+                        const int i = i0 + lane;
+                        const unsigned long long w = (i < L) ? sp[i] : kSentinel;
+                        bool head = false;
+                        if (w != kSentinel) head = (i == 0) || pair_key(w) != pair_key(sp[i - 1]);
+                        const unsigned hb = __ballot_sync(FULL, head);
+                        const int slot = running + __popc(hb & lanemask_le(lane)) - 1;
+                        if (w != kSentinel) {
+                            if (head) {
+                                uint32_t orv = 0;
+                                const int key = pair_key(w);
+                                for (int jj = i; jj < L && sp[jj] != kSentinel && pair_key(sp[jj]) == key; ++jj)
+                                    orv |= pair_map(sp[jj]);
+                                bidx[base + slot] = key;
+                                bmap[base + slot] = (uint16_t)orv;
+                            }
+                            const int bit = __ffs(pair_map(w)) - 1;
+                            bval[(size_t)16 * (base + slot) + bit] = a[p0 + pair_tag(w)];
+                        }
+                        running += __popc(hb);
+                    }
                 }
-                running += __popc(hb);
             }
         }
     }
@@ -555,7 +633,8 @@ int amgt_csr_to_bsr(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream)
     AMGT_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(int64_t) * 4, s));
     AMGT_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * (brow + 1), s));
     if (brow > 0) {
-        AMGT_LAUNCH(csr2bsr_count_kernel, grid_for(kCvtWarps, brow, st->sm_count, 16), 32 * kCvtWarps, 0, s, m, n,
+        AMGT_LAUNCH(csr2bsr_count_kernel, grid_for(kCvtWarps, (brow + kCvtGroup - 1) / kCvtGroup, st->sm_count, 16),
+                    32 * kCvtWarps, 0, s, m, n,
                     A->i, A->j, brow, cnt, large, stats, st->err, sorted);
         AMGT_LAUNCH(csr2bsr_large_kernel<false>, 2 * st->sm_count, kLargeThreads, 2 * kWin * sizeof(uint32_t), s,
                     m, n, A->i, A->j, A->data, large, stats, cnt, nullptr, nullptr, nullptr, nullptr, stats);
@@ -580,8 +659,9 @@ int amgt_csr_to_bsr(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream)
         (rc = alloc_n(&out->blcVal, (size_t)16 * nb, s)))
         goto fail;
     if (brow > 0) {
-        AMGT_LAUNCH(csr2bsr_fill_kernel, grid_for(kCvtWarps, brow, st->sm_count, 16), 32 * kCvtWarps, 0, s, m, n,
-                    A->i, A->data, brow, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal, sorted);
+        AMGT_LAUNCH(csr2bsr_fill_kernel, grid_for(kCvtWarps, (brow + kCvtGroup - 1) / kCvtGroup, st->sm_count, 16),
+                    32 * kCvtWarps, 0, s, m, n,
+                    A->i, A->j, A->data, brow, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal, sorted, st->err);
         AMGT_LAUNCH(csr2bsr_large_kernel<true>, 2 * st->sm_count, kLargeThreads, 2 * kWin * sizeof(uint32_t), s, m,
                     n, A->i, A->j, A->data, large, stats, nullptr, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal,
                     nullptr);
