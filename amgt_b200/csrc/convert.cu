@@ -69,7 +69,7 @@ constexpr int kCvtGroup = 4;
 __global__ void __launch_bounds__(32 * kCvtWarps)
 csr2bsr_count_kernel(int m, int n, const int *__restrict__ ia, const int *__restrict__ ja, int brow,
                      int *__restrict__ cnt, int *__restrict__ large, int64_t *__restrict__ stats, int *err,
-                     unsigned long long *__restrict__ sorted)
+                     unsigned long long *__restrict__ sorted, unsigned char *__restrict__ slotb)
 {
     __shared__ unsigned long long sbuf[kCvtWarps][kWarpCap];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -115,9 +115,19 @@ csr2bsr_count_kernel(int m, int n, const int *__restrict__ ia, const int *__rest
             if (L <= 32) {
                 // distinct block columns: lanes with equal columns match,
                 // the lowest lane of each group counts it (no sort needed)
-                const int key = (v[j] != kSentinel) ? pair_key(v[j]) : -1 - lane;
+                const bool valid = v[j] != kSentinel;
+                const int key = valid ? pair_key(v[j]) : -1 - lane;
                 const unsigned peers = __match_any_sync(FULL, key);
-                u = __popc(__ballot_sync(FULL, v[j] != kSentinel && (__ffs(peers) - 1) == lane));
+                const bool leader = valid && (__ffs(peers) - 1) == lane;
+                unsigned lm = __ballot_sync(FULL, leader);
+                u = __popc(lm);
+                int slot = 0;  // rank of the entry's column among the row's distinct columns
+                while (lm) {   // warp-uniform
+                    const int l = __ffs(lm) - 1;
+                    lm &= lm - 1;
+                    slot += __shfl_sync(FULL, key, l) < key;
+                }
+                if (valid) slotb[Rj.p0 + lane] = (unsigned char)(slot | (leader ? 0x80 : 0));
             } else {
                 const int N = next_pow2_min64(L);
                 for (int i = lane; i < N; i += 32) {
@@ -283,7 +293,7 @@ __global__ void __launch_bounds__(32 * kCvtWarps)
 csr2bsr_fill_kernel(int m, int n, const int *__restrict__ ia, const int *__restrict__ ja,
                     const double *__restrict__ a, int brow, const int *__restrict__ bptr, int *__restrict__ bidx,
                     uint16_t *__restrict__ bmap, double *__restrict__ bval,
-                    const unsigned long long *__restrict__ sorted, int *err)
+                    const unsigned long long *__restrict__ sorted, const unsigned char *__restrict__ slotb, int *err)
 {
     __shared__ unsigned sorv[kCvtWarps][32];  // per-slot OR of the bitmaps
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -299,6 +309,7 @@ csr2bsr_fill_kernel(int m, int n, const int *__restrict__ ia, const int *__restr
         const int bpv = (lane <= nb) ? bptr[b0 + lane] : 0;
         unsigned long long v[kCvtGroup];
         double av[kCvtGroup];
+        int sl[kCvtGroup];  // slot | 0x80 on the first entry of its column (from the count pass)
 #pragma unroll
         for (int j = 0; j < kCvtGroup; ++j) {
             const int p0 = __shfl_sync(FULL, iav, 4 * j), e1 = __shfl_sync(FULL, iav, 4 * j + 1),
@@ -307,10 +318,12 @@ csr2bsr_fill_kernel(int m, int n, const int *__restrict__ ia, const int *__restr
             const int L = p1 - p0;
             v[j] = kSentinel;
             av[j] = 0.0;
+            sl[j] = 0;
             if (j < nb && L <= 32 && lane < L) {  // short rows: entries straight from ja / a
                 const int p = p0 + lane;
                 v[j] = csr_entry_pair(ja, p, p0, row_in_block(p, e1, e2, e3), n, err);
                 av[j] = a[p];
+                sl[j] = slotb[p];
             }
         }
 #pragma unroll
@@ -327,16 +340,9 @@ csr2bsr_fill_kernel(int m, int n, const int *__restrict__ ia, const int *__restr
                     // group's bits, rank the column among the row's distinct
                     // columns by comparing with each group's leader
                     const bool valid = v[j] != kSentinel;
-                    const int key = valid ? pair_key(v[j]) : -1 - lane;
-                    const unsigned peers = __match_any_sync(FULL, key);
-                    const bool leader = valid && (__ffs(peers) - 1) == lane;
-                    unsigned lm = __ballot_sync(FULL, leader);
-                    int slot = 0;
-                    while (lm) {  // warp-uniform: the row's distinct columns
-                        const int l = __ffs(lm) - 1;
-                        lm &= lm - 1;
-                        slot += __shfl_sync(FULL, key, l) < key;
-                    }
+                    const int key = pair_key(v[j]);
+                    const int slot = sl[j] & 0x1F;
+                    const bool leader = valid && (sl[j] & 0x80);
                     so[lane] = 0;
                     __syncwarp();
                     if (valid) atomicOr(&so[slot], pair_map(v[j]));
@@ -614,28 +620,32 @@ int amgt_csr_to_bsr(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream)
 
     int *cnt = nullptr, *large = nullptr;
     int64_t *stats = nullptr;
-    unsigned long long *sorted = nullptr;
+    unsigned long long *sorted = nullptr;  // sorted entries of rows of 33..512 entries
+    unsigned char *slotb = nullptr;        // per entry of shorter rows: block slot | first-of-column flag
     int rc = AMGT_OK;
     const int64_t *h = nullptr;
     int nb = 0;
-    static bool smem_set = false;
-    if (!smem_set) {
+    static bool smem_set[64];  // per device: the large-row kernels' shared-memory opt-in
+    int dev = 0;
+    AMGT_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && !smem_set[dev]) {
         AMGT_CUDA_TRY(cudaFuncSetAttribute(csr2bsr_large_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            2 * kWin * (int)sizeof(uint32_t)));
         AMGT_CUDA_TRY(cudaFuncSetAttribute(csr2bsr_large_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            2 * kWin * (int)sizeof(uint32_t)));
-        smem_set = true;
+        smem_set[dev] = true;
     }
     if ((rc = alloc_n(&out->blcPtr, brow + 1, s)) || (rc = alloc_n(&cnt, brow + 1, s)) ||
         (rc = alloc_n(&large, brow, s)) || (rc = alloc_n(&stats, 4, s)) ||
-        (rc = alloc_n(&sorted, (size_t)A->num_nonzeros, s)))
+        (rc = alloc_n(&sorted, (size_t)A->num_nonzeros, s)) ||
+        (rc = alloc_n(&slotb, (size_t)A->num_nonzeros, s)))
         goto fail;
     AMGT_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(int64_t) * 4, s));
     AMGT_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * (brow + 1), s));
     if (brow > 0) {
         AMGT_LAUNCH(csr2bsr_count_kernel, grid_for(kCvtWarps, (brow + kCvtGroup - 1) / kCvtGroup, st->sm_count, 16),
                     32 * kCvtWarps, 0, s, m, n,
-                    A->i, A->j, brow, cnt, large, stats, st->err, sorted);
+                    A->i, A->j, brow, cnt, large, stats, st->err, sorted, slotb);
         AMGT_LAUNCH(csr2bsr_large_kernel<false>, 2 * st->sm_count, kLargeThreads, 2 * kWin * sizeof(uint32_t), s,
                     m, n, A->i, A->j, A->data, large, stats, cnt, nullptr, nullptr, nullptr, nullptr, stats);
     }
@@ -661,7 +671,8 @@ int amgt_csr_to_bsr(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream)
     if (brow > 0) {
         AMGT_LAUNCH(csr2bsr_fill_kernel, grid_for(kCvtWarps, (brow + kCvtGroup - 1) / kCvtGroup, st->sm_count, 16),
                     32 * kCvtWarps, 0, s, m, n,
-                    A->i, A->j, A->data, brow, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal, sorted, st->err);
+                    A->i, A->j, A->data, brow, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal, sorted, slotb,
+                    st->err);
         AMGT_LAUNCH(csr2bsr_large_kernel<true>, 2 * st->sm_count, kLargeThreads, 2 * kWin * sizeof(uint32_t), s, m,
                     n, A->i, A->j, A->data, large, stats, nullptr, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal,
                     nullptr);
@@ -670,12 +681,14 @@ int amgt_csr_to_bsr(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream)
     free_ptr(large, s);
     free_ptr(stats, s);
     free_ptr(sorted, s);
+    free_ptr(slotb, s);
     return AMGT_OK;
 fail:
     free_ptr(cnt, s);
     free_ptr(large, s);
     free_ptr(stats, s);
     free_ptr(sorted, s);
+    free_ptr(slotb, s);
     amgt_bsr_free(out, stream);
     return rc;
 }
