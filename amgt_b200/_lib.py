@@ -32,7 +32,7 @@ class AmgtBsr(ctypes.Structure):
                 ("blcPtr", c_void_p), ("blcIdx", c_void_p), ("blcVal", c_void_p), ("blcMap", c_void_p),
                 ("warpnum", c_int), ("rowPtrbyWarp", c_void_p), ("rowIdxbyWarp", c_void_p),
                 ("blcVal_fp32", c_void_p), ("blcVal_fp16", c_void_p), ("blcVal_bf16", c_void_p),
-                ("max_blc_per_row", c_int), ("csr_nnz", c_int)]
+                ("max_blc_per_row", c_int), ("csr_nnz", c_int), ("exact_prec", c_int)]
 
 
 class AmgtVector(ctypes.Structure):
@@ -48,7 +48,8 @@ class AmgtCSRMatrix(ctypes.Structure):
 class AmgtAmgParams(ctypes.Structure):
     _fields_ = [("max_levels", c_int), ("max_coarse_rows", c_int), ("tol", c_double), ("max_iter", c_int),
                 ("relax_weight", c_double), ("flexible", c_int), ("use_graph", c_int),
-                ("galerkin_by_level", c_int), ("smooth_prec0", c_int), ("packed", c_int)]
+                ("galerkin_by_level", c_int), ("smooth_prec0", c_int), ("packed", c_int),
+                ("exact_storage", c_int)]
 
 
 class AmgtPbsr(ctypes.Structure):
@@ -71,6 +72,7 @@ SIGNATURES = {
     "amgt_bsr_balance": (c_int, [P(AmgtBsr), c_void_p]),
     "amgt_bsr_make_shadow": (c_int, [P(AmgtBsr), c_int, c_void_p]),
     "amgt_bsr_transpose": (c_int, [P(AmgtBsr), P(AmgtBsr), c_void_p]),
+    "amgt_bsr_make_exact": (c_int, [P(AmgtBsr), c_void_p]),
     "amgt_bsr_free": (c_int, [P(AmgtBsr), c_void_p]),
     "amgt_csr_free": (c_int, [P(AmgtCsr), c_void_p]),
     "amgt_spmv": (c_int, [c_int, c_double, P(AmgtBsr), c_void_p, c_double, c_void_p, c_void_p]),

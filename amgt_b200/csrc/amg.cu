@@ -398,6 +398,7 @@ void amgt_amg_default_params(amgt_amg_params *p)
     p->galerkin_by_level = 0;
     p->smooth_prec0 = AMGT_DOUBLE;
     p->packed = 0;
+    p->exact_storage = 1;
 }
 
 int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const amgt_amg_params *params,
@@ -449,6 +450,32 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     }
     h->lv[L - 1].prec = amgt_precision_for_level(L - 1);
     t0 = now_ms();
+    // exact narrow storage of the operators used in fp64 (level 0, fp64
+    // levels and transfers): one value check each, one read-back per 15
+    if (h->prm.exact_storage) {
+        std::vector<amgt_bsr *> mats;
+        for (int l = 0; l < L; ++l) {
+            if (l == 0 || h->lv[l].prec == AMGT_DOUBLE) mats.push_back(&h->lv[l].A);
+            if (l < L - 1 && h->lv[l].prec_transfer == AMGT_DOUBLE) {
+                mats.push_back(&h->lv[l].P);
+                mats.push_back(&h->lv[l].R);
+            }
+        }
+        int64_t *flags = nullptr;
+        if ((rc = alloc_n(&flags, mats.size(), s))) goto fail;
+        AMGT_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int64_t) * mats.size(), s));
+        for (size_t i = 0; i < mats.size() && !rc; ++i) rc = bsr_exact_check(mats[i], flags + i, s, h->sm_count);
+        for (size_t i0 = 0; i0 < mats.size() && !rc; i0 += 15) {
+            const int k = (int)std::min<size_t>(15, mats.size() - i0);
+            const int64_t *hf = nullptr;
+            if ((rc = read_back(flags + i0, k, s, &hf))) break;
+            int64_t f[15];
+            for (int i = 0; i < k; ++i) f[i] = hf[i];  // the pinned slots are reused by the calls below
+            for (int i = 0; i < k && !rc; ++i) rc = bsr_exact_apply(mats[i0 + i], f[i], s);
+        }
+        free_ptr(flags, s);
+        if (rc) goto fail;
+    }
     // smoother data, shadows, work vectors
     for (int l = 0; l < L; ++l) {
         Level &v = h->lv[l];

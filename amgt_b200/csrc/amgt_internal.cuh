@@ -114,6 +114,13 @@ int pbsr_jacobi(const amgt_pbsr *A, const double *inv_l1, double w, const double
                 cudaStream_t s, int sm_count);
 int pbsr_dot(const amgt_pbsr *A, const double *u, double *out, double *partial, int grid, cudaStream_t s);
 
+// Exact narrow storage (convert.cu): launch the value check of A into
+// *flag (bit 0: not all fp32 values, bit 1: not all fp16 values; *flag
+// zeroed by the caller), then, with the flag read back, build the exact
+// shadow and set A->exact_prec.
+int bsr_exact_check(const amgt_bsr *A, int64_t *flag, cudaStream_t s, int sm_count);
+int bsr_exact_apply(amgt_bsr *A, int64_t flag, cudaStream_t s);
+
 // Exclusive scan of n ints (in may equal out), CUB with allocator scratch.
 int exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s);
 // Exclusive scan of n 64-bit ints.

@@ -481,6 +481,42 @@ __global__ void shadow_kernel(long long n, const double *__restrict__ v, void *_
     }
 }
 
+// Exactness of stored values: bit 0 of *flags set when some value is not
+// an fp32 value, bit 1 when some value is not an fp16 value (round trip
+// through the format changes it; NaN counts as inexact).
+__global__ void exact_check_kernel(long long n, const double *__restrict__ v, unsigned long long *flags)
+{
+    bool not32 = false, not16 = false;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double d = v[i];
+        if ((double)__double2float_rn(d) != d) not32 = true;
+        if ((double)__half2float(__double2half(d)) != d) not16 = true;
+    }
+    const unsigned b32 = __ballot_sync(FULL, not32), b16 = __ballot_sync(FULL, not16);
+    if ((threadIdx.x & 31) == 0 && (b32 | b16))
+        atomicOr(flags, (b32 ? 1ull : 0ull) | (b16 ? 2ull : 0ull));
+}
+
+int bsr_exact_check(const amgt_bsr *A, int64_t *flag, cudaStream_t s, int sm_count)
+{
+    if (A->blc_num == 0) return AMGT_OK;
+    const long long n = 16LL * A->blc_num;
+    AMGT_LAUNCH(exact_check_kernel, grid_for(256 * 4, n, sm_count, 8), 256, 0, s, n, A->blcVal,
+                (unsigned long long *)flag);
+    return AMGT_OK;
+}
+
+int bsr_exact_apply(amgt_bsr *A, int64_t flag, cudaStream_t s)
+{
+    A->exact_prec = AMGT_DOUBLE;
+    if (A->blc_num == 0) return AMGT_OK;
+    const int prec = !(flag & 2) ? AMGT_HALF : !(flag & 1) ? AMGT_FLOAT : AMGT_DOUBLE;
+    if (prec == AMGT_DOUBLE) return AMGT_OK;
+    AMGT_TRY(amgt_bsr_make_shadow(A, prec, (amgt_stream_t)s));  // exact, so equal to any existing shadow
+    A->exact_prec = prec;
+    return AMGT_OK;
+}
+
 // ------------------------------------------------- block-row statistics
 // out[0] = longest block row (max), out[1] = sum of squared lengths.
 __global__ void row_stats_kernel(int brow, const int *__restrict__ bptr, int64_t *__restrict__ out)
@@ -796,6 +832,23 @@ int amgt_bsr_make_shadow(amgt_bsr *A, int prec, amgt_stream_t stream)
     default:
         return AMGT_ERR_INVALID;
     }
+}
+
+int amgt_bsr_make_exact(amgt_bsr *A, amgt_stream_t stream)
+{
+    if (!A || (A->blc_num > 0 && !A->blcVal)) return AMGT_ERR_INVALID;
+    DeviceState *st;
+    AMGT_TRY(device_state(&st));
+    cudaStream_t s = (cudaStream_t)stream;
+    int64_t *flag = nullptr;
+    const int64_t *h = nullptr;
+    int rc;
+    if ((rc = alloc_n(&flag, 1, s))) return rc;
+    if (!(rc = (cudaMemsetAsync(flag, 0, sizeof(int64_t), s) == cudaSuccess) ? AMGT_OK : AMGT_ERR_CUDA) &&
+        !(rc = bsr_exact_check(A, flag, s, st->sm_count)) && !(rc = read_back(flag, 1, s, &h)))
+        rc = bsr_exact_apply(A, h[0], s);
+    free_ptr(flag, s);
+    return rc;
 }
 
 int amgt_bsr_transpose(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream)

@@ -43,6 +43,24 @@ __device__ __forceinline__ typename ValTraits<PREC>::acc_t block_row_dot(const v
     return acc;
 }
 
+// A lane group's blocks k, k + G, k + 2G, ... of one block row, two per
+// step so that both loads are in flight before the FMAs; products are
+// added in block order.
+template <int PREC, int G, bool SAFE>
+__device__ __forceinline__ typename ValTraits<PREC>::acc_t row_dot(const void *__restrict__ val,
+                                                                   const int *__restrict__ idx,
+                                                                   const double *__restrict__ x, int n, int k,
+                                                                   int end, int q, typename ValTraits<PREC>::acc_t acc)
+{
+    for (; k + G < end; k += 2 * G) {
+        const int c0 = __ldcs(idx + k), c1 = __ldcs(idx + k + G);
+        acc = block_row_dot<PREC, SAFE>(val, x, n, k, q, c0, acc);
+        acc = block_row_dot<PREC, SAFE>(val, x, n, k + G, q, c1, acc);
+    }
+    if (k < end) acc = block_row_dot<PREC, SAFE>(val, x, n, k, q, __ldcs(idx + k), acc);
+    return acc;
+}
+
 template <int PREC, int LPR, bool SAFE>
 __global__ void __launch_bounds__(256)
 spmv_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__restrict__ idx,
@@ -60,15 +78,7 @@ spmv_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__re
         const int b = b0 + sub;
         acc_t acc = 0;
         if (b < brow) {
-            const int start = ptr[b], end = ptr[b + 1];
-            int k = start + g;
-            // two blocks per group per step: both loads in flight before the FMAs
-            for (; k + G < end; k += 2 * G) {
-                const int c0 = __ldcs(idx + k), c1 = __ldcs(idx + k + G);
-                acc = block_row_dot<PREC, SAFE>(val, x, n, k, q, c0, acc);
-                acc = block_row_dot<PREC, SAFE>(val, x, n, k + G, q, c1, acc);
-            }
-            if (k < end) acc = block_row_dot<PREC, SAFE>(val, x, n, k, q, __ldcs(idx + k), acc);
+            acc = row_dot<PREC, G, SAFE>(val, idx, x, n, ptr[b] + g, ptr[b + 1], q, acc);
         }
 #pragma unroll
         for (int o = 4; o < LPR; o <<= 1) acc += __shfl_xor_sync(FULL, acc, o);
@@ -208,14 +218,7 @@ spmv_epi_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *
         const int b = b0 + sub;
         acc_t acc = 0;
         if (b < brow) {
-            const int start = ptr[b], end = ptr[b + 1];
-            int k = start + g;
-            for (; k + G < end; k += 2 * G) {
-                const int c0 = __ldcs(idx + k), c1 = __ldcs(idx + k + G);
-                acc = block_row_dot<PREC, SAFE>(val, x, n, k, q, c0, acc);
-                acc = block_row_dot<PREC, SAFE>(val, x, n, k + G, q, c1, acc);
-            }
-            if (k < end) acc = block_row_dot<PREC, SAFE>(val, x, n, k, q, __ldcs(idx + k), acc);
+            acc = row_dot<PREC, G, SAFE>(val, idx, x, n, ptr[b] + g, ptr[b + 1], q, acc);
         }
 #pragma unroll
         for (int o = 4; o < LPR; o <<= 1) acc += __shfl_xor_sync(FULL, acc, o);
@@ -277,14 +280,30 @@ static const void *value_array(const amgt_bsr *A, int prec)
     case AMGT_FLOAT: return A->blcVal_fp32;
     case AMGT_HALF: return A->blcVal_fp16;
     case AMGT_BF16: return A->blcVal_bf16;
+    case kExact32: return A->blcVal_fp32;
+    case kExact16: return A->blcVal_fp16;
     default: return nullptr;
     }
 }
 
+// Storage read by an fp64 product: the shadow that holds every value
+// exactly when amgt_bsr_make_exact found one (same results, fewer bytes).
+static int storage_mode(const amgt_bsr *A, int prec)
+{
+    if (prec != AMGT_DOUBLE) return prec;
+    if (A->exact_prec == AMGT_HALF && A->blcVal_fp16) return kExact16;
+    if (A->exact_prec == AMGT_FLOAT && A->blcVal_fp32) return kExact32;
+    return AMGT_DOUBLE;
+}
+
+
 // Lanes per block row from the mean block-row length (overridable with
 // AMGT_SPMV_LPR for tuning runs).
-static int pick_lpr(const amgt_bsr *A)
+static int pick_lpr(const amgt_bsr *A, int mode)
 {
+    // the choice depends on the structure only: with the same segment length
+    // the exact narrow storage sums a row in the fp64 order, bit for bit
+    (void)mode;
     static int env = -1;
     if (env < 0) {
         const char *e = getenv("AMGT_SPMV_LPR");
@@ -293,8 +312,8 @@ static int pick_lpr(const amgt_bsr *A)
     if (env == 4 || env == 8 || env == 16 || env == 32) return env;
     const double avg = A->blc_row ? (double)A->blc_num / A->blc_row : 0.0;
     if (avg <= 1.5) return 4;
-    if (avg <= 3.0) return 8;
-    if (avg <= 10.0) return 16;
+    if (avg <= 10.0) return 8;   // 7-point 128^3 (6.9): 8 beat 16 for 8- and 2-byte values
+    if (avg <= 20.0) return 16;
     return 32;
 }
 
@@ -304,7 +323,7 @@ static int launch_spmv(const amgt_bsr *A, const void *val, double alpha, const d
 {
     const int brow = A->blc_row;
     const bool safe = (A->col % 4 != 0) || ((uintptr_t)x % 16 != 0);
-    const int lpr = pick_lpr(A);
+    const int lpr = pick_lpr(A, PREC);
     const int rows_per_cta = 8 * (32 / lpr);
     const int grid = grid_for(rows_per_cta, brow, sm_count, 8);
 #define AMGT_SPMV_CASE(L)                                                                                   \
@@ -379,7 +398,7 @@ template <int PREC>
 static int launch_spmm(const amgt_bsr *A, const void *val, double alpha, int nvec, const double *x, int ldx,
                        double beta, double *y, int ldy, cudaStream_t s, int sm_count)
 {
-    const int lpr = pick_lpr(A);
+    const int lpr = pick_lpr(A, AMGT_DOUBLE);
     const int grid = grid_for(8 * (32 / lpr), A->blc_row, sm_count, 8);
     switch (lpr) {
     case 4: return launch_spmm_lpr<PREC, 4>(A, val, alpha, nvec, x, ldx, beta, y, ldy, s, grid);
@@ -428,7 +447,7 @@ static int launch_epi(const amgt_bsr *A, const void *val, const double *x, const
                       cudaStream_t s)
 {
     const bool safe = (A->col % 4 != 0) || ((uintptr_t)x % 16 != 0);
-    const int lpr = pick_lpr(A);
+    const int lpr = pick_lpr(A, PREC);
 #define AMGT_EPI_CASE(L)                                                                                     \
     if (lpr == L) {                                                                                          \
         if (safe)                                                                                            \
@@ -451,20 +470,23 @@ template <int EPI>
 static int launch_epi_prec(int prec, const amgt_bsr *A, const double *x, const EpiArgs &e, int grid,
                            cudaStream_t s)
 {
-    const void *val = value_array(A, prec);
+    const int mode = storage_mode(A, prec);
+    const void *val = value_array(A, mode);
     if (!val) return AMGT_ERR_INVALID;
-    switch (prec) {
+    switch (mode) {
     case AMGT_DOUBLE: return launch_epi<AMGT_DOUBLE, EPI>(A, val, x, e, grid, s);
     case AMGT_FLOAT: return launch_epi<AMGT_FLOAT, EPI>(A, val, x, e, grid, s);
     case AMGT_HALF: return launch_epi<AMGT_HALF, EPI>(A, val, x, e, grid, s);
     case AMGT_BF16: return launch_epi<AMGT_BF16, EPI>(A, val, x, e, grid, s);
+    case kExact32: return launch_epi<kExact32, EPI>(A, val, x, e, grid, s);
+    case kExact16: return launch_epi<kExact16, EPI>(A, val, x, e, grid, s);
     default: return AMGT_ERR_INVALID;
     }
 }
 
 int epi_grid(const amgt_bsr *A, int sm_count)
 {
-    const int lpr = pick_lpr(A);
+    const int lpr = pick_lpr(A, storage_mode(A, AMGT_DOUBLE));
     return grid_for(8 * (32 / lpr), A->blc_row, sm_count, 8);
 }
 
@@ -514,10 +536,13 @@ int amgt_spmv(int prec, double alpha, const amgt_bsr *A, const double *x, double
         AMGT_LAUNCH(scale_kernel, grid_for(256, A->row, st->sm_count, 8), 256, 0, s, (long long)A->row, beta, y);
         return AMGT_OK;
     }
-    const void *val = value_array(A, prec);
-    if (!val || !x || !A->blcPtr || !A->blcIdx) return AMGT_ERR_INVALID;
     const bool seg = A->rowPtrbyWarp && A->rowIdxbyWarp && A->warpnum > 0 && A->max_blc_per_row > 256;
-    switch (prec) {
+    const int mode = seg ? prec : storage_mode(A, prec);
+    const void *val = value_array(A, mode);
+    if (!val || !x || !A->blcPtr || !A->blcIdx) return AMGT_ERR_INVALID;
+    switch (mode) {
+    case kExact32: return launch_spmv<kExact32>(A, val, alpha, x, beta, y, s, st->sm_count);
+    case kExact16: return launch_spmv<kExact16>(A, val, alpha, x, beta, y, s, st->sm_count);
     case AMGT_DOUBLE:
         return seg ? launch_spmv_segmented<AMGT_DOUBLE>(A, val, alpha, x, beta, y, s, st->sm_count)
                    : launch_spmv<AMGT_DOUBLE>(A, val, alpha, x, beta, y, s, st->sm_count);

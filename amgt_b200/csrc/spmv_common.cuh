@@ -23,6 +23,19 @@ template <>
 struct ValTraits<AMGT_BF16> {
     using acc_t = float;
 };
+// Internal storage modes for fp64 arithmetic on values that the fp32 or
+// fp16 shadow holds exactly (amgt_bsr.exact_prec): the shadow is read and
+// widened exactly, the sums are the fp64 kernel's, bit for bit.
+constexpr int kExact32 = 4;
+constexpr int kExact16 = 5;
+template <>
+struct ValTraits<kExact32> {
+    using acc_t = double;
+};
+template <>
+struct ValTraits<kExact16> {
+    using acc_t = double;
+};
 
 // Row q of block k as 4 values in the accumulation type.
 template <int PREC>
@@ -33,12 +46,12 @@ __device__ __forceinline__ void load_block_row(const void *__restrict__ val, lon
         const double2 *p = reinterpret_cast<const double2 *>(val) + (k * 8 + q * 2);
         const double2 a = __ldcs(p), b = __ldcs(p + 1);
         v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-    } else if constexpr (PREC == AMGT_FLOAT) {
+    } else if constexpr (PREC == AMGT_FLOAT || PREC == kExact32) {
         const float4 a = __ldcs(reinterpret_cast<const float4 *>(val) + (k * 4 + q));
         v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
     } else {
         const uint2 a = __ldcs(reinterpret_cast<const uint2 *>(val) + (k * 4 + q));
-        if constexpr (PREC == AMGT_HALF) {
+        if constexpr (PREC == AMGT_HALF || PREC == kExact16) {
             const float2 f0 = __half22float2(*reinterpret_cast<const __half2 *>(&a.x));
             const float2 f1 = __half22float2(*reinterpret_cast<const __half2 *>(&a.y));
             v[0] = f0.x; v[1] = f0.y; v[2] = f1.x; v[3] = f1.y;

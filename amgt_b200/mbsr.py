@@ -113,6 +113,11 @@ class Bsr:
     def make_shadow(self, prec: int, stream=None) -> None:
         check(L.lib().amgt_bsr_make_shadow(ctypes.byref(self.s), prec, _stream(stream)), "amgt_bsr_make_shadow")
 
+    def make_exact(self, stream=None) -> int:
+        """Exact narrow storage (amgt_bsr_make_exact); returns exact_prec."""
+        check(L.lib().amgt_bsr_make_exact(ctypes.byref(self.s), _stream(stream)), "amgt_bsr_make_exact")
+        return int(self.s.exact_prec)
+
     def balance(self, stream=None) -> None:
         check(L.lib().amgt_bsr_balance(ctypes.byref(self.s), _stream(stream)), "amgt_bsr_balance")
 

@@ -126,6 +126,10 @@ typedef struct {
     uint16_t *blcVal_bf16; /* [16 * blc_num] bfloat16 bits or NULL   */
     int max_blc_per_row; /* longest block row                        */
     int csr_nnz;         /* number of set bitmap bits (CSR nonzeros) */
+    int exact_prec;      /* AMGT_HALF / AMGT_FLOAT: that shadow holds every
+                            value exactly (amgt_bsr_make_exact), and fp64
+                            products read it with unchanged results;
+                            AMGT_DOUBLE (0): none                     */
 } amgt_bsr;
 
 /* Dense vector / column-major multivector, mirrors the fields of
@@ -169,6 +173,15 @@ AMGT_API int amgt_bsr_make_shadow(amgt_bsr *A, int prec, amgt_stream_t stream);
 AMGT_API int amgt_bsr_transpose(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream);
 
 /* Frees every array of *A (through the allocator) and zeroes the struct. */
+/* Exact narrow storage (no counterpart in the reference): checks whether
+ * every value of A is an fp16 value (else an fp32 value); if so builds that
+ * shadow and sets A->exact_prec, after which fp64 products (amgt_spmv,
+ * amgt_bsr_residual / _jacobi at AMGT_DOUBLE) read 2 or 4 bytes per value
+ * instead of 8 with bit-identical results.  Stencil operators with
+ * dyadic-rational coefficients and their interpolation / Galerkin
+ * products qualify.  One host read-back.  Call again after changing the
+ * values (or set exact_prec to AMGT_DOUBLE). */
+AMGT_API int amgt_bsr_make_exact(amgt_bsr *A, amgt_stream_t stream);
 AMGT_API int amgt_bsr_free(amgt_bsr *A, amgt_stream_t stream);
 AMGT_API int amgt_csr_free(amgt_csr *A, amgt_stream_t stream);
 
@@ -304,6 +317,9 @@ typedef struct {
     int smooth_prec0;      /* precision of the finest-level smoother SpMV   */
     int packed;            /* cycle / Krylov SpMVs on bitmap-packed values
                               (amgt_pbsr), default 0                        */
+    int exact_storage;     /* fp64 operators whose values fp16 / fp32 hold
+                              exactly are read from that shadow
+                              (amgt_bsr_make_exact; same results), default 1 */
 } amgt_amg_params;
 
 typedef struct amgt_amg amgt_amg;

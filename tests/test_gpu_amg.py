@@ -111,6 +111,24 @@ def test_amg_graph_and_direct_launches_agree_bit_for_bit(amgt, orc):
     assert torch.equal(x1, x2)
 
 
+def test_amg_exact_storage_changes_no_bit(amgt, orc):
+    """fp64 AMG-PCG with the operators read from exact fp16 / fp32 shadows
+    (exact_storage = 1, the default) returns the same x, bit for bit, and
+    the same iteration count as with 8-byte values."""
+    amgt.set_level_policy([0])
+    try:
+        dims = (40, 36, 32)
+        A = orc.laplacian(*dims)
+        Ps = orc.geometric_hierarchy(*dims)
+        b = torch.from_numpy(A.to_scipy() @ orc.rand_uniform(4, A.n)).cuda()
+        x1, it1, r1 = _gpu_solver(amgt, A, Ps, exact_storage=1).solve(b)
+        x0, it0, r0 = _gpu_solver(amgt, A, Ps, exact_storage=0).solve(b)
+        assert it1 == it0 and r1 == r0
+        assert torch.equal(x1.view(torch.int64), x0.view(torch.int64))
+    finally:
+        amgt.set_level_policy([])
+
+
 @pytest.mark.parametrize("policy,flexible", [([0, 1], 0), ([0, 1, 1, 2], 1), ([0, 1, 1, 3], 1)])
 def test_amg_mixed_precision_converges_fp64_verified(amgt, orc, policy, flexible):
     amgt.set_level_policy(policy)

@@ -4,6 +4,8 @@ fp64: |y_gpu - y_oracle| <= 1e-12 * (|alpha| sum|a||x| + |beta||y|) per row
 (the two sum in different fixed orders).  fp32 / fp16 / bf16: the values are
 the same rounded shadows on both sides and both accumulate in fp32, so the
 bound is 1e-5 of the same scale (fp32 summation-order differences)."""
+import ctypes
+
 import numpy as np
 import pytest
 import torch
@@ -125,3 +127,35 @@ def test_spmv_empty_matrix_scales_y(amgt, orc):
     y = torch.arange(10, dtype=torch.float64, device="cuda")
     G.spmv(torch.ones(7, dtype=torch.float64, device="cuda"), y, alpha=1.0, beta=3.0)
     np.testing.assert_array_equal(y.cpu().numpy(), 3.0 * np.arange(10))
+
+
+@pytest.mark.parametrize("name,want", [("7pt_24x20x16", 2), ("interp_T", 2), ("scaled_7pt", 1),
+                                       ("varcoef27_17x13x11", 0)])
+def test_exact_storage_is_bit_identical(amgt, orc, mats, name, want):
+    """amgt_bsr_make_exact picks the narrowest shadow that holds every value
+    exactly (fp16: 7-point and interpolation weights; fp32: a 7-point
+    operator scaled by 1 + 2^-12; none: variable coefficients), and fp64
+    products that read it give the fp64 results bit for bit."""
+    from amgt_b200 import _lib as L
+
+    if name == "scaled_7pt":
+        A = mats["7pt_24x20x16"]
+        A = orc.CSR(A.m, A.n, A.ia, A.ja, A.a * (1.0 + 2.0 ** -12))
+    else:
+        A = mats[name]
+    ref = amgt.Bsr.from_csr(*to_dev(A))
+    G = amgt.Bsr.from_csr(*to_dev(A))
+    assert G.make_exact() == want
+    x = torch.from_numpy(orc.rand_uniform(21, A.n)).cuda()
+    y0 = torch.from_numpy(orc.rand_uniform(22, A.m)).cuda()
+    for alpha, beta in ((1.0, 0.0), (-0.7, 1.0)):
+        y_ref, y = y0.clone(), y0.clone()
+        ref.spmv(x, y_ref, alpha=alpha, beta=beta)
+        G.spmv(x, y, alpha=alpha, beta=beta)
+        assert torch.equal(y.view(torch.int64), y_ref.view(torch.int64))
+    if A.m == A.n:  # fused residual r = f - A u
+        s = torch.cuda.current_stream().cuda_stream
+        r_ref, r = torch.empty_like(y0), torch.empty_like(y0)
+        assert L.lib().amgt_bsr_residual(0, ctypes.byref(ref.s), y0.data_ptr(), x.data_ptr(), r_ref.data_ptr(), s) == 0
+        assert L.lib().amgt_bsr_residual(0, ctypes.byref(G.s), y0.data_ptr(), x.data_ptr(), r.data_ptr(), s) == 0
+        assert torch.equal(r.view(torch.int64), r_ref.view(torch.int64))
