@@ -286,10 +286,37 @@ void destroy_handle(amgt_amg *h, cudaStream_t s)
     delete h;
 }
 
-double now_ms()
-{
-    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
-}
+// Setup phase times from events recorded in stream order (no host
+// synchronisation between phases): mark(p) closes an interval of phase p.
+struct PhaseMarks {
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> phase;
+    void mark(int p, cudaStream_t s)
+    {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess || cudaEventRecord(e, s) != cudaSuccess) {
+            cudaGetLastError();
+            if (e) cudaEventDestroy(e);
+            return;
+        }
+        ev.push_back(e);
+        phase.push_back(p);
+    }
+    void accumulate(double *ms)
+    {
+        if (!ev.empty() && cudaEventSynchronize(ev.back()) == cudaSuccess)
+            for (size_t i = 1; i < ev.size(); ++i) {
+                float t = 0.f;
+                if (phase[i] >= 0 && cudaEventElapsedTime(&t, ev[i - 1], ev[i]) == cudaSuccess) ms[phase[i]] += t;
+            }
+        cudaGetLastError();
+    }
+    ~PhaseMarks()
+    {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+};
+
 
 int grid_n(amgt_amg *h, long long n) { return grid_for(256, n, h->sm_count, 8); }
 
@@ -418,25 +445,21 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     int L = num_interp + 1;
     if (h->prm.max_levels > 0 && L > h->prm.max_levels) L = h->prm.max_levels;
     int rc = AMGT_OK;
-    double t0 = now_ms(), t1;
+    PhaseMarks pm;
+    pm.mark(-1, s);
     h->lv.resize(L);
     // hierarchy
     if ((rc = amgt_csr_to_bsr(A, &h->lv[0].A, stream))) goto fail;
     h->lv[0].n = A->num_rows;
-    AMGT_CUDA_TRY(cudaStreamSynchronize(s));
-    t1 = now_ms();
-    h->setup_ms[0] += t1 - t0;
+    pm.mark(0, s);
     for (int l = 0; l < L - 1; ++l) {
         Level &v = h->lv[l];
         if (P[l].num_rows != v.n || P[l].num_cols <= 0) { rc = AMGT_ERR_INVALID; goto fail; }
         v.prec = amgt_precision_for_level(l);
         v.prec_transfer = amgt_precision_for_level(l + 1);
-        t0 = now_ms();
         if ((rc = amgt_csr_to_bsr(&P[l], &v.P, stream))) goto fail;
         if ((rc = amgt_bsr_transpose(&v.P, &v.R, stream))) goto fail;
-        AMGT_CUDA_TRY(cudaStreamSynchronize(s));
-        t1 = now_ms();
-        h->setup_ms[1] += t1 - t0;
+        pm.mark(1, s);
         const int gp = h->prm.galerkin_by_level ? v.prec : AMGT_DOUBLE;
         amgt_bsr AP{};
         if ((rc = amgt_spgemm(gp, &v.A, &v.P, &AP, nullptr, stream))) goto fail;
@@ -444,12 +467,9 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         amgt_bsr_free(&AP, stream);
         if (rc) goto fail;
         h->lv[l + 1].n = h->lv[l + 1].A.row;
-        AMGT_CUDA_TRY(cudaStreamSynchronize(s));
-        t0 = now_ms();
-        h->setup_ms[2] += t0 - t1;
+        pm.mark(2, s);
     }
     h->lv[L - 1].prec = amgt_precision_for_level(L - 1);
-    t0 = now_ms();
     // exact narrow storage of the operators used in fp64 (level 0, fp64
     // levels and transfers): one value check each, one read-back per 15
     if (h->prm.exact_storage) {
@@ -464,14 +484,19 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         int64_t *flags = nullptr;
         if ((rc = alloc_n(&flags, mats.size(), s))) goto fail;
         AMGT_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int64_t) * mats.size(), s));
-        for (size_t i = 0; i < mats.size() && !rc; ++i) rc = bsr_exact_check(mats[i], flags + i, s, h->sm_count);
-        for (size_t i0 = 0; i0 < mats.size() && !rc; i0 += 15) {
-            const int k = (int)std::min<size_t>(15, mats.size() - i0);
+        std::vector<char> own16(mats.size(), 0);
+        for (size_t i = 0; i < mats.size() && !rc; ++i) {
+            bool o = false;
+            rc = bsr_exact_check(mats[i], flags + i, &o, s, h->sm_count);
+            own16[i] = o;
+        }
+        for (size_t i0 = 0; i0 < mats.size() && !rc; i0 += 63) {
+            const int k = (int)std::min<size_t>(63, mats.size() - i0);
             const int64_t *hf = nullptr;
             if ((rc = read_back(flags + i0, k, s, &hf))) break;
-            int64_t f[15];
+            int64_t f[63];
             for (int i = 0; i < k; ++i) f[i] = hf[i];  // the pinned slots are reused by the calls below
-            for (int i = 0; i < k && !rc; ++i) rc = bsr_exact_apply(mats[i0 + i], f[i], s);
+            for (int i = 0; i < k && !rc; ++i) rc = bsr_exact_apply(mats[i0 + i], f[i], own16[i0 + i] != 0, s);
         }
         free_ptr(flags, s);
         if (rc) goto fail;
@@ -530,8 +555,8 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         goto fail;
     AMGT_CUDA_TRY(cudaMemsetAsync(h->scal, 0, sizeof(double) * S_NSCAL, s));
     AMGT_CUDA_TRY(cudaMallocHost(&h->pinned, sizeof(double) * 4));
-    AMGT_CUDA_TRY(cudaStreamSynchronize(s));
-    h->setup_ms[3] += now_ms() - t0;
+    pm.mark(3, s);
+    pm.accumulate(h->setup_ms);  // waits for the setup's last work
     *out = h;
     return AMGT_OK;
 fail:

@@ -63,7 +63,7 @@ void free_ptr(T *&p, cudaStream_t s)
 // must read back.
 struct DeviceState {
     int *err;            // device: 0 = ok, else first error code raised
-    int64_t *pinned;     // host pinned, 16 slots
+    int64_t *pinned;     // host pinned, 64 slots (the last holds the error word)
     int sm_count;
 };
 int device_state(DeviceState **st);
@@ -118,16 +118,19 @@ int pbsr_dot(const amgt_pbsr *A, const double *u, double *out, double *partial, 
 // *flag (bit 0: not all fp32 values, bit 1: not all fp16 values; *flag
 // zeroed by the caller), then, with the flag read back, build the exact
 // shadow and set A->exact_prec.
-int bsr_exact_check(const amgt_bsr *A, int64_t *flag, cudaStream_t s, int sm_count);
-int bsr_exact_apply(amgt_bsr *A, int64_t flag, cudaStream_t s);
+// bsr_exact_check also writes the fp16 shadow (allocating it when absent:
+// *own16 set), so that fp16-exact matrices need no second pass.
+int bsr_exact_check(amgt_bsr *A, int64_t *flag, bool *own16, cudaStream_t s, int sm_count);
+int bsr_exact_apply(amgt_bsr *A, int64_t flag, bool own16, cudaStream_t s);
 
 // Exclusive scan of n ints (in may equal out), CUB with allocator scratch.
 int exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s);
 // Exclusive scan of n 64-bit ints.
 int exclusive_scan_i64(const int64_t *in, int64_t *out, int n, cudaStream_t s);
 
-// Device-to-host read of `count` int64 slots into DeviceState::pinned and a
-// stream synchronize; returns pointer to the pinned slots.
+// Device-to-host read of `count` (<= 63) int64 slots into
+// DeviceState::pinned and a stream synchronize; returns pointer to the
+// pinned slots.
 int read_back(const int64_t *dev, int count, cudaStream_t s, const int64_t **host);
 
 // ----------------------------------------------------------------- bitmaps

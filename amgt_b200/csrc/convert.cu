@@ -481,39 +481,52 @@ __global__ void shadow_kernel(long long n, const double *__restrict__ v, void *_
     }
 }
 
-// Exactness of stored values: bit 0 of *flags set when some value is not
-// an fp32 value, bit 1 when some value is not an fp16 value (round trip
+// Exactness of stored values, fused with the fp16 shadow: writes the
+// fp16 rounding of every value and sets bit 0 of *flags when some value is
+// not an fp32 value, bit 1 when some value is not an fp16 value (round trip
 // through the format changes it; NaN counts as inexact).
-__global__ void exact_check_kernel(long long n, const double *__restrict__ v, unsigned long long *flags)
+__global__ void exact_check_kernel(long long n, const double *__restrict__ v, __half *__restrict__ v16,
+                                   unsigned long long *flags)
 {
     bool not32 = false, not16 = false;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const double d = v[i];
+        const __half h = __double2half(d);
+        v16[i] = h;
         if ((double)__double2float_rn(d) != d) not32 = true;
-        if ((double)__half2float(__double2half(d)) != d) not16 = true;
+        if ((double)__half2float(h) != d) not16 = true;
     }
     const unsigned b32 = __ballot_sync(FULL, not32), b16 = __ballot_sync(FULL, not16);
     if ((threadIdx.x & 31) == 0 && (b32 | b16))
         atomicOr(flags, (b32 ? 1ull : 0ull) | (b16 ? 2ull : 0ull));
 }
 
-int bsr_exact_check(const amgt_bsr *A, int64_t *flag, cudaStream_t s, int sm_count)
+int bsr_exact_check(amgt_bsr *A, int64_t *flag, bool *own16, cudaStream_t s, int sm_count)
 {
+    *own16 = false;
     if (A->blc_num == 0) return AMGT_OK;
     const long long n = 16LL * A->blc_num;
+    if (!A->blcVal_fp16) {
+        AMGT_TRY(alloc_n(&A->blcVal_fp16, (size_t)n, s));
+        *own16 = true;
+    }
     AMGT_LAUNCH(exact_check_kernel, grid_for(256 * 4, n, sm_count, 8), 256, 0, s, n, A->blcVal,
-                (unsigned long long *)flag);
+                reinterpret_cast<__half *>(A->blcVal_fp16), (unsigned long long *)flag);
     return AMGT_OK;
 }
 
-int bsr_exact_apply(amgt_bsr *A, int64_t flag, cudaStream_t s)
+int bsr_exact_apply(amgt_bsr *A, int64_t flag, bool own16, cudaStream_t s)
 {
     A->exact_prec = AMGT_DOUBLE;
     if (A->blc_num == 0) return AMGT_OK;
-    const int prec = !(flag & 2) ? AMGT_HALF : !(flag & 1) ? AMGT_FLOAT : AMGT_DOUBLE;
-    if (prec == AMGT_DOUBLE) return AMGT_OK;
-    AMGT_TRY(amgt_bsr_make_shadow(A, prec, (amgt_stream_t)s));  // exact, so equal to any existing shadow
-    A->exact_prec = prec;
+    if (!(flag & 2)) {
+        A->exact_prec = AMGT_HALF;  // the fp16 shadow written by the check holds every value
+        return AMGT_OK;
+    }
+    if (own16) free_ptr(A->blcVal_fp16, s);  // speculative shadow not needed
+    if (flag & 1) return AMGT_OK;
+    AMGT_TRY(amgt_bsr_make_shadow(A, AMGT_FLOAT, (amgt_stream_t)s));  // exact, so equal to any existing shadow
+    A->exact_prec = AMGT_FLOAT;
     return AMGT_OK;
 }
 
@@ -844,9 +857,10 @@ int amgt_bsr_make_exact(amgt_bsr *A, amgt_stream_t stream)
     const int64_t *h = nullptr;
     int rc;
     if ((rc = alloc_n(&flag, 1, s))) return rc;
+    bool own16 = false;
     if (!(rc = (cudaMemsetAsync(flag, 0, sizeof(int64_t), s) == cudaSuccess) ? AMGT_OK : AMGT_ERR_CUDA) &&
-        !(rc = bsr_exact_check(A, flag, s, st->sm_count)) && !(rc = read_back(flag, 1, s, &h)))
-        rc = bsr_exact_apply(A, h[0], s);
+        !(rc = bsr_exact_check(A, flag, &own16, s, st->sm_count)) && !(rc = read_back(flag, 1, s, &h)))
+        rc = bsr_exact_apply(A, h[0], own16, s);
     free_ptr(flag, s);
     return rc;
 }

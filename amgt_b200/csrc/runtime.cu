@@ -197,7 +197,7 @@ int device_state(DeviceState **st)
         DeviceState &s = g_states[dev];
         AMGT_CUDA_TRY(cudaMalloc(&s.err, sizeof(int) * 4));
         AMGT_CUDA_TRY(cudaMemset(s.err, 0, sizeof(int) * 4));
-        AMGT_CUDA_TRY(cudaMallocHost(&s.pinned, sizeof(int64_t) * 16));
+        AMGT_CUDA_TRY(cudaMallocHost(&s.pinned, sizeof(int64_t) * 64));
         AMGT_CUDA_TRY(cudaDeviceGetAttribute(&s.sm_count, cudaDevAttrMultiProcessorCount, dev));
         g_state_ready[dev] = true;
     }
@@ -208,7 +208,7 @@ int device_state(DeviceState **st)
 // The error word as of the last read_back on this device (copied with it
 // into pinned slot kErrSlot, so no second synchronisation is needed); a
 // raised word is cleared on the stream and reported once.
-static constexpr int kErrSlot = 15;
+static constexpr int kErrSlot = 63;
 
 int check_device_error(cudaStream_t s)
 {
