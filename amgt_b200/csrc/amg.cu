@@ -20,7 +20,6 @@
 // Dots are deterministic: fixed grids, per-CTA partials reduced in a fixed
 // order by one CTA.
 #include <algorithm>
-#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
