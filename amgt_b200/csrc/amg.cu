@@ -285,6 +285,29 @@ void destroy_handle(amgt_amg *h, cudaStream_t s)
     delete h;
 }
 
+// The next level's interpolation, converted and transposed on a second
+// stream while the current level's products run (called from inside the
+// A * P SpGEMM, between its queued symbolic pass and its wait for C's
+// size); `ready` is recorded on that stream when P and R are complete.
+struct NextInterp {
+    const amgt_csr *P = nullptr;
+    amgt_bsr *Pb = nullptr, *Rb = nullptr;
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t ready = nullptr;
+    bool done = false;
+};
+
+int convert_next_interp(void *ctx)
+{
+    NextInterp *nx = static_cast<NextInterp *>(ctx);
+    if (!nx->P || nx->done) return AMGT_OK;
+    nx->done = true;
+    AMGT_TRY(amgt_csr_to_bsr(nx->P, nx->Pb, (amgt_stream_t)nx->s2));
+    AMGT_TRY(amgt_bsr_transpose(nx->Pb, nx->Rb, (amgt_stream_t)nx->s2));
+    AMGT_CUDA_TRY(cudaEventRecord(nx->ready, nx->s2));
+    return AMGT_OK;
+}
+
 // Setup phase times from events recorded in stream order (no host
 // synchronisation between phases): mark(p) closes an interval of phase p.
 struct PhaseMarks {
@@ -445,7 +468,14 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     if (h->prm.max_levels > 0 && L > h->prm.max_levels) L = h->prm.max_levels;
     int rc = AMGT_OK;
     PhaseMarks pm;
+    NextInterp nx;
     pm.mark(-1, s);
+    if (L > 2 && (cudaStreamCreateWithFlags(&nx.s2, cudaStreamNonBlocking) != cudaSuccess ||
+                  cudaEventCreateWithFlags(&nx.ready, cudaEventDisableTiming) != cudaSuccess)) {
+        cudaGetLastError();
+        rc = AMGT_ERR_CUDA;
+        goto fail;
+    }
     h->lv.resize(L);
     // hierarchy
     if ((rc = amgt_csr_to_bsr(A, &h->lv[0].A, stream))) goto fail;
@@ -456,12 +486,24 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         if (P[l].num_rows != v.n || P[l].num_cols <= 0) { rc = AMGT_ERR_INVALID; goto fail; }
         v.prec = amgt_precision_for_level(l);
         v.prec_transfer = amgt_precision_for_level(l + 1);
-        if ((rc = amgt_csr_to_bsr(&P[l], &v.P, stream))) goto fail;
-        if ((rc = amgt_bsr_transpose(&v.P, &v.R, stream))) goto fail;
-        pm.mark(1, s);
+        if (l == 0) {
+            if ((rc = amgt_csr_to_bsr(&P[l], &v.P, stream))) goto fail;
+            if ((rc = amgt_bsr_transpose(&v.P, &v.R, stream))) goto fail;
+            pm.mark(1, s);
+        } else {  // converted on the second stream during the previous level
+            if ((rc = convert_next_interp(&nx))) goto fail;
+            if (cudaStreamWaitEvent(s, nx.ready, 0) != cudaSuccess) {
+                rc = AMGT_ERR_CUDA;
+                goto fail;
+            }
+        }
         const int gp = h->prm.galerkin_by_level ? v.prec : AMGT_DOUBLE;
         amgt_bsr AP{};
-        if ((rc = amgt_spgemm(gp, &v.A, &v.P, &AP, nullptr, stream))) goto fail;
+        nx.P = (l + 1 < L - 1) ? &P[l + 1] : nullptr;
+        nx.Pb = &h->lv[l + 1].P;
+        nx.Rb = &h->lv[l + 1].R;
+        nx.done = false;
+        if ((rc = spgemm_impl(gp, &v.A, &v.P, &AP, nullptr, stream, convert_next_interp, &nx))) goto fail;
         rc = amgt_spgemm(gp, &v.R, &AP, &h->lv[l + 1].A, nullptr, stream);
         amgt_bsr_free(&AP, stream);
         if (rc) goto fail;
@@ -556,9 +598,17 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     AMGT_CUDA_TRY(cudaMallocHost(&h->pinned, sizeof(double) * 4));
     pm.mark(3, s);
     pm.accumulate(h->setup_ms);  // waits for the setup's last work
+    if (nx.s2) cudaStreamDestroy(nx.s2);
+    if (nx.ready) cudaEventDestroy(nx.ready);
     *out = h;
     return AMGT_OK;
 fail:
+    if (nx.s2) {  // its conversions may still use arrays the handle frees
+        cudaStreamSynchronize(nx.s2);
+        cudaStreamDestroy(nx.s2);
+    }
+    if (nx.ready) cudaEventDestroy(nx.ready);
+    cudaGetLastError();
     destroy_handle(h, s);
     return rc;
 }

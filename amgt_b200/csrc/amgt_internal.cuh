@@ -123,6 +123,11 @@ int pbsr_dot(const amgt_pbsr *A, const double *u, double *out, double *partial, 
 int bsr_exact_check(amgt_bsr *A, int64_t *flag, bool *own16, cudaStream_t s, int sm_count);
 int bsr_exact_apply(amgt_bsr *A, int64_t flag, bool own16, cudaStream_t s);
 
+// amgt_spgemm with a host callback run between the queued symbolic pass
+// and the wait for C's size (spgemm.cu).
+int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amgt_csr *Ccsr, amgt_stream_t stream,
+                int (*between)(void *), void *ctx);
+
 // Exclusive scan of n ints (in may equal out), CUB with allocator scratch.
 int exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s);
 // Exclusive scan of n 64-bit ints.

@@ -781,9 +781,14 @@ static void *shadow_of(const amgt_bsr *A, int prec)
 
 using namespace amgt;
 
-extern "C" {
+namespace amgt {
 
-int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amgt_csr *Ccsr, amgt_stream_t stream)
+// amgt_spgemm with an optional host callback `between`, run after the
+// symbolic kernels are queued and before the host waits for C's size:
+// host work that can overlap them (the AMG setup converts the next
+// level's interpolation there, on its own stream).
+int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amgt_csr *Ccsr, amgt_stream_t stream,
+                int (*between)(void *), void *ctx)
 {
     if (!A || !B || !C || prec < AMGT_DOUBLE || prec > AMGT_BF16) return AMGT_ERR_INVALID;
     if (A->col != B->row) return AMGT_ERR_INVALID;
@@ -879,6 +884,7 @@ int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     }
     if ((rc = exclusive_scan_int(csrcnt, csr_i, m + 1, s))) goto fail;
     AMGT_CUDA_TRY(cudaMemcpyAsync((int *)&stats[2] + 1, csr_i + m, sizeof(int), cudaMemcpyDeviceToDevice, s));
+    if (between && (rc = between(ctx))) goto fail;
     if ((rc = read_back(stats, 4, s, &h))) goto fail;
     nbC = (int)(h[2] & 0xFFFFFFFF);
     nnzC = (int)(h[2] >> 32);
@@ -942,6 +948,15 @@ fail:
     amgt_bsr_free(C, stream);
     if (Ccsr) amgt_csr_free(Ccsr, stream);
     return rc;
+}
+
+}  // namespace amgt
+
+extern "C" {
+
+int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amgt_csr *Ccsr, amgt_stream_t stream)
+{
+    return amgt::spgemm_impl(prec, A, B, C, Ccsr, stream, nullptr, nullptr);
 }
 
 }  // extern "C"
