@@ -470,15 +470,19 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     PhaseMarks pm;
     NextInterp nx;
     pm.mark(-1, s);
-    if (L > 2 && (cudaStreamCreateWithFlags(&nx.s2, cudaStreamNonBlocking) != cudaSuccess ||
+    if (L > 1 && (cudaStreamCreateWithFlags(&nx.s2, cudaStreamNonBlocking) != cudaSuccess ||
                   cudaEventCreateWithFlags(&nx.ready, cudaEventDisableTiming) != cudaSuccess)) {
         cudaGetLastError();
         rc = AMGT_ERR_CUDA;
         goto fail;
     }
     h->lv.resize(L);
-    // hierarchy
-    if ((rc = amgt_csr_to_bsr(A, &h->lv[0].A, stream))) goto fail;
+    // hierarchy; P_0 is converted and transposed on the second stream while
+    // A's conversion runs, P_{l+1} while level l's products run
+    nx.P = (L > 1) ? &P[0] : nullptr;
+    nx.Pb = &h->lv[0].P;
+    nx.Rb = &h->lv[0].R;
+    if ((rc = csr_to_bsr_impl(A, &h->lv[0].A, stream, convert_next_interp, &nx))) goto fail;
     h->lv[0].n = A->num_rows;
     pm.mark(0, s);
     for (int l = 0; l < L - 1; ++l) {
@@ -486,17 +490,13 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         if (P[l].num_rows != v.n || P[l].num_cols <= 0) { rc = AMGT_ERR_INVALID; goto fail; }
         v.prec = amgt_precision_for_level(l);
         v.prec_transfer = amgt_precision_for_level(l + 1);
-        if (l == 0) {
-            if ((rc = amgt_csr_to_bsr(&P[l], &v.P, stream))) goto fail;
-            if ((rc = amgt_bsr_transpose(&v.P, &v.R, stream))) goto fail;
-            pm.mark(1, s);
-        } else {  // converted on the second stream during the previous level
-            if ((rc = convert_next_interp(&nx))) goto fail;
-            if (cudaStreamWaitEvent(s, nx.ready, 0) != cudaSuccess) {
-                rc = AMGT_ERR_CUDA;
-                goto fail;
-            }
+        // P_l and R_l: converted on the second stream (no-op when done)
+        if ((rc = convert_next_interp(&nx))) goto fail;
+        if (cudaStreamWaitEvent(s, nx.ready, 0) != cudaSuccess) {
+            rc = AMGT_ERR_CUDA;
+            goto fail;
         }
+        pm.mark(1, s);
         const int gp = h->prm.galerkin_by_level ? v.prec : AMGT_DOUBLE;
         amgt_bsr AP{};
         nx.P = (l + 1 < L - 1) ? &P[l + 1] : nullptr;

@@ -128,6 +128,10 @@ int bsr_exact_apply(amgt_bsr *A, int64_t flag, bool own16, cudaStream_t s);
 int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amgt_csr *Ccsr, amgt_stream_t stream,
                 int (*between)(void *), void *ctx);
 
+// amgt_csr_to_bsr with a host callback run between the queued count pass
+// and the wait for the block count (convert.cu).
+int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int (*between)(void *), void *ctx);
+
 // Exclusive scan of n ints (in may equal out), CUB with allocator scratch.
 int exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s);
 // Exclusive scan of n 64-bit ints.

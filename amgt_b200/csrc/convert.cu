@@ -653,7 +653,15 @@ int amgt_csr_free(amgt_csr *A, amgt_stream_t stream)
     return AMGT_OK;
 }
 
-int amgt_csr_to_bsr(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream)
+}  // extern "C"
+
+namespace amgt {
+
+// amgt_csr_to_bsr with an optional host callback `between`, run after the
+// count pass is queued and before the host waits for the block count (host
+// work that can overlap it; the AMG setup converts the first
+// interpolation there, on its own stream).
+int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int (*between)(void *), void *ctx)
 {
     if (!csr_valid(A) || !out) return AMGT_ERR_INVALID;
     DeviceState *st;
@@ -700,6 +708,7 @@ int amgt_csr_to_bsr(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream)
     }
     if ((rc = exclusive_scan_int(cnt, out->blcPtr, brow + 1, s))) goto fail;
     AMGT_CUDA_TRY(cudaMemcpyAsync(&stats[2], out->blcPtr + brow, sizeof(int), cudaMemcpyDeviceToDevice, s));
+    if (between && (rc = between(ctx))) goto fail;
     if ((rc = read_back(stats, 4, s, &h))) goto fail;
     nb = (int)h[2];
     out->max_blc_per_row = (int)h[0];
@@ -740,6 +749,15 @@ fail:
     free_ptr(slotb, s);
     amgt_bsr_free(out, stream);
     return rc;
+}
+
+}  // namespace amgt
+
+extern "C" {
+
+int amgt_csr_to_bsr(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream)
+{
+    return amgt::csr_to_bsr_impl(A, out, stream, nullptr, nullptr);
 }
 
 int amgt_bsr_to_csr(const amgt_bsr *A, amgt_csr *out, amgt_stream_t stream)

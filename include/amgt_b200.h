@@ -336,8 +336,10 @@ AMGT_API int amgt_amg_solve(amgt_amg *amg, const double *b, double *x,
 AMGT_API int amgt_amg_num_levels(const amgt_amg *amg);
 /* Borrowed view of level `level`'s operator and its cycle precision. */
 AMGT_API int amgt_amg_level(const amgt_amg *amg, int level, amgt_bsr *A_view, int *prec);
-/* ms[0..3]: conversion of A, P conversion + transpose, Galerkin SpGEMMs,
- * smoother data + shadows + coarse inverse + vectors. */
+/* ms[0..3], stream time between phase ends: conversion of A, waits for the
+ * interpolation operators (converted and transposed on a second stream,
+ * overlapping the other phases), Galerkin SpGEMMs, smoother data + exact
+ * and reduced-precision shadows + coarse inverse + vectors. */
 AMGT_API int amgt_amg_setup_times(const amgt_amg *amg, double *ms);
 /* Relative residual per iteration (entry 0 = initial); returns the count. */
 AMGT_API int amgt_amg_residual_history(const amgt_amg *amg, double *hist, int cap);
