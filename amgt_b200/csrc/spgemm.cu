@@ -122,29 +122,49 @@ __device__ __forceinline__ long long sym_upper_bound(int lane, int a0, int a1, c
 }
 
 // Sorted distinct keys with OR-ed bitmaps of the warp's list s[0..cnt),
-// cnt <= 32 (one pair per lane, a register sort).  Writes them to
-// cidx/cmap, the index of each pair's C block to pslot (by the pair's tag,
-// its ordinal in the row), and returns the distinct count and the
-// per-scalar-row CSR counts (popcount of each bitmap nibble).
+// cnt <= 32 (one pair per lane).  Lanes with equal keys match
+// (__match_any_sync); the lowest lane of each group is its leader, and a
+// key's rank among the distinct keys comes from comparing it with every
+// leader's key, so no sort is needed.  The group's bitmaps are OR-ed in
+// shared memory (s[] is reused for that once the pairs are in registers).
+// Writes the distinct keys in ascending order to cidx/cmap, the index of
+// each pair's C block to pslot (by the pair's tag, its ordinal in the row),
+// and returns the distinct count and the per-scalar-row CSR counts
+// (popcount of each bitmap nibble).
 __device__ __forceinline__ int sym_reduce32(int lane, int cnt, unsigned long long *s, int *__restrict__ cidx,
                                             uint16_t *__restrict__ cmap, int csr[4], uint16_t *__restrict__ pslot)
 {
-    csr[0] = csr[1] = csr[2] = csr[3] = 0;
-    unsigned long long v = (lane < cnt) ? s[lane] : kSentinel;
+    const bool valid = lane < cnt;
+    const unsigned long long v = valid ? s[lane] : kSentinel;
+    const int key = valid ? pair_key(v) : -1 - lane;
+    const unsigned peers = __match_any_sync(FULL, key);
+    const bool leader = valid && (__ffs(peers) - 1) == lane;
+    unsigned lm = __ballot_sync(FULL, leader);
+    const int u = __popc(lm);
+    int rank = 0;
+    while (lm) {  // warp-uniform: the distinct keys
+        const int l = __ffs(lm) - 1;
+        lm &= lm - 1;
+        rank += __shfl_sync(FULL, key, l) < key;
+    }
+    unsigned *so = reinterpret_cast<unsigned *>(s);
     __syncwarp();
-    v = warp_sort32(v, lane);
-    uint32_t orv;
-    const bool head = warp_runs32(v, lane, &orv);
-    const unsigned hb = __ballot_sync(FULL, head);
-    const int u = __popc(hb);
-    if (v != kSentinel) pslot[pair_tag(v)] = (uint16_t)(__popc(hb & ((2u << lane) - 1u)) - 1);
-    if (head) {
-        const int slot = __popc(hb & lanemask_lt(lane));
-        cidx[slot] = pair_key(v);
-        cmap[slot] = (uint16_t)orv;
+    so[lane] = 0;
+    __syncwarp();
+    if (valid) {
+        atomicOr(&so[rank], pair_map(v));
+        pslot[pair_tag(v)] = (uint16_t)rank;
+    }
+    __syncwarp();
+    csr[0] = csr[1] = csr[2] = csr[3] = 0;
+    if (leader) {
+        const uint32_t orv = so[rank];
+        cidx[rank] = key;
+        cmap[rank] = (uint16_t)orv;
 #pragma unroll
         for (int q = 0; q < 4; ++q) csr[q] = __popc((orv >> (4 * q)) & 0xFu);
     }
+    __syncwarp();
 #pragma unroll
     for (int q = 0; q < 4; ++q) csr[q] = warp_sum(csr[q]);
     return u;
@@ -199,15 +219,16 @@ __device__ int sym_reduce_hashed(int lane, int cnt, unsigned long long *s, int *
     }
     __syncwarp();
     csr[0] = csr[1] = csr[2] = csr[3] = 0;
-    if (u <= 32) {
-        unsigned long long v = (lane < u) ? s[lane] : kSentinel;
-        __syncwarp();
-        v = warp_sort32(v, lane);
-        if (v != kSentinel) {
+    if (u <= 32) {  // distinct keys: rank each by comparing with all u
+        const unsigned long long v = (lane < u) ? s[lane] : kSentinel;
+        const int key = pair_key(v);
+        int rank = 0;
+        for (int l = 0; l < u; ++l) rank += __shfl_sync(FULL, key, l) < key;
+        if (lane < u) {
             const uint32_t mp = pair_map(v);
-            cidx[lane] = pair_key(v);
-            cmap[lane] = (uint16_t)mp;
-            tval[pair_tag(v)] = (unsigned)lane;  // rank of the column
+            cidx[rank] = key;
+            cmap[rank] = (uint16_t)mp;
+            tval[pair_tag(v)] = (unsigned)rank;  // rank of the column
 #pragma unroll
             for (int q = 0; q < 4; ++q) csr[q] = __popc((mp >> (4 * q)) & 0xFu);
         }
