@@ -38,6 +38,7 @@ enum { OP_STORE = 0, OP_ALPHA = 1, OP_BETA = 2, OP_BETA_FLEX = 3 };
 __global__ void __launch_bounds__(kDotThreads) dot_kernel(long long n, const double *__restrict__ a,
                                                          const double *__restrict__ b, double *__restrict__ part)
 {
+    grid_dependency_wait();
     __shared__ double sred[kDotThreads / 32];
     double s = 0.0;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -57,6 +58,7 @@ __global__ void __launch_bounds__(kDotThreads) dot_kernel(long long n, const dou
 __global__ void __launch_bounds__(kDotThreads) reduce_kernel(const double *__restrict__ part, int np,
                                                             double *__restrict__ scal, int slot, int op)
 {
+    grid_dependency_wait();
     __shared__ double sred[kDotThreads / 32];
     double s = 0.0;
     for (int i = threadIdx.x; i < np; i += blockDim.x) s += part[i];
@@ -87,6 +89,7 @@ __global__ void __launch_bounds__(kDotThreads) axpy2_dot_kernel(long long n, con
                                                                const double *__restrict__ q, double *__restrict__ x,
                                                                double *__restrict__ r, double *__restrict__ part)
 {
+    grid_dependency_wait();
     __shared__ double sred[kDotThreads / 32];
     const double alpha = scal[S_ALPHA];
     double s = 0.0;
@@ -111,6 +114,7 @@ __global__ void __launch_bounds__(kDotThreads) axpy2_dot_kernel(long long n, con
 __global__ void xpby_kernel(long long n, const double *__restrict__ z, const double *__restrict__ scal,
                             double *__restrict__ p)
 {
+    grid_dependency_wait();
     const double beta = scal[S_BETA];
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         p[i] = z[i] + beta * p[i];
@@ -120,6 +124,7 @@ __global__ void xpby_kernel(long long n, const double *__restrict__ z, const dou
 __global__ void jacobi_zero_kernel(long long n, const double *__restrict__ f, const double *__restrict__ inv_l1,
                                    double w, double *__restrict__ u)
 {
+    grid_dependency_wait();
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         u[i] = w * f[i] * inv_l1[i];
 }
@@ -128,6 +133,7 @@ __global__ void jacobi_zero_kernel(long long n, const double *__restrict__ f, co
 __global__ void dense_mv_kernel(int nc, const double *__restrict__ M, const double *__restrict__ f,
                                 double *__restrict__ u)
 {
+    grid_dependency_wait();
     const int lane = threadIdx.x & 31;
     for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nc; row += (gridDim.x * blockDim.x) >> 5) {
         double s = 0.0;
@@ -352,7 +358,7 @@ int cycle(amgt_amg *h, const double *rhs0, double *out0, cudaStream_t s)
     for (int l = 0; l < L - 1; ++l) {
         Level &v = lv[l];
         const double *f = (l == 0) ? rhs0 : v.f;
-        AMGT_LAUNCH(jacobi_zero_kernel, grid_n(h, v.n), 256, 0, s, (long long)v.n, f, v.inv_l1, w, v.u);
+        AMGT_LAUNCH_PDL(jacobi_zero_kernel, grid_n(h, v.n), 256, 0, s, (long long)v.n, f, v.inv_l1, w, v.u);
         if (pk) {
             AMGT_TRY(pbsr_residual(&v.pA, f, v.u, v.t, s, h->sm_count));
             AMGT_TRY(pbsr_spmv(&v.pR, 1.0, v.t, 0.0, lv[l + 1].f, s, h->sm_count));
@@ -364,7 +370,7 @@ int cycle(amgt_amg *h, const double *rhs0, double *out0, cudaStream_t s)
     Level &c = lv[L - 1];
     const double *fc = (L == 1) ? rhs0 : c.f;
     double *uc = (L == 1) ? out0 : c.s;
-    AMGT_LAUNCH(dense_mv_kernel, grid_for(8, c.n, h->sm_count, 8), 256, 0, s, c.n, h->coarse_inv, fc, uc);
+    AMGT_LAUNCH_PDL(dense_mv_kernel, grid_for(8, c.n, h->sm_count, 8), 256, 0, s, c.n, h->coarse_inv, fc, uc);
     for (int l = L - 2; l >= 0; --l) {
         Level &v = lv[l];
         const double *f = (l == 0) ? rhs0 : v.f;
@@ -383,8 +389,8 @@ int cycle(amgt_amg *h, const double *rhs0, double *out0, cudaStream_t s)
 
 int dot(amgt_amg *h, const double *a, const double *b, int slot, int op, cudaStream_t s)
 {
-    AMGT_LAUNCH(dot_kernel, kDotGrid, kDotThreads, 0, s, h->n0, a, b, h->part);
-    AMGT_LAUNCH(reduce_kernel, 1, kDotThreads, 0, s, h->part, kDotGrid, h->scal, slot, op);
+    AMGT_LAUNCH_PDL(dot_kernel, kDotGrid, kDotThreads, 0, s, h->n0, a, b, h->part);
+    AMGT_LAUNCH_PDL(reduce_kernel, 1, kDotThreads, 0, s, h->part, kDotGrid, h->scal, slot, op);
     return AMGT_OK;
 }
 
@@ -394,14 +400,14 @@ int pcg_iteration(amgt_amg *h, double *x, cudaStream_t s)
     Level &v0 = h->lv[0];
     if (h->prm.packed) AMGT_TRY(pbsr_dot(&v0.pA, h->p, h->q, h->part, h->grid0, s));
     else AMGT_TRY(spmv_dot(AMGT_DOUBLE, &v0.A, h->p, h->q, h->part, h->grid0, s));
-    AMGT_LAUNCH(reduce_kernel, 1, kDotThreads, 0, s, h->part, h->grid0, h->scal, (int)S_PQ, (int)OP_ALPHA);
-    AMGT_LAUNCH(axpy2_dot_kernel, kDotGrid, kDotThreads, 0, s, h->n0, h->scal, h->p, h->q, x, h->r, h->part);
-    AMGT_LAUNCH(reduce_kernel, 1, kDotThreads, 0, s, h->part, kDotGrid, h->scal, (int)S_RR, (int)OP_STORE);
+    AMGT_LAUNCH_PDL(reduce_kernel, 1, kDotThreads, 0, s, h->part, h->grid0, h->scal, (int)S_PQ, (int)OP_ALPHA);
+    AMGT_LAUNCH_PDL(axpy2_dot_kernel, kDotGrid, kDotThreads, 0, s, h->n0, h->scal, h->p, h->q, x, h->r, h->part);
+    AMGT_LAUNCH_PDL(reduce_kernel, 1, kDotThreads, 0, s, h->part, kDotGrid, h->scal, (int)S_RR, (int)OP_STORE);
     AMGT_CUDA_TRY(cudaMemcpyAsync(h->pinned, h->scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, s));
     if (h->prm.flexible) AMGT_TRY(dot(h, h->z, h->r, S_ZRPREV, OP_STORE, s));
     AMGT_TRY(cycle(h, h->r, h->z, s));
     AMGT_TRY(dot(h, h->r, h->z, S_RZ, h->prm.flexible ? OP_BETA_FLEX : OP_BETA, s));
-    AMGT_LAUNCH(xpby_kernel, grid_n(h, h->n0), 256, 0, s, h->n0, h->z, h->scal, h->p);
+    AMGT_LAUNCH_PDL(xpby_kernel, grid_n(h, h->n0), 256, 0, s, h->n0, h->z, h->scal, h->p);
     return AMGT_OK;
 }
 

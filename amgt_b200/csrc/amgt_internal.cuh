@@ -38,6 +38,33 @@ void count_launch();
         AMGT_CUDA_TRY(cudaGetLastError());                                    \
     } while (0)
 
+// Launch with programmatic dependent launch (solve-path kernels): the grid
+// may be scheduled while the previous kernel on the stream is finishing,
+// which hides most of the launch gap between dependent kernels (also inside
+// CUDA graphs, where capture turns it into a programmatic edge).  Every
+// kernel launched this way calls grid_dependency_wait() before it touches
+// memory; without a programmatic dependency the wait returns at once.
+#define AMGT_LAUNCH_PDL(kernel, grid, block, smem, strm, ...)                 \
+    do {                                                                      \
+        amgt::count_launch();                                                 \
+        cudaLaunchConfig_t _cfg = {};                                         \
+        _cfg.gridDim = dim3(grid);                                            \
+        _cfg.blockDim = dim3(block);                                          \
+        _cfg.dynamicSmemBytes = (smem);                                       \
+        _cfg.stream = (strm);                                                 \
+        cudaLaunchAttribute _at[1];                                           \
+        _at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;       \
+        _at[0].val.programmaticStreamSerializationAllowed = 1;                \
+        _cfg.attrs = _at;                                                     \
+        _cfg.numAttrs = 1;                                                    \
+        AMGT_CUDA_TRY(cudaLaunchKernelEx(&_cfg, kernel, __VA_ARGS__));        \
+    } while (0)
+
+__device__ __forceinline__ void grid_dependency_wait()
+{
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+}
+
 // ------------------------------------------------------------- allocation
 void *dev_alloc(size_t bytes, cudaStream_t s);
 void dev_free(void *p, cudaStream_t s);

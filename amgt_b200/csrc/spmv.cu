@@ -67,6 +67,7 @@ spmv_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__re
             const void *__restrict__ val, double alpha, const double *__restrict__ x, double beta,
             double *__restrict__ y)
 {
+    grid_dependency_wait();
     using acc_t = typename ValTraits<PREC>::acc_t;
     constexpr int RPW = 32 / LPR;  // block rows per warp
     constexpr int G = LPR / 4;     // blocks in flight per row
@@ -205,6 +206,7 @@ __global__ void __launch_bounds__(256)
 spmv_epi_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__restrict__ idx,
                 const void *__restrict__ val, const double *__restrict__ x, EpiArgs e)
 {
+    grid_dependency_wait();
     using acc_t = typename ValTraits<PREC>::acc_t;
     constexpr int RPW = 32 / LPR;
     constexpr int G = LPR / 4;
@@ -329,10 +331,10 @@ static int launch_spmv(const amgt_bsr *A, const void *val, double alpha, const d
 #define AMGT_SPMV_CASE(L)                                                                                   \
     if (lpr == L) {                                                                                         \
         if (safe)                                                                                           \
-            AMGT_LAUNCH((spmv_kernel<PREC, L, true>), grid, 256, 0, s, A->row, A->col, brow, A->blcPtr,     \
+            AMGT_LAUNCH_PDL((spmv_kernel<PREC, L, true>), grid, 256, 0, s, A->row, A->col, brow, A->blcPtr,     \
                         A->blcIdx, val, alpha, x, beta, y);                                                 \
         else                                                                                                \
-            AMGT_LAUNCH((spmv_kernel<PREC, L, false>), grid, 256, 0, s, A->row, A->col, brow, A->blcPtr,    \
+            AMGT_LAUNCH_PDL((spmv_kernel<PREC, L, false>), grid, 256, 0, s, A->row, A->col, brow, A->blcPtr,    \
                         A->blcIdx, val, alpha, x, beta, y);                                                 \
         return AMGT_OK;                                                                                     \
     }
@@ -451,10 +453,10 @@ static int launch_epi(const amgt_bsr *A, const void *val, const double *x, const
 #define AMGT_EPI_CASE(L)                                                                                     \
     if (lpr == L) {                                                                                          \
         if (safe)                                                                                            \
-            AMGT_LAUNCH((spmv_epi_kernel<PREC, L, true, EPI>), grid, 256, 0, s, A->row, A->col, A->blc_row,  \
+            AMGT_LAUNCH_PDL((spmv_epi_kernel<PREC, L, true, EPI>), grid, 256, 0, s, A->row, A->col, A->blc_row,  \
                         A->blcPtr, A->blcIdx, val, x, e);                                                    \
         else                                                                                                 \
-            AMGT_LAUNCH((spmv_epi_kernel<PREC, L, false, EPI>), grid, 256, 0, s, A->row, A->col, A->blc_row, \
+            AMGT_LAUNCH_PDL((spmv_epi_kernel<PREC, L, false, EPI>), grid, 256, 0, s, A->row, A->col, A->blc_row, \
                         A->blcPtr, A->blcIdx, val, x, e);                                                    \
         return AMGT_OK;                                                                                      \
     }
