@@ -476,8 +476,11 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     PhaseMarks pm;
     NextInterp nx;
     pm.mark(-1, s);
+    // the second stream starts after everything the caller queued on `s`
+    // before this call (the inputs may still be arriving there)
     if (L > 1 && (cudaStreamCreateWithFlags(&nx.s2, cudaStreamNonBlocking) != cudaSuccess ||
-                  cudaEventCreateWithFlags(&nx.ready, cudaEventDisableTiming) != cudaSuccess)) {
+                  cudaEventCreateWithFlags(&nx.ready, cudaEventDisableTiming) != cudaSuccess ||
+                  cudaEventRecord(nx.ready, s) != cudaSuccess || cudaStreamWaitEvent(nx.s2, nx.ready, 0) != cudaSuccess)) {
         cudaGetLastError();
         rc = AMGT_ERR_CUDA;
         goto fail;

@@ -111,6 +111,37 @@ def test_amg_graph_and_direct_launches_agree_bit_for_bit(amgt, orc):
     assert torch.equal(x1, x2)
 
 
+def test_amg_setup_orders_inputs_still_being_copied(amgt, orc):
+    """Setup runs part of its work on a second stream; inputs whose copies
+    from pinned host memory are still in flight on the caller's stream must
+    be complete before that stream reads them (same x, bit for bit, as with
+    blocking copies)."""
+    from amgt_b200.amg import AmgSolver, default_params
+
+    amgt.set_level_policy([0])
+    try:
+        dims = (40, 36, 32)
+        A = orc.laplacian(*dims)
+        Ps = orc.geometric_hierarchy(*dims)
+        b = orc.rand_uniform(4, A.n)
+
+        def pinned(M):
+            return (M.m, M.n) + tuple(torch.from_numpy(v).pin_memory() for v in (M.ia, M.ja, M.a))
+
+        def nonblocking(M):
+            return M[:2] + tuple(t.cuda(non_blocking=True) for t in M[2:])
+
+        hA, hPs = pinned(A), [pinned(P) for P in Ps]
+        torch.cuda.synchronize()
+        S = AmgSolver(nonblocking(hA), [nonblocking(P) for P in hPs], default_params())
+        x1, it1, _ = S.solve(torch.from_numpy(b).pin_memory().cuda(non_blocking=True))
+        x0, it0, _ = _gpu_solver(amgt, A, Ps).solve(torch.from_numpy(b).cuda())
+        assert it1 == it0
+        assert torch.equal(x1.view(torch.int64), x0.view(torch.int64))
+    finally:
+        amgt.set_level_policy([])
+
+
 def test_amg_exact_storage_changes_no_bit(amgt, orc):
     """fp64 AMG-PCG with the operators read from exact fp16 / fp32 shadows
     (exact_storage = 1, the default) returns the same x, bit for bit, and
