@@ -181,7 +181,31 @@ def run_reference(args):
 
 
 # -------------------------------------------------------------------- GPU
-def build_hierarchy(amgt, torch, A, grid, max_levels=8, min_rows=512):
+def spgemm_work(Ah: dict, Bh: dict) -> dict:
+    """Work of C = A * B on mBSR (host arrays from Bsr.host()): the (A block,
+    B block) pairs, those with a non-zero bitmap product, and the flop counts
+    useful = 2 * sum over pairs and k of popc(column k of A's bitmap) *
+    popc(row k of B's bitmap), block = 128 per pair with a non-zero product."""
+    bptr = Bh["bptr"].astype(np.int64)
+    lens = bptr[Ah["bidx"] + 1] - bptr[Ah["bidx"]]
+    npairs = int(lens.sum())
+    if npairs == 0:
+        return {"pairs": 0, "pairs_nonzero": 0, "flops_useful": 0, "flops_block": 0}
+    a_of = np.repeat(np.arange(len(lens)), lens)
+    first = np.repeat(np.cumsum(lens) - lens, lens)
+    b_of = bptr[Ah["bidx"]][a_of] + (np.arange(npairs) - first)
+    ma = Ah["bmap"].astype(np.int64)[a_of]
+    mb = Bh["bmap"].astype(np.int64)[b_of]
+    pc = np.array([bin(i).count("1") for i in range(16)], dtype=np.int64)
+    useful = np.zeros(npairs, dtype=np.int64)
+    for k in range(4):
+        colk = ((ma >> k) & 1) + ((ma >> (k + 4)) & 1) + ((ma >> (k + 8)) & 1) + ((ma >> (k + 12)) & 1)
+        useful += colk * pc[(mb >> (4 * k)) & 0xF]
+    nz = int(np.count_nonzero(useful))
+    return {"pairs": npairs, "pairs_nonzero": nz, "flops_useful": int(2 * useful.sum()), "flops_block": 128 * nz}
+
+
+def build_hierarchy(amgt, torch, A, grid, max_levels=8, min_rows=512, work=False):
     """Galerkin hierarchy A_{l+1} = P^T (A_l P) with linear interpolation P;
     returns (per-level info, [A_0, A_1, ...])."""
     from amgt_b200 import problems
@@ -209,6 +233,12 @@ def build_hierarchy(amgt, torch, A, grid, max_levels=8, min_rows=512):
         RAP, _ = amgt.spgemm(R, AP, want_csr=True)
         torch.cuda.synchronize()
         t3 = time.perf_counter()
+        if work:  # host-side counts, outside the timed products
+            Ah, Ph, Rh, APh = Ab.host(), P.host(), R.host(), AP.host()
+            wa, wr = spgemm_work(Ah, Ph), spgemm_work(Rh, APh)
+            info.update({"AP_work": wa, "RAP_work": wr,
+                         "AP_gflops_block": round(wa["flops_block"] / (t1 - t0) / 1e9, 1),
+                         "RAP_gflops_block": round(wr["flops_block"] / (t3 - t2) / 1e9, 1)})
         info.update({"AP_ms": round(1e3 * (t1 - t0), 3), "PT_ms": round(1e3 * (t2 - t1), 3),
                      "RAP_ms": round(1e3 * (t3 - t2), 3), "P_blocks": P.nblk, "AP_blocks": AP.nblk})
         mats.append(RAP)
@@ -401,7 +431,7 @@ def run_amgt(args):
     levels, mats = [], []
     if not args.no_levels:
         build_hierarchy(amgt, torch, A, GRID)  # warm-up pass, result dropped
-        levels, mats = build_hierarchy(amgt, torch, A, GRID)
+        levels, mats = build_hierarchy(amgt, torch, A, GRID, work=True)
     for lvl, Ab in enumerate(mats):
         xx = torch.zeros(Ab.s.col, dtype=torch.float64, device="cuda").uniform_(-1, 1)
         yy = torch.zeros(Ab.s.row, dtype=torch.float64, device="cuda")
