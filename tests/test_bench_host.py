@@ -69,3 +69,27 @@ def test_reference_arm_rank_nonzero_prints_nothing():
                         "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=300, cwd=ROOT,
                        env=env)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_spgemm_work_counts_match_brute_force(orc):
+    """bench.spgemm_work (pairs, non-zero bitmap products, useful and block
+    flops of an mBSR product) against a per-entry count."""
+    import bench
+
+    A = orc.varcoef27(9, 8, 7, seed=2)
+    P, _ = orc.interp(9, 8, 7)
+    BA, BP = orc.csr2bsr(A), orc.csr2bsr(P)
+    w = bench.spgemm_work({"bptr": BA.bptr, "bidx": BA.bidx, "bmap": BA.bmap},
+                          {"bptr": BP.bptr, "bidx": BP.bidx, "bmap": BP.bmap})
+    pairs = nz = useful = 0
+    for i in range(BA.brow):
+        for p in range(BA.bptr[i], BA.bptr[i + 1]):
+            ma, k = int(BA.bmap[p]), BA.bidx[p]
+            for q in range(BP.bptr[k], BP.bptr[k + 1]):
+                mb = int(BP.bmap[q])
+                u = sum(((ma >> (4 * r + kk)) & 1) * ((mb >> (4 * kk + c)) & 1)
+                        for r in range(4) for kk in range(4) for c in range(4))
+                pairs += 1
+                nz += u > 0
+                useful += u
+    assert w == {"pairs": pairs, "pairs_nonzero": nz, "flops_useful": 2 * useful, "flops_block": 128 * nz}
