@@ -238,9 +238,55 @@ int read_back(const int64_t *dev, int count, cudaStream_t s, const int64_t **hos
 }
 
 // ------------------------------------------------------------------ scans
+// Exclusive sum of up to kSmallScan entries in one launch of one CTA
+// (CUB's scan takes two launches and a scratch allocation, which dominates
+// the small arrays of coarse AMG levels).  Thread t sums a contiguous
+// segment, the CTA scans the segment sums, and each thread writes its
+// segment; in == out is allowed (every entry is read before it is written).
+constexpr int kSmallScan = 32768;
+
+template <typename T>
+__global__ void __launch_bounds__(1024) scan_small_kernel(const T *in, T *out, int n)
+{
+    __shared__ T wsum[32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int per = (n + 1023) / 1024;
+    const int b = min(t * per, n), e = min(b + per, n);
+    T sum = 0;
+    for (int i = b; i < e; ++i) sum += in[i];
+    T incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const T y = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        T w = wsum[lane], wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const T y = __shfl_up_sync(FULL, wi, o);
+            if (lane >= o) wi += y;
+        }
+        wsum[lane] = wi - w;  // exclusive over warps
+    }
+    __syncthreads();
+    T run = wsum[warp] + incl - sum;
+    for (int i = b; i < e; ++i) {
+        const T v = in[i];
+        out[i] = run;
+        run += v;
+    }
+}
+
 int exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s)
 {
     if (n <= 0) return AMGT_OK;
+    if (n <= kSmallScan) {
+        AMGT_LAUNCH(scan_small_kernel<int>, 1, 1024, 0, s, in, out, n);
+        return AMGT_OK;
+    }
     size_t bytes = 0;
     AMGT_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, s));
     void *tmp = dev_alloc(bytes ? bytes : 16, s);
@@ -255,6 +301,11 @@ int exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s)
 int exclusive_scan_i64(const int64_t *in, int64_t *out, int n, cudaStream_t s)
 {
     if (n <= 0) return AMGT_OK;
+    if (n <= kSmallScan) {
+        AMGT_LAUNCH(scan_small_kernel<long long>, 1, 1024, 0, s, reinterpret_cast<const long long *>(in),
+                    reinterpret_cast<long long *>(out), n);
+        return AMGT_OK;
+    }
     size_t bytes = 0;
     AMGT_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, s));
     void *tmp = dev_alloc(bytes ? bytes : 16, s);
