@@ -406,25 +406,44 @@ def run_amgt(args):
               "speedup_vs_16_value_blocks": round(ms / pms, 3)}
     del Apk
 
-    # e2e: host x in, host y out, through the C ABI, every step
+    # e2e: host x in, host y out, through the C ABI, every step.  Serial:
+    # upload, product, download on one stream.  Pipelined: steps alternate
+    # between two streams with their own x / y, so one step's y download
+    # (device -> host) runs while the next step's x upload (host -> device)
+    # does; every step still moves its full x and y across PCIe.
     xh = torch.from_numpy(x_host).pin_memory()
-    yh = torch.empty(m, dtype=torch.float64).pin_memory()
-    for _ in range(2):
-        x.copy_(xh, non_blocking=True)
-        A.spmv(x, y)
-        yh.copy_(y, non_blocking=True)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    ev0.record(stream)
-    for _ in range(args.steps):
-        x.copy_(xh, non_blocking=True)
-        A.spmv(x, y)
-        yh.copy_(y, non_blocking=True)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = ev0.elapsed_time(ev1) / args.steps
-    e2e_value = whole_job_gbs(nbytes, max_over_ranks(e2e_ms, device="cuda"), world)
+    yhs = [torch.empty(m, dtype=torch.float64).pin_memory() for _ in range(2)]
+    xs, ys = [x, torch.empty_like(x)], [y, torch.empty_like(y)]
+    streams = [stream, torch.cuda.Stream()]
+
+    def e2e_step(i, pipelined):
+        j = i % 2 if pipelined else 0
+        with torch.cuda.stream(streams[j]):
+            xs[j].copy_(xh, non_blocking=True)
+            A.spmv(xs[j], ys[j])
+            yhs[j].copy_(ys[j], non_blocking=True)
+
+    def e2e_time(pipelined):
+        for i in range(2):
+            e2e_step(i, pipelined)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ev0.record(stream)
+        streams[1].wait_event(ev0)
+        for i in range(args.steps):
+            e2e_step(i, pipelined)
+        stream.wait_stream(streams[1])
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(ev0.elapsed_time(ev1) / args.steps, device="cuda")
+
+    e2e_serial_ms = e2e_time(False)
+    e2e_ms = e2e_time(True)
+    e2e_value = whole_job_gbs(nbytes, e2e_ms, world)
+    e2e_serial = whole_job_gbs(nbytes, e2e_serial_ms, world)
+    if not torch.equal(yhs[0], yhs[1]):
+        raise RuntimeError("pipelined e2e steps disagree")
 
     # hierarchy: RAP per level and SpMV GB/s per level (not part of `value`);
     # built twice, the first pass loading the kernels' modules
@@ -514,7 +533,8 @@ def run_amgt(args):
                      else "fallback"},
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": 8 * n,
-                "d2h_bytes_per_step": 8 * m},
+                "d2h_bytes_per_step": 8 * m, "pipelined": "two streams: step k's y download overlaps step k+1's "
+                "x upload", "serial_value": round(e2e_serial, 2)},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "levels": levels,
