@@ -57,37 +57,152 @@ __device__ __forceinline__ BlockRowRange block_row_range(const int *ia, int m, i
     return r;
 }
 
+// ------------------------------------------------- sorted count pass
+// One thread per block row.  When each of its 4 CSR rows lists block
+// columns in non-decreasing order after its first entry (sorted CSR, or
+// HYPRE's diagonal-first order), the block row's distinct block columns are
+// an 8-way merge (each row's first entry, and the rest of the row): every
+// entry gets its column's rank (slot) and a first-of-column flag in slotb,
+// and the count goes to cnt[b], with no sorting and no warp-wide matching.  The
+// entries of a warp's 32 block rows are first copied into shared memory
+// with coalesced loads.  Block rows of more than 32 entries, with unsorted
+// columns or with an index out of range go to slow[] for the warp kernel
+// below (which writes their slotb / cnt, or reports the bad index).
+constexpr int kStWarps = 4;
+constexpr int kStCap = 1024;  // entries of a warp's 32 block rows held in shared memory
+
+__global__ void __launch_bounds__(32 * kStWarps)
+csr2bsr_count_sorted_kernel(int m, int n, const int *__restrict__ ia, const int *__restrict__ ja, int brow,
+                            int *__restrict__ cnt, int *__restrict__ slow, int *__restrict__ nslow,
+                            int64_t *__restrict__ stats, unsigned char *__restrict__ slotb)
+{
+    __shared__ int scol[kStWarps][kStCap];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int *sc = scol[warp];
+    unsigned long long wmax = 0, wsq = 0;
+    const int ngroups = (brow + 31) / 32;
+    for (int gi = blockIdx.x * kStWarps + warp; gi < ngroups; gi += gridDim.x * kStWarps) {
+        const int b = gi * 32 + lane;
+        const bool live = b < brow;
+        int r[5];
+#pragma unroll
+        for (int o = 0; o < 5; ++o) r[o] = live ? __ldg(ia + min(4 * b + o, m)) : 0;
+        const int P0 = __shfl_sync(FULL, r[0], 0);
+        const int P1 = __shfl_sync(FULL, r[4], min(31, brow - 1 - gi * 32));
+        const bool staged = P1 - P0 <= kStCap;  // warp-uniform
+        if (staged)
+            for (int e = P0 + lane; e < P1; e += 32) sc[e - P0] = __ldg(ja + e);
+        __syncwarp();
+        auto col_at = [&](int p) { return staged ? sc[p - P0] : __ldg(ja + p); };
+        bool ok = live && r[4] - r[0] <= 32;
+        int u = 0;
+        if (ok) {
+            // lists in entry order: row q's first entry (list 2q) and the
+            // rest of row q (list 2q + 1), so that the first entry popped
+            // for a column is its lowest-numbered one
+            int h[8], e[8], c[8];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                h[2 * q] = r[q];
+                e[2 * q] = min(r[q] + 1, r[q + 1]);
+                h[2 * q + 1] = r[q] + 1;
+                e[2 * q + 1] = r[q + 1];
+            }
+#pragma unroll
+            for (int l = 0; l < 8; ++l) {
+                c[l] = 0x7FFFFFFF;
+                if (h[l] < e[l]) {
+                    const int col = col_at(h[l]);
+                    if (col < 0 || col >= n) ok = false;
+                    c[l] = col >> 2;
+                }
+            }
+            while (ok) {
+                int mn = c[0];
+#pragma unroll
+                for (int l = 1; l < 8; ++l) mn = min(mn, c[l]);
+                if (mn == 0x7FFFFFFF) break;
+                unsigned lead = 0x80;
+#pragma unroll
+                for (int l = 0; l < 8; ++l) {
+                    while (c[l] == mn) {
+                        slotb[h[l]] = (unsigned char)(u | lead);
+                        lead = 0;
+                        int next = 0x7FFFFFFF;
+                        if (++h[l] < e[l]) {
+                            const int col = col_at(h[l]);
+                            if (col < 0 || col >= n || (col >> 2) < mn) ok = false;  // bad index / unsorted
+                            next = (col >> 2) < mn ? 0x7FFFFFFF : col >> 2;
+                        }
+                        c[l] = next;
+                    }
+                }
+                ++u;
+            }
+        }
+        if (ok) {
+            cnt[b] = u;
+            wmax = wmax > (unsigned long long)u ? wmax : (unsigned long long)u;
+            wsq += (unsigned long long)u * (unsigned long long)u;
+        }
+        const unsigned left = __ballot_sync(FULL, live && !ok);
+        if (left) {
+            int at = 0;
+            if (lane == 0) at = atomicAdd(nslow, __popc(left));
+            at = __shfl_sync(FULL, at, 0);
+            if (live && !ok) slow[at + __popc(left & ((1u << lane) - 1))] = b;
+        }
+        __syncwarp();  // the shared entries are reused by the next group
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long om = __shfl_xor_sync(FULL, wmax, o);
+        wmax = wmax > om ? wmax : om;
+        wsq += __shfl_xor_sync(FULL, wsq, o);
+    }
+    if (lane == 0 && wsq) {
+        atomicMax((unsigned long long *)&stats[0], wmax);
+        atomicAdd((unsigned long long *)&stats[1], wsq);
+    }
+}
+
 // ------------------------------------------------------------ count pass
-// A warp takes kCvtGroup consecutive block rows at a time: their 4 * G + 1
-// row pointers arrive in one coalesced load and their entries (rows of at
-// most 32) in independent loads, so G block rows cost two memory round
-// trips instead of 2 G.  Each block row is then sorted on its own
+// A warp takes kCvtGroup block rows at a time: their row pointers arrive
+// in one load and their entries (rows of at most 32) in independent loads,
+// so G block rows cost two memory round trips instead of 2 G.  Each block row is then sorted on its own
 // (registers for <= 32 entries, the warp's shared-memory slice for <= 512);
 // longer ones go to the large list.
 constexpr int kCvtGroup = 4;
 
+// rows == nullptr: every block row, in groups of kCvtGroup consecutive ones;
+// else the *nrows block rows listed in rows[] (those the one-thread-per-row
+// pass below left: unsorted columns, more than 32 entries, bad indices).
 __global__ void __launch_bounds__(32 * kCvtWarps)
 csr2bsr_count_kernel(int m, int n, const int *__restrict__ ia, const int *__restrict__ ja, int brow,
-                     int *__restrict__ cnt, int *__restrict__ large, int64_t *__restrict__ stats, int *err,
+                     const int *__restrict__ rows, const int *__restrict__ nrows, int *__restrict__ cnt,
+                     int *__restrict__ large, int64_t *__restrict__ stats, int *err,
                      unsigned long long *__restrict__ sorted, unsigned char *__restrict__ slotb)
 {
     __shared__ unsigned long long sbuf[kCvtWarps][kWarpCap];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned long long *s = sbuf[warp];
     unsigned long long wmax = 0, wsq = 0;  // per-warp statistics, one atomic each at the end
-    const int ngroups = (brow + kCvtGroup - 1) / kCvtGroup;
+    const int total = rows ? *nrows : brow;
+    const int ngroups = (total + kCvtGroup - 1) / kCvtGroup;
     for (int g = blockIdx.x * kCvtWarps + warp; g < ngroups; g += gridDim.x * kCvtWarps) {
-        const int b0 = g * kCvtGroup;
-        const int nb = min(kCvtGroup, brow - b0);
-        // lane i holds ia[min(4 b0 + i, m)], i <= 4 nb (rows past m are empty)
-        const int iav = (lane <= 4 * nb) ? ia[min(4 * b0 + lane, m)] : 0;
-        auto range = [&](int j) {  // block row b0 + j's entries and row ends
+        const int nb = min(kCvtGroup, total - g * kCvtGroup);
+        // lanes 5j .. 5j + 4 hold ia[min(4 b_j + o, m)], o = 0..4, for the
+        // group's block rows b_j, j < nb (rows past m are empty)
+        const int jl = lane / 5, ol = lane - 5 * jl;
+        const int bl = (jl < nb) ? (rows ? rows[g * kCvtGroup + jl] : g * kCvtGroup + jl) : 0;
+        const int iav = (jl < nb) ? ia[min(4 * bl + ol, m)] : 0;
+        auto range = [&](int j) {  // block row b_j's entries and row ends
             BlockRowRange r;
-            r.p0 = __shfl_sync(FULL, iav, 4 * j);
-            r.e1 = __shfl_sync(FULL, iav, 4 * j + 1);
-            r.e2 = __shfl_sync(FULL, iav, 4 * j + 2);
-            r.e3 = __shfl_sync(FULL, iav, 4 * j + 3);
-            r.p1 = __shfl_sync(FULL, iav, 4 * j + 4);
+            r.p0 = __shfl_sync(FULL, iav, 5 * j);
+            r.e1 = __shfl_sync(FULL, iav, 5 * j + 1);
+            r.e2 = __shfl_sync(FULL, iav, 5 * j + 2);
+            r.e3 = __shfl_sync(FULL, iav, 5 * j + 3);
+            r.p1 = __shfl_sync(FULL, iav, 5 * j + 4);
             return r;
         };
         unsigned long long v[kCvtGroup];
@@ -104,7 +219,7 @@ csr2bsr_count_kernel(int m, int n, const int *__restrict__ ia, const int *__rest
 #pragma unroll
         for (int j = 0; j < kCvtGroup; ++j) {
             const BlockRowRange Rj = range(j);
-            const int b = b0 + j;
+            const int b = __shfl_sync(FULL, bl, 5 * j);
             const int L = Rj.p1 - Rj.p0;
             if (j >= nb) {
                 // past the last block row (warp-uniform)
@@ -692,24 +807,29 @@ int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int 
                                            2 * kWin * (int)sizeof(uint32_t)));
         smem_set[dev] = true;
     }
+    // stats: [0] longest block row, [1] sum of squares, [2] block count,
+    // [3] large-row count (int), [4] slow-row count (int)
     if ((rc = alloc_n(&out->blcPtr, brow + 1, s)) || (rc = alloc_n(&cnt, brow + 1, s)) ||
-        (rc = alloc_n(&large, brow, s)) || (rc = alloc_n(&stats, 4, s)) ||
+        (rc = alloc_n(&large, 2 * (size_t)brow, s)) || (rc = alloc_n(&stats, 5, s)) ||
         (rc = alloc_n(&sorted, (size_t)A->num_nonzeros, s)) ||
         (rc = alloc_n(&slotb, (size_t)A->num_nonzeros, s)))
         goto fail;
-    AMGT_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(int64_t) * 4, s));
+    AMGT_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(int64_t) * 5, s));
     AMGT_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * (brow + 1), s));
     if (brow > 0) {
-        AMGT_LAUNCH(csr2bsr_count_kernel, grid_for(kCvtWarps, (brow + kCvtGroup - 1) / kCvtGroup, st->sm_count, 16),
-                    32 * kCvtWarps, 0, s, m, n,
-                    A->i, A->j, brow, cnt, large, stats, st->err, sorted, slotb);
+        // slow-row list behind the large-row list (2 brow ints)
+        int *slow = large + brow, *nslow = (int *)&stats[4];
+        AMGT_LAUNCH(csr2bsr_count_sorted_kernel, grid_for(32 * kStWarps, brow, st->sm_count, 12), 32 * kStWarps, 0,
+                    s, m, n, A->i, A->j, brow, cnt, slow, nslow, stats, slotb);
+        AMGT_LAUNCH(csr2bsr_count_kernel, 2 * st->sm_count, 32 * kCvtWarps, 0, s, m, n, A->i, A->j, brow, slow,
+                    nslow, cnt, large, stats, st->err, sorted, slotb);
         AMGT_LAUNCH(csr2bsr_large_kernel<false>, 2 * st->sm_count, kLargeThreads, 2 * kWin * sizeof(uint32_t), s,
                     m, n, A->i, A->j, A->data, large, stats, cnt, nullptr, nullptr, nullptr, nullptr, stats);
     }
     if ((rc = exclusive_scan_int(cnt, out->blcPtr, brow + 1, s))) goto fail;
     AMGT_CUDA_TRY(cudaMemcpyAsync(&stats[2], out->blcPtr + brow, sizeof(int), cudaMemcpyDeviceToDevice, s));
     if (between && (rc = between(ctx))) goto fail;
-    if ((rc = read_back(stats, 4, s, &h))) goto fail;
+    if ((rc = read_back(stats, 5, s, &h))) goto fail;
     nb = (int)h[2];
     out->max_blc_per_row = (int)h[0];
     {

@@ -9,8 +9,35 @@ from gpu_util import assert_bsr_equal, random_csr, to_dev
 pytestmark = pytest.mark.gpu
 
 
+def _reverse_rows(orc, A, rows):
+    """A with the entries of the given rows in reverse (unsorted) order."""
+    ja, a = A.ja.copy(), A.a.copy()
+    for r in rows:
+        lo, hi = A.ia[r], A.ia[r + 1]
+        ja[lo:hi] = ja[lo:hi][::-1]
+        a[lo:hi] = a[lo:hi][::-1]
+    return orc.CSR(A.m, A.n, A.ia, ja, a)
+
+
+def _with_long_row(orc, A, r, length, seed):
+    """A with row r replaced by `length` sorted random columns."""
+    rng = np.random.default_rng(seed)
+    cols = np.sort(rng.choice(A.n, size=length, replace=False)).astype(np.int32)
+    rows_ja = [A.ja[A.ia[i]:A.ia[i + 1]] for i in range(A.m)]
+    rows_a = [A.a[A.ia[i]:A.ia[i + 1]] for i in range(A.m)]
+    rows_ja[r], rows_a[r] = cols, rng.standard_normal(length)
+    ia = np.concatenate([[0], np.cumsum([len(x) for x in rows_ja])]).astype(np.int32)
+    return orc.CSR(A.m, A.n, ia, np.concatenate(rows_ja).astype(np.int32), np.concatenate(rows_a))
+
+
 def _cases(orc):
+    lap = orc.laplacian(16, 16, 16)
     return {
+        # sorted rows (one thread per block row) mixed with reversed ones in
+        # the same warps (the warp kernel), and a warp whose entries do not
+        # fit the shared-memory copy because of one long row
+        "sorted_some_reversed": _reverse_rows(orc, lap, [7, 100, 101, 102, 103, 2000, 4095]),
+        "sorted_one_long": _with_long_row(orc, lap, 300, 1500, seed=5),
         "hypre7pt_10x10x10": orc.laplacian(10, 10, 10),
         "5pt_64x64": orc.laplacian(64, 64, 1),
         "varcoef27_13x11x9": orc.varcoef27(13, 11, 9, seed=4),
@@ -31,7 +58,7 @@ def cases(orc):
 
 
 CASE_NAMES = ["hypre7pt_10x10x10", "5pt_64x64", "varcoef27_13x11x9", "27pt_20x20x20", "interp_13x11x9",
-              "ragged_rect", "long_rows", "empty"]
+              "ragged_rect", "long_rows", "empty", "sorted_some_reversed", "sorted_one_long"]
 
 
 @pytest.mark.parametrize("name", CASE_NAMES)
@@ -96,3 +123,20 @@ def test_balance_segments(amgt, orc, cases):
     idx = view(G.s.rowIdxbyWarp, G.s.warpnum, torch.int32).cpu().numpy()
     np.testing.assert_array_equal(ptr, np.concatenate([[0], np.cumsum(segs)]))
     np.testing.assert_array_equal(idx, np.repeat(np.arange(len(lens)), segs))
+
+
+@pytest.mark.parametrize("bad", [-1, "n"])
+def test_csr_to_bsr_reports_bad_column(amgt, orc, bad):
+    """A column index outside [0, n) in an otherwise sorted matrix: the
+    kernels check the index before using it and the call returns
+    AMGT_ERR_DEVICE; the next conversion on the device is unaffected."""
+    from amgt_b200._lib import AmgtError
+
+    A = orc.laplacian(16, 16, 16)
+    ja = A.ja.copy()
+    ja[A.ia[500] + 1] = A.n if bad == "n" else bad
+    with pytest.raises(AmgtError) as ei:
+        amgt.Bsr.from_csr(*to_dev(orc.CSR(A.m, A.n, A.ia, ja, A.a)))
+    assert ei.value.status == 4  # AMGT_ERR_DEVICE
+    G = amgt.Bsr.from_csr(*to_dev(A))
+    assert_bsr_equal(G, orc.csr2bsr(A))
