@@ -66,15 +66,17 @@ __device__ __forceinline__ BlockRowRange block_row_range(const int *ia, int m, i
 // and the count goes to cnt[b], with no sorting and no warp-wide matching.  The
 // entries of a warp's 32 block rows are first copied into shared memory
 // with coalesced loads.  Block rows of more than 32 entries, with unsorted
-// columns or with an index out of range go to slow[] for the warp kernel
-// below (which writes their slotb / cnt, or reports the bad index).
+// columns or with an index out of range go to slow[] (and slowf[b] = 1)
+// for the warp kernel below (which writes their slotb / cnt, or reports the
+// bad index).
 constexpr int kStWarps = 4;
 constexpr int kStCap = 1024;  // entries of a warp's 32 block rows held in shared memory
 
 __global__ void __launch_bounds__(32 * kStWarps)
 csr2bsr_count_sorted_kernel(int m, int n, const int *__restrict__ ia, const int *__restrict__ ja, int brow,
                             int *__restrict__ cnt, int *__restrict__ slow, int *__restrict__ nslow,
-                            int64_t *__restrict__ stats, unsigned char *__restrict__ slotb)
+                            unsigned char *__restrict__ slowf, int64_t *__restrict__ stats,
+                            unsigned char *__restrict__ slotb)
 {
     __shared__ int scol[kStWarps][kStCap];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -140,6 +142,7 @@ csr2bsr_count_sorted_kernel(int m, int n, const int *__restrict__ ia, const int 
                 ++u;
             }
         }
+        if (live) slowf[b] = ok ? 0 : 1;
         if (ok) {
             cnt[b] = u;
             wmax = wmax > (unsigned long long)u ? wmax : (unsigned long long)u;
@@ -401,35 +404,143 @@ csr2bsr_large_kernel(int m, int n, const int *__restrict__ ia, const int *__rest
 }
 
 // ------------------------------------------------------------- fill pass
+// Fill for the block rows of the sorted count pass (slowf[b] == 0): 4 lanes
+// per block row, lane q walks CSR row q (its first entry, then the rest in
+// column order, so in slot order) slot by slot and writes row q of every
+// block once, zeros included; the 4 lanes together write whole 128-byte
+// blocks.  A block's bitmap is the OR of the 4 lanes' nibbles (shuffles in
+// the group), and the first entry of a column writes the block column.  A
+// warp takes 8 block rows at a time and first copies their entries (column,
+// value, slot byte) into shared memory with coalesced loads.
+constexpr int kFsWarps = 4;
+constexpr int kFsCap = 256;  // entries of a warp's 8 block rows held in shared memory
+
+__global__ void __launch_bounds__(32 * kFsWarps)
+csr2bsr_fill_sorted_kernel(int m, const int *__restrict__ ia, const int *__restrict__ ja,
+                           const double *__restrict__ a, int brow, const unsigned char *__restrict__ slowf,
+                           const int *__restrict__ bptr, int *__restrict__ bidx, uint16_t *__restrict__ bmap,
+                           double *__restrict__ bval, const unsigned char *__restrict__ slotb)
+{
+    __shared__ double sval[kFsWarps][kFsCap];
+    __shared__ int scol[kFsWarps][kFsCap];
+    __shared__ unsigned char sslot[kFsWarps][kFsCap];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, q = lane & 3;
+    const unsigned gmask = 0xFu << (lane & ~3);
+    const int nwg = (brow + 7) / 8;
+    for (int wg = blockIdx.x * kFsWarps + warp; wg < nwg; wg += gridDim.x * kFsWarps) {
+        const int b0 = 8 * wg;
+        const int E0 = __ldg(ia + 4 * b0), E1 = __ldg(ia + min(4 * (b0 + 8), m));
+        const bool staged = E1 - E0 <= kFsCap;  // warp-uniform
+        if (staged)
+            for (int e = E0 + lane; e < E1; e += 32) {
+                scol[warp][e - E0] = __ldg(ja + e);
+                sval[warp][e - E0] = __ldg(a + e);
+                sslot[warp][e - E0] = __ldg(slotb + e);
+            }
+        __syncwarp();
+        auto entry = [&](int p, int &sb, int &c, double &v) {
+            if (staged) {
+                sb = sslot[warp][p - E0];
+                c = scol[warp][p - E0];
+                v = sval[warp][p - E0];
+            } else {
+                sb = __ldg(slotb + p);
+                c = __ldg(ja + p);
+                v = __ldg(a + p);
+            }
+        };
+        const int b = b0 + (lane >> 2);
+        if (b < brow && !slowf[b]) {  // the same for the 4 lanes of a group
+            const int base = bptr[b], u = bptr[b + 1] - base;
+            const int r = 4 * b + q;
+            int p = 0, pe = 0;
+            if (r < m) {
+                p = ia[r];
+                pe = ia[r + 1];
+            }
+            int hs = -1, hc = 0, hsb = 0;
+            double hv = 0.0;
+            if (p < pe) {
+                entry(p, hsb, hc, hv);
+                hs = hsb & 0x1F;
+                ++p;
+            }
+            int ts = -1, tc = 0, tsb = 0;
+            double tv = 0.0;
+            if (p < pe) {
+                entry(p, tsb, tc, tv);
+                ts = tsb & 0x1F;
+            }
+            for (int sl = 0; sl < u; ++sl) {
+                double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+                unsigned bits = 0;
+                if (hs == sl) {
+                    const int c = hc & 3;
+                    v0 = c == 0 ? hv : v0; v1 = c == 1 ? hv : v1; v2 = c == 2 ? hv : v2; v3 = c == 3 ? hv : v3;
+                    bits |= 1u << c;
+                    if (hsb & 0x80) bidx[base + sl] = hc >> 2;
+                }
+                while (ts == sl) {
+                    const int c = tc & 3;
+                    v0 = c == 0 ? tv : v0; v1 = c == 1 ? tv : v1; v2 = c == 2 ? tv : v2; v3 = c == 3 ? tv : v3;
+                    bits |= 1u << c;
+                    if (tsb & 0x80) bidx[base + sl] = tc >> 2;
+                    ts = -1;
+                    if (++p < pe) {
+                        entry(p, tsb, tc, tv);
+                        ts = tsb & 0x1F;
+                    }
+                }
+                double2 *dst = reinterpret_cast<double2 *>(bval + 16LL * (base + sl) + 4 * q);
+                dst[0] = make_double2(v0, v1);
+                dst[1] = make_double2(v2, v3);
+                unsigned mp = bits << (4 * q);
+                mp |= __shfl_xor_sync(gmask, mp, 1);
+                mp |= __shfl_xor_sync(gmask, mp, 2);
+                if (q == 0) bmap[base + sl] = (uint16_t)mp;
+            }
+        }
+        __syncwarp();  // the shared entries are reused by the next group
+    }
+}
+
 // Takes each block row's pairs as the count pass sorted them (scratch at the
 // block row's CSR offset) and writes block columns, OR-ed bitmaps and the
 // zero-padded values.
+// rows == nullptr: every block row; else the *nrows listed ones (as in the
+// count pass).
 __global__ void __launch_bounds__(32 * kCvtWarps)
 csr2bsr_fill_kernel(int m, int n, const int *__restrict__ ia, const int *__restrict__ ja,
-                    const double *__restrict__ a, int brow, const int *__restrict__ bptr, int *__restrict__ bidx,
+                    const double *__restrict__ a, int brow, const int *__restrict__ rows,
+                    const int *__restrict__ nrows, const int *__restrict__ bptr, int *__restrict__ bidx,
                     uint16_t *__restrict__ bmap, double *__restrict__ bval,
                     const unsigned long long *__restrict__ sorted, const unsigned char *__restrict__ slotb, int *err)
 {
     __shared__ unsigned sorv[kCvtWarps][32];  // per-slot OR of the bitmaps
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned *so = sorv[warp];
-    const int ngroups = (brow + kCvtGroup - 1) / kCvtGroup;
+    const int total = rows ? *nrows : brow;
+    const int ngroups = (total + kCvtGroup - 1) / kCvtGroup;
     for (int g = blockIdx.x * kCvtWarps + warp; g < ngroups; g += gridDim.x * kCvtWarps) {
         // kCvtGroup block rows at a time, as in the count pass: row pointers
-        // and block offsets in one load each, sorted pairs and values of the
-        // short rows in independent loads
-        const int b0 = g * kCvtGroup;
-        const int nb = min(kCvtGroup, brow - b0);
-        const int iav = (lane <= 4 * nb) ? ia[min(4 * b0 + lane, m)] : 0;
-        const int bpv = (lane <= nb) ? bptr[b0 + lane] : 0;
+        // (lanes 5j .. 5j + 4) and block offsets (lanes 2j, 2j + 1) in one
+        // load each, sorted pairs and values of the short rows in
+        // independent loads
+        const int nb = min(kCvtGroup, total - g * kCvtGroup);
+        const int jl = lane / 5, ol = lane - 5 * jl;
+        const int bl = (jl < nb) ? (rows ? rows[g * kCvtGroup + jl] : g * kCvtGroup + jl) : 0;
+        const int iav = (jl < nb) ? ia[min(4 * bl + ol, m)] : 0;
+        const int jb = lane >> 1;
+        const int bb = __shfl_sync(FULL, bl, 5 * min(jb, kCvtGroup - 1));  // every lane shuffles
+        const int bpv = (jb < nb) ? bptr[bb + (lane & 1)] : 0;
         unsigned long long v[kCvtGroup];
         double av[kCvtGroup];
         int sl[kCvtGroup];  // slot | 0x80 on the first entry of its column (from the count pass)
 #pragma unroll
         for (int j = 0; j < kCvtGroup; ++j) {
-            const int p0 = __shfl_sync(FULL, iav, 4 * j), e1 = __shfl_sync(FULL, iav, 4 * j + 1),
-                      e2 = __shfl_sync(FULL, iav, 4 * j + 2), e3 = __shfl_sync(FULL, iav, 4 * j + 3),
-                      p1 = __shfl_sync(FULL, iav, 4 * j + 4);
+            const int p0 = __shfl_sync(FULL, iav, 5 * j), e1 = __shfl_sync(FULL, iav, 5 * j + 1),
+                      e2 = __shfl_sync(FULL, iav, 5 * j + 2), e3 = __shfl_sync(FULL, iav, 5 * j + 3),
+                      p1 = __shfl_sync(FULL, iav, 5 * j + 4);
             const int L = p1 - p0;
             v[j] = kSentinel;
             av[j] = 0.0;
@@ -443,9 +554,9 @@ csr2bsr_fill_kernel(int m, int n, const int *__restrict__ ia, const int *__restr
         }
 #pragma unroll
         for (int j = 0; j < kCvtGroup; ++j) {
-            const int p0 = __shfl_sync(FULL, iav, 4 * j), p1 = __shfl_sync(FULL, iav, 4 * j + 4);
+            const int p0 = __shfl_sync(FULL, iav, 5 * j), p1 = __shfl_sync(FULL, iav, 5 * j + 4);
             const int L = p1 - p0;
-            const int base = __shfl_sync(FULL, bpv, j), u = __shfl_sync(FULL, bpv, j + 1) - base;
+            const int base = __shfl_sync(FULL, bpv, 2 * j), u = __shfl_sync(FULL, bpv, 2 * j + 1) - base;
             if (j < nb && L <= kWarpCap) {  // warp-uniform; longer rows: large-row kernel
                 double2 *z = reinterpret_cast<double2 *>(bval + (size_t)16 * base);
                 for (int i = lane; i < 8 * u; i += 32) z[i] = make_double2(0.0, 0.0);
@@ -791,6 +902,7 @@ int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int 
     out->blc_col = (n + 3) / 4;
 
     int *cnt = nullptr, *large = nullptr;
+    unsigned char *slowf = nullptr;  // per block row: left to the warp kernels
     int64_t *stats = nullptr;
     unsigned long long *sorted = nullptr;  // sorted entries of rows of 33..512 entries
     unsigned char *slotb = nullptr;        // per entry of shorter rows: block slot | first-of-column flag
@@ -812,7 +924,7 @@ int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int 
     if ((rc = alloc_n(&out->blcPtr, brow + 1, s)) || (rc = alloc_n(&cnt, brow + 1, s)) ||
         (rc = alloc_n(&large, 2 * (size_t)brow, s)) || (rc = alloc_n(&stats, 5, s)) ||
         (rc = alloc_n(&sorted, (size_t)A->num_nonzeros, s)) ||
-        (rc = alloc_n(&slotb, (size_t)A->num_nonzeros, s)))
+        (rc = alloc_n(&slotb, (size_t)A->num_nonzeros, s)) || (rc = alloc_n(&slowf, (size_t)brow, s)))
         goto fail;
     AMGT_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(int64_t) * 5, s));
     AMGT_CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(int) * (brow + 1), s));
@@ -820,7 +932,7 @@ int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int 
         // slow-row list behind the large-row list (2 brow ints)
         int *slow = large + brow, *nslow = (int *)&stats[4];
         AMGT_LAUNCH(csr2bsr_count_sorted_kernel, grid_for(32 * kStWarps, brow, st->sm_count, 12), 32 * kStWarps, 0,
-                    s, m, n, A->i, A->j, brow, cnt, slow, nslow, stats, slotb);
+                    s, m, n, A->i, A->j, brow, cnt, slow, nslow, slowf, stats, slotb);
         AMGT_LAUNCH(csr2bsr_count_kernel, 2 * st->sm_count, 32 * kCvtWarps, 0, s, m, n, A->i, A->j, brow, slow,
                     nslow, cnt, large, stats, st->err, sorted, slotb);
         AMGT_LAUNCH(csr2bsr_large_kernel<false>, 2 * st->sm_count, kLargeThreads, 2 * kWin * sizeof(uint32_t), s,
@@ -847,10 +959,12 @@ int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int 
         (rc = alloc_n(&out->blcVal, (size_t)16 * nb, s)))
         goto fail;
     if (brow > 0) {
-        AMGT_LAUNCH(csr2bsr_fill_kernel, grid_for(kCvtWarps, (brow + kCvtGroup - 1) / kCvtGroup, st->sm_count, 16),
-                    32 * kCvtWarps, 0, s, m, n,
-                    A->i, A->j, A->data, brow, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal, sorted, slotb,
-                    st->err);
+        const int *slow = large + brow, *nslow = (const int *)&stats[4];
+        AMGT_LAUNCH(csr2bsr_fill_sorted_kernel, grid_for(8 * kFsWarps, brow, st->sm_count, 16), 32 * kFsWarps, 0, s,
+                    m, A->i, A->j,
+                    A->data, brow, slowf, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal, slotb);
+        AMGT_LAUNCH(csr2bsr_fill_kernel, 2 * st->sm_count, 32 * kCvtWarps, 0, s, m, n, A->i, A->j, A->data, brow,
+                    slow, nslow, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal, sorted, slotb, st->err);
         AMGT_LAUNCH(csr2bsr_large_kernel<true>, 2 * st->sm_count, kLargeThreads, 2 * kWin * sizeof(uint32_t), s, m,
                     n, A->i, A->j, A->data, large, stats, nullptr, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal,
                     nullptr);
@@ -860,6 +974,7 @@ int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int 
     free_ptr(stats, s);
     free_ptr(sorted, s);
     free_ptr(slotb, s);
+    free_ptr(slowf, s);
     return AMGT_OK;
 fail:
     free_ptr(cnt, s);
@@ -867,6 +982,7 @@ fail:
     free_ptr(stats, s);
     free_ptr(sorted, s);
     free_ptr(slotb, s);
+    free_ptr(slowf, s);
     amgt_bsr_free(out, stream);
     return rc;
 }
