@@ -61,7 +61,54 @@ __device__ __forceinline__ typename ValTraits<PREC>::acc_t row_dot(const void *_
     return acc;
 }
 
-template <int PREC, int LPR, bool SAFE>
+// The same walk with the blocks dealt alternately to two sums (a lane group
+// standing for two of the row's segments: blocks k, k + 2G, ... and
+// k + G, k + 3G, ...), with the loads and the order of each sum unchanged.
+template <int PREC, int G, bool SAFE>
+__device__ __forceinline__ void row_dot2(const void *__restrict__ val, const int *__restrict__ idx,
+                                         const double *__restrict__ x, int n, int k, int end, int q,
+                                         typename ValTraits<PREC>::acc_t &a0, typename ValTraits<PREC>::acc_t &a1)
+{
+    for (; k + G < end; k += 2 * G) {
+        const int c0 = __ldcs(idx + k), c1 = __ldcs(idx + k + G);
+        a0 = block_row_dot<PREC, SAFE>(val, x, n, k, q, c0, a0);
+        a1 = block_row_dot<PREC, SAFE>(val, x, n, k + G, q, c1, a1);
+    }
+    if (k < end) a0 = block_row_dot<PREC, SAFE>(val, x, n, k, q, __ldcs(idx + k), a0);
+}
+
+// Row sum of a block row: V == 1, LPR lanes per row as the row's segments;
+// V == 2, LPR lanes stand for the 2 LPR-lane layout (each lane group holds
+// segments g and g + LPR/4 of it): the segment sums are combined in that
+// layout's order (first across groups, then the two halves), so both give
+// the same bits.  Lanes with g == 0 hold the result.
+template <int PREC, int LPR, bool SAFE, int V>
+__device__ __forceinline__ typename ValTraits<PREC>::acc_t row_sum(const void *__restrict__ val,
+                                                                   const int *__restrict__ idx,
+                                                                   const double *__restrict__ x, int n, bool live,
+                                                                   int k, int end, int q)
+{
+    using acc_t = typename ValTraits<PREC>::acc_t;
+    constexpr int G = LPR / 4;
+    if constexpr (V == 1) {
+        acc_t acc = 0;
+        if (live) acc = row_dot<PREC, G, SAFE>(val, idx, x, n, k, end, q, acc);
+#pragma unroll
+        for (int o = 4; o < LPR; o <<= 1) acc += __shfl_xor_sync(FULL, acc, o);
+        return acc;
+    } else {
+        acc_t a0 = 0, a1 = 0;
+        if (live) row_dot2<PREC, G, SAFE>(val, idx, x, n, k, end, q, a0, a1);
+#pragma unroll
+        for (int o = 4; o < LPR; o <<= 1) {
+            a0 += __shfl_xor_sync(FULL, a0, o);
+            a1 += __shfl_xor_sync(FULL, a1, o);
+        }
+        return a0 + a1;
+    }
+}
+
+template <int PREC, int LPR, bool SAFE, int V = 1>
 __global__ void __launch_bounds__(256)
 spmv_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__restrict__ idx,
             const void *__restrict__ val, double alpha, const double *__restrict__ x, double beta,
@@ -70,20 +117,16 @@ spmv_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__re
     grid_dependency_wait();
     using acc_t = typename ValTraits<PREC>::acc_t;
     constexpr int RPW = 32 / LPR;  // block rows per warp
-    constexpr int G = LPR / 4;     // blocks in flight per row
     const int lane = threadIdx.x & 31;
     const int sub = lane / LPR, l = lane % LPR, g = l >> 2, q = l & 3;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     for (int b0 = warp * RPW; b0 < brow; b0 += nwarps * RPW) {
         const int b = b0 + sub;
-        acc_t acc = 0;
-        if (b < brow) {
-            acc = row_dot<PREC, G, SAFE>(val, idx, x, n, ptr[b] + g, ptr[b + 1], q, acc);
-        }
-#pragma unroll
-        for (int o = 4; o < LPR; o <<= 1) acc += __shfl_xor_sync(FULL, acc, o);
-        if (b < brow && g == 0) {
+        const bool live = b < brow;
+        const acc_t acc = row_sum<PREC, LPR, SAFE, V>(val, idx, x, n, live, live ? ptr[b] + g : 0,
+                                                      live ? ptr[b + 1] : 0, q);
+        if (live && g == 0) {
             const int row = 4 * b + q;
             if (row < m) {
                 const double t = alpha * (double)acc;
@@ -201,15 +244,15 @@ struct EpiArgs {
     double *partial;       // DOT: [gridDim.x]
 };
 
-template <int PREC, int LPR, bool SAFE, int EPI>
+template <int PREC, int LPR, bool SAFE, int EPI, int V = 1>
 __global__ void __launch_bounds__(256)
 spmv_epi_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__restrict__ idx,
                 const void *__restrict__ val, const double *__restrict__ x, EpiArgs e)
 {
+    static_assert(V == 1 || EPI != EPI_DOT, "dot partials follow the one-segment-per-group layout");
     grid_dependency_wait();
     using acc_t = typename ValTraits<PREC>::acc_t;
     constexpr int RPW = 32 / LPR;
-    constexpr int G = LPR / 4;
     __shared__ double sred[8];
     const int lane = threadIdx.x & 31;
     const int sub = lane / LPR, l = lane % LPR, g = l >> 2, q = l & 3;
@@ -218,13 +261,10 @@ spmv_epi_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *
     double dot = 0.0;
     for (int b0 = warp * RPW; b0 < brow; b0 += nwarps * RPW) {
         const int b = b0 + sub;
-        acc_t acc = 0;
-        if (b < brow) {
-            acc = row_dot<PREC, G, SAFE>(val, idx, x, n, ptr[b] + g, ptr[b + 1], q, acc);
-        }
-#pragma unroll
-        for (int o = 4; o < LPR; o <<= 1) acc += __shfl_xor_sync(FULL, acc, o);
-        if (b < brow && g == 0) {
+        const bool live = b < brow;
+        const acc_t acc = row_sum<PREC, LPR, SAFE, V>(val, idx, x, n, live, live ? ptr[b] + g : 0,
+                                                      live ? ptr[b + 1] : 0, q);
+        if (live && g == 0) {
             const int row = 4 * b + q;
             if (row < m) {
                 const double ax = (double)acc;
@@ -313,10 +353,22 @@ static int pick_lpr(const amgt_bsr *A, int mode)
     }
     if (env == 4 || env == 8 || env == 16 || env == 32) return env;
     const double avg = A->blc_row ? (double)A->blc_num / A->blc_row : 0.0;
-    if (avg <= 1.5) return 4;
-    if (avg <= 10.0) return 8;   // 7-point 128^3 (6.9): 8 beat 16 for 8- and 2-byte values
+    if (avg <= 4.0) return 4;    // interpolation 128^3 (3.3): 4 beat 8 for 8- and 2-byte values
+    if (avg <= 10.0) return 8;   // 7-point 128^3 (6.9): 8 beat 4 and 16 for 8-byte values
     if (avg <= 20.0) return 16;
     return 32;
+}
+
+// Lanes a row is given when it runs: 2-byte values move few bytes per
+// lane, so with the 8-lane segment layout half the lanes (each group
+// holding two of its segments, same sums) keep more rows in flight
+// (7-point 128^3, fp16 exact: 43.7 -> 37.0 us; at 32 lanes the same split
+// measured 22.4 -> 23.5 us and is not used).  The fused dot form keeps the
+// segment layout (its partials follow it).
+static int run_lpr(int lpr, int mode)
+{
+    const bool narrow = mode == AMGT_HALF || mode == AMGT_BF16 || mode == kExact16;
+    return (narrow && lpr == 8) ? 4 : lpr;
 }
 
 template <int PREC>
@@ -325,23 +377,26 @@ static int launch_spmv(const amgt_bsr *A, const void *val, double alpha, const d
 {
     const int brow = A->blc_row;
     const bool safe = (A->col % 4 != 0) || ((uintptr_t)x % 16 != 0);
-    const int lpr = pick_lpr(A, PREC);
-    const int rows_per_cta = 8 * (32 / lpr);
+    const int lpr = pick_lpr(A, PREC), run = run_lpr(lpr, PREC);
+    const int rows_per_cta = 8 * (32 / run);
     const int grid = grid_for(rows_per_cta, brow, sm_count, 8);
-#define AMGT_SPMV_CASE(L)                                                                                   \
-    if (lpr == L) {                                                                                         \
+#define AMGT_SPMV_CASE(L, V)                                                                                \
+    if (run == L && lpr == L * V) {                                                                         \
         if (safe)                                                                                           \
-            AMGT_LAUNCH_PDL((spmv_kernel<PREC, L, true>), grid, 256, 0, s, A->row, A->col, brow, A->blcPtr,     \
-                        A->blcIdx, val, alpha, x, beta, y);                                                 \
+            AMGT_LAUNCH_PDL((spmv_kernel<PREC, L, true, V>), grid, 256, 0, s, A->row, A->col, brow,          \
+                            A->blcPtr, A->blcIdx, val, alpha, x, beta, y);                                  \
         else                                                                                                \
-            AMGT_LAUNCH_PDL((spmv_kernel<PREC, L, false>), grid, 256, 0, s, A->row, A->col, brow, A->blcPtr,    \
-                        A->blcIdx, val, alpha, x, beta, y);                                                 \
+            AMGT_LAUNCH_PDL((spmv_kernel<PREC, L, false, V>), grid, 256, 0, s, A->row, A->col, brow,         \
+                            A->blcPtr, A->blcIdx, val, alpha, x, beta, y);                                  \
         return AMGT_OK;                                                                                     \
     }
-    AMGT_SPMV_CASE(4)
-    AMGT_SPMV_CASE(8)
-    AMGT_SPMV_CASE(16)
-    AMGT_SPMV_CASE(32)
+    AMGT_SPMV_CASE(4, 1)
+    AMGT_SPMV_CASE(8, 1)
+    AMGT_SPMV_CASE(16, 1)
+    AMGT_SPMV_CASE(32, 1)
+    if constexpr (PREC == AMGT_HALF || PREC == AMGT_BF16 || PREC == kExact16) {
+        AMGT_SPMV_CASE(4, 2)
+    }
 #undef AMGT_SPMV_CASE
     return AMGT_ERR_INVALID;
 }
@@ -446,42 +501,47 @@ int spmv_segmented_with_scratch(int prec, double alpha, const amgt_bsr *A, const
 
 template <int PREC, int EPI>
 static int launch_epi(const amgt_bsr *A, const void *val, const double *x, const EpiArgs &e, int grid,
-                      cudaStream_t s)
+                      cudaStream_t s, int sm_count)
 {
     const bool safe = (A->col % 4 != 0) || ((uintptr_t)x % 16 != 0);
     const int lpr = pick_lpr(A, PREC);
-#define AMGT_EPI_CASE(L)                                                                                     \
-    if (lpr == L) {                                                                                          \
+    const int run = EPI == EPI_DOT ? lpr : run_lpr(lpr, PREC);
+    if (run != lpr) grid = grid_for(8 * (32 / run), A->blc_row, sm_count, 8);  // no partials: any grid
+#define AMGT_EPI_CASE(L, V)                                                                                  \
+    if (run == L && lpr == L * V) {                                                                          \
         if (safe)                                                                                            \
-            AMGT_LAUNCH_PDL((spmv_epi_kernel<PREC, L, true, EPI>), grid, 256, 0, s, A->row, A->col, A->blc_row,  \
-                        A->blcPtr, A->blcIdx, val, x, e);                                                    \
+            AMGT_LAUNCH_PDL((spmv_epi_kernel<PREC, L, true, EPI, V>), grid, 256, 0, s, A->row, A->col,        \
+                            A->blc_row, A->blcPtr, A->blcIdx, val, x, e);                                    \
         else                                                                                                 \
-            AMGT_LAUNCH_PDL((spmv_epi_kernel<PREC, L, false, EPI>), grid, 256, 0, s, A->row, A->col, A->blc_row, \
-                        A->blcPtr, A->blcIdx, val, x, e);                                                    \
+            AMGT_LAUNCH_PDL((spmv_epi_kernel<PREC, L, false, EPI, V>), grid, 256, 0, s, A->row, A->col,       \
+                            A->blc_row, A->blcPtr, A->blcIdx, val, x, e);                                    \
         return AMGT_OK;                                                                                      \
     }
-    AMGT_EPI_CASE(4)
-    AMGT_EPI_CASE(8)
-    AMGT_EPI_CASE(16)
-    AMGT_EPI_CASE(32)
+    AMGT_EPI_CASE(4, 1)
+    AMGT_EPI_CASE(8, 1)
+    AMGT_EPI_CASE(16, 1)
+    AMGT_EPI_CASE(32, 1)
+    if constexpr (EPI != EPI_DOT && (PREC == AMGT_HALF || PREC == AMGT_BF16 || PREC == kExact16)) {
+        AMGT_EPI_CASE(4, 2)
+    }
 #undef AMGT_EPI_CASE
     return AMGT_ERR_INVALID;
 }
 
 template <int EPI>
 static int launch_epi_prec(int prec, const amgt_bsr *A, const double *x, const EpiArgs &e, int grid,
-                           cudaStream_t s)
+                           cudaStream_t s, int sm_count)
 {
     const int mode = storage_mode(A, prec);
     const void *val = value_array(A, mode);
     if (!val) return AMGT_ERR_INVALID;
     switch (mode) {
-    case AMGT_DOUBLE: return launch_epi<AMGT_DOUBLE, EPI>(A, val, x, e, grid, s);
-    case AMGT_FLOAT: return launch_epi<AMGT_FLOAT, EPI>(A, val, x, e, grid, s);
-    case AMGT_HALF: return launch_epi<AMGT_HALF, EPI>(A, val, x, e, grid, s);
-    case AMGT_BF16: return launch_epi<AMGT_BF16, EPI>(A, val, x, e, grid, s);
-    case kExact32: return launch_epi<kExact32, EPI>(A, val, x, e, grid, s);
-    case kExact16: return launch_epi<kExact16, EPI>(A, val, x, e, grid, s);
+    case AMGT_DOUBLE: return launch_epi<AMGT_DOUBLE, EPI>(A, val, x, e, grid, s, sm_count);
+    case AMGT_FLOAT: return launch_epi<AMGT_FLOAT, EPI>(A, val, x, e, grid, s, sm_count);
+    case AMGT_HALF: return launch_epi<AMGT_HALF, EPI>(A, val, x, e, grid, s, sm_count);
+    case AMGT_BF16: return launch_epi<AMGT_BF16, EPI>(A, val, x, e, grid, s, sm_count);
+    case kExact32: return launch_epi<kExact32, EPI>(A, val, x, e, grid, s, sm_count);
+    case kExact16: return launch_epi<kExact16, EPI>(A, val, x, e, grid, s, sm_count);
     default: return AMGT_ERR_INVALID;
     }
 }
@@ -496,20 +556,20 @@ int spmv_residual(int prec, const amgt_bsr *A, const double *f, const double *u,
                   int sm_count)
 {
     EpiArgs e{f, nullptr, 0.0, r, nullptr};
-    return launch_epi_prec<EPI_RESID>(prec, A, u, e, epi_grid(A, sm_count), s);
+    return launch_epi_prec<EPI_RESID>(prec, A, u, e, epi_grid(A, sm_count), s, sm_count);
 }
 
 int spmv_jacobi(int prec, const amgt_bsr *A, const double *inv_l1, double w, const double *f, const double *u,
                 double *u_out, cudaStream_t s, int sm_count)
 {
     EpiArgs e{f, inv_l1, w, u_out, nullptr};
-    return launch_epi_prec<EPI_JACOBI>(prec, A, u, e, epi_grid(A, sm_count), s);
+    return launch_epi_prec<EPI_JACOBI>(prec, A, u, e, epi_grid(A, sm_count), s, sm_count);
 }
 
 int spmv_dot(int prec, const amgt_bsr *A, const double *u, double *out, double *partial, int grid, cudaStream_t s)
 {
     EpiArgs e{nullptr, nullptr, 0.0, out, partial};
-    return launch_epi_prec<EPI_DOT>(prec, A, u, e, grid, s);
+    return launch_epi_prec<EPI_DOT>(prec, A, u, e, grid, s, 0);  // the segment layout: grid as given
 }
 
 int bsr_l1_norms(const amgt_bsr *A, double *l1, int invert, cudaStream_t s, int sm_count)
