@@ -291,26 +291,46 @@ void destroy_handle(amgt_amg *h, cudaStream_t s)
     delete h;
 }
 
-// The next level's interpolation, converted and transposed on a second
-// stream while the current level's products run (called from inside the
-// A * P SpGEMM, between its queued symbolic pass and its wait for C's
-// size); `ready` is recorded on that stream when P and R are complete.
+// Interpolations are converted and transposed on a second stream while the
+// first stream converts A and runs the products.  The work is issued from
+// inside amgt_csr_to_bsr / amgt_spgemm (after their first kernels are
+// queued and before they wait for a size), so that the host
+// synchronisations of the second stream's own calls delay no work on the
+// first: the pending transpose first (R_l, for level l's R (A P)), then the
+// pending conversion (P_{l+1}), whose transpose waits for the next call.
+// Events by level parity, so that level l + 1's records do not move the
+// ones level l still waits on: p_ready[l % 2] after P_l, r_ready[l % 2]
+// after R_l.
 struct NextInterp {
-    const amgt_csr *P = nullptr;
-    amgt_bsr *Pb = nullptr, *Rb = nullptr;
     cudaStream_t s2 = nullptr;
-    cudaEvent_t ready = nullptr;
-    bool done = false;
+    cudaEvent_t p_ready[2] = {nullptr, nullptr}, r_ready[2] = {nullptr, nullptr};
+    const amgt_csr *P = nullptr;  // pending conversion into Pb (R later into PRb)
+    amgt_bsr *Pb = nullptr, *PRb = nullptr;
+    int pslot = 0;
+    amgt_bsr *Tb = nullptr, *TRb = nullptr;  // pending transpose Tb -> TRb
+    int rslot = 0;
 };
 
-int convert_next_interp(void *ctx)
+int transpose_pending(NextInterp *nx)
+{
+    if (!nx->Tb) return AMGT_OK;
+    AMGT_TRY(amgt_bsr_transpose(nx->Tb, nx->TRb, (amgt_stream_t)nx->s2));
+    AMGT_CUDA_TRY(cudaEventRecord(nx->r_ready[nx->rslot], nx->s2));
+    nx->Tb = nullptr;
+    return AMGT_OK;
+}
+
+int prepare_interp(void *ctx)
 {
     NextInterp *nx = static_cast<NextInterp *>(ctx);
-    if (!nx->P || nx->done) return AMGT_OK;
-    nx->done = true;
+    AMGT_TRY(transpose_pending(nx));
+    if (!nx->P) return AMGT_OK;
     AMGT_TRY(amgt_csr_to_bsr(nx->P, nx->Pb, (amgt_stream_t)nx->s2));
-    AMGT_TRY(amgt_bsr_transpose(nx->Pb, nx->Rb, (amgt_stream_t)nx->s2));
-    AMGT_CUDA_TRY(cudaEventRecord(nx->ready, nx->s2));
+    AMGT_CUDA_TRY(cudaEventRecord(nx->p_ready[nx->pslot], nx->s2));
+    nx->Tb = nx->Pb;
+    nx->TRb = nx->PRb;
+    nx->rslot = nx->pslot;
+    nx->P = nullptr;
     return AMGT_OK;
 }
 
@@ -479,19 +499,26 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     // the second stream starts after everything the caller queued on `s`
     // before this call (the inputs may still be arriving there)
     if (L > 1 && (cudaStreamCreateWithFlags(&nx.s2, cudaStreamNonBlocking) != cudaSuccess ||
-                  cudaEventCreateWithFlags(&nx.ready, cudaEventDisableTiming) != cudaSuccess ||
-                  cudaEventRecord(nx.ready, s) != cudaSuccess || cudaStreamWaitEvent(nx.s2, nx.ready, 0) != cudaSuccess)) {
+                  cudaEventCreateWithFlags(&nx.p_ready[0], cudaEventDisableTiming) != cudaSuccess ||
+                  cudaEventCreateWithFlags(&nx.p_ready[1], cudaEventDisableTiming) != cudaSuccess ||
+                  cudaEventCreateWithFlags(&nx.r_ready[0], cudaEventDisableTiming) != cudaSuccess ||
+                  cudaEventCreateWithFlags(&nx.r_ready[1], cudaEventDisableTiming) != cudaSuccess ||
+                  cudaEventRecord(nx.p_ready[0], s) != cudaSuccess ||
+                  cudaStreamWaitEvent(nx.s2, nx.p_ready[0], 0) != cudaSuccess)) {
         cudaGetLastError();
         rc = AMGT_ERR_CUDA;
         goto fail;
     }
     h->lv.resize(L);
-    // hierarchy; P_0 is converted and transposed on the second stream while
-    // A's conversion runs, P_{l+1} while level l's products run
-    nx.P = (L > 1) ? &P[0] : nullptr;
-    nx.Pb = &h->lv[0].P;
-    nx.Rb = &h->lv[0].R;
-    if ((rc = csr_to_bsr_impl(A, &h->lv[0].A, stream, convert_next_interp, &nx))) goto fail;
+    // hierarchy: P_0 converted while A's conversion runs, R_l transposed
+    // and P_{l+1} converted while level l's A P runs
+    if (L > 1) {
+        nx.P = &P[0];
+        nx.Pb = &h->lv[0].P;
+        nx.PRb = &h->lv[0].R;
+        nx.pslot = 0;
+    }
+    if ((rc = csr_to_bsr_impl(A, &h->lv[0].A, stream, prepare_interp, &nx))) goto fail;
     h->lv[0].n = A->num_rows;
     pm.mark(0, s);
     for (int l = 0; l < L - 1; ++l) {
@@ -499,20 +526,32 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         if (P[l].num_rows != v.n || P[l].num_cols <= 0) { rc = AMGT_ERR_INVALID; goto fail; }
         v.prec = amgt_precision_for_level(l);
         v.prec_transfer = amgt_precision_for_level(l + 1);
-        // P_l and R_l: converted on the second stream (no-op when done)
-        if ((rc = convert_next_interp(&nx))) goto fail;
-        if (cudaStreamWaitEvent(s, nx.ready, 0) != cudaSuccess) {
+        // A P waits for P_l only (converted now if no call issued it),
+        // R (A P) for R_l (transposed now if A P's call did not)
+        if (nx.P && (rc = prepare_interp(&nx))) goto fail;
+        if (cudaStreamWaitEvent(s, nx.p_ready[l % 2], 0) != cudaSuccess) {
             rc = AMGT_ERR_CUDA;
             goto fail;
         }
         pm.mark(1, s);
         const int gp = h->prm.galerkin_by_level ? v.prec : AMGT_DOUBLE;
         amgt_bsr AP{};
-        nx.P = (l + 1 < L - 1) ? &P[l + 1] : nullptr;
-        nx.Pb = &h->lv[l + 1].P;
-        nx.Rb = &h->lv[l + 1].R;
-        nx.done = false;
-        if ((rc = spgemm_impl(gp, &v.A, &v.P, &AP, nullptr, stream, convert_next_interp, &nx))) goto fail;
+        if (l + 1 < L - 1) {
+            nx.P = &P[l + 1];
+            nx.Pb = &h->lv[l + 1].P;
+            nx.PRb = &h->lv[l + 1].R;
+            nx.pslot = (l + 1) % 2;
+        }
+        if ((rc = spgemm_impl(gp, &v.A, &v.P, &AP, nullptr, stream, prepare_interp, &nx))) goto fail;
+        if (nx.Tb == &v.P && (rc = transpose_pending(&nx))) {
+            amgt_bsr_free(&AP, stream);
+            goto fail;
+        }
+        if (cudaStreamWaitEvent(s, nx.r_ready[l % 2], 0) != cudaSuccess) {
+            amgt_bsr_free(&AP, stream);
+            rc = AMGT_ERR_CUDA;
+            goto fail;
+        }
         rc = amgt_spgemm(gp, &v.R, &AP, &h->lv[l + 1].A, nullptr, stream);
         amgt_bsr_free(&AP, stream);
         if (rc) goto fail;
@@ -608,7 +647,10 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     pm.mark(3, s);
     pm.accumulate(h->setup_ms);  // waits for the setup's last work
     if (nx.s2) cudaStreamDestroy(nx.s2);
-    if (nx.ready) cudaEventDestroy(nx.ready);
+    for (int i = 0; i < 2; ++i) {
+        if (nx.p_ready[i]) cudaEventDestroy(nx.p_ready[i]);
+        if (nx.r_ready[i]) cudaEventDestroy(nx.r_ready[i]);
+    }
     *out = h;
     return AMGT_OK;
 fail:
@@ -616,7 +658,10 @@ fail:
         cudaStreamSynchronize(nx.s2);
         cudaStreamDestroy(nx.s2);
     }
-    if (nx.ready) cudaEventDestroy(nx.ready);
+    for (int i = 0; i < 2; ++i) {
+        if (nx.p_ready[i]) cudaEventDestroy(nx.p_ready[i]);
+        if (nx.r_ready[i]) cudaEventDestroy(nx.r_ready[i]);
+    }
     cudaGetLastError();
     destroy_handle(h, s);
     return rc;
