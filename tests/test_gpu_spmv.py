@@ -20,6 +20,7 @@ TOL = {0: 1e-12, 1: 1e-5, 2: 1e-5, 3: 1e-5}
 def _mats(orc):
     return {
         "7pt_24x20x16": orc.laplacian(24, 20, 16),
+        "7pt_23x19x15": orc.laplacian(23, 19, 15),  # n % 4 != 0: scalar x loads, 2-byte 4-lane run
         "varcoef27_17x13x11": orc.varcoef27(17, 13, 11, seed=6),
         "ragged_rect": random_csr(orc, 1001, 1234, 20, seed=3),  # n % 4 != 0
         "long_rows": random_csr(orc, 400, 40000, 6, seed=4, dense_rows={8: 3000, 9: 2000, 200: 1500}),
@@ -45,7 +46,8 @@ def _check(orc, R, x, y0, alpha, beta, prec, got):
     assert np.all(err <= TOL[prec] * scale + 1e-300), f"max err/scale {np.max(err / (scale + 1e-300))}"
 
 
-@pytest.mark.parametrize("name", ["7pt_24x20x16", "varcoef27_17x13x11", "ragged_rect", "long_rows", "interp_T"])
+@pytest.mark.parametrize("name", ["7pt_24x20x16", "7pt_23x19x15", "varcoef27_17x13x11", "ragged_rect", "long_rows",
+                                  "interp_T"])
 @pytest.mark.parametrize("prec", [0, 1, 2, 3])
 @pytest.mark.parametrize("alpha,beta", [(1.0, 0.0), (-0.7, 1.0), (2.5, -0.3)])
 def test_spmv_matches_oracle(amgt, orc, mats, name, prec, alpha, beta):
@@ -129,8 +131,8 @@ def test_spmv_empty_matrix_scales_y(amgt, orc):
     np.testing.assert_array_equal(y.cpu().numpy(), 3.0 * np.arange(10))
 
 
-@pytest.mark.parametrize("name,want", [("7pt_24x20x16", 2), ("interp_T", 2), ("scaled_7pt", 1),
-                                       ("varcoef27_17x13x11", 0)])
+@pytest.mark.parametrize("name,want", [("7pt_24x20x16", 2), ("7pt_23x19x15", 2), ("interp_T", 2),
+                                       ("scaled_7pt", 1), ("varcoef27_17x13x11", 0)])
 def test_exact_storage_is_bit_identical(amgt, orc, mats, name, want):
     """amgt_bsr_make_exact picks the narrowest shadow that holds every value
     exactly (fp16: 7-point and interpolation weights; fp32: a 7-point
