@@ -15,8 +15,12 @@
 //          (fused), as hypre_BoomerAMGCycle does with relax 18
 //          (par_cycle.c:678-751, par_relax.c:1178-1260);
 //   solve  PCG (krylov/pcg.c:405-580), optionally flexible (Polak-Ribiere
-//          beta), with the scalars kept on the device and every iteration
-//          one CUDA graph launch plus one 8-byte read of ||r||^2.
+//          beta), with the scalars kept on the device; the whole iteration
+//          loop is one CUDA graph launch (a conditional while node whose
+//          body ends with the convergence test) and one read-back of the
+//          iteration count and the ||r||^2 history (if the runtime does
+//          not take the loop graph: one graph launch and one 8-byte read
+//          per iteration).
 // Dots are deterministic: fixed grids, per-CTA partials reduced in a fixed
 // order by one CTA.
 #include <algorithm>
@@ -250,6 +254,15 @@ struct amgt_amg {
     cudaStream_t graph_stream = nullptr;
     const double *graph_b = nullptr;
     double *graph_xout = nullptr;
+    // the whole iteration loop as one graph (a conditional while node); the
+    // loop's iteration count and ||r||^2 per iteration stay on the device
+    cudaGraphExec_t loop = nullptr;
+    double *loop_xout = nullptr;
+    bool loop_failed = false;
+    int *loop_it = nullptr;     // device: iterations done
+    double *loop_rr = nullptr;  // device: ||r||^2 after iteration k, k = 1 .. max_iter
+    double *loop_pinned = nullptr;
+    uint64_t graph_launches = 0, loop_launches = 0;  // our kernels per iteration in each graph
     double setup_ms[5] = {0, 0, 0, 0, 0};
     std::vector<double> hist;
 };
@@ -278,7 +291,11 @@ void destroy_handle(amgt_amg *h, cudaStream_t s)
 {
     if (!h) return;
     if (h->graph) cudaGraphExecDestroy(h->graph);
+    if (h->loop) cudaGraphExecDestroy(h->loop);
     if (h->graph_stream) cudaStreamDestroy(h->graph_stream);
+    if (h->loop_it) cudaFree(h->loop_it);
+    if (h->loop_rr) cudaFree(h->loop_rr);
+    if (h->loop_pinned) cudaFreeHost(h->loop_pinned);
     for (auto &v : h->lv) free_level(v, s);
     free_ptr(h->coarse_inv, s);
     free_ptr(h->r, s);
@@ -431,6 +448,79 @@ int pcg_iteration(amgt_amg *h, double *x, cudaStream_t s)
     return AMGT_OK;
 }
 
+// End of a loop iteration inside the loop graph: counts it, keeps ||r||^2
+// and sets the while condition with the host loop's test (relative
+// residual above tol and fewer than max_iter iterations).
+__global__ void pcg_continue_kernel(cudaGraphConditionalHandle cond, const double *__restrict__ scal, double tol,
+                                    int max_iter, int *__restrict__ it, double *__restrict__ rr_hist)
+{
+    const int k = ++*it;
+    const double rr = scal[S_RR];
+    rr_hist[k] = rr;
+    const double rel = sqrt(fmax(0.0, rr) / scal[S_BB]);
+    cudaGraphSetConditional(cond, (k < max_iter && !(rel <= tol)) ? 1u : 0u);
+}
+
+// Builds h->loop: a while node whose body is one PCG iteration plus
+// pcg_continue_kernel.  Returns an error (and the caller keeps the
+// one-graph-per-iteration loop) if the runtime does not take it.
+int build_loop_graph(amgt_amg *h, double *x)
+{
+    if (h->loop && h->loop_xout == x) return AMGT_OK;
+    if (h->loop) {
+        cudaGraphExecDestroy(h->loop);
+        h->loop = nullptr;
+    }
+    if (!h->graph_stream) AMGT_CUDA_TRY(cudaStreamCreateWithFlags(&h->graph_stream, cudaStreamNonBlocking));
+    if (!h->loop_it) AMGT_CUDA_TRY(cudaMalloc(&h->loop_it, sizeof(int)));
+    if (!h->loop_rr) AMGT_CUDA_TRY(cudaMalloc(&h->loop_rr, sizeof(double) * (h->prm.max_iter + 1)));
+    if (!h->loop_pinned) AMGT_CUDA_TRY(cudaMallocHost(&h->loop_pinned, sizeof(double) * (h->prm.max_iter + 2)));
+    cudaGraph_t g = nullptr;
+    AMGT_CUDA_TRY(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle cond;
+    cudaGraphNodeParams np = {};
+    cudaGraphNode_t node;
+    cudaGraph_t body = nullptr;
+    int rc = AMGT_OK;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = cond;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+    }
+    if (e == cudaSuccess) {
+        body = np.conditional.phGraph_out[0];
+        e = cudaStreamBeginCaptureToGraph(h->graph_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    }
+    if (e == cudaSuccess) {
+        const uint64_t c0 = amgt_kernel_launch_count();
+        rc = pcg_iteration(h, x, h->graph_stream);
+        if (rc == AMGT_OK) {
+            count_launch();
+            h->loop_launches = amgt_kernel_launch_count() - c0;
+            pcg_continue_kernel<<<1, 1, 0, h->graph_stream>>>(cond, h->scal, h->prm.tol, h->prm.max_iter, h->loop_it,
+                                                              h->loop_rr);
+            e = cudaGetLastError();
+        }
+        cudaGraph_t captured = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(h->graph_stream, &captured);
+        if (e == cudaSuccess) e = ee;
+    }
+    if (e == cudaSuccess && rc == AMGT_OK) e = cudaGraphInstantiate(&h->loop, g, 0);
+    cudaGraphDestroy(g);
+    if (rc != AMGT_OK) return rc;
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        h->loop = nullptr;
+        set_last_cuda_error(e, "loop graph", __FILE__, __LINE__);
+        return AMGT_ERR_CUDA;
+    }
+    h->loop_xout = x;
+    return AMGT_OK;
+}
+
 int build_graph(amgt_amg *h, double *x)
 {
     if (h->graph && h->graph_xout == x) return AMGT_OK;
@@ -441,7 +531,9 @@ int build_graph(amgt_amg *h, double *x)
     if (!h->graph_stream) AMGT_CUDA_TRY(cudaStreamCreateWithFlags(&h->graph_stream, cudaStreamNonBlocking));
     cudaGraph_t g = nullptr;
     AMGT_CUDA_TRY(cudaStreamBeginCapture(h->graph_stream, cudaStreamCaptureModeThreadLocal));
+    const uint64_t c0 = amgt_kernel_launch_count();
     const int rc = pcg_iteration(h, x, h->graph_stream);
+    h->graph_launches = amgt_kernel_launch_count() - c0;
     const cudaError_t e = cudaStreamEndCapture(h->graph_stream, &g);
     if (rc != AMGT_OK) {
         if (g) cudaGraphDestroy(g);
@@ -688,10 +780,34 @@ int amgt_amg_solve(amgt_amg *h, const double *b, double *x, int *iterations, dou
         AMGT_TRY(dot(h, h->r, h->z, S_RZ, OP_STORE, s));
         AMGT_CUDA_TRY(cudaMemcpyAsync(h->p, h->z, sizeof(double) * h->n0, cudaMemcpyDeviceToDevice, s));
         uint64_t per_iter = 0;
+        if (h->prm.use_graph && !h->loop_failed) {
+            // one launch for the whole loop; one read-back at its end
+            const int lrc = build_loop_graph(h, x);
+            per_iter = h->loop_launches;
+            if (lrc == AMGT_OK) {
+                AMGT_CUDA_TRY(cudaMemsetAsync(h->loop_it, 0, sizeof(int), s));
+                AMGT_CUDA_TRY(cudaGraphLaunch(h->loop, s));
+                AMGT_CUDA_TRY(cudaMemcpyAsync(h->loop_pinned, h->loop_it, sizeof(int), cudaMemcpyDeviceToHost, s));
+                AMGT_CUDA_TRY(cudaMemcpyAsync(h->loop_pinned + 1, h->loop_rr + 1, sizeof(double) * h->prm.max_iter,
+                                              cudaMemcpyDeviceToHost, s));
+                AMGT_CUDA_TRY(cudaStreamSynchronize(s));
+                it = *reinterpret_cast<const int *>(h->loop_pinned);
+                for (int k = 1; k <= it; ++k) {
+                    rel = std::sqrt(std::max(0.0, h->loop_pinned[k]) / bb);
+                    h->hist.push_back(rel);
+                }
+                for (int k = 0; k < it; ++k)
+                    for (uint64_t j = 0; j < per_iter; ++j) count_launch();
+                if (iterations) *iterations = it;
+                if (rel_res) *rel_res = rel;
+                return AMGT_OK;
+            }
+            if (lrc != AMGT_ERR_CUDA) return lrc;
+            h->loop_failed = true;  // the runtime did not take the loop graph: one graph per iteration
+        }
         if (h->prm.use_graph) {
-            const uint64_t c0 = amgt_kernel_launch_count();
             AMGT_TRY(build_graph(h, x));
-            per_iter = amgt_kernel_launch_count() - c0;
+            per_iter = h->graph_launches;
         }
         for (it = 1; it <= h->prm.max_iter; ++it) {
             if (h->prm.use_graph) {

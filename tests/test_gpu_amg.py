@@ -99,16 +99,37 @@ def test_amg_levels_match_oracle_galerkin(amgt, orc):
         assert (info["rows"], info["blocks"]) == (n, nb)
 
 
-def test_amg_graph_and_direct_launches_agree_bit_for_bit(amgt, orc):
+@pytest.mark.parametrize("max_iter", [100, 4])
+def test_amg_graph_and_direct_launches_agree_bit_for_bit(amgt, orc, max_iter):
+    """The graph path (the whole PCG loop as one launch: a conditional while
+    node whose body ends with the convergence test) and direct launches with
+    a host test per iteration give the same x, iteration count and residual
+    history, also when max_iter stops the loop and on a second solve that
+    reuses the built graph."""
     amgt.set_level_policy([0])
-    dims = (40, 36, 32)
-    A = orc.laplacian(*dims)
-    Ps = orc.geometric_hierarchy(*dims)
-    b = torch.from_numpy(A.to_scipy() @ orc.rand_uniform(4, A.n)).cuda()
-    x1, it1, _ = _gpu_solver(amgt, A, Ps, use_graph=1).solve(b)
-    x2, it2, _ = _gpu_solver(amgt, A, Ps, use_graph=0).solve(b)
-    assert it1 == it2
-    assert torch.equal(x1, x2)
+    try:
+        dims = (40, 36, 32)
+        A = orc.laplacian(*dims)
+        Ps = orc.geometric_hierarchy(*dims)
+        S1 = _gpu_solver(amgt, A, Ps, use_graph=1, max_iter=max_iter)
+        S2 = _gpu_solver(amgt, A, Ps, use_graph=0, max_iter=max_iter)
+        x1 = torch.zeros(A.n, dtype=torch.float64, device="cuda")  # the same x buffer: the graph is reused
+        x2 = torch.zeros_like(x1)
+        for seed in (4, 5):
+            b = torch.from_numpy(A.to_scipy() @ orc.rand_uniform(seed, A.n)).cuda()
+            x1.zero_()
+            x2.zero_()
+            _, it1, r1 = S1.solve(b, x1)
+            _, it2, r2 = S2.solve(b, x2)
+            assert it1 == it2 and r1 == r2
+            if max_iter == 4:
+                assert it1 == 4 and r1 > 1e-8
+            else:
+                assert it1 < max_iter and r1 <= 1e-8
+            assert torch.equal(x1, x2)
+            assert np.array_equal(S1.history(), S2.history())
+    finally:
+        amgt.set_level_policy([])
 
 
 def test_amg_setup_orders_inputs_still_being_copied(amgt, orc):
