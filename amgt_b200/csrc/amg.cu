@@ -587,6 +587,8 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     int rc = AMGT_OK;
     PhaseMarks pm;
     NextInterp nx;
+    double *dense = nullptr, *dense_h = nullptr;  // the coarsest operator, dense, on device / host
+    cudaEvent_t dense_ready = nullptr;
     pm.mark(-1, s);
     // the second stream starts after everything the caller queued on `s`
     // before this call (the inputs may still be arriving there)
@@ -651,6 +653,24 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         pm.mark(2, s);
     }
     h->lv[L - 1].prec = amgt_precision_for_level(L - 1);
+    // coarsest: its dense form goes to the host now and is inverted there
+    // while the GPU runs the exactness checks, norms and shadows queued below
+    h->nc = h->lv[L - 1].n;
+    if (h->nc > h->prm.max_coarse_rows) {
+        rc = AMGT_ERR_TOO_LARGE;
+        goto fail;
+    }
+    if ((rc = alloc_n(&dense, (size_t)h->nc * h->nc, s))) goto fail;
+    if (cudaMallocHost(&dense_h, sizeof(double) * h->nc * h->nc) != cudaSuccess ||
+        cudaEventCreateWithFlags(&dense_ready, cudaEventDisableTiming) != cudaSuccess) {
+        rc = AMGT_ERR_CUDA;
+        goto fail;
+    }
+    AMGT_CUDA_TRY(cudaMemsetAsync(dense, 0, sizeof(double) * h->nc * h->nc, s));
+    AMGT_LAUNCH(bsr_to_dense_kernel, grid_for(256, h->nc, h->sm_count, 8), 256, 0, s, h->nc, h->nc,
+                h->lv[L - 1].A.blcPtr, h->lv[L - 1].A.blcIdx, h->lv[L - 1].A.blcVal, dense);
+    AMGT_CUDA_TRY(cudaMemcpyAsync(dense_h, dense, sizeof(double) * h->nc * h->nc, cudaMemcpyDeviceToHost, s));
+    AMGT_CUDA_TRY(cudaEventRecord(dense_ready, s));
     // exact narrow storage of the operators used in fp64 (level 0, fp64
     // levels and transfers): one value check each, one read-back per 15
     if (h->prm.exact_storage) {
@@ -705,27 +725,24 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         if ((rc = alloc_n(&v.u, v.n, s)) || (rc = alloc_n(&v.t, v.n, s))) goto fail;
         if (l > 0 && ((rc = alloc_n(&v.f, v.n, s)) || (rc = alloc_n(&v.s, v.n, s)))) goto fail;
     }
-    // coarsest: dense inverse
+    // coarsest: inverted on the host (the GPU still runs the work queued
+    // above), back to the device
+    if (cudaEventSynchronize(dense_ready) != cudaSuccess) {
+        rc = AMGT_ERR_CUDA;
+        goto fail;
+    }
     {
-        Level &c = h->lv[L - 1];
-        h->nc = c.n;
-        if (c.n > h->prm.max_coarse_rows) { rc = AMGT_ERR_TOO_LARGE; goto fail; }
-        double *D = nullptr;
-        if ((rc = alloc_n(&D, (size_t)c.n * c.n, s))) goto fail;
-        AMGT_CUDA_TRY(cudaMemsetAsync(D, 0, sizeof(double) * c.n * c.n, s));
-        AMGT_LAUNCH(bsr_to_dense_kernel, grid_for(256, c.n, h->sm_count, 8), 256, 0, s, c.n, c.n, c.A.blcPtr,
-                    c.A.blcIdx, c.A.blcVal, D);
-        std::vector<double> hd((size_t)c.n * c.n);
-        AMGT_CUDA_TRY(cudaMemcpyAsync(hd.data(), D, sizeof(double) * hd.size(), cudaMemcpyDeviceToHost, s));
-        AMGT_CUDA_TRY(cudaStreamSynchronize(s));
-        if (!host_invert(c.n, hd)) {
-            free_ptr(D, s);
+        const size_t nn = (size_t)h->nc * h->nc;
+        std::vector<double> hd(dense_h, dense_h + nn);
+        if (!host_invert(h->nc, hd)) {
             rc = AMGT_ERR_INVALID;
             goto fail;
         }
-        AMGT_CUDA_TRY(cudaMemcpyAsync(D, hd.data(), sizeof(double) * hd.size(), cudaMemcpyHostToDevice, s));
-        h->coarse_inv = D;
-        if (L == 1) c.s = nullptr;
+        std::copy(hd.begin(), hd.end(), dense_h);
+        AMGT_CUDA_TRY(cudaMemcpyAsync(dense, dense_h, sizeof(double) * nn, cudaMemcpyHostToDevice, s));
+        h->coarse_inv = dense;
+        dense = nullptr;
+        if (L == 1) h->lv[L - 1].s = nullptr;
     }
     // Krylov vectors and scalars
     h->n0 = h->lv[0].n;
@@ -737,7 +754,9 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     AMGT_CUDA_TRY(cudaMemsetAsync(h->scal, 0, sizeof(double) * S_NSCAL, s));
     AMGT_CUDA_TRY(cudaMallocHost(&h->pinned, sizeof(double) * 4));
     pm.mark(3, s);
-    pm.accumulate(h->setup_ms);  // waits for the setup's last work
+    pm.accumulate(h->setup_ms);  // waits for the setup's last work (the inverse's copy from dense_h included)
+    cudaFreeHost(dense_h);
+    cudaEventDestroy(dense_ready);
     if (nx.s2) cudaStreamDestroy(nx.s2);
     for (int i = 0; i < 2; ++i) {
         if (nx.p_ready[i]) cudaEventDestroy(nx.p_ready[i]);
@@ -750,6 +769,10 @@ fail:
         cudaStreamSynchronize(nx.s2);
         cudaStreamDestroy(nx.s2);
     }
+    cudaStreamSynchronize(s);  // no copy from or to dense_h in flight
+    if (dense) free_ptr(dense, s);
+    if (dense_h) cudaFreeHost(dense_h);
+    if (dense_ready) cudaEventDestroy(dense_ready);
     for (int i = 0; i < 2; ++i) {
         if (nx.p_ready[i]) cudaEventDestroy(nx.p_ready[i]);
         if (nx.r_ready[i]) cudaEventDestroy(nx.r_ready[i]);

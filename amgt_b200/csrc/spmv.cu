@@ -295,14 +295,18 @@ spmv_epi_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *
 
 // l1 row norms sum_j |a_ij| (hypre_ParCSRComputeL1Norms option 1,
 // AmgT_HYPRE/src/parcsr_ls/ams.c:627-636), one thread per scalar row.
-__global__ void l1_norm_kernel(int m, const int *__restrict__ ptr, const double *__restrict__ val,
+// PREC: the 8-byte values or an exact narrow shadow (same values, widened
+// exactly: the same sums with fewer bytes read).
+template <int PREC>
+__global__ void l1_norm_kernel(int m, const int *__restrict__ ptr, const void *__restrict__ val,
                                double *__restrict__ l1, int invert)
 {
     for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < m; row += gridDim.x * blockDim.x) {
         const int b = row >> 2, q = row & 3;
         double s = 0.0;
         for (int k = ptr[b]; k < ptr[b + 1]; ++k) {
-            const double *v = val + 16LL * k + 4 * q;
+            double v[4];
+            load_block_row<PREC>(val, k, q, v);
             s += fabs(v[0]) + fabs(v[1]) + fabs(v[2]) + fabs(v[3]);
         }
         l1[row] = invert ? (s != 0.0 ? 1.0 / s : 0.0) : s;
@@ -574,8 +578,15 @@ int spmv_dot(int prec, const amgt_bsr *A, const double *u, double *out, double *
 
 int bsr_l1_norms(const amgt_bsr *A, double *l1, int invert, cudaStream_t s, int sm_count)
 {
-    AMGT_LAUNCH(l1_norm_kernel, grid_for(256, A->row, sm_count, 8), 256, 0, s, A->row, A->blcPtr, A->blcVal, l1,
-                invert);
+    const int mode = storage_mode(A, AMGT_DOUBLE);
+    const void *val = value_array(A, mode);
+    const int grid = grid_for(256, A->row, sm_count, 8);
+    if (mode == kExact16)
+        AMGT_LAUNCH(l1_norm_kernel<kExact16>, grid, 256, 0, s, A->row, A->blcPtr, val, l1, invert);
+    else if (mode == kExact32)
+        AMGT_LAUNCH(l1_norm_kernel<kExact32>, grid, 256, 0, s, A->row, A->blcPtr, val, l1, invert);
+    else
+        AMGT_LAUNCH(l1_norm_kernel<AMGT_DOUBLE>, grid, 256, 0, s, A->row, A->blcPtr, A->blcVal, l1, invert);
     return AMGT_OK;
 }
 

@@ -216,3 +216,44 @@ def test_amg_solve_reuses_setup_and_initial_guess(amgt, orc):
     b3 = torch.from_numpy(A.to_scipy() @ orc.rand_uniform(9, A.n)).cuda()
     _, it3, rel3 = S.solve(b3)
     assert rel3 <= 1e-8 and abs(it3 - it) <= 2
+
+
+def test_amg_single_level_dense_inverse_exact(amgt, orc):
+    """One level: the coarsest (only) operator is inverted exactly (Cholesky
+    when it exists, else Gauss-Jordan with partial pivoting), so PCG with
+    that preconditioner converges in one iteration, also for a
+    non-symmetric matrix with a zero first pivot."""
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(7)
+    n = 40
+    M = rng.standard_normal((n, n))
+    M[0, 0] = 0.0  # first pivot would be zero without row exchanges
+    M += np.diag(np.where(np.arange(n) == 0, 0.0, n))
+    S = sp.csr_matrix(M)
+    A = orc.CSR(n, n, S.indptr.astype(np.int32), S.indices.astype(np.int32), S.data.copy())
+    b = rng.standard_normal(n)
+    amgt.set_level_policy([0])
+    try:
+        x, it, rel = _gpu_solver(amgt, A, []).solve(torch.from_numpy(b).cuda())
+        assert it == 1 and rel <= 1e-12
+        np.testing.assert_allclose(x.cpu().numpy(), np.linalg.solve(M, b), rtol=1e-10, atol=1e-12)
+    finally:
+        amgt.set_level_policy([])
+
+
+def test_amg_singular_coarsest_is_reported(amgt, orc):
+    """A zero row makes the coarsest operator singular: setup returns
+    AMGT_ERR_INVALID (the elimination finds a zero pivot)."""
+    from amgt_b200._lib import AmgtError
+
+    A = orc.laplacian(4, 4, 2)
+    a = A.a.copy()
+    a[A.ia[5]:A.ia[6]] = 0.0
+    amgt.set_level_policy([0])
+    try:
+        with pytest.raises(AmgtError) as ei:
+            _gpu_solver(amgt, orc.CSR(A.m, A.n, A.ia, A.ja, a), [])
+        assert ei.value.status == 1
+    finally:
+        amgt.set_level_policy([])
