@@ -45,6 +45,8 @@ constexpr int kNumWin = 256;      // pairs per window of the numeric pair -> A b
 
 __device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
 
+inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
 // Appends the row's non-zero-product pairs to the warp's list s[]; returns
 // the count (the caller bounds it via the upper bound).  Up to 32 A blocks
 // at a time: lane i fetches A block i's B row range, a warp scan of the
@@ -260,8 +262,11 @@ __device__ int sym_reduce_hashed(int lane, int cnt, unsigned long long *s, int *
 
 // Upper bound of pairs per A block row (sum of the selected B row
 // lengths); ub[brA] = 0 so that an exclusive scan gives scratch offsets.
-__global__ void spgemm_ub_kernel(int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
-                                 const int *__restrict__ bptr, int64_t *__restrict__ ub)
+// Also clears the symbolic pass's counters: ccnt[0 .. brA], csrcnt[0 .. m],
+// stats[0 .. 3] and *nmedium.
+__global__ void spgemm_ub_kernel(int m, int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
+                                 const int *__restrict__ bptr, int64_t *__restrict__ ub, int *__restrict__ ccnt,
+                                 int *__restrict__ csrcnt, int64_t *__restrict__ stats, int *__restrict__ nmedium)
 {
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= brA; b += gridDim.x * blockDim.x) {
         long long t = 0;
@@ -271,6 +276,14 @@ __global__ void spgemm_ub_kernel(int brA, const int *__restrict__ aptr, const in
                 t += bptr[k + 1] - bptr[k];
             }
         ub[b] = t;
+        ccnt[b] = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (4 * b + q <= m) csrcnt[4 * b + q] = 0;
+        if (b == 0) {
+            stats[0] = stats[1] = stats[2] = stats[3] = 0;
+            *nmedium = 0;
+        }
     }
 }
 
@@ -828,6 +841,7 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     amgt_bsr Atmp = *A, Btmp = *B;
     bool ownA = false, ownB = false;
     int rc = AMGT_OK;
+    unsigned char *arena = nullptr, *arena2 = nullptr;  // scratch (pieces below point into them)
     int *ccnt = nullptr, *csrcnt = nullptr, *large = nullptr, *csr_i = nullptr, *csr_tmp = nullptr;
     int64_t *stats = nullptr, *ub = nullptr, *ub_off = nullptr;
     int *skey = nullptr;
@@ -847,17 +861,25 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
             ownB = true;
         }
     }
-    if ((rc = alloc_n(&C->blcPtr, brA + 1, s)) || (rc = alloc_n(&ccnt, brA + 1, s)) ||
-        (rc = alloc_n(&csrcnt, m + 1, s)) || (rc = alloc_n(&large, 2 * (size_t)brA + 1, s)) ||
-        (rc = alloc_n(&stats, 4, s)) || (rc = alloc_n(&ub, (size_t)brA + 1, s)) ||
-        (rc = alloc_n(&ub_off, (size_t)brA + 1, s)))
-        goto fail;
-    AMGT_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(int64_t) * 4, s));
-    AMGT_CUDA_TRY(cudaMemsetAsync(ccnt, 0, sizeof(int) * (brA + 1), s));
-    AMGT_CUDA_TRY(cudaMemsetAsync(csrcnt, 0, sizeof(int) * (m + 1), s));
+    {
+        // the per-row scratch in one allocation (256-byte aligned pieces)
+        const size_t o_stats = 0, o_ub = o_stats + 256, o_uboff = o_ub + align256(8 * ((size_t)brA + 1)),
+                     o_ccnt = o_uboff + align256(8 * ((size_t)brA + 1)),
+                     o_csr = o_ccnt + align256(4 * ((size_t)brA + 1)),
+                     o_large = o_csr + align256(4 * ((size_t)m + 1)),
+                     o_end = o_large + align256(4 * (2 * (size_t)brA + 1));
+        if ((rc = alloc_n(&C->blcPtr, brA + 1, s)) || (rc = alloc_n(&arena, o_end, s))) goto fail;
+        stats = reinterpret_cast<int64_t *>(arena + o_stats);
+        ub = reinterpret_cast<int64_t *>(arena + o_ub);
+        ub_off = reinterpret_cast<int64_t *>(arena + o_uboff);
+        ccnt = reinterpret_cast<int *>(arena + o_ccnt);
+        csrcnt = reinterpret_cast<int *>(arena + o_csr);
+        large = reinterpret_cast<int *>(arena + o_large);
+    }
     // per-row pair bounds -> scratch offsets for the rows' sorted patterns
-    AMGT_LAUNCH(spgemm_ub_kernel, grid_for(256, brA + 1LL, st->sm_count, 8), 256, 0, s, brA, A->blcPtr, A->blcIdx,
-                B->blcPtr, ub);
+    // (the kernel also clears the counters)
+    AMGT_LAUNCH(spgemm_ub_kernel, grid_for(256, brA + 1LL, st->sm_count, 8), 256, 0, s, m, brA, A->blcPtr,
+                A->blcIdx, B->blcPtr, ub, ccnt, csrcnt, stats, large + 2 * brA);
     if ((rc = exclusive_scan_i64(ub, ub_off, brA + 1, s))) goto fail;
     {
         // scratch size: the host-side bound nblk(A) * longest B row when it is
@@ -871,14 +893,17 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
             cap = h[2];
             AMGT_CUDA_TRY(cudaMemsetAsync(&stats[2], 0, sizeof(int64_t), s));
         }
-        if ((rc = alloc_n(&skey, (size_t)cap, s)) || (rc = alloc_n(&smap, (size_t)cap, s)) ||
-            (rc = alloc_n(&pslot, (size_t)cap, s)))
-            goto fail;
+        // pattern keys, bitmaps and pair slots in one allocation
+        const size_t o_map = align256(4 * (size_t)cap), o_slot = o_map + align256(2 * (size_t)cap),
+                     o_end = o_slot + align256(2 * (size_t)cap);
+        if ((rc = alloc_n(&arena2, o_end, s))) goto fail;
+        skey = reinterpret_cast<int *>(arena2);
+        smap = reinterpret_cast<uint16_t *>(arena2 + o_map);
+        pslot = reinterpret_cast<uint16_t *>(arena2 + o_slot);
     }
     if (brA > 0) {
         // medium-row list and count live behind the large list (2 * brA + 1 ints)
-        int *medium = large + brA, *nmedium = large + 2 * brA;
-        AMGT_CUDA_TRY(cudaMemsetAsync(nmedium, 0, sizeof(int), s));
+        int *medium = large + brA, *nmedium = large + 2 * brA;  // *nmedium cleared by spgemm_ub_kernel
         AMGT_LAUNCH((spgemm_symbolic_kernel<256, kSymWarps>), grid_for(kSymWarps, brA, st->sm_count, 16),
                     32 * kSymWarps, 0, s, m, brA, A->blcPtr, A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap,
                     ccnt, csrcnt, large, stats, ub_off, skey, smap, nullptr, nullptr, medium, nmedium, pslot,
@@ -956,14 +981,12 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     if (rc) goto fail;
     C->csr_nnz = nnzC;
     C->avg_nnz = nbC ? (double)nnzC / nbC : 0.0;
-    free_ptr(ccnt, s); free_ptr(csrcnt, s); free_ptr(large, s); free_ptr(stats, s); free_ptr(csr_tmp, s);
-    free_ptr(ub, s); free_ptr(ub_off, s); free_ptr(skey, s); free_ptr(smap, s); free_ptr(pslot, s);
+    free_ptr(arena, s); free_ptr(arena2, s); free_ptr(csr_tmp, s);
     if (ownA) { free_ptr(Atmp.blcVal_fp32, s); free_ptr(Atmp.blcVal_fp16, s); free_ptr(Atmp.blcVal_bf16, s); }
     if (ownB) { free_ptr(Btmp.blcVal_fp32, s); free_ptr(Btmp.blcVal_fp16, s); free_ptr(Btmp.blcVal_bf16, s); }
     return AMGT_OK;
 fail:
-    free_ptr(ccnt, s); free_ptr(csrcnt, s); free_ptr(large, s); free_ptr(stats, s); free_ptr(csr_tmp, s);
-    free_ptr(ub, s); free_ptr(ub_off, s); free_ptr(skey, s); free_ptr(smap, s); free_ptr(pslot, s);
+    free_ptr(arena, s); free_ptr(arena2, s); free_ptr(csr_tmp, s);
     if (ownA) { free_ptr(Atmp.blcVal_fp32, s); free_ptr(Atmp.blcVal_fp16, s); free_ptr(Atmp.blcVal_bf16, s); }
     if (ownB) { free_ptr(Btmp.blcVal_fp32, s); free_ptr(Btmp.blcVal_fp16, s); free_ptr(Btmp.blcVal_bf16, s); }
     amgt_bsr_free(C, stream);
