@@ -86,18 +86,16 @@ void free_ptr(T *&p, cudaStream_t s)
 }
 
 // Per-device state: a device error word that kernels raise instead of
-// trapping, and a pinned host staging buffer for the few scalars the host
-// must read back.
+// trapping, and the SM count.
 struct DeviceState {
     int *err;            // device: 0 = ok, else first error code raised
-    int64_t *pinned;     // host pinned, 64 slots (the last holds the error word)
     int sm_count;
 };
 int device_state(DeviceState **st);
 
-// Reports the device error word as the last read_back on this device
-// copied it (no further synchronisation) and clears a raised word.  Call
-// right after a read_back.
+// Reports the device error word as the calling thread's last read_back on
+// this device copied it (no further synchronisation) and clears a raised
+// word.  Call right after a read_back.
 int check_device_error(cudaStream_t s);
 
 // Error codes a kernel may raise into DeviceState::err
@@ -164,9 +162,10 @@ int exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s);
 // Exclusive scan of n 64-bit ints.
 int exclusive_scan_i64(const int64_t *in, int64_t *out, int n, cudaStream_t s);
 
-// Device-to-host read of `count` (<= 63) int64 slots into
-// DeviceState::pinned and a stream synchronize; returns pointer to the
-// pinned slots.
+// Device-to-host read of `count` (<= 63) int64 slots into the calling
+// thread's pinned staging for this device, and a stream synchronize;
+// returns a pointer to the pinned slots (valid until the thread's next
+// read_back on the device).
 int read_back(const int64_t *dev, int count, cudaStream_t s, const int64_t **host);
 
 // ----------------------------------------------------------------- bitmaps

@@ -10,6 +10,8 @@
 // bitmap table.  Two passes: count (sorts, keeps the sorted pairs in
 // scratch, sizes the arrays with one host read-back), then fill (block
 // columns, bitmaps, zero-padded values from the kept pairs).
+#include <atomic>
+
 #include <cub/device/device_radix_sort.cuh>
 
 #include "rowunion.cuh"
@@ -909,7 +911,7 @@ int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int 
     int rc = AMGT_OK;
     const int64_t *h = nullptr;
     int nb = 0;
-    static bool smem_set[64];  // per device: the large-row kernels' shared-memory opt-in
+    static std::atomic<bool> smem_set[64];  // per device: the large-row kernels' shared-memory opt-in
     int dev = 0;
     AMGT_CUDA_TRY(cudaGetDevice(&dev));
     if (dev >= 0 && dev < 64 && !smem_set[dev]) {

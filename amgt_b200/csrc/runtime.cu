@@ -197,7 +197,6 @@ int device_state(DeviceState **st)
         DeviceState &s = g_states[dev];
         AMGT_CUDA_TRY(cudaMalloc(&s.err, sizeof(int) * 4));
         AMGT_CUDA_TRY(cudaMemset(s.err, 0, sizeof(int) * 4));
-        AMGT_CUDA_TRY(cudaMallocHost(&s.pinned, sizeof(int64_t) * 64));
         AMGT_CUDA_TRY(cudaDeviceGetAttribute(&s.sm_count, cudaDevAttrMultiProcessorCount, dev));
         g_state_ready[dev] = true;
     }
@@ -210,13 +209,41 @@ int device_state(DeviceState **st)
 // raised word is cleared on the stream and reported once.
 static constexpr int kErrSlot = 63;
 
+// Pinned staging for read-backs, per host thread and device, so that two
+// host threads can read back on one device at once (the AMG setup converts
+// its interpolations on a second thread); freed when the thread exits.
+struct Staging {
+    int64_t *p[kMaxDevices] = {};
+    ~Staging()
+    {
+        for (int64_t *q : p)
+            if (q) cudaFreeHost(q);
+    }
+};
+static thread_local Staging g_staging;
+
+static int staging(int64_t **out)
+{
+    int dev = 0;
+    AMGT_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return AMGT_ERR_NO_DEVICE;
+    if (!g_staging.p[dev]) {
+        AMGT_CUDA_TRY(cudaMallocHost(&g_staging.p[dev], sizeof(int64_t) * 64));
+        for (int i = 0; i < 64; ++i) g_staging.p[dev][i] = 0;
+    }
+    *out = g_staging.p[dev];
+    return AMGT_OK;
+}
+
 int check_device_error(cudaStream_t s)
 {
     DeviceState *st;
     AMGT_TRY(device_state(&st));
-    const int h = (int)st->pinned[kErrSlot];
+    int64_t *pin;
+    AMGT_TRY(staging(&pin));
+    const int h = (int)pin[kErrSlot];
     if (h != 0) {
-        st->pinned[kErrSlot] = 0;
+        pin[kErrSlot] = 0;
         AMGT_CUDA_TRY(cudaMemsetAsync(st->err, 0, sizeof(int), s));
         snprintf(g_cuda_msg, sizeof(g_cuda_msg), "device error word raised: %d", h);
         return AMGT_ERR_DEVICE;
@@ -229,11 +256,13 @@ int read_back(const int64_t *dev, int count, cudaStream_t s, const int64_t **hos
     DeviceState *st;
     AMGT_TRY(device_state(&st));
     if (count > kErrSlot) return AMGT_ERR_INVALID;
-    st->pinned[kErrSlot] = 0;
-    AMGT_CUDA_TRY(cudaMemcpyAsync(st->pinned, dev, sizeof(int64_t) * count, cudaMemcpyDeviceToHost, s));
-    AMGT_CUDA_TRY(cudaMemcpyAsync(&st->pinned[kErrSlot], st->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    int64_t *pin;
+    AMGT_TRY(staging(&pin));
+    pin[kErrSlot] = 0;
+    AMGT_CUDA_TRY(cudaMemcpyAsync(pin, dev, sizeof(int64_t) * count, cudaMemcpyDeviceToHost, s));
+    AMGT_CUDA_TRY(cudaMemcpyAsync(&pin[kErrSlot], st->err, sizeof(int), cudaMemcpyDeviceToHost, s));
     AMGT_CUDA_TRY(cudaStreamSynchronize(s));
-    *host = st->pinned;
+    *host = pin;
     return AMGT_OK;
 }
 

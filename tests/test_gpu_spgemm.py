@@ -126,3 +126,41 @@ def test_spgemm_structure_matches_hypre_known_answers(amgt, orc, case):
     assert C.s.csr_nnz == case["nnz_cpu"]
     C.free()
     torch.cuda.empty_cache()
+
+
+def test_two_host_threads_on_one_device(amgt, orc):
+    """Two host threads convert and multiply at once, each on its own
+    stream: every size read-back goes through that thread's own pinned
+    staging, so both results stay bit-exact."""
+    import threading
+
+    A = orc.laplacian(24, 20, 16)
+    P, _ = orc.interp(24, 20, 16)
+    RC, _ = orc.spgemm(orc.csr2bsr(A), orc.csr2bsr(P))
+    results, errors = [None, None], []
+
+    def work(i):
+        try:
+            torch.cuda.set_device(0)
+            st = torch.cuda.Stream()
+            with torch.cuda.stream(st):
+                outs = []
+                for _ in range(20):
+                    GA = amgt.Bsr.from_csr(*to_dev(A), stream=st)
+                    GP = amgt.Bsr.from_csr(*to_dev(P), stream=st)
+                    GC, _ = amgt.spgemm(GA, GP, want_csr=False, stream=st)
+                    outs.append(GC)
+                st.synchronize()
+                results[i] = outs
+        except Exception as e:  # reported by the main thread
+            errors.append(e)
+
+    threads = [threading.Thread(target=work, args=(i,)) for i in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for outs in results:
+        for GC in outs:
+            assert_bsr_equal(GC, RC)
