@@ -7,7 +7,10 @@
  * otherwise.  Every entry point returns an amgt_status (0 = success) and is
  * stream-ordered on the stream it is given (NULL = the legacy default
  * stream); an entry point only blocks the host where it must learn a size
- * that decides an allocation (noted per function).
+ * that decides an allocation (noted per function).  Host threads may call
+ * the library at the same time on one device (each thread stages its
+ * read-backs in its own pinned buffer); one handle (amgt_amg) belongs to
+ * one thread at a time.
  *
  * Reference interfaces replaced (paths inside the AmgT repository,
  * R = AmgT_HYPRE/src):
