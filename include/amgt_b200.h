@@ -9,8 +9,9 @@
  * stream); an entry point only blocks the host where it must learn a size
  * that decides an allocation (noted per function).  Host threads may call
  * the library at the same time on one device (each thread stages its
- * read-backs in its own pinned buffer); one handle (amgt_amg) belongs to
- * one thread at a time.
+ * read-backs in its own pinned buffer; the device error word is shared, so
+ * AMGT_ERR_DEVICE may reach the thread that reads back first); one handle
+ * (amgt_amg) belongs to one thread at a time.
  *
  * Reference interfaces replaced (paths inside the AmgT repository,
  * R = AmgT_HYPRE/src):
