@@ -6,7 +6,10 @@ seeded uniform x.  One step = one SpMV y = A*x on the finest level, the
 operation that drives smoothing and residuals in solve.  The run also
 builds the Galerkin hierarchy (A_{l+1} = P^T (A_l P), linear interpolation
 P, mBSR SpGEMM) and reports per level the A P, P^T and R (A P) times (best
-of three calls, after a warm-up build) and SpMV GB/s.
+of three calls, after a warm-up build) and SpMV GB/s; then AMG-PCG setup +
+solve to 1e-8 in fp64 and in the mixed form, on this operator and on the
+27-point variable-coefficient 96^3 operator (the mixed-precision
+configuration).
 
 python bench.py [--gpus N] [--steps K] [--warmup W] [--impl amgt|reference]
 Under torchrun (N > 1) every rank runs the same workload on its own GPU
@@ -511,6 +514,23 @@ def run_amgt(args):
         setup_solve["e2e_fp64"] = amg_e2e(amgt, torch, A_host, Ps_host, b_host, [0], 0, 0)
         setup_solve["problem"] = (f"3D 7-point Poisson {GRID[0]}^3, b uniform[-1,1] seed 0, linear-interpolation "
                                   f"hierarchy ({len(Ps_host) + 1} levels), PCG + V(1,1) l1-Jacobi, tol 1e-8")
+        # the mixed-precision configuration: 27-point variable-coefficient
+        # diffusion 96^3 (log-normal cell coefficients, seed 1), whose values
+        # no narrow format holds exactly
+        vdims = (96, 96, 96)
+        V_host = problems.varcoef27(*vdims, seed=1)
+        VPs_host = geometric_interps(problems, vdims)
+        vb_host = problems.rand_uniform(0, V_host[0])
+        vf64 = amg_setup_solve(amgt, torch, V_host, VPs_host, vb_host, [0], 0, 0)
+        vmix = amg_setup_solve(amgt, torch, V_host, VPs_host, vb_host, MIXED_POLICY, 1, 1)
+        vc = {"problem": "3D 27-point variable-coefficient diffusion 96^3 (884,736 rows, 23.4 M nonzeros), "
+                         "b uniform[-1,1] seed 0, linear-interpolation hierarchy, PCG + V(1,1) l1-Jacobi, tol 1e-8"}
+        for name, rres in (("fp64", vf64), ("mixed", vmix)):
+            vc[name] = {k: round(rres[k], 6) if isinstance(rres[k], float) else rres[k]
+                        for k in ("setup_s", "solve_s", "iters", "relres_fp64_verified")}
+            vc[name]["total_s"] = round(rres["setup_s"] + rres["solve_s"], 5)
+        vc["mixed"]["speedup_vs_fp64"] = round(vc["fp64"]["total_s"] / vc["mixed"]["total_s"], 3)
+        setup_solve["varcoef27_96"] = vc
         if world == 1 and rank == 0 and not args.no_cpu:
             setup_solve["cpu_oracle"], xo = cpu_amg(GRID, b_host)
             setup_solve["fp64"]["rel_err_vs_cpu_oracle"] = float(
