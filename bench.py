@@ -268,7 +268,7 @@ def geometric_interps(problems, dims, coarse_rows=64):
 MIXED_POLICY = [0, 1, 1, 2]  # level 0 fp64, 1-2 fp32, >= 3 fp16 (values); fp32 accumulation
 
 
-def amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, policy, smooth0, flexible, reps=2, exact=1):
+def amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, policy, smooth0, flexible, reps=2, exact=1, galerkin=0):
     """Setup + solve to ||b - A x|| / ||b|| <= 1e-8 through the library;
     device-resident inputs.  Returns timings, iterations and the residual
     recomputed in fp64 from the returned x."""
@@ -278,7 +278,7 @@ def amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, policy, smooth0, flexi
     dev = lambda M: (M[0], M[1]) + tuple(torch.from_numpy(v).cuda() for v in M[2:])  # noqa: E731
     dA, dPs = dev(A_host), [dev(P) for P in Ps_host]
     b = torch.from_numpy(b_host).cuda()
-    prm = default_params(flexible=flexible, smooth_prec0=smooth0, exact_storage=exact)
+    prm = default_params(flexible=flexible, smooth_prec0=smooth0, exact_storage=exact, galerkin_by_level=galerkin)
     S = AmgSolver(dA, dPs, prm)  # warm-up: module loads, pools
     S.solve(b)
     S.free()
@@ -494,7 +494,7 @@ def run_amgt(args):
         b_host = problems.rand_uniform(0, n)
         f64 = amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, [0], 0, 0)
         f64_8 = amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, [0], 0, 0, exact=0)
-        mix = amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, MIXED_POLICY, 1, 1)
+        mix = amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, MIXED_POLICY, 1, 1, galerkin=1)
         err = float(torch.linalg.vector_norm(mix["x"] - f64["x"]) / torch.linalg.vector_norm(f64["x"]))
         setup_solve = {}
         for name, rres in (("fp64", f64), ("fp64_8byte_values", f64_8), ("mixed", mix)):
@@ -508,7 +508,8 @@ def run_amgt(args):
         setup_solve["fp64_8byte_values"]["storage"] = "exact_storage=0: every operator read as 8-byte values"
         setup_solve["fp64_8byte_values"]["x_bit_identical_to_fp64"] = bool(
             torch.equal(f64["x"].view(torch.int64), f64_8["x"].view(torch.int64)))
-        setup_solve["mixed"]["policy"] = "levels 0 fp64 (residual) / fp32 smoother, 1-2 fp32, >=3 fp16; flexible CG"
+        setup_solve["mixed"]["policy"] = ("levels 0 fp64 (residual) / fp32 smoother, 1-2 fp32, >=3 fp16; Galerkin "
+                                          "products at each level's precision; flexible CG")
         setup_solve["mixed"]["rel_err_vs_fp64_solution"] = err
         setup_solve["mixed"]["speedup_vs_fp64"] = round(setup_solve["fp64"]["total_s"] / setup_solve["mixed"]["total_s"], 3)
         setup_solve["e2e_fp64"] = amg_e2e(amgt, torch, A_host, Ps_host, b_host, [0], 0, 0)
@@ -522,7 +523,7 @@ def run_amgt(args):
         VPs_host = geometric_interps(problems, vdims)
         vb_host = problems.rand_uniform(0, V_host[0])
         vf64 = amg_setup_solve(amgt, torch, V_host, VPs_host, vb_host, [0], 0, 0)
-        vmix = amg_setup_solve(amgt, torch, V_host, VPs_host, vb_host, MIXED_POLICY, 1, 1)
+        vmix = amg_setup_solve(amgt, torch, V_host, VPs_host, vb_host, MIXED_POLICY, 1, 1, galerkin=1)
         vc = {"problem": "3D 27-point variable-coefficient diffusion 96^3 (884,736 rows, 23.4 M nonzeros), "
                          "b uniform[-1,1] seed 0, linear-interpolation hierarchy, PCG + V(1,1) l1-Jacobi, tol 1e-8"}
         for name, rres in (("fp64", vf64), ("mixed", vmix)):
