@@ -318,12 +318,19 @@ void destroy_handle(amgt_amg *h, cudaStream_t s)
 // Events by level parity, so that level l + 1's records do not move the
 // ones level l still waits on: p_ready[l % 2] after P_l, r_ready[l % 2]
 // after R_l.
+// With exact storage, a conversion whose every block row takes the sorted
+// fill path also writes P_l's fp16 shadow and exactness bits (flag slot
+// 3 l + 1 of xflags; fused16 records it).
 struct NextInterp {
     cudaStream_t s2 = nullptr;
     cudaEvent_t p_ready[2] = {nullptr, nullptr}, r_ready[2] = {nullptr, nullptr};
     const amgt_csr *P = nullptr;  // pending conversion into Pb (R later into PRb)
     amgt_bsr *Pb = nullptr, *PRb = nullptr;
     int pslot = 0;
+    int plevel = 0;  // level of the pending conversion
+    bool exact = false;
+    int64_t *xflags = nullptr;
+    std::vector<char> *fused16 = nullptr;
     amgt_bsr *Tb = nullptr, *TRb = nullptr;  // pending transpose Tb -> TRb
     int rslot = 0;
 };
@@ -342,7 +349,11 @@ int prepare_interp(void *ctx)
     NextInterp *nx = static_cast<NextInterp *>(ctx);
     AMGT_TRY(transpose_pending(nx));
     if (!nx->P) return AMGT_OK;
-    AMGT_TRY(amgt_csr_to_bsr(nx->P, nx->Pb, (amgt_stream_t)nx->s2));
+    CvtFuse f;
+    f.want16 = nx->exact && amgt_precision_for_level(nx->plevel + 1) == AMGT_DOUBLE;
+    f.flags = nx->xflags + 3 * nx->plevel + 1;
+    AMGT_TRY(csr_to_bsr_impl(nx->P, nx->Pb, (amgt_stream_t)nx->s2, nullptr, nullptr, f.want16 ? &f : nullptr));
+    if (f.want16 && f.fused) (*nx->fused16)[3 * nx->plevel + 1] = 1;
     AMGT_CUDA_TRY(cudaEventRecord(nx->p_ready[nx->pslot], nx->s2));
     nx->Tb = nx->Pb;
     nx->TRb = nx->PRb;
@@ -589,7 +600,17 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     NextInterp nx;
     double *dense = nullptr, *dense_h = nullptr;  // the coarsest operator, dense, on device / host
     cudaEvent_t dense_ready = nullptr;
+    // exactness bits per operator (flag slots 3 l, 3 l + 1, 3 l + 2: A_l,
+    // P_l, R_l), some written by the conversions' fill passes (fused16)
+    int64_t *xflags = nullptr;
+    std::vector<char> fused16(3 * (size_t)(num_interp + 1), 0);
+    bool l1_fused0 = false;  // level 0's l1 norms written by A's conversion
     pm.mark(-1, s);
+    if ((rc = alloc_n(&xflags, fused16.size(), s))) goto fail;
+    if (cudaMemsetAsync(xflags, 0, sizeof(int64_t) * fused16.size(), s) != cudaSuccess) {
+        rc = AMGT_ERR_CUDA;
+        goto fail;
+    }
     // the second stream starts after everything the caller queued on `s`
     // before this call (the inputs may still be arriving there)
     if (L > 1 && (cudaStreamCreateWithFlags(&nx.s2, cudaStreamNonBlocking) != cudaSuccess ||
@@ -604,6 +625,9 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         goto fail;
     }
     h->lv.resize(L);
+    nx.exact = h->prm.exact_storage != 0;
+    nx.xflags = xflags;
+    nx.fused16 = &fused16;
     // hierarchy: P_0 converted while A's conversion runs, R_l transposed
     // and P_{l+1} converted while level l's A P runs
     if (L > 1) {
@@ -611,8 +635,21 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         nx.Pb = &h->lv[0].P;
         nx.PRb = &h->lv[0].R;
         nx.pslot = 0;
+        nx.plevel = 0;
     }
-    if ((rc = csr_to_bsr_impl(A, &h->lv[0].A, stream, prepare_interp, &nx))) goto fail;
+    if ((rc = alloc_n(&h->lv[0].inv_l1, A->num_rows, s))) goto fail;
+    {
+        // A's fill pass also writes level 0's inverse l1 norms and, with
+        // exact storage, A's fp16 shadow and exactness bits
+        CvtFuse f0;
+        f0.want16 = h->prm.exact_storage != 0;
+        f0.flags = xflags;
+        f0.l1 = h->lv[0].inv_l1;
+        f0.invert = 1;
+        if ((rc = csr_to_bsr_impl(A, &h->lv[0].A, stream, prepare_interp, &nx, &f0))) goto fail;
+        l1_fused0 = f0.fused;
+        fused16[0] = f0.fused && f0.want16;
+    }
     h->lv[0].n = A->num_rows;
     pm.mark(0, s);
     for (int l = 0; l < L - 1; ++l) {
@@ -635,6 +672,7 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
             nx.Pb = &h->lv[l + 1].P;
             nx.PRb = &h->lv[l + 1].R;
             nx.pslot = (l + 1) % 2;
+            nx.plevel = l + 1;
         }
         if ((rc = spgemm_impl(gp, &v.A, &v.P, &AP, nullptr, stream, prepare_interp, &nx))) goto fail;
         if (nx.Tb == &v.P && (rc = transpose_pending(&nx))) {
@@ -674,39 +712,43 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     // exact narrow storage of the operators used in fp64 (level 0, fp64
     // levels and transfers): one value check each, one read-back per 15
     if (h->prm.exact_storage) {
-        std::vector<amgt_bsr *> mats;
+        std::vector<std::pair<amgt_bsr *, int>> mats;  // operator, flag slot
         for (int l = 0; l < L; ++l) {
-            if (l == 0 || h->lv[l].prec == AMGT_DOUBLE) mats.push_back(&h->lv[l].A);
+            if (l == 0 || h->lv[l].prec == AMGT_DOUBLE) mats.push_back({&h->lv[l].A, 3 * l});
             if (l < L - 1 && h->lv[l].prec_transfer == AMGT_DOUBLE) {
-                mats.push_back(&h->lv[l].P);
-                mats.push_back(&h->lv[l].R);
+                mats.push_back({&h->lv[l].P, 3 * l + 1});
+                mats.push_back({&h->lv[l].R, 3 * l + 2});
             }
         }
-        int64_t *flags = nullptr;
-        if ((rc = alloc_n(&flags, mats.size(), s))) goto fail;
-        AMGT_CUDA_TRY(cudaMemsetAsync(flags, 0, sizeof(int64_t) * mats.size(), s));
-        std::vector<char> own16(mats.size(), 0);
+        std::vector<char> own16(fused16.size(), 0);
         for (size_t i = 0; i < mats.size() && !rc; ++i) {
+            const int slot = mats[i].second;
+            if (fused16[slot]) {
+                own16[slot] = 1;  // checked by its conversion, which allocated the shadow
+                continue;
+            }
             bool o = false;
-            rc = bsr_exact_check(mats[i], flags + i, &o, s, h->sm_count);
-            own16[i] = o;
+            rc = bsr_exact_check(mats[i].first, xflags + slot, &o, s, h->sm_count);
+            own16[slot] = o;
         }
-        for (size_t i0 = 0; i0 < mats.size() && !rc; i0 += 63) {
-            const int k = (int)std::min<size_t>(63, mats.size() - i0);
+        std::vector<int64_t> f(fused16.size(), 0);
+        for (size_t i0 = 0; i0 < f.size() && !rc; i0 += 63) {
+            const int k = (int)std::min<size_t>(63, f.size() - i0);
             const int64_t *hf = nullptr;
-            if ((rc = read_back(flags + i0, k, s, &hf))) break;
-            int64_t f[63];
-            for (int i = 0; i < k; ++i) f[i] = hf[i];  // the pinned slots are reused by the calls below
-            for (int i = 0; i < k && !rc; ++i) rc = bsr_exact_apply(mats[i0 + i], f[i], own16[i0 + i] != 0, s);
+            if ((rc = read_back(xflags + i0, k, s, &hf))) break;
+            for (int i = 0; i < k; ++i) f[i0 + i] = hf[i];  // the pinned slots are reused by later calls
         }
-        free_ptr(flags, s);
+        for (size_t i = 0; i < mats.size() && !rc; ++i)
+            rc = bsr_exact_apply(mats[i].first, f[mats[i].second], own16[mats[i].second] != 0, s);
         if (rc) goto fail;
     }
     // smoother data, shadows, work vectors
     for (int l = 0; l < L; ++l) {
         Level &v = h->lv[l];
-        if ((rc = alloc_n(&v.inv_l1, v.n, s))) goto fail;
-        if ((rc = bsr_l1_norms(&v.A, v.inv_l1, 1, s, h->sm_count))) goto fail;
+        if (!(l == 0 && l1_fused0)) {
+            if (!v.inv_l1 && (rc = alloc_n(&v.inv_l1, v.n, s))) goto fail;
+            if ((rc = bsr_l1_norms(&v.A, v.inv_l1, 1, s, h->sm_count))) goto fail;
+        }
         if ((rc = amgt_bsr_make_shadow(&v.A, v.prec, stream))) goto fail;
         if (l == 0 && (rc = amgt_bsr_make_shadow(&v.A, h->prm.smooth_prec0, stream))) goto fail;
         if (l < L - 1) {
@@ -753,6 +795,7 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         goto fail;
     AMGT_CUDA_TRY(cudaMemsetAsync(h->scal, 0, sizeof(double) * S_NSCAL, s));
     AMGT_CUDA_TRY(cudaMallocHost(&h->pinned, sizeof(double) * 4));
+    free_ptr(xflags, s);
     pm.mark(3, s);
     pm.accumulate(h->setup_ms);  // waits for the setup's last work (the inverse's copy from dense_h included)
     cudaFreeHost(dense_h);
@@ -770,6 +813,7 @@ fail:
         cudaStreamDestroy(nx.s2);
     }
     cudaStreamSynchronize(s);  // no copy from or to dense_h in flight
+    if (xflags) free_ptr(xflags, s);
     if (dense) free_ptr(dense, s);
     if (dense_h) cudaFreeHost(dense_h);
     if (dense_ready) cudaEventDestroy(dense_ready);

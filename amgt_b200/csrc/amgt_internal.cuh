@@ -153,9 +153,25 @@ int bsr_exact_apply(amgt_bsr *A, int64_t flag, bool own16, cudaStream_t s);
 int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amgt_csr *Ccsr, amgt_stream_t stream,
                 int (*between)(void *), void *ctx);
 
+// Work the conversion's fill pass can do on the values it writes, when
+// every block row takes the sorted path (else `fused` stays false and the
+// caller runs the separate passes): with want16, the exactness check of
+// bsr_exact_check (the fp16 shadow, allocated here, and the flag bits in
+// *flags); with l1, the row norms of bsr_l1_norms (1 / norm when invert),
+// the same bits.
+struct CvtFuse {
+    bool want16 = false;
+    int64_t *flags = nullptr;
+    double *l1 = nullptr;
+    int invert = 0;
+    bool fused = false;  // out
+};
+
 // amgt_csr_to_bsr with a host callback run between the queued count pass
-// and the wait for the block count (convert.cu).
-int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int (*between)(void *), void *ctx);
+// and the wait for the block count, and the optional fused work above
+// (convert.cu).
+int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int (*between)(void *), void *ctx,
+                    CvtFuse *fuse = nullptr);
 
 // Exclusive scan of n ints (in may equal out), CUB with allocator scratch.
 int exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s);

@@ -414,15 +414,28 @@ csr2bsr_large_kernel(int m, int n, const int *__restrict__ ia, const int *__rest
 // the group), and the first entry of a column writes the block column.  A
 // warp takes 8 block rows at a time and first copies their entries (column,
 // value, slot byte) into shared memory with coalesced loads.
+// With every block row on this path the pass can also write, from the
+// values it holds: the fp16 rounding of each stored value and the
+// exactness bits of exact_check_kernel (v16, flags), and each row's l1 norm
+// summed as l1_norm_kernel sums it (blocks in order, |v0| + |v1| + |v2| +
+// |v3| per block; 1 / norm with l1_invert).
 constexpr int kFsWarps = 4;
 constexpr int kFsCap = 256;  // entries of a warp's 8 block rows held in shared memory
+
+struct FillExtras {
+    __half *v16;                // nullable
+    unsigned long long *flags;  // with v16
+    double *l1;                 // nullable
+    int l1_invert;
+};
 
 __global__ void __launch_bounds__(32 * kFsWarps)
 csr2bsr_fill_sorted_kernel(int m, const int *__restrict__ ia, const int *__restrict__ ja,
                            const double *__restrict__ a, int brow, const unsigned char *__restrict__ slowf,
                            const int *__restrict__ bptr, int *__restrict__ bidx, uint16_t *__restrict__ bmap,
-                           double *__restrict__ bval, const unsigned char *__restrict__ slotb)
+                           double *__restrict__ bval, const unsigned char *__restrict__ slotb, FillExtras fx)
 {
+    bool not32 = false, not16 = false;
     __shared__ double sval[kFsWarps][kFsCap];
     __shared__ int scol[kFsWarps][kFsCap];
     __shared__ unsigned char sslot[kFsWarps][kFsCap];
@@ -473,6 +486,7 @@ csr2bsr_fill_sorted_kernel(int m, const int *__restrict__ ia, const int *__restr
                 entry(p, tsb, tc, tv);
                 ts = tsb & 0x1F;
             }
+            double l1s = 0.0;
             for (int sl = 0; sl < u; ++sl) {
                 double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
                 unsigned bits = 0;
@@ -496,13 +510,32 @@ csr2bsr_fill_sorted_kernel(int m, const int *__restrict__ ia, const int *__restr
                 double2 *dst = reinterpret_cast<double2 *>(bval + 16LL * (base + sl) + 4 * q);
                 dst[0] = make_double2(v0, v1);
                 dst[1] = make_double2(v2, v3);
+                if (fx.v16) {
+                    const double vv[4] = {v0, v1, v2, v3};
+                    __half hh[4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        hh[c] = __double2half(vv[c]);
+                        if ((double)__double2float_rn(vv[c]) != vv[c]) not32 = true;
+                        if ((double)__half2float(hh[c]) != vv[c]) not16 = true;
+                    }
+                    __half2 *d16 = reinterpret_cast<__half2 *>(fx.v16 + 16LL * (base + sl) + 4 * q);
+                    d16[0] = __halves2half2(hh[0], hh[1]);
+                    d16[1] = __halves2half2(hh[2], hh[3]);
+                }
+                l1s += fabs(v0) + fabs(v1) + fabs(v2) + fabs(v3);
                 unsigned mp = bits << (4 * q);
                 mp |= __shfl_xor_sync(gmask, mp, 1);
                 mp |= __shfl_xor_sync(gmask, mp, 2);
                 if (q == 0) bmap[base + sl] = (uint16_t)mp;
             }
+            if (fx.l1 && r < m) fx.l1[r] = fx.l1_invert ? (l1s != 0.0 ? 1.0 / l1s : 0.0) : l1s;
         }
         __syncwarp();  // the shared entries are reused by the next group
+    }
+    if (fx.v16) {  // the warp's loop trip count is uniform: all lanes are here
+        const unsigned b32 = __ballot_sync(FULL, not32), b16 = __ballot_sync(FULL, not16);
+        if (lane == 0 && (b32 | b16)) atomicOr(fx.flags, (b32 ? 1ull : 0ull) | (b16 ? 2ull : 0ull));
     }
 }
 
@@ -889,7 +922,8 @@ namespace amgt {
 // count pass is queued and before the host waits for the block count (host
 // work that can overlap it; the AMG setup converts the first
 // interpolation there, on its own stream).
-int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int (*between)(void *), void *ctx)
+int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int (*between)(void *), void *ctx,
+                    CvtFuse *fuse)
 {
     if (!csr_valid(A) || !out) return AMGT_ERR_INVALID;
     DeviceState *st;
@@ -911,6 +945,8 @@ int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int 
     int rc = AMGT_OK;
     const int64_t *h = nullptr;
     int nb = 0;
+    FillExtras fx{nullptr, nullptr, nullptr, 0};
+    bool all_sorted = false;  // no block row left to the warp or large-row kernels
     static std::atomic<bool> smem_set[64];  // per device: the large-row kernels' shared-memory opt-in
     int dev = 0;
     AMGT_CUDA_TRY(cudaGetDevice(&dev));
@@ -945,6 +981,7 @@ int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int 
     if (between && (rc = between(ctx))) goto fail;
     if ((rc = read_back(stats, 5, s, &h))) goto fail;
     nb = (int)h[2];
+    all_sorted = h[3] == 0 && h[4] == 0;
     out->max_blc_per_row = (int)h[0];
     {
         const double S2 = (double)h[1];
@@ -960,11 +997,24 @@ int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int 
     if ((rc = alloc_n(&out->blcIdx, nb, s)) || (rc = alloc_n(&out->blcMap, nb, s)) ||
         (rc = alloc_n(&out->blcVal, (size_t)16 * nb, s)))
         goto fail;
+    if (fuse) {
+        fuse->fused = false;
+        if (all_sorted && brow > 0) {
+            fx.l1 = fuse->l1;
+            fx.l1_invert = fuse->invert;
+            if (fuse->want16 && nb > 0) {
+                if ((rc = alloc_n(&out->blcVal_fp16, (size_t)16 * nb, s))) goto fail;
+                fx.v16 = reinterpret_cast<__half *>(out->blcVal_fp16);
+                fx.flags = reinterpret_cast<unsigned long long *>(fuse->flags);
+            }
+            fuse->fused = true;
+        }
+    }
     if (brow > 0) {
         const int *slow = large + brow, *nslow = (const int *)&stats[4];
         AMGT_LAUNCH(csr2bsr_fill_sorted_kernel, grid_for(8 * kFsWarps, brow, st->sm_count, 16), 32 * kFsWarps, 0, s,
                     m, A->i, A->j,
-                    A->data, brow, slowf, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal, slotb);
+                    A->data, brow, slowf, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal, slotb, fx);
         AMGT_LAUNCH(csr2bsr_fill_kernel, 2 * st->sm_count, 32 * kCvtWarps, 0, s, m, n, A->i, A->j, A->data, brow,
                     slow, nslow, out->blcPtr, out->blcIdx, out->blcMap, out->blcVal, sorted, slotb, st->err);
         AMGT_LAUNCH(csr2bsr_large_kernel<true>, 2 * st->sm_count, kLargeThreads, 2 * kWin * sizeof(uint32_t), s, m,

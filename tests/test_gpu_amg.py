@@ -181,6 +181,42 @@ def test_amg_exact_storage_changes_no_bit(amgt, orc):
         amgt.set_level_policy([])
 
 
+def _reverse_some_rows(orc, M, count):
+    """M with the entries of its first `count` rows of two or more entries
+    in reverse (unsorted) order."""
+    lens = np.diff(M.ia)
+    rows = np.nonzero(lens >= 2)[0][:count]
+    ja, a = M.ja.copy(), M.a.copy()
+    for r in rows:
+        lo, hi = M.ia[r], M.ia[r + 1]
+        ja[lo:hi] = ja[lo:hi][::-1]
+        a[lo:hi] = a[lo:hi][::-1]
+    return orc.CSR(M.m, M.n, M.ia, ja, a)
+
+
+@pytest.mark.parametrize("exact", [1, 0])
+def test_amg_setup_work_fused_into_conversion_changes_no_bit(amgt, orc, exact):
+    """When every block row of A (of P) takes the conversion's sorted path,
+    its fill pass also writes level 0's l1 norms and, with exact storage,
+    the fp16 shadow and exactness bits; with a few rows given in reverse
+    order the separate passes run instead.  Both setups give the same x,
+    iteration count and residual, bit for bit."""
+    amgt.set_level_policy([0])
+    try:
+        dims = (40, 36, 32)
+        A = orc.laplacian(*dims)
+        Ps = orc.geometric_hierarchy(*dims)
+        Ar = _reverse_some_rows(orc, A, 5)
+        Psr = [_reverse_some_rows(orc, P, 3) for P in Ps]
+        b = torch.from_numpy(A.to_scipy() @ orc.rand_uniform(6, A.n)).cuda()
+        x1, it1, r1 = _gpu_solver(amgt, A, Ps, exact_storage=exact).solve(b)
+        x2, it2, r2 = _gpu_solver(amgt, Ar, Psr, exact_storage=exact).solve(b)
+        assert it1 == it2 and r1 == r2
+        assert torch.equal(x1.view(torch.int64), x2.view(torch.int64))
+    finally:
+        amgt.set_level_policy([])
+
+
 @pytest.mark.parametrize("policy,flexible", [([0, 1], 0), ([0, 1, 1, 2], 1), ([0, 1, 1, 3], 1)])
 def test_amg_mixed_precision_converges_fp64_verified(amgt, orc, policy, flexible):
     amgt.set_level_policy(policy)
