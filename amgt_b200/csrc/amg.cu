@@ -320,7 +320,8 @@ void destroy_handle(amgt_amg *h, cudaStream_t s)
 // after R_l.
 // With exact storage, a conversion whose every block row takes the sorted
 // fill path also writes P_l's fp16 shadow and exactness bits (flag slot
-// 3 l + 1 of xflags; fused16 records it).
+// 3 l + 1 of xflags; fused16 records it), and the transpose then carries
+// the shadow to R_l, whose values are P_l's: R_l's bits are P_l's.
 struct NextInterp {
     cudaStream_t s2 = nullptr;
     cudaEvent_t p_ready[2] = {nullptr, nullptr}, r_ready[2] = {nullptr, nullptr};
@@ -333,12 +334,15 @@ struct NextInterp {
     std::vector<char> *fused16 = nullptr;
     amgt_bsr *Tb = nullptr, *TRb = nullptr;  // pending transpose Tb -> TRb
     int rslot = 0;
+    int tlevel = 0;  // level of the pending transpose
 };
 
 int transpose_pending(NextInterp *nx)
 {
     if (!nx->Tb) return AMGT_OK;
-    AMGT_TRY(amgt_bsr_transpose(nx->Tb, nx->TRb, (amgt_stream_t)nx->s2));
+    const bool with16 = (*nx->fused16)[3 * nx->tlevel + 1] != 0;
+    AMGT_TRY(bsr_transpose_impl(nx->Tb, nx->TRb, (amgt_stream_t)nx->s2, with16));
+    if (with16) (*nx->fused16)[3 * nx->tlevel + 2] = 1;
     AMGT_CUDA_TRY(cudaEventRecord(nx->r_ready[nx->rslot], nx->s2));
     nx->Tb = nullptr;
     return AMGT_OK;
@@ -358,6 +362,7 @@ int prepare_interp(void *ctx)
     nx->Tb = nx->Pb;
     nx->TRb = nx->PRb;
     nx->rslot = nx->pslot;
+    nx->tlevel = nx->plevel;
     nx->P = nullptr;
     return AMGT_OK;
 }
@@ -684,7 +689,16 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
             rc = AMGT_ERR_CUDA;
             goto fail;
         }
-        rc = amgt_spgemm(gp, &v.R, &AP, &h->lv[l + 1].A, nullptr, stream);
+        {
+            // A_{l+1} in fp64 is checked for exact storage by the numeric pass
+            CvtFuse fz;
+            fz.want16 = h->prm.exact_storage && gp == AMGT_DOUBLE &&
+                        amgt_precision_for_level(l + 1) == AMGT_DOUBLE;
+            fz.flags = xflags + 3 * (l + 1);
+            rc = spgemm_impl(gp, &v.R, &AP, &h->lv[l + 1].A, nullptr, stream, nullptr, nullptr,
+                             fz.want16 ? &fz : nullptr);
+            if (!rc && fz.fused) fused16[3 * (l + 1)] = 1;
+        }
         amgt_bsr_free(&AP, stream);
         if (rc) goto fail;
         h->lv[l + 1].n = h->lv[l + 1].A.row;
@@ -738,8 +752,11 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
             if ((rc = read_back(xflags + i0, k, s, &hf))) break;
             for (int i = 0; i < k; ++i) f[i0 + i] = hf[i];  // the pinned slots are reused by later calls
         }
-        for (size_t i = 0; i < mats.size() && !rc; ++i)
-            rc = bsr_exact_apply(mats[i].first, f[mats[i].second], own16[mats[i].second] != 0, s);
+        for (size_t i = 0; i < mats.size() && !rc; ++i) {
+            const int slot = mats[i].second;
+            const int fs = (slot % 3 == 2 && fused16[slot]) ? slot - 1 : slot;  // R_l carried P_l's shadow
+            rc = bsr_exact_apply(mats[i].first, f[fs], own16[slot] != 0, s);
+        }
         if (rc) goto fail;
     }
     // smoother data, shadows, work vectors

@@ -148,11 +148,6 @@ int pbsr_dot(const amgt_pbsr *A, const double *u, double *out, double *partial, 
 int bsr_exact_check(amgt_bsr *A, int64_t *flag, bool *own16, cudaStream_t s, int sm_count);
 int bsr_exact_apply(amgt_bsr *A, int64_t flag, bool own16, cudaStream_t s);
 
-// amgt_spgemm with a host callback run between the queued symbolic pass
-// and the wait for C's size (spgemm.cu).
-int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amgt_csr *Ccsr, amgt_stream_t stream,
-                int (*between)(void *), void *ctx);
-
 // Work the conversion's fill pass can do on the values it writes, when
 // every block row takes the sorted path (else `fused` stays false and the
 // caller runs the separate passes): with want16, the exactness check of
@@ -172,6 +167,17 @@ struct CvtFuse {
 // (convert.cu).
 int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int (*between)(void *), void *ctx,
                     CvtFuse *fuse = nullptr);
+
+// amgt_spgemm with a host callback run between the queued symbolic pass
+// and the wait for C's size (spgemm.cu); at fp64 with fuse->want16 the
+// numeric pass also writes C's fp16 shadow and exactness bits (fuse->l1
+// unused).
+int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amgt_csr *Ccsr, amgt_stream_t stream,
+                int (*between)(void *), void *ctx, CvtFuse *fuse = nullptr);
+
+// amgt_bsr_transpose; with16: A's fp16 shadow, when present, is
+// transposed with the values (convert.cu).
+int bsr_transpose_impl(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream, bool with16);
 
 // Exclusive scan of n ints (in may equal out), CUB with allocator scratch.
 int exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s);

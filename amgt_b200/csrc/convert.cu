@@ -852,11 +852,13 @@ __global__ void col_hist_kernel(int nblk, const int *__restrict__ bidx, int *__r
         atomicAdd(&hist[bidx[k]], 1);
 }
 
-// out block d takes source block src[d]: row -> column, values transposed.
+// out block d takes source block src[d]: row -> column, values transposed
+// (and the fp16 shadow with them when aval16 is given).
 __global__ void transpose_gather_kernel(int nblk, const int *__restrict__ src, const int *__restrict__ rowid,
                                         const uint16_t *__restrict__ amap, const double *__restrict__ aval,
                                         int *__restrict__ tidx, uint16_t *__restrict__ tmap,
-                                        double *__restrict__ tval)
+                                        double *__restrict__ tval, const __half *__restrict__ aval16,
+                                        __half *__restrict__ tval16)
 {
     // 16 threads per block: thread e writes entry e of the transposed block
     const long long total = (long long)nblk * 16;
@@ -865,6 +867,7 @@ __global__ void transpose_gather_kernel(int nblk, const int *__restrict__ src, c
         const int sidx = src[d];
         const int r = e >> 2, c = e & 3;  // entry (r, c) of the transpose = (c, r) of the source
         tval[t] = aval[(size_t)16 * sidx + 4 * c + r];
+        if (aval16) tval16[t] = aval16[(size_t)16 * sidx + 4 * c + r];
         if (e == 0) {
             tidx[d] = rowid[sidx];
             tmap[d] = (uint16_t)bitmap_transpose(amap[sidx]);
@@ -1171,7 +1174,11 @@ int amgt_bsr_make_exact(amgt_bsr *A, amgt_stream_t stream)
     return rc;
 }
 
-int amgt_bsr_transpose(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream)
+}  // extern "C"
+
+namespace amgt {
+
+int bsr_transpose_impl(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream, bool with16)
 {
     if (!A || !out || (A->blc_row > 0 && !A->blcPtr)) return AMGT_ERR_INVALID;
     DeviceState *st;
@@ -1209,8 +1216,12 @@ int amgt_bsr_transpose(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream)
         if (!tmp) { rc = AMGT_ERR_ALLOC; goto fail; }
         count_launch();
         AMGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys_in, keys_out, iota, src, nb, 0, bits, s));
+        const bool g16 = with16 && A->blcVal_fp16;
+        if (g16 && (rc = alloc_n(&out->blcVal_fp16, (size_t)16 * nb, s))) goto fail;
         AMGT_LAUNCH(transpose_gather_kernel, grid_for(256, 16LL * nb, st->sm_count, 8), 256, 0, s, nb, src, rowid,
-                    A->blcMap, A->blcVal, out->blcIdx, out->blcMap, out->blcVal);
+                    A->blcMap, A->blcVal, out->blcIdx, out->blcMap, out->blcVal,
+                    g16 ? reinterpret_cast<const __half *>(A->blcVal_fp16) : nullptr,
+                    g16 ? reinterpret_cast<__half *>(out->blcVal_fp16) : nullptr);
     }
     if ((rc = exclusive_scan_int(hist, out->blcPtr, bcol + 1, s))) goto fail;
     free_ptr(rowid, s); free_ptr(iota, s); free_ptr(keys_out, s); free_ptr(src, s); free_ptr(hist, s);
@@ -1221,6 +1232,15 @@ fail:
     if (tmp) dev_free(tmp, s);
     amgt_bsr_free(out, stream);
     return rc;
+}
+
+}  // namespace amgt
+
+extern "C" {
+
+int amgt_bsr_transpose(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream)
+{
+    return amgt::bsr_transpose_impl(A, out, stream, false);
 }
 
 }  // extern "C"

@@ -580,7 +580,9 @@ struct NumSmem {
 // step that hit the same C block row are applied in rounds, lowest lane
 // first (match_any), so the accumulation order is the sequential one.  Rows
 // of up to 32 C blocks accumulate in shared memory, longer rows in place in
-// C.
+// C.  For fp64 with cshadow given, the final store also writes the fp16
+// rounding of every C value and the exactness bits of exact_check_kernel
+// into *cflags (bit 0: some value not an fp32 value, bit 1: not fp16).
 template <int PREC>
 __global__ void __launch_bounds__(32 * kNumWarps, 6)
 spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
@@ -590,8 +592,9 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                       double *__restrict__ cval, void *__restrict__ cshadow, const int *__restrict__ csr_i,
                       int *__restrict__ csr_j, double *__restrict__ csr_a, const int64_t *__restrict__ ub_off,
                       const int *__restrict__ skey, const uint16_t *__restrict__ smap,
-                      const uint16_t *__restrict__ pslot)
+                      const uint16_t *__restrict__ pslot, unsigned long long *__restrict__ cflags)
 {
+    bool not32 = false, not16 = false;
     using T = NumT<PREC>;
     using V = typename T::val_t;
     using acc_t = typename T::acc_t;
@@ -750,7 +753,16 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
         for (int t = lane; t < 16 * cn; t += 32) {
             const acc_t v = small ? sa[(t >> 4) * SS + (t & 15)] : (acc_t)ga[t];
             ga[t] = (double)v;
-            if (PREC != AMGT_DOUBLE && cshadow) store_shadow<PREC>(cshadow, 16LL * c0 + t, v);
+            if constexpr (PREC == AMGT_DOUBLE) {
+                if (cshadow) {
+                    const __half hv = __double2half(v);
+                    static_cast<__half *>(cshadow)[16LL * c0 + t] = hv;
+                    if ((double)__double2float_rn(v) != v) not32 = true;
+                    if ((double)__half2float(hv) != v) not16 = true;
+                }
+            } else if (cshadow) {
+                store_shadow<PREC>(cshadow, 16LL * c0 + t, v);
+            }
         }
         __syncwarp();
         // CSR rows 4b..4b+3 (BSR2CSR fused)
@@ -783,12 +795,17 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
         }
         __syncwarp();
     }
+    if (PREC == AMGT_DOUBLE && cshadow) {  // the row loop is warp-uniform: all lanes are here
+        const unsigned b32 = __ballot_sync(FULL, not32), b16 = __ballot_sync(FULL, not16);
+        if (lane == 0 && (b32 | b16)) atomicOr(cflags, (b32 ? 1ull : 0ull) | (b16 ? 2ull : 0ull));
+    }
 }
 
 template <int PREC>
 static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B, const void *bval, amgt_bsr *C,
                           void *cshadow, amgt_csr *Ccsr, const int64_t *ub_off, const int *skey,
-                          const uint16_t *smap, const uint16_t *pslot, cudaStream_t s, int sm_count)
+                          const uint16_t *smap, const uint16_t *pslot, cudaStream_t s, int sm_count,
+                          unsigned long long *cflags = nullptr)
 {
     using V = typename NumT<PREC>::val_t;
     if (A->blc_row == 0) return AMGT_OK;
@@ -797,7 +814,7 @@ static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B
     AMGT_LAUNCH(spgemm_numeric_kernel<PREC>, grid_for(kNumWarps, A->blc_row, sm_count, 6), 32 * kNumWarps, smem, s,
                 A->row, A->blc_row, A->blcPtr, A->blcIdx, (const V *)aval, B->blcPtr, B->blcIdx, (const V *)bval,
                 C->blcPtr, C->blcIdx, C->blcMap, C->blcVal, cshadow, Ccsr ? Ccsr->i : nullptr,
-                Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr, ub_off, skey, smap, pslot);
+                Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr, ub_off, skey, smap, pslot, cflags);
     return AMGT_OK;
 }
 
@@ -822,7 +839,7 @@ namespace amgt {
 // host work that can overlap them (the AMG setup converts the next
 // level's interpolation there, on its own stream).
 int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amgt_csr *Ccsr, amgt_stream_t stream,
-                int (*between)(void *), void *ctx)
+                int (*between)(void *), void *ctx, CvtFuse *fuse)
 {
     if (!A || !B || !C || prec < AMGT_DOUBLE || prec > AMGT_BF16) return AMGT_ERR_INVALID;
     if (A->col != B->row) return AMGT_ERR_INVALID;
@@ -955,6 +972,10 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     } else if (prec == AMGT_BF16) {
         if ((rc = alloc_n(&C->blcVal_bf16, 16LL * nbC, s))) goto fail;
         cshadow = C->blcVal_bf16;
+    } else if (fuse && fuse->want16 && nbC > 0) {  // fp64: exactness check fused into the store
+        if ((rc = alloc_n(&C->blcVal_fp16, 16LL * nbC, s))) goto fail;
+        cshadow = C->blcVal_fp16;
+        fuse->fused = true;
     }
     if (Ccsr) {
         Ccsr->num_nonzeros = nnzC;
@@ -962,8 +983,9 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     }
     switch (prec) {
     case AMGT_DOUBLE:
-        rc = launch_numeric<AMGT_DOUBLE>(A, A->blcVal, B, B->blcVal, C, nullptr, Ccsr, ub_off, skey, smap, pslot, s,
-                                         st->sm_count);
+        rc = launch_numeric<AMGT_DOUBLE>(A, A->blcVal, B, B->blcVal, C, cshadow, Ccsr, ub_off, skey, smap, pslot, s,
+                                         st->sm_count, fuse ? reinterpret_cast<unsigned long long *>(fuse->flags)
+                                                            : nullptr);
         break;
     case AMGT_FLOAT:
         rc = launch_numeric<AMGT_FLOAT>(A, Atmp.blcVal_fp32, B, Btmp.blcVal_fp32, C, cshadow, Ccsr, ub_off, skey,

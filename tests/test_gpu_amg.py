@@ -163,14 +163,17 @@ def test_amg_setup_orders_inputs_still_being_copied(amgt, orc):
         amgt.set_level_policy([])
 
 
-def test_amg_exact_storage_changes_no_bit(amgt, orc):
+@pytest.mark.parametrize("problem", ["laplacian", "varcoef27"])
+def test_amg_exact_storage_changes_no_bit(amgt, orc, problem):
     """fp64 AMG-PCG with the operators read from exact fp16 / fp32 shadows
     (exact_storage = 1, the default) returns the same x, bit for bit, and
-    the same iteration count as with 8-byte values."""
+    the same iteration count as with 8-byte values: on the 7-point operator
+    (fp16-exact levels) and on a variable-coefficient one whose values no
+    narrow format holds (every exactness check, fused or not, must say so)."""
     amgt.set_level_policy([0])
     try:
         dims = (40, 36, 32)
-        A = orc.laplacian(*dims)
+        A = orc.laplacian(*dims) if problem == "laplacian" else orc.varcoef27(*dims, seed=3)
         Ps = orc.geometric_hierarchy(*dims)
         b = torch.from_numpy(A.to_scipy() @ orc.rand_uniform(4, A.n)).cuda()
         x1, it1, r1 = _gpu_solver(amgt, A, Ps, exact_storage=1).solve(b)
