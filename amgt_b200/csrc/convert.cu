@@ -67,12 +67,15 @@ __device__ __forceinline__ BlockRowRange block_row_range(const int *ia, int m, i
 // entry gets its column's rank (slot) and a first-of-column flag in slotb,
 // and the count goes to cnt[b], with no sorting and no warp-wide matching.  The
 // entries of a warp's 32 block rows are first copied into shared memory
-// with coalesced loads.  Block rows of more than 32 entries, with unsorted
-// columns or with an index out of range go to slow[] (and slowf[b] = 1)
-// for the warp kernel below (which writes their slotb / cnt, or reports the
-// bad index).
+// with coalesced loads when they fit.  Block rows of more than kStRowMax
+// entries or more than 32 block columns (a slot byte holds 5 bits), with
+// unsorted columns or with an index out of range go to slow[] (and
+// slowf[b] = 1) for the warp kernel below (which writes their slotb / cnt,
+// or reports the bad index).  27-point operators (108 entries and about 27
+// block columns per block row) stay on this path.
 constexpr int kStWarps = 4;
-constexpr int kStCap = 1024;  // entries of a warp's 32 block rows held in shared memory
+constexpr int kStCap = 1024;    // entries of a warp's 32 block rows held in shared memory
+constexpr int kStRowMax = 128;  // entries of a block row on this path
 
 __global__ void __launch_bounds__(32 * kStWarps)
 csr2bsr_count_sorted_kernel(int m, int n, const int *__restrict__ ia, const int *__restrict__ ja, int brow,
@@ -98,7 +101,7 @@ csr2bsr_count_sorted_kernel(int m, int n, const int *__restrict__ ia, const int 
             for (int e = P0 + lane; e < P1; e += 32) sc[e - P0] = __ldg(ja + e);
         __syncwarp();
         auto col_at = [&](int p) { return staged ? sc[p - P0] : __ldg(ja + p); };
-        bool ok = live && r[4] - r[0] <= 32;
+        bool ok = live && r[4] - r[0] <= kStRowMax;
         int u = 0;
         if (ok) {
             // lists in entry order: row q's first entry (list 2q) and the
@@ -126,6 +129,10 @@ csr2bsr_count_sorted_kernel(int m, int n, const int *__restrict__ ia, const int 
 #pragma unroll
                 for (int l = 1; l < 8; ++l) mn = min(mn, c[l]);
                 if (mn == 0x7FFFFFFF) break;
+                if (u == 32) {  // a 33rd block column: slot bytes hold 0..31
+                    ok = false;
+                    break;
+                }
                 unsigned lead = 0x80;
 #pragma unroll
                 for (int l = 0; l < 8; ++l) {

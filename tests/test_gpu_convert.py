@@ -30,6 +30,18 @@ def _with_long_row(orc, A, r, length, seed):
     return orc.CSR(A.m, A.n, ia, np.concatenate(rows_ja).astype(np.int32), np.concatenate(rows_a))
 
 
+def _with_rows(orc, A, new_rows, seed):
+    """A with the rows in new_rows (row -> sorted columns) replaced."""
+    rng = np.random.default_rng(seed)
+    rows_ja = [A.ja[A.ia[i]:A.ia[i + 1]] for i in range(A.m)]
+    rows_a = [A.a[A.ia[i]:A.ia[i + 1]] for i in range(A.m)]
+    for r, cols in new_rows.items():
+        rows_ja[r] = np.asarray(cols, np.int32)
+        rows_a[r] = rng.standard_normal(len(cols))
+    ia = np.concatenate([[0], np.cumsum([len(x) for x in rows_ja])]).astype(np.int32)
+    return orc.CSR(A.m, A.n, ia, np.concatenate(rows_ja).astype(np.int32), np.concatenate(rows_a))
+
+
 def _cases(orc):
     lap = orc.laplacian(16, 16, 16)
     return {
@@ -38,6 +50,14 @@ def _cases(orc):
         # fit the shared-memory copy because of one long row
         "sorted_some_reversed": _reverse_rows(orc, lap, [7, 100, 101, 102, 103, 2000, 4095]),
         "sorted_one_long": _with_long_row(orc, lap, 300, 1500, seed=5),
+        # sorted block rows of more than 32 entries: 128 entries in 32 block
+        # columns (the most the one-thread path takes), and 61 entries in
+        # more than 32 block columns (left to the warp kernel mid-merge)
+        "sorted_wide_block_rows": _with_rows(
+            orc, lap, {**{44 + q: [4 * j + c for j in range(100 + 8 * q, 108 + 8 * q) for c in range(4)]
+                          for q in range(4)},
+                       40: sorted(np.random.default_rng(7).choice(np.arange(0, 4096, 4), 40, replace=False))},
+            seed=8),
         "hypre7pt_10x10x10": orc.laplacian(10, 10, 10),
         "5pt_64x64": orc.laplacian(64, 64, 1),
         "varcoef27_13x11x9": orc.varcoef27(13, 11, 9, seed=4),
@@ -58,7 +78,8 @@ def cases(orc):
 
 
 CASE_NAMES = ["hypre7pt_10x10x10", "5pt_64x64", "varcoef27_13x11x9", "27pt_20x20x20", "interp_13x11x9",
-              "ragged_rect", "long_rows", "empty", "sorted_some_reversed", "sorted_one_long"]
+              "ragged_rect", "long_rows", "empty", "sorted_some_reversed", "sorted_one_long",
+              "sorted_wide_block_rows"]
 
 
 @pytest.mark.parametrize("name", CASE_NAMES)
