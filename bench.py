@@ -268,7 +268,7 @@ def geometric_interps(problems, dims, coarse_rows=64):
 MIXED_POLICY = [0, 1, 1, 2]  # level 0 fp64, 1-2 fp32, >= 3 fp16 (values); fp32 accumulation
 
 
-def amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, policy, smooth0, flexible, reps=2, exact=1, galerkin=0):
+def amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, policy, smooth0, flexible, reps=3, exact=1, galerkin=0):
     """Setup + solve to ||b - A x|| / ||b|| <= 1e-8 through the library;
     device-resident inputs.  Returns timings, iterations and the residual
     recomputed in fp64 from the returned x."""
