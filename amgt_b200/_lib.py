@@ -63,6 +63,7 @@ SIGNATURES = {
     "amgt_status_string": (ctypes.c_char_p, [c_int]),
     "amgt_init": (c_int, []),
     "amgt_kernel_launch_count": (ctypes.c_uint64, []),
+    "amgt_kernel_arch": (c_int, [P(c_int)]),
     "amgt_set_allocator": (c_int, [c_void_p, c_void_p, c_void_p]),
     "amgt_trim_pool": (c_int, [ctypes.c_size_t]),
     "amgt_precision_for_level": (c_int, [c_int]),

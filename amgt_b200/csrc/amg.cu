@@ -162,69 +162,176 @@ __global__ void bsr_to_dense_kernel(int m, int n, const int *__restrict__ ptr, c
     }
 }
 
-// Inverse of an SPD matrix by Cholesky (A = L L^T), then L^-T L^-1; falls
-// back to Gauss-Jordan with partial pivoting when a pivot is not positive.
-static bool host_invert(int n, std::vector<double> &A)
+// Dense inverse of the coarsest operator on the GPU: Gauss-Jordan in
+// exchange form with partial pivoting.  The table T starts as D (y = D x);
+// a pivot (p, c), p the largest |T[r][c]| among rows not yet pivoted,
+// exchanges unknown x_c with equation y_p:
+//   T'[p][c] = 1/a, T'[p][k] = -T[p][k]/a, T'[r][c] = T[r][c]/a,
+//   T'[r][k] = T[r][k] - T[r][c] T[p][k]/a          (a = T[p][c]).
+// After every column has been pivoted, row p_c expresses x_c in the
+// equations y_{p_k}: D^-1[c][p_k] = T[p_c][k] (gj_gather_kernel).  Each
+// update needs only the element itself, the pivot row and the pivot column,
+// which the pivot phase stages first, so the update runs in place.  A zero
+// (or non-finite) pivot marks D singular in *bad and continues with a = 1.
+// Candidate (v2, i2) beats (v1, i1): a row beats none, a number beats NaN,
+// then the larger |value|, then the lower row.
+__device__ __forceinline__ bool gj_better(double v2, int i2, double v1, int i1, int none)
 {
-    std::vector<double> L(A);
-    bool spd = true;
-    for (int j = 0; j < n && spd; ++j) {
-        double d = L[(size_t)j * n + j];
-        for (int k = 0; k < j; ++k) d -= L[(size_t)j * n + k] * L[(size_t)j * n + k];
-        if (!(d > 0.0)) { spd = false; break; }
-        d = std::sqrt(d);
-        L[(size_t)j * n + j] = d;
-        for (int i = j + 1; i < n; ++i) {
-            double s = L[(size_t)i * n + j];
-            for (int k = 0; k < j; ++k) s -= L[(size_t)i * n + k] * L[(size_t)j * n + k];
-            L[(size_t)i * n + j] = s / d;
+    if (i2 == none) return false;
+    if (i1 == none) return true;
+    if (isnan(v1) != isnan(v2)) return isnan(v1);
+    return v2 > v1 || (v2 == v1 && i2 < i1);
+}
+
+__device__ void gj_pivot_phase(int nc, int c, const double *__restrict__ T, int *__restrict__ used,
+                               int *__restrict__ piv, double *__restrict__ rowp, double *__restrict__ colc,
+                               int *__restrict__ bad, double *sval, int *sidx)
+{
+    const int t = threadIdx.x, nt = blockDim.x;  // nt: a power of two
+    double best = 0.0;
+    int bi = nc;
+    for (int r = t; r < nc; r += nt) {
+        if (used[r]) continue;
+        const double v = fabs(T[(long long)r * nc + c]);
+        if (gj_better(v, r, best, bi, nc)) { best = v; bi = r; }
+    }
+    sval[t] = best;
+    sidx[t] = bi;
+    __syncthreads();
+    for (int o = nt / 2; o > 0; o >>= 1) {
+        if (t < o && gj_better(sval[t + o], sidx[t + o], sval[t], sidx[t], nc)) {
+            sval[t] = sval[t + o];
+            sidx[t] = sidx[t + o];
+        }
+        __syncthreads();
+    }
+    // c < nc columns done so far leave at least one unpivoted row, so p < nc
+    const int p = min(sidx[0], nc - 1);
+    __syncthreads();
+    for (int k = t; k < nc; k += nt) {
+        rowp[k] = T[(long long)p * nc + k];
+        colc[k] = T[(long long)k * nc + c];
+    }
+    if (t == 0) {
+        used[p] = 1;
+        piv[c] = p;
+        const double a = T[(long long)p * nc + c];
+        if (!(a != 0.0) || !isfinite(a)) *bad = 1;
+    }
+}
+
+__device__ __forceinline__ double gj_update(double v, int r, int k, int p, int c, double a, const double *rowp,
+                                            const double *colc)
+{
+    if (r == p) return (k == c) ? 1.0 / a : -rowp[k] / a;
+    if (k == c) return colc[r] / a;
+    return v - colc[r] * rowp[k] / a;
+}
+
+__device__ __forceinline__ double gj_pivot_value(int c, const double *rowp)
+{
+    const double a = rowp[c];
+    return (a != 0.0 && isfinite(a)) ? a : 1.0;
+}
+
+// Whole inverse in one CTA (small coarsest levels): pivot phase, barrier,
+// in-place update, barrier, per column.
+__global__ void __launch_bounds__(1024) gj_small_kernel(int nc, double *__restrict__ T, int *__restrict__ used,
+                                                       int *__restrict__ piv, double *__restrict__ rowp,
+                                                       double *__restrict__ colc, int *__restrict__ bad)
+{
+    __shared__ double sval[1024];
+    __shared__ int sidx[1024];
+    for (int r = threadIdx.x; r < nc; r += blockDim.x) used[r] = 0;
+    __syncthreads();
+    for (int c = 0; c < nc; ++c) {
+        gj_pivot_phase(nc, c, T, used, piv, rowp, colc, bad, sval, sidx);
+        __syncthreads();
+        const int p = piv[c];
+        const double a = gj_pivot_value(c, rowp);
+        for (long long e = threadIdx.x; e < (long long)nc * nc; e += blockDim.x) {
+            const int r = (int)(e / nc), k = (int)(e % nc);
+            T[e] = gj_update(T[e], r, k, p, c, a, rowp, colc);
+        }
+        __syncthreads();
+    }
+}
+
+// Larger coarsest levels: one CTA finds and stages the pivot of column c ...
+__global__ void __launch_bounds__(1024) gj_pivot_kernel(int nc, int c, const double *__restrict__ T,
+                                                       int *__restrict__ used, int *__restrict__ piv,
+                                                       double *__restrict__ rowp, double *__restrict__ colc,
+                                                       int *__restrict__ bad)
+{
+    __shared__ double sval[1024];
+    __shared__ int sidx[1024];
+    gj_pivot_phase(nc, c, T, used, piv, rowp, colc, bad, sval, sidx);
+}
+
+// ... and the whole grid updates the table in place.
+__global__ void gj_update_kernel(int nc, int c, double *__restrict__ T, const int *__restrict__ piv,
+                                 const double *__restrict__ rowp, const double *__restrict__ colc)
+{
+    const int p = piv[c];
+    const double a = gj_pivot_value(c, rowp);
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < (long long)nc * nc;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(e / nc), k = (int)(e % nc);
+        T[e] = gj_update(T[e], r, k, p, c, a, rowp, colc);
+    }
+}
+
+__global__ void clear_int_kernel(int n, int *__restrict__ a)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = 0;
+}
+
+// D^-1[c][p_k] = T[p_c][k]
+__global__ void gj_gather_kernel(int nc, const double *__restrict__ T, const int *__restrict__ piv,
+                                 double *__restrict__ inv)
+{
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < (long long)nc * nc;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(e / nc), k = (int)(e % nc);
+        inv[(long long)c * nc + piv[k]] = T[(long long)piv[c] * nc + k];
+    }
+}
+
+constexpr int kGjSmall = 256;  // one CTA up to this order, a launch pair per column above
+
+// inv = D^-1 for the dense nc x nc matrix T (overwritten); *bad (device,
+// zeroed by the caller) is raised when D is singular.
+int dense_invert(int nc, double *T, double *inv, int *bad, int sm_count, cudaStream_t s)
+{
+    int *used = nullptr, *piv = nullptr;
+    double *rowp = nullptr, *colc = nullptr;
+    int rc = AMGT_OK;
+    if ((rc = alloc_n(&used, nc, s)) || (rc = alloc_n(&piv, nc, s)) || (rc = alloc_n(&rowp, nc, s)) ||
+        (rc = alloc_n(&colc, nc, s)))
+        goto done;
+    if (nc <= kGjSmall) {
+        count_launch();
+        gj_small_kernel<<<1, 1024, 0, s>>>(nc, T, used, piv, rowp, colc, bad);
+    } else {
+        count_launch();
+        clear_int_kernel<<<grid_for(256, nc, sm_count, 4), 256, 0, s>>>(nc, used);
+        const int grid = grid_for(256, (long long)nc * nc, sm_count, 8);
+        for (int c = 0; c < nc; ++c) {
+            count_launch();
+            gj_pivot_kernel<<<1, 1024, 0, s>>>(nc, c, T, used, piv, rowp, colc, bad);
+            count_launch();
+            gj_update_kernel<<<grid, 256, 0, s>>>(nc, c, T, piv, rowp, colc);
         }
     }
-    if (spd) {
-        // Linv (lower), then Ainv = Linv^T Linv
-        std::vector<double> Li((size_t)n * n, 0.0);
-        for (int j = 0; j < n; ++j) {
-            Li[(size_t)j * n + j] = 1.0 / L[(size_t)j * n + j];
-            for (int i = j + 1; i < n; ++i) {
-                double s = 0.0;
-                for (int k = j; k < i; ++k) s -= L[(size_t)i * n + k] * Li[(size_t)k * n + j];
-                Li[(size_t)i * n + j] = s / L[(size_t)i * n + i];
-            }
-        }
-        for (int i = 0; i < n; ++i)
-            for (int j = 0; j < n; ++j) {
-                double s = 0.0;
-                for (int k = std::max(i, j); k < n; ++k) s += Li[(size_t)k * n + i] * Li[(size_t)k * n + j];
-                A[(size_t)i * n + j] = s;
-            }
-        return true;
-    }
-    std::vector<double> M(A), I((size_t)n * n, 0.0);
-    for (int i = 0; i < n; ++i) I[(size_t)i * n + i] = 1.0;
-    for (int c = 0; c < n; ++c) {
-        int piv = c;
-        for (int r = c + 1; r < n; ++r)
-            if (std::fabs(M[(size_t)r * n + c]) > std::fabs(M[(size_t)piv * n + c])) piv = r;
-        if (M[(size_t)piv * n + c] == 0.0) return false;
-        if (piv != c)
-            for (int k = 0; k < n; ++k) {
-                std::swap(M[(size_t)c * n + k], M[(size_t)piv * n + k]);
-                std::swap(I[(size_t)c * n + k], I[(size_t)piv * n + k]);
-            }
-        const double inv = 1.0 / M[(size_t)c * n + c];
-        for (int k = 0; k < n; ++k) { M[(size_t)c * n + k] *= inv; I[(size_t)c * n + k] *= inv; }
-        for (int r = 0; r < n; ++r) {
-            if (r == c) continue;
-            const double fct = M[(size_t)r * n + c];
-            if (fct == 0.0) continue;
-            for (int k = 0; k < n; ++k) {
-                M[(size_t)r * n + k] -= fct * M[(size_t)c * n + k];
-                I[(size_t)r * n + k] -= fct * I[(size_t)c * n + k];
-            }
-        }
-    }
-    A.swap(I);
-    return true;
+    count_launch();
+    gj_gather_kernel<<<grid_for(256, (long long)nc * nc, sm_count, 8), 256, 0, s>>>(nc, T, piv, inv);
+    if (cudaGetLastError() != cudaSuccess) rc = AMGT_ERR_CUDA;
+done:
+    free_ptr(used, s);
+    free_ptr(piv, s);
+    free_ptr(rowp, s);
+    free_ptr(colc, s);
+    return rc;
 }
 
 struct Level {
@@ -293,8 +400,8 @@ void destroy_handle(amgt_amg *h, cudaStream_t s)
     if (h->graph) cudaGraphExecDestroy(h->graph);
     if (h->loop) cudaGraphExecDestroy(h->loop);
     if (h->graph_stream) cudaStreamDestroy(h->graph_stream);
-    if (h->loop_it) cudaFree(h->loop_it);
-    if (h->loop_rr) cudaFree(h->loop_rr);
+    free_ptr(h->loop_it, s);
+    free_ptr(h->loop_rr, s);
     if (h->loop_pinned) cudaFreeHost(h->loop_pinned);
     for (auto &v : h->lv) free_level(v, s);
     free_ptr(h->coarse_inv, s);
@@ -488,8 +595,7 @@ int build_loop_graph(amgt_amg *h, double *x)
         h->loop = nullptr;
     }
     if (!h->graph_stream) AMGT_CUDA_TRY(cudaStreamCreateWithFlags(&h->graph_stream, cudaStreamNonBlocking));
-    if (!h->loop_it) AMGT_CUDA_TRY(cudaMalloc(&h->loop_it, sizeof(int)));
-    if (!h->loop_rr) AMGT_CUDA_TRY(cudaMalloc(&h->loop_rr, sizeof(double) * (h->prm.max_iter + 1)));
+    if (!h->loop_it || !h->loop_rr) return AMGT_ERR_INVALID;  // allocated by the setup
     if (!h->loop_pinned) AMGT_CUDA_TRY(cudaMallocHost(&h->loop_pinned, sizeof(double) * (h->prm.max_iter + 2)));
     cudaGraph_t g = nullptr;
     AMGT_CUDA_TRY(cudaGraphCreate(&g, 0));
@@ -590,6 +696,12 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     if (!A || !out || num_interp < 0 || (num_interp > 0 && !P) || A->num_rows != A->num_cols || A->num_rows <= 0)
         return AMGT_ERR_INVALID;
     *out = nullptr;
+    // the loop graph's body runs at least once and keeps max_iter + 1
+    // residual norms: max_iter must be >= 1 (and bounded, so that its
+    // buffers stay small)
+    if (params && (params->max_iter < 1 || params->max_iter > 1000000 || !(params->tol >= 0.0) ||
+                   params->max_coarse_rows < 1 || params->max_coarse_rows > 16384))
+        return AMGT_ERR_INVALID;
     DeviceState *st;
     AMGT_TRY(device_state(&st));
     cudaStream_t s = (cudaStream_t)stream;
@@ -603,8 +715,7 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     int rc = AMGT_OK;
     PhaseMarks pm;
     NextInterp nx;
-    double *dense = nullptr, *dense_h = nullptr;  // the coarsest operator, dense, on device / host
-    cudaEvent_t dense_ready = nullptr;
+    double *dense = nullptr;  // the coarsest operator, dense (inverted into h->coarse_inv)
     // exactness bits per operator (flag slots 3 l, 3 l + 1, 3 l + 2: A_l,
     // P_l, R_l), some written by the conversions' fill passes (fused16)
     int64_t *xflags = nullptr;
@@ -705,24 +816,30 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         pm.mark(2, s);
     }
     h->lv[L - 1].prec = amgt_precision_for_level(L - 1);
-    // coarsest: its dense form goes to the host now and is inverted there
-    // while the GPU runs the exactness checks, norms and shadows queued below
+    // coarsest: dense form and its inverse, on the GPU (Gauss-Jordan); the
+    // singularity flag is read back with the exactness bits below
     h->nc = h->lv[L - 1].n;
     if (h->nc > h->prm.max_coarse_rows) {
         rc = AMGT_ERR_TOO_LARGE;
         goto fail;
     }
-    if ((rc = alloc_n(&dense, (size_t)h->nc * h->nc, s))) goto fail;
-    if (cudaMallocHost(&dense_h, sizeof(double) * h->nc * h->nc) != cudaSuccess ||
-        cudaEventCreateWithFlags(&dense_ready, cudaEventDisableTiming) != cudaSuccess) {
-        rc = AMGT_ERR_CUDA;
-        goto fail;
+    {
+        const size_t nn = (size_t)h->nc * h->nc;
+        if ((rc = alloc_n(&dense, nn, s)) || (rc = alloc_n(&h->coarse_inv, nn, s))) goto fail;
+        if (cudaMemsetAsync(dense, 0, sizeof(double) * nn, s) != cudaSuccess ||
+            cudaMemsetAsync(xflags + 3 * num_interp + 2, 0, sizeof(int64_t), s) != cudaSuccess) {
+            rc = AMGT_ERR_CUDA;
+            goto fail;
+        }
+        AMGT_LAUNCH(bsr_to_dense_kernel, grid_for(256, h->nc, h->sm_count, 8), 256, 0, s, h->nc, h->nc,
+                    h->lv[L - 1].A.blcPtr, h->lv[L - 1].A.blcIdx, h->lv[L - 1].A.blcVal, dense);
+        // the flag slot after the last operator's (never a P or R slot: the
+        // coarsest level has none) holds the singular mark
+        if ((rc = dense_invert(h->nc, dense, h->coarse_inv, reinterpret_cast<int *>(xflags + 3 * num_interp + 2),
+                               h->sm_count, s)))
+            goto fail;
+        free_ptr(dense, s);
     }
-    AMGT_CUDA_TRY(cudaMemsetAsync(dense, 0, sizeof(double) * h->nc * h->nc, s));
-    AMGT_LAUNCH(bsr_to_dense_kernel, grid_for(256, h->nc, h->sm_count, 8), 256, 0, s, h->nc, h->nc,
-                h->lv[L - 1].A.blcPtr, h->lv[L - 1].A.blcIdx, h->lv[L - 1].A.blcVal, dense);
-    AMGT_CUDA_TRY(cudaMemcpyAsync(dense_h, dense, sizeof(double) * h->nc * h->nc, cudaMemcpyDeviceToHost, s));
-    AMGT_CUDA_TRY(cudaEventRecord(dense_ready, s));
     // exact narrow storage of the operators used in fp64 (level 0, fp64
     // levels and transfers): one value check each, one read-back per 15
     if (h->prm.exact_storage) {
@@ -784,23 +901,14 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         if ((rc = alloc_n(&v.u, v.n, s)) || (rc = alloc_n(&v.t, v.n, s))) goto fail;
         if (l > 0 && ((rc = alloc_n(&v.f, v.n, s)) || (rc = alloc_n(&v.s, v.n, s)))) goto fail;
     }
-    // coarsest: inverted on the host (the GPU still runs the work queued
-    // above), back to the device
-    if (cudaEventSynchronize(dense_ready) != cudaSuccess) {
-        rc = AMGT_ERR_CUDA;
-        goto fail;
-    }
+    // coarsest: the inverse's singularity mark (one read-back)
     {
-        const size_t nn = (size_t)h->nc * h->nc;
-        std::vector<double> hd(dense_h, dense_h + nn);
-        if (!host_invert(h->nc, hd)) {
-            rc = AMGT_ERR_INVALID;
+        const int64_t *hf = nullptr;
+        if ((rc = read_back(xflags + 3 * num_interp + 2, 1, s, &hf))) goto fail;
+        if (hf[0] != 0) {
+            rc = AMGT_ERR_INVALID;  // singular coarsest operator
             goto fail;
         }
-        std::copy(hd.begin(), hd.end(), dense_h);
-        AMGT_CUDA_TRY(cudaMemcpyAsync(dense, dense_h, sizeof(double) * nn, cudaMemcpyHostToDevice, s));
-        h->coarse_inv = dense;
-        dense = nullptr;
         if (L == 1) h->lv[L - 1].s = nullptr;
     }
     // Krylov vectors and scalars
@@ -808,15 +916,14 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     h->grid0 = h->prm.packed ? pbsr_grid(&h->lv[0].pA, h->sm_count) : epi_grid(&h->lv[0].A, h->sm_count);
     if ((rc = alloc_n(&h->r, h->n0, s)) || (rc = alloc_n(&h->z, h->n0, s)) || (rc = alloc_n(&h->p, h->n0, s)) ||
         (rc = alloc_n(&h->q, h->n0, s)) || (rc = alloc_n(&h->scal, S_NSCAL, s)) ||
-        (rc = alloc_n(&h->part, std::max(h->grid0, kDotGrid), s)))
+        (rc = alloc_n(&h->part, std::max(h->grid0, kDotGrid), s)) || (rc = alloc_n(&h->loop_it, 1, s)) ||
+        (rc = alloc_n(&h->loop_rr, (size_t)h->prm.max_iter + 1, s)))
         goto fail;
     AMGT_CUDA_TRY(cudaMemsetAsync(h->scal, 0, sizeof(double) * S_NSCAL, s));
     AMGT_CUDA_TRY(cudaMallocHost(&h->pinned, sizeof(double) * 4));
     free_ptr(xflags, s);
     pm.mark(3, s);
-    pm.accumulate(h->setup_ms);  // waits for the setup's last work (the inverse's copy from dense_h included)
-    cudaFreeHost(dense_h);
-    cudaEventDestroy(dense_ready);
+    pm.accumulate(h->setup_ms);  // waits for the setup's last work
     if (nx.s2) cudaStreamDestroy(nx.s2);
     for (int i = 0; i < 2; ++i) {
         if (nx.p_ready[i]) cudaEventDestroy(nx.p_ready[i]);
@@ -829,11 +936,9 @@ fail:
         cudaStreamSynchronize(nx.s2);
         cudaStreamDestroy(nx.s2);
     }
-    cudaStreamSynchronize(s);  // no copy from or to dense_h in flight
+    cudaStreamSynchronize(s);  // no kernel of this setup in flight
     if (xflags) free_ptr(xflags, s);
     if (dense) free_ptr(dense, s);
-    if (dense_h) cudaFreeHost(dense_h);
-    if (dense_ready) cudaEventDestroy(dense_ready);
     for (int i = 0; i < 2; ++i) {
         if (nx.p_ready[i]) cudaEventDestroy(nx.p_ready[i]);
         if (nx.r_ready[i]) cudaEventDestroy(nx.r_ready[i]);

@@ -119,6 +119,9 @@ int block_row_stats(amgt_bsr *A, cudaStream_t s);
 int spmv_segmented_with_scratch(int prec, double alpha, const amgt_bsr *A, const double *x, double beta, double *y,
                                 double *part, int sm_count, cudaStream_t s);
 
+// y = beta * y (y = 0 when beta == 0) over n entries (spmv.cu).
+int scale_vector(long long n, double beta, double *y, int sm_count, cudaStream_t s);
+
 // Fused SpMV forms (spmv.cu): r = f - A u; u_out = u + w (f - A u) .* inv_l1;
 // out = A u with per-CTA partials of u . out (grid CTAs, from epi_grid);
 // l1 row norms (or their inverses).

@@ -75,11 +75,18 @@ extern "C" int amgt_spmv_segmented_noalloc(int prec, double alpha, const amgt_bs
 {
     if (!A || prec < AMGT_DOUBLE || prec > AMGT_BF16) return AMGT_ERR_INVALID;
     if (A->row == 0) return AMGT_OK;
-    if (!x || !y || !A->blcPtr || !A->blcIdx || !A->rowPtrbyWarp || !A->rowIdxbyWarp || A->warpnum <= 0)
-        return AMGT_ERR_INVALID;  // needs the segment table of amgt_bsr_balance
-    if (A->warpnum > AMGT_NOALLOC_MAX_SEGMENTS) return AMGT_ERR_TOO_LARGE;
+    if (!y) return AMGT_ERR_INVALID;
     double *part = nullptr;
     int sm_count = 0;
+    if (A->blc_num == 0 || A->col == 0) {
+        // no stored block: y = beta * y, as amgt_spmv does (no scratch needed)
+        const int rc = noalloc_setup(&part, &sm_count);
+        if (rc != AMGT_OK) return rc;
+        return amgt::scale_vector(A->row, beta, y, sm_count, (cudaStream_t)stream);
+    }
+    if (!x || !A->blcPtr || !A->blcIdx || !A->rowPtrbyWarp || !A->rowIdxbyWarp || A->warpnum <= 0)
+        return AMGT_ERR_INVALID;  // needs the segment table of amgt_bsr_balance
+    if (A->warpnum > AMGT_NOALLOC_MAX_SEGMENTS) return AMGT_ERR_TOO_LARGE;
     const int rc = noalloc_setup(&part, &sm_count);
     if (rc != AMGT_OK) return rc;
     return amgt::spmv_segmented_with_scratch(prec, alpha, A, x, beta, y, part, sm_count, (cudaStream_t)stream);

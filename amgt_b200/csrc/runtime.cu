@@ -170,12 +170,29 @@ static void default_free(void *p, amgt_stream_t s, void *)
     cudaFreeAsync(p, (cudaStream_t)s);
 }
 
-static amgt_alloc_fn g_alloc = default_alloc;
-static amgt_free_fn g_free = default_free;
-static void *g_alloc_ctx = nullptr;
+// The installed hooks, swapped as one pointer so that a call never pairs
+// one installation's function with another's context.  Replaced hook sets
+// are kept (a concurrent call may still hold one); each is three words.
+struct AllocHooks {
+    amgt_alloc_fn alloc;
+    amgt_free_fn free;
+    void *ctx;
+};
+static const AllocHooks g_default_hooks{default_alloc, default_free, nullptr};
+static std::atomic<const AllocHooks *> g_hooks{&g_default_hooks};
+static std::mutex g_hooks_mu;
+static std::vector<AllocHooks *> g_hooks_kept;
 
-void *dev_alloc(size_t bytes, cudaStream_t s) { return g_alloc(bytes, (amgt_stream_t)s, g_alloc_ctx); }
-void dev_free(void *p, cudaStream_t s) { g_free(p, (amgt_stream_t)s, g_alloc_ctx); }
+void *dev_alloc(size_t bytes, cudaStream_t s)
+{
+    const AllocHooks *h = g_hooks.load(std::memory_order_acquire);
+    return h->alloc(bytes, (amgt_stream_t)s, h->ctx);
+}
+void dev_free(void *p, cudaStream_t s)
+{
+    const AllocHooks *h = g_hooks.load(std::memory_order_acquire);
+    h->free(p, (amgt_stream_t)s, h->ctx);
+}
 
 // ---------------------------------------------------------- device state
 static constexpr int kMaxDevices = 64;
@@ -384,6 +401,21 @@ int amgt_init(void)
 
 uint64_t amgt_kernel_launch_count(void) { return g_launches.load(); }
 
+int amgt_kernel_arch(int *binary_version)
+{
+    if (!binary_version) return AMGT_ERR_INVALID;
+    *binary_version = 0;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return AMGT_ERR_NO_DEVICE;
+    }
+    cudaFuncAttributes fa;
+    AMGT_CUDA_TRY(cudaFuncGetAttributes(&fa, scan_small_kernel<int>));
+    *binary_version = fa.binaryVersion;
+    return AMGT_OK;
+}
+
 int amgt_trim_pool(size_t keep_bytes)
 {
     cudaMemPool_t pool = library_pool();
@@ -400,9 +432,14 @@ int amgt_set_allocator(amgt_alloc_fn alloc_fn, amgt_free_fn free_fn, void *ctx)
 {
     if ((alloc_fn == nullptr) != (free_fn == nullptr)) return AMGT_ERR_INVALID;
     if (alloc_fn) flush_cache(-1);  // the default allocator's kept blocks go back to its pool
-    g_alloc = alloc_fn ? alloc_fn : default_alloc;
-    g_free = free_fn ? free_fn : default_free;
-    g_alloc_ctx = alloc_fn ? ctx : nullptr;
+    if (!alloc_fn) {
+        g_hooks.store(&g_default_hooks, std::memory_order_release);
+        return AMGT_OK;
+    }
+    std::lock_guard<std::mutex> lk(g_hooks_mu);
+    AllocHooks *h = new AllocHooks{alloc_fn, free_fn, ctx};
+    g_hooks_kept.push_back(h);
+    g_hooks.store(h, std::memory_order_release);
     return AMGT_OK;
 }
 

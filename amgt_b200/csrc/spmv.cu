@@ -576,6 +576,12 @@ int spmv_dot(int prec, const amgt_bsr *A, const double *u, double *out, double *
     return launch_epi_prec<EPI_DOT>(prec, A, u, e, grid, s, 0);  // the segment layout: grid as given
 }
 
+int scale_vector(long long n, double beta, double *y, int sm_count, cudaStream_t s)
+{
+    AMGT_LAUNCH(scale_kernel, grid_for(256, n, sm_count, 8), 256, 0, s, n, beta, y);
+    return AMGT_OK;
+}
+
 int bsr_l1_norms(const amgt_bsr *A, double *l1, int invert, cudaStream_t s, int sm_count)
 {
     const int mode = storage_mode(A, AMGT_DOUBLE);

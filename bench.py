@@ -33,7 +33,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "setup+solve s to rtol 1e-8, mixed/learned vs FP64 on 1 B200; SpMV HBM GB/s"
 GRID = (128, 128, 128)  # the workload; --grid changes it only for profiling captures
-PROFILE_MD = os.path.join(ROOT, "profiles", "spmv_fp64_7pt128.md")
+PROFILE_JSON = os.path.join(ROOT, "profiles", "spmv_fp64_7pt128.json")
 
 
 def spmv_bytes(nblk: int, brow: int, m: int, n: int, val_bytes: int = 8, beta: bool = False) -> int:
@@ -76,16 +76,12 @@ def read_peaks():
 
 
 def read_traffic():
-    """traffic_bytes_per_launch recorded from the ncu capture of the SpMV."""
-    if not os.path.exists(PROFILE_MD):
+    """DRAM read + write bytes per launch of the SpMV from its ncu capture
+    (profiles/spmv_fp64_7pt128.json), or None."""
+    try:
+        return int(json.load(open(PROFILE_JSON))["traffic_bytes_per_launch"])
+    except (OSError, KeyError, ValueError):
         return None
-    for line in open(PROFILE_MD):
-        if line.strip().startswith("traffic_bytes_per_launch:"):
-            try:
-                return int(line.split(":", 1)[1].strip().split()[0])
-            except ValueError:
-                return None
-    return None
 
 
 class ClockSampler:

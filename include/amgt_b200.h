@@ -62,11 +62,25 @@ AMGT_API int amgt_init(void);
  * all streams).  Used to prove that a measured region ran native kernels. */
 AMGT_API uint64_t amgt_kernel_launch_count(void);
 
+/* Architecture of the device code the current device runs for this library
+ * (cudaFuncGetAttributes().binaryVersion of one of its kernels: 100 for the
+ * sm_100a build).  AMGT_ERR_NO_DEVICE without a device. */
+AMGT_API int amgt_kernel_arch(int *binary_version);
+
 /* ---------------------------------------------------------- allocation */
-/* Every array the library returns or uses as scratch comes from this
+/* Every DEVICE array the library returns or uses as scratch comes from this
  * allocator.  HYPRE plugs hypre_TAlloc/hypre_TFree here so that
  * hypre_CSRMatrixDestroy can free an SpGEMM result (the reference allocates C
- * with hypre_TAlloc, R/seq_mv/csr_spgemm_device.c:1808-1839). */
+ * with hypre_TAlloc, R/seq_mv/csr_spgemm_device.c:1808-1839).  Exceptions,
+ * all small and all pinned HOST memory from cudaMallocHost: each host
+ * thread's 512-byte read-back staging per device (freed when the thread
+ * exits), and an AMG handle's read-back slots (32 bytes plus
+ * 8 * (max_iter + 2) bytes, freed by amgt_amg_destroy); the per-device
+ * error word (16 bytes, cudaMalloc, held until exit); and the fixed array of
+ * amgt_spmv_segmented_noalloc.
+ * Install or remove an allocator only while no other library call runs and
+ * no array the library allocated is still live: a block is always freed
+ * through the allocator installed when the free happens. */
 /* Default: a stream-ordered memory pool owned by the library (one per
  * device) that keeps freed memory for reuse; amgt_trim_pool(keep) returns
  * all but `keep` bytes of it to the driver (synchronises the device). */
@@ -176,7 +190,6 @@ AMGT_API int amgt_bsr_make_shadow(amgt_bsr *A, int prec, amgt_stream_t stream);
  * keeps it in mBSR.  Host-blocking once. */
 AMGT_API int amgt_bsr_transpose(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream);
 
-/* Frees every array of *A (through the allocator) and zeroes the struct. */
 /* Exact narrow storage (no counterpart in the reference): checks whether
  * every value of A is an fp16 value (else an fp32 value); if so builds that
  * shadow and sets A->exact_prec, after which fp64 products (amgt_spmv,
@@ -186,6 +199,7 @@ AMGT_API int amgt_bsr_transpose(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t 
  * products qualify.  One host read-back.  Call again after changing the
  * values (or set exact_prec to AMGT_DOUBLE). */
 AMGT_API int amgt_bsr_make_exact(amgt_bsr *A, amgt_stream_t stream);
+/* Frees every array of *A (through the allocator) and zeroes the struct. */
 AMGT_API int amgt_bsr_free(amgt_bsr *A, amgt_stream_t stream);
 AMGT_API int amgt_csr_free(amgt_csr *A, amgt_stream_t stream);
 
@@ -310,9 +324,10 @@ AMGT_API int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bs
  * dots, and the coarsest (dense, inverted) solve are always fp64. */
 typedef struct {
     int max_levels;        /* cap on levels (default 25)                    */
-    int max_coarse_rows;   /* largest coarsest level (dense inverse), 4096  */
+    int max_coarse_rows;   /* largest coarsest level (dense inverse), 4096;
+                              a larger coarsest level: AMGT_ERR_TOO_LARGE   */
     double tol;            /* ||b - A x|| / ||b|| target (default 1e-8)     */
-    int max_iter;          /* default 200                                   */
+    int max_iter;          /* default 200, at least 1                       */
     double relax_weight;   /* l1-Jacobi weight (default 1)                  */
     int flexible;          /* flexible CG (Polak-Ribiere beta), default 0   */
     int use_graph;         /* one CUDA graph per iteration (default 1)      */
@@ -329,7 +344,10 @@ typedef struct {
 typedef struct amgt_amg amgt_amg;
 
 AMGT_API void amgt_amg_default_params(amgt_amg_params *p);
-/* Host-blocking (sizes of every level; coarsest inverse on the host). */
+/* Host-blocking (sizes of every level).  The coarsest operator is inverted
+ * on the GPU (Gauss-Jordan, partial pivoting); a singular one returns
+ * AMGT_ERR_INVALID.  Rejected with AMGT_ERR_INVALID: max_iter outside
+ * 1 .. 1000000, tol negative or NaN, max_coarse_rows outside 1 .. 16384. */
 AMGT_API int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P,
                             const amgt_amg_params *params, amgt_amg **out,
                             amgt_stream_t stream);

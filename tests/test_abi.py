@@ -36,12 +36,38 @@ def test_library_exports_every_declared_symbol():
     assert exported == set(_declared())
 
 
-def test_library_targets_sm100a():
+def test_library_is_built_for_sm100a_only():
+    # the build passes exactly one -gencode, sm_100a; the device side of
+    # this is test_gpu_hypre.py::test_kernels_run_sm100_code (binaryVersion)
+    from amgt_b200 import build
+
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def test_amg_setup_rejects_bad_params_without_a_device():
     from amgt_b200 import _lib
 
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", _lib.LIB_PATH], capture_output=True,
-                         text=True).stdout
-    assert "sm_100a" in out
+    L = _lib.lib()
+    A = _lib.AmgtCsr(8, 8, 0, None, None, None)
+    h = ctypes.c_void_p()
+    for field, bad in (("max_iter", 0), ("max_iter", -3), ("tol", -1.0), ("tol", float("nan")),
+                       ("max_coarse_rows", 0)):
+        p = _lib.AmgtAmgParams()
+        L.amgt_amg_default_params(ctypes.byref(p))
+        setattr(p, field, bad)
+        assert L.amgt_amg_setup(ctypes.byref(A), 0, None, ctypes.byref(p), ctypes.byref(h), None) == 1, field
+        assert not h.value
+
+
+def test_kernel_arch_query_without_a_device():
+    import torch
+
+    from amgt_b200 import _lib
+
+    v = ctypes.c_int(-1)
+    rc = _lib.lib().amgt_kernel_arch(ctypes.byref(v))
+    if not torch.cuda.is_available():
+        assert rc == 6 and v.value == 0
 
 
 def test_precision_policy_defaults_and_override():

@@ -117,3 +117,13 @@ def test_mixed_level_matvec_uses_shadow(amgt, orc):
     want = orc.spmv(R, x, prec=2)
     scale = orc.spmv_bound(R, x, None)
     assert np.all(np.abs(y.cpu().numpy() - want) <= 1e-5 * scale)
+
+
+def test_kernels_run_sm100_code(amgt):
+    """The device code the B200 runs for this library is the sm_100a build
+    (cudaFuncGetAttributes binaryVersion 100), queried at run time."""
+    import ctypes
+
+    v = ctypes.c_int(0)
+    assert amgt.lib().amgt_kernel_arch(ctypes.byref(v)) == 0
+    assert v.value == 100

@@ -75,8 +75,35 @@ def test_noalloc_spmv_matches_allocating_spmv_twice(amgt, orc):
     finally:
         assert L.amgt_set_allocator(None, None, None) == 0
     assert calls == {"alloc": 0, "free": 0}
+    # against the oracle's mBSR SpMV directly (not only the allocating path,
+    # which runs the same two kernels), and against the allocating path
+    y_orc = orc.spmv(R, x.cpu().numpy(), y0, alpha=alpha, beta=beta)
     for y in outs:
+        assert np.all(np.abs(y - y_orc) <= 1e-12 * scale + 1e-300)
         assert np.all(np.abs(y - y_ref) <= 1e-12 * scale + 1e-300)
+
+
+def test_noalloc_spmv_matrix_without_blocks_scales_y(amgt, orc):
+    """Rows but no stored block: y = beta * y, as amgt_spmv gives."""
+    L = amgt.lib()
+    m, n = 37, 21
+    E = orc.CSR(m, n, np.zeros(m + 1, np.int32), np.zeros(0, np.int32), np.zeros(0))
+    G = amgt.Bsr.from_csr(*to_dev(E))
+    G.balance()
+    assert G.s.blc_num == 0
+    x = torch.ones(n, dtype=torch.float64, device="cuda")
+    y0 = orc.rand_uniform(51, m)
+    for beta in (0.75, 0.0):
+        outs = []
+        for _ in range(2):
+            y = torch.from_numpy(y0).cuda()
+            assert _spmv_noalloc(L, 0, 2.0, G, x, beta, y) == 0
+            outs.append(y.cpu().numpy())
+        y_ref = torch.from_numpy(y0).cuda()
+        G.spmv(x, y_ref, alpha=2.0, beta=beta)
+        for y in outs:
+            np.testing.assert_array_equal(y, y_ref.cpu().numpy())
+            np.testing.assert_array_equal(y, beta * y0)
 
 
 def test_noalloc_spmv_reduced_precision(amgt, orc):
