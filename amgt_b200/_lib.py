@@ -16,6 +16,7 @@ STATUS = {0: "AMGT_OK", 1: "AMGT_ERR_INVALID", 2: "AMGT_ERR_ALLOC", 3: "AMGT_ERR
           5: "AMGT_ERR_UNSUPPORTED", 6: "AMGT_ERR_NO_DEVICE", 7: "AMGT_ERR_TOO_LARGE"}
 NOALLOC_MAX_SEGMENTS = 1 << 18  # AMGT_NOALLOC_MAX_SEGMENTS
 DOUBLE, FLOAT, HALF, BF16 = 0, 1, 2, 3
+SOLVER_PCG, SOLVER_FGMRES_IR = 0, 1
 
 c_int, c_double, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
 P = ctypes.POINTER
@@ -49,7 +50,8 @@ class AmgtAmgParams(ctypes.Structure):
     _fields_ = [("max_levels", c_int), ("max_coarse_rows", c_int), ("tol", c_double), ("max_iter", c_int),
                 ("relax_weight", c_double), ("flexible", c_int), ("use_graph", c_int),
                 ("galerkin_by_level", c_int), ("smooth_prec0", c_int), ("packed", c_int),
-                ("exact_storage", c_int)]
+                ("exact_storage", c_int), ("solver", c_int), ("restart", c_int), ("inner_tol", c_double),
+                ("inner_prec0", c_int), ("max_outer", c_int)]
 
 
 class AmgtPbsr(ctypes.Structure):

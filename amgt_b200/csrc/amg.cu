@@ -334,6 +334,252 @@ done:
     return rc;
 }
 
+// ------------------------------------------------ FGMRES with refinement
+// The inner solve of FGMRES-IR: flexible GMRES(m) (R/krylov/flexgmres.c)
+// with the Krylov basis V (m + 1 vectors) and the preconditioned vectors Z
+// (m vectors) stored in fp32, inner products and the Hessenberg
+// least-squares problem in fp64.  The iteration index j lives on the device
+// so that one captured iteration serves every j (the body of a while node):
+//   vin (fixed, fp64) = V_j      written by the previous iteration's scale
+//   zout = M vin                 V-cycle
+//   Z_j = zout                   (fp32)
+//   w = A zout                   level-0 matvec at the inner precision
+//   H[i][j] = V_i . w, i <= j    classical Gram-Schmidt, one pass
+//   w -= sum H[i][j] V_i; ||w||
+//   Givens rotations on column j, residual estimate |g[j+1]|, j += 1
+//   V_j = vin = w / ||w||
+// Scalars (gm): H column-major (m + 1) x m, then cs[m], sn[m], g[m + 1],
+// y[m], and the slots below.
+constexpr int kGmMaxRestart = 32;
+enum { GM_BETA0 = 0, GM_INVH = 1, GM_RES = 2, GM_NSLOT = 4 };
+
+struct GmLayout {
+    int m;
+    __host__ __device__ int H(int i, int j) const { return i + j * (m + 1); }
+    __host__ __device__ int cs() const { return (m + 1) * m; }
+    __host__ __device__ int sn() const { return cs() + m; }
+    __host__ __device__ int g() const { return sn() + m; }
+    __host__ __device__ int y() const { return g() + m + 1; }
+    __host__ __device__ int slot() const { return y() + m; }
+    __host__ __device__ int size() const { return slot() + GM_NSLOT; }
+};
+
+// partials of V_i . w for i = 0 .. j, one row of partials per i; the basis
+// is taken 8 vectors per sweep (w re-read from L2 between sweeps)
+__global__ void __launch_bounds__(kDotThreads) gm_mdot_kernel(long long n, const float *__restrict__ V,
+                                                             const int *__restrict__ jdev,
+                                                             const double *__restrict__ w, double *__restrict__ part)
+{
+    grid_dependency_wait();
+    __shared__ double sred[kDotThreads / 32][8];
+    const int j = *jdev;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i0 = 0; i0 <= j; i0 += 8) {
+        double acc[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) acc[t] = 0.0;
+        for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+             e += (long long)gridDim.x * blockDim.x) {
+            const double we = w[e];
+#pragma unroll
+            for (int t = 0; t < 8; ++t)
+                if (i0 + t <= j) acc[t] += (double)V[(long long)(i0 + t) * n + e] * we;
+        }
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+            double v = acc[t];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+            if (lane == 0) sred[warp][t] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < 8 && i0 + (int)threadIdx.x <= j) {
+            double t = 0.0;
+            for (int w8 = 0; w8 < kDotThreads / 32; ++w8) t += sred[w8][threadIdx.x];
+            part[(long long)(i0 + threadIdx.x) * gridDim.x + blockIdx.x] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// H[i][j] = sum of the partials of vector i (warp i, fixed order)
+__global__ void __launch_bounds__(1024) gm_mdot_reduce_kernel(const double *__restrict__ part, int np,
+                                                             const int *__restrict__ jdev, int m,
+                                                             double *__restrict__ gm)
+{
+    grid_dependency_wait();
+    const int j = *jdev, lane = threadIdx.x & 31;
+    const GmLayout L{m};
+    for (int i = threadIdx.x >> 5; i <= j; i += blockDim.x >> 5) {
+        double t = 0.0;
+        for (int k = lane; k < np; k += 32) t += part[(long long)i * np + k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(FULL, t, o);
+        if (lane == 0) gm[L.H(i, j)] = t;
+    }
+}
+
+// w -= sum_{i <= j} H[i][j] V_i; partials of ||w||^2
+__global__ void __launch_bounds__(kDotThreads) gm_orth_kernel(long long n, const float *__restrict__ V,
+                                                             const int *__restrict__ jdev, int m,
+                                                             const double *__restrict__ gm, double *__restrict__ w,
+                                                             double *__restrict__ part)
+{
+    grid_dependency_wait();
+    __shared__ double hc[kGmMaxRestart + 1];
+    __shared__ double sred[kDotThreads / 32];
+    const int j = *jdev;
+    const GmLayout L{m};
+    for (int i = threadIdx.x; i <= j; i += blockDim.x) hc[i] = gm[L.H(i, j)];
+    __syncthreads();
+    double s = 0.0;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        double we = w[e];
+        for (int i = 0; i <= j; ++i) we -= hc[i] * (double)V[(long long)i * n + e];
+        w[e] = we;
+        s += we * we;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+    if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < kDotThreads / 32; ++k) t += sred[k];
+        part[blockIdx.x] = t;
+    }
+}
+
+// ||w|| from its partials, Givens rotations on column j, the residual
+// estimate; j += 1; the while condition (inner tolerance, basis size,
+// breakdown, total iteration cap).
+__global__ void __launch_bounds__(kDotThreads) gm_givens_kernel(cudaGraphConditionalHandle cond, int use_cond,
+                                                               const double *__restrict__ part, int np,
+                                                               int *__restrict__ jdev, int m, double *__restrict__ gm,
+                                                               double inner_tol, int *__restrict__ it_total,
+                                                               int max_iter, double *__restrict__ hist)
+{
+    grid_dependency_wait();
+    __shared__ double sred[kDotThreads / 32];
+    double s = 0.0;
+    for (int k = threadIdx.x; k < np; k += blockDim.x) s += part[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+    if ((threadIdx.x & 31) == 0) sred[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    double wsq = 0.0;
+    for (int k = 0; k < kDotThreads / 32; ++k) wsq += sred[k];
+    const int j = *jdev;
+    const GmLayout L{m};
+    double *cs = gm + L.cs(), *sn = gm + L.sn(), *g = gm + L.g(), *sl = gm + L.slot();
+    const double hn = sqrt(fmax(wsq, 0.0));
+    for (int i = 0; i < j; ++i) {
+        const double a = gm[L.H(i, j)], b = gm[L.H(i + 1, j)];
+        gm[L.H(i, j)] = cs[i] * a + sn[i] * b;
+        gm[L.H(i + 1, j)] = -sn[i] * a + cs[i] * b;
+    }
+    const double a = gm[L.H(j, j)];
+    const double r = hypot(a, hn);
+    const double c = r > 0.0 ? a / r : 1.0, sg = r > 0.0 ? hn / r : 0.0;
+    cs[j] = c;
+    sn[j] = sg;
+    gm[L.H(j, j)] = r;
+    gm[L.H(j + 1, j)] = 0.0;
+    g[j + 1] = -sg * g[j];
+    g[j] = c * g[j];
+    const double res = fabs(g[j + 1]);
+    sl[GM_RES] = res;
+    sl[GM_INVH] = hn > 0.0 ? 1.0 / hn : 0.0;
+    const int k = ++*it_total;
+    hist[k] = res;
+    *jdev = j + 1;
+    const bool more = (j + 1 < m) && res > inner_tol * sl[GM_BETA0] && hn > 0.0 && k < max_iter;
+    if (use_cond) cudaGraphSetConditional(cond, more ? 1u : 0u);
+}
+
+// V_j = vin = w / ||w|| (j already advanced)
+__global__ void gm_scale_kernel(long long n, const double *__restrict__ w, const int *__restrict__ jdev, int m,
+                                const double *__restrict__ gm, float *__restrict__ V, double *__restrict__ vin)
+{
+    grid_dependency_wait();
+    const int j = *jdev;
+    const double inv = gm[GmLayout{m}.slot() + GM_INVH];
+    float *vj = V + (long long)j * n;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const double v = w[e] * inv;
+        const float f = (float)v;
+        vj[e] = f;
+        vin[e] = (double)f;  // the cycle sees the stored basis vector
+    }
+}
+
+// Z_j = zout (fp32)
+__global__ void gm_store_z_kernel(long long n, const double *__restrict__ zout, const int *__restrict__ jdev,
+                                  float *__restrict__ Z)
+{
+    grid_dependency_wait();
+    float *zj = Z + (long long)(*jdev) * n;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        zj[e] = (float)zout[e];
+}
+
+// start of an inner solve: r (fp64) in vin and V_0 = r / ||r||; g = (beta0, 0, ...)
+__global__ void gm_start_kernel(int m, const double *__restrict__ scal, int slot_rr, double *__restrict__ gm,
+                                int *__restrict__ jdev)
+{
+    const GmLayout L{m};
+    const double beta0 = sqrt(fmax(scal[slot_rr], 0.0));
+    double *g = gm + L.g();
+    for (int i = 0; i <= m; ++i) g[i] = 0.0;
+    g[0] = beta0;
+    gm[L.slot() + GM_BETA0] = beta0;
+    gm[L.slot() + GM_INVH] = beta0 > 0.0 ? 1.0 / beta0 : 0.0;
+    *jdev = 0;
+}
+
+__global__ void gm_scale_first_kernel(long long n, const double *__restrict__ r, int m, const double *__restrict__ gm,
+                                      float *__restrict__ V, double *__restrict__ vin)
+{
+    const double inv = gm[GmLayout{m}.slot() + GM_INVH];
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const float f = (float)(r[e] * inv);
+        V[e] = f;
+        vin[e] = (double)f;
+    }
+}
+
+// y = R^-1 g over the k = j columns done (R: the rotated Hessenberg)
+__global__ void gm_backsolve_kernel(int m, const int *__restrict__ jdev, double *__restrict__ gm)
+{
+    const GmLayout L{m};
+    const int k = *jdev;
+    const double *g = gm + L.g();
+    double *y = gm + L.y();
+    for (int i = k - 1; i >= 0; --i) {
+        double t = g[i];
+        for (int l = i + 1; l < k; ++l) t -= gm[L.H(i, l)] * y[l];
+        const double d = gm[L.H(i, i)];
+        y[i] = d != 0.0 ? t / d : 0.0;
+    }
+}
+
+// x += sum_{i < k} y_i Z_i  (fp64 update of x)
+__global__ void gm_update_kernel(long long n, const float *__restrict__ Z, const int *__restrict__ jdev, int m,
+                                 const double *__restrict__ gm, double *__restrict__ x)
+{
+    __shared__ double ys[kGmMaxRestart];
+    const int k = *jdev;
+    const double *y = gm + GmLayout{m}.y();
+    for (int i = threadIdx.x; i < k; i += blockDim.x) ys[i] = y[i];
+    __syncthreads();
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        double t = 0.0;
+        for (int i = 0; i < k; ++i) t += ys[i] * (double)Z[(long long)i * n + e];
+        x[e] += t;
+    }
+}
+
 struct Level {
     amgt_bsr A{}, P{}, R{};
     amgt_pbsr pA{}, pAs{}, pP{}, pR{};  // packed: cycle operator, level-0 smoother, transfers
@@ -372,6 +618,15 @@ struct amgt_amg {
     uint64_t graph_launches = 0, loop_launches = 0;  // our kernels per iteration in each graph
     double setup_ms[5] = {0, 0, 0, 0, 0};
     std::vector<double> hist;
+    // FGMRES with iterative refinement (solver = AMGT_SOLVER_FGMRES_IR)
+    int resid_prec0 = AMGT_DOUBLE;  // the cycle's level-0 residual precision
+    float *gmV = nullptr, *gmZ = nullptr;  // basis (m + 1 vectors), preconditioned vectors (m)
+    double *gm = nullptr;                  // Hessenberg, rotations, g, y, slots (GmLayout)
+    double *gm_vin = nullptr, *gm_zout = nullptr, *gm_w = nullptr, *gm_part = nullptr;
+    int *gm_j = nullptr;                   // device: inner iteration index
+    cudaGraphExec_t gm_loop = nullptr;
+    bool gm_loop_failed = false;
+    uint64_t gm_loop_launches = 0;
 };
 
 using namespace amgt;
@@ -399,6 +654,15 @@ void destroy_handle(amgt_amg *h, cudaStream_t s)
     if (!h) return;
     if (h->graph) cudaGraphExecDestroy(h->graph);
     if (h->loop) cudaGraphExecDestroy(h->loop);
+    if (h->gm_loop) cudaGraphExecDestroy(h->gm_loop);
+    free_ptr(h->gmV, s);
+    free_ptr(h->gmZ, s);
+    free_ptr(h->gm, s);
+    free_ptr(h->gm_vin, s);
+    free_ptr(h->gm_zout, s);
+    free_ptr(h->gm_w, s);
+    free_ptr(h->gm_part, s);
+    free_ptr(h->gm_j, s);
     if (h->graph_stream) cudaStreamDestroy(h->graph_stream);
     free_ptr(h->loop_it, s);
     free_ptr(h->loop_rr, s);
@@ -508,6 +772,14 @@ struct PhaseMarks {
 
 int grid_n(amgt_amg *h, long long n) { return grid_for(256, n, h->sm_count, 8); }
 
+// The value shadow a level's products at `prec` read; none for fp32 when
+// the exact fp16 shadow serves them (the SpMV reads it instead).
+int level_shadow(amgt_bsr *A, int prec, amgt_stream_t stream)
+{
+    if (prec == AMGT_FLOAT && A->exact_prec == AMGT_HALF && A->blcVal_fp16) return AMGT_OK;
+    return amgt_bsr_make_shadow(A, prec, stream);
+}
+
 // z = M f: one V(1,1) cycle
 int cycle(amgt_amg *h, const double *rhs0, double *out0, cudaStream_t s)
 {
@@ -523,7 +795,7 @@ int cycle(amgt_amg *h, const double *rhs0, double *out0, cudaStream_t s)
             AMGT_TRY(pbsr_residual(&v.pA, f, v.u, v.t, s, h->sm_count));
             AMGT_TRY(pbsr_spmv(&v.pR, 1.0, v.t, 0.0, lv[l + 1].f, s, h->sm_count));
         } else {
-            AMGT_TRY(spmv_residual(l == 0 ? AMGT_DOUBLE : v.prec, &v.A, f, v.u, v.t, s, h->sm_count));
+            AMGT_TRY(spmv_residual(l == 0 ? h->resid_prec0 : v.prec, &v.A, f, v.u, v.t, s, h->sm_count));
             AMGT_TRY(amgt_spmv(v.prec_transfer, 1.0, &v.R, v.t, 0.0, lv[l + 1].f, (amgt_stream_t)s));
         }
     }
@@ -669,6 +941,145 @@ int build_graph(amgt_amg *h, double *x)
     return AMGT_OK;
 }
 
+// One inner FGMRES iteration (the body of the inner loop graph); see the
+// kernel comments above.  use_cond: the Givens kernel sets the while node's
+// condition.
+int gm_iteration(amgt_amg *h, cudaStream_t s, int use_cond, cudaGraphConditionalHandle cond)
+{
+    const int m = h->prm.restart;
+    const long long n = h->n0;
+    AMGT_TRY(cycle(h, h->gm_vin, h->gm_zout, s));
+    AMGT_LAUNCH_PDL(gm_store_z_kernel, grid_n(h, n), 256, 0, s, n, (const double *)h->gm_zout, (const int *)h->gm_j,
+                    h->gmZ);
+    AMGT_TRY(amgt_spmv(h->prm.inner_prec0, 1.0, &h->lv[0].A, h->gm_zout, 0.0, h->gm_w, (amgt_stream_t)s));
+    AMGT_LAUNCH_PDL(gm_mdot_kernel, kDotGrid, kDotThreads, 0, s, n, (const float *)h->gmV, (const int *)h->gm_j,
+                    (const double *)h->gm_w, h->gm_part);
+    AMGT_LAUNCH_PDL(gm_mdot_reduce_kernel, 1, 1024, 0, s, (const double *)h->gm_part, kDotGrid, (const int *)h->gm_j,
+                    m, h->gm);
+    AMGT_LAUNCH_PDL(gm_orth_kernel, kDotGrid, kDotThreads, 0, s, n, (const float *)h->gmV, (const int *)h->gm_j, m,
+                    (const double *)h->gm, h->gm_w, h->gm_part);
+    AMGT_LAUNCH_PDL(gm_givens_kernel, 1, kDotThreads, 0, s, cond, use_cond, (const double *)h->gm_part, kDotGrid,
+                    h->gm_j, m, h->gm, h->prm.inner_tol, h->loop_it, h->prm.max_iter, h->loop_rr);
+    AMGT_LAUNCH_PDL(gm_scale_kernel, grid_n(h, n), 256, 0, s, n, (const double *)h->gm_w, (const int *)h->gm_j, m,
+                    (const double *)h->gm, h->gmV, h->gm_vin);
+    return AMGT_OK;
+}
+
+// The inner loop as one graph: a while node whose body is gm_iteration.
+int build_gm_loop(amgt_amg *h)
+{
+    if (h->gm_loop) return AMGT_OK;
+    if (!h->graph_stream) AMGT_CUDA_TRY(cudaStreamCreateWithFlags(&h->graph_stream, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    AMGT_CUDA_TRY(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle cond;
+    cudaGraphNodeParams np = {};
+    cudaGraphNode_t node;
+    int rc = AMGT_OK;
+    cudaError_t e = cudaGraphConditionalHandleCreate(&cond, g, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = cond;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+    }
+    if (e == cudaSuccess)
+        e = cudaStreamBeginCaptureToGraph(h->graph_stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        const uint64_t c0 = amgt_kernel_launch_count();
+        rc = gm_iteration(h, h->graph_stream, 1, cond);
+        h->gm_loop_launches = amgt_kernel_launch_count() - c0;
+        cudaGraph_t captured = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(h->graph_stream, &captured);
+        if (e == cudaSuccess) e = ee;
+    }
+    if (e == cudaSuccess && rc == AMGT_OK) e = cudaGraphInstantiate(&h->gm_loop, g, 0);
+    cudaGraphDestroy(g);
+    if (rc != AMGT_OK) return rc;
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        h->gm_loop = nullptr;
+        set_last_cuda_error(e, "FGMRES loop graph", __FILE__, __LINE__);
+        return AMGT_ERR_CUDA;
+    }
+    return AMGT_OK;
+}
+
+// FGMRES(m) with iterative refinement: see amgt_amg_params.solver.
+int fgmres_ir_solve(amgt_amg *h, const double *b, double *x, int *iterations, double *rel_res, cudaStream_t s)
+{
+    Level &v0 = h->lv[0];
+    const int m = h->prm.restart;
+    const long long n = h->n0;
+    const int max_iter = h->prm.max_iter;
+    if (!h->loop_pinned) AMGT_CUDA_TRY(cudaMallocHost(&h->loop_pinned, sizeof(double) * (max_iter + 2)));
+    h->hist.clear();
+    AMGT_CUDA_TRY(cudaMemsetAsync(h->loop_it, 0, sizeof(int), s));
+    AMGT_TRY(dot(h, b, b, S_BB, OP_STORE, s));
+    double bb = 0.0, rel = 0.0;
+    int total = 0, seen = 0;
+    bool graph_ran = false;
+    for (int outer = 0; outer < h->prm.max_outer + 1; ++outer) {
+        // fp64 residual of the current x (the refinement's residual)
+        AMGT_TRY(spmv_residual(AMGT_DOUBLE, &v0.A, b, x, h->r, s, h->sm_count));
+        AMGT_TRY(dot(h, h->r, h->r, S_RR, OP_STORE, s));
+        AMGT_CUDA_TRY(cudaMemcpyAsync(h->pinned, h->scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        AMGT_CUDA_TRY(cudaMemcpyAsync(h->loop_pinned, h->loop_it, sizeof(int), cudaMemcpyDeviceToHost, s));
+        AMGT_CUDA_TRY(cudaMemcpyAsync(h->loop_pinned + 1, h->loop_rr + 1, sizeof(double) * max_iter,
+                                      cudaMemcpyDeviceToHost, s));
+        AMGT_CUDA_TRY(cudaStreamSynchronize(s));
+        bb = h->pinned[S_BB];
+        const double sb = bb > 0.0 ? std::sqrt(bb) : 1.0;
+        total = *reinterpret_cast<const int *>(h->loop_pinned);
+        for (int k = seen + 1; k <= total; ++k) h->hist.push_back(h->loop_pinned[k] / sb);  // inner estimates
+        if (graph_ran)  // the kernels the graph launched, per inner iteration
+            for (long long k = 0; k < (long long)(total - seen) * (long long)h->gm_loop_launches; ++k) count_launch();
+        graph_ran = false;
+        seen = total;
+        rel = bb > 0.0 ? std::sqrt(std::max(0.0, h->pinned[S_RR]) / bb) : 0.0;
+        h->hist.push_back(rel);
+        if (rel <= h->prm.tol || total >= max_iter || outer == h->prm.max_outer) break;
+        // inner solve of A d = r; x += d
+        AMGT_LAUNCH(gm_start_kernel, 1, 1, 0, s, m, (const double *)h->scal, (int)S_RR, h->gm, h->gm_j);
+        AMGT_LAUNCH(gm_scale_first_kernel, grid_n(h, n), 256, 0, s, n, (const double *)h->r, m,
+                    (const double *)h->gm, h->gmV, h->gm_vin);
+        bool done = false;
+        if (h->prm.use_graph && !h->gm_loop_failed) {
+            const int lrc = build_gm_loop(h);
+            if (lrc == AMGT_OK) {
+                AMGT_CUDA_TRY(cudaGraphLaunch(h->gm_loop, s));
+                done = graph_ran = true;
+            } else if (lrc != AMGT_ERR_CUDA) {
+                return lrc;
+            } else {
+                h->gm_loop_failed = true;
+            }
+        }
+        if (!done) {
+            // direct launches, the while test on the host
+            for (int j = 0; j < m; ++j) {
+                AMGT_TRY(gm_iteration(h, s, 0, 0));
+                AMGT_CUDA_TRY(cudaMemcpyAsync(h->pinned + 2, h->gm + GmLayout{m}.slot(), 3 * sizeof(double),
+                                              cudaMemcpyDeviceToHost, s));
+                AMGT_CUDA_TRY(cudaMemcpyAsync(h->loop_pinned, h->loop_it, sizeof(int), cudaMemcpyDeviceToHost, s));
+                AMGT_CUDA_TRY(cudaStreamSynchronize(s));
+                const double beta0 = h->pinned[2 + GM_BETA0], invh = h->pinned[2 + GM_INVH],
+                             res = h->pinned[2 + GM_RES];
+                const int k = *reinterpret_cast<const int *>(h->loop_pinned);
+                if (!(j + 1 < m && res > h->prm.inner_tol * beta0 && invh > 0.0 && k < max_iter)) break;
+            }
+        }
+        AMGT_LAUNCH(gm_backsolve_kernel, 1, 1, 0, s, m, (const int *)h->gm_j, h->gm);
+        AMGT_LAUNCH(gm_update_kernel, grid_n(h, n), 256, 0, s, n, (const float *)h->gmZ, (const int *)h->gm_j, m,
+                    (const double *)h->gm, x);
+    }
+    if (iterations) *iterations = total;
+    if (rel_res) *rel_res = rel;
+    return AMGT_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -688,6 +1099,11 @@ void amgt_amg_default_params(amgt_amg_params *p)
     p->smooth_prec0 = AMGT_DOUBLE;
     p->packed = 0;
     p->exact_storage = 1;
+    p->solver = AMGT_SOLVER_PCG;
+    p->restart = 30;
+    p->inner_tol = 1e-4;
+    p->inner_prec0 = AMGT_FLOAT;
+    p->max_outer = 20;
 }
 
 int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const amgt_amg_params *params,
@@ -700,7 +1116,12 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     // residual norms: max_iter must be >= 1 (and bounded, so that its
     // buffers stay small)
     if (params && (params->max_iter < 1 || params->max_iter > 1000000 || !(params->tol >= 0.0) ||
-                   params->max_coarse_rows < 1 || params->max_coarse_rows > 16384))
+                   params->max_coarse_rows < 1 || params->max_coarse_rows > 16384 ||
+                   (params->solver != AMGT_SOLVER_PCG && params->solver != AMGT_SOLVER_FGMRES_IR)))
+        return AMGT_ERR_INVALID;
+    if (params && params->solver == AMGT_SOLVER_FGMRES_IR &&
+        (params->restart < 1 || params->restart > kGmMaxRestart || params->inner_prec0 < AMGT_DOUBLE ||
+         params->inner_prec0 > AMGT_BF16 || !(params->inner_tol >= 0.0) || params->max_outer < 1))
         return AMGT_ERR_INVALID;
     DeviceState *st;
     AMGT_TRY(device_state(&st));
@@ -709,6 +1130,8 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     if (params) h->prm = *params;
     else amgt_amg_default_params(&h->prm);
     if (h->prm.smooth_prec0 < AMGT_DOUBLE || h->prm.smooth_prec0 > AMGT_BF16) h->prm.smooth_prec0 = AMGT_DOUBLE;
+    const bool fgm = h->prm.solver == AMGT_SOLVER_FGMRES_IR;
+    h->resid_prec0 = fgm ? h->prm.inner_prec0 : AMGT_DOUBLE;
     h->sm_count = st->sm_count;
     int L = num_interp + 1;
     if (h->prm.max_levels > 0 && L > h->prm.max_levels) L = h->prm.max_levels;
@@ -844,9 +1267,12 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
     // levels and transfers): one value check each, one read-back per 15
     if (h->prm.exact_storage) {
         std::vector<std::pair<amgt_bsr *, int>> mats;  // operator, flag slot
+        // fp32 operators too: one whose values fp16 holds is read from the
+        // fp16 shadow (the same fp32 sums at half the bytes)
         for (int l = 0; l < L; ++l) {
-            if (l == 0 || h->lv[l].prec == AMGT_DOUBLE) mats.push_back({&h->lv[l].A, 3 * l});
-            if (l < L - 1 && h->lv[l].prec_transfer == AMGT_DOUBLE) {
+            if (l == 0 || h->lv[l].prec == AMGT_DOUBLE || h->lv[l].prec == AMGT_FLOAT)
+                mats.push_back({&h->lv[l].A, 3 * l});
+            if (l < L - 1 && (h->lv[l].prec_transfer == AMGT_DOUBLE || h->lv[l].prec_transfer == AMGT_FLOAT)) {
                 mats.push_back({&h->lv[l].P, 3 * l + 1});
                 mats.push_back({&h->lv[l].R, 3 * l + 2});
             }
@@ -883,11 +1309,12 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
             if (!v.inv_l1 && (rc = alloc_n(&v.inv_l1, v.n, s))) goto fail;
             if ((rc = bsr_l1_norms(&v.A, v.inv_l1, 1, s, h->sm_count))) goto fail;
         }
-        if ((rc = amgt_bsr_make_shadow(&v.A, v.prec, stream))) goto fail;
-        if (l == 0 && (rc = amgt_bsr_make_shadow(&v.A, h->prm.smooth_prec0, stream))) goto fail;
+        if ((rc = level_shadow(&v.A, v.prec, stream))) goto fail;
+        if (l == 0 && (rc = level_shadow(&v.A, h->prm.smooth_prec0, stream))) goto fail;
+        if (l == 0 && fgm && (rc = level_shadow(&v.A, h->prm.inner_prec0, stream))) goto fail;
         if (l < L - 1) {
-            if ((rc = amgt_bsr_make_shadow(&v.P, v.prec_transfer, stream))) goto fail;
-            if ((rc = amgt_bsr_make_shadow(&v.R, v.prec_transfer, stream))) goto fail;
+            if ((rc = level_shadow(&v.P, v.prec_transfer, stream))) goto fail;
+            if ((rc = level_shadow(&v.R, v.prec_transfer, stream))) goto fail;
         }
         if (h->prm.packed) {
             // level 0: fp64 for the residual and the Krylov product, the
@@ -919,8 +1346,20 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         (rc = alloc_n(&h->part, std::max(h->grid0, kDotGrid), s)) || (rc = alloc_n(&h->loop_it, 1, s)) ||
         (rc = alloc_n(&h->loop_rr, (size_t)h->prm.max_iter + 1, s)))
         goto fail;
+    if (fgm) {
+        const int m = h->prm.restart;
+        if ((rc = alloc_n(&h->gmV, (size_t)(m + 1) * h->n0, s)) || (rc = alloc_n(&h->gmZ, (size_t)m * h->n0, s)) ||
+            (rc = alloc_n(&h->gm, (size_t)GmLayout{m}.size(), s)) || (rc = alloc_n(&h->gm_vin, h->n0, s)) ||
+            (rc = alloc_n(&h->gm_zout, h->n0, s)) || (rc = alloc_n(&h->gm_w, h->n0, s)) ||
+            (rc = alloc_n(&h->gm_part, (size_t)(m + 1) * kDotGrid, s)) || (rc = alloc_n(&h->gm_j, 1, s)))
+            goto fail;
+        if (cudaMemsetAsync(h->gm, 0, sizeof(double) * GmLayout{m}.size(), s) != cudaSuccess) {
+            rc = AMGT_ERR_CUDA;
+            goto fail;
+        }
+    }
     AMGT_CUDA_TRY(cudaMemsetAsync(h->scal, 0, sizeof(double) * S_NSCAL, s));
-    AMGT_CUDA_TRY(cudaMallocHost(&h->pinned, sizeof(double) * 4));
+    AMGT_CUDA_TRY(cudaMallocHost(&h->pinned, sizeof(double) * 8));
     free_ptr(xflags, s);
     pm.mark(3, s);
     pm.accumulate(h->setup_ms);  // waits for the setup's last work
@@ -952,6 +1391,7 @@ int amgt_amg_solve(amgt_amg *h, const double *b, double *x, int *iterations, dou
 {
     if (!h || !b || !x) return AMGT_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
+    if (h->prm.solver == AMGT_SOLVER_FGMRES_IR) return fgmres_ir_solve(h, b, x, iterations, rel_res, s);
     Level &v0 = h->lv[0];
     h->hist.clear();
     // r = b - A x, ||b||^2, ||r||^2

@@ -21,12 +21,16 @@
 // Numeric.  One warp per A block row; the row's (A block, B block) pairs
 // are flattened and taken 8 at a time, 4 lanes per pair (lane r: row r of
 // the 4x4 product), B blocks staged through shared memory, so that every
-// load of a step is in flight at once.  Entry (r, c) of a product is the
-// sum over k ascending of a[r][k] * b[k][c] with separate multiply and add
-// (no FMA); products are added to their C block in A block order, the
-// arithmetic of the reference's scalar branch (:1289-1339), so the fp64
-// result equals the CPU oracle bit for bit (for finite values: unstored
-// entries are zero and their products change no sum).  C rows of up to 32
+// load of a step is in flight at once.  In fp64, entry (r, c) of a product
+// is the fused multiply-add chain t = fma(a[r][k], b[k][c], t) over k
+// ascending from zero, and products are added to their C block in A block
+// order: the arithmetic of the reference's fp64 kernel, whose scalar
+// branch's `temp += a * b` (:1317) nvcc contracts into that chain and
+// whose m8n8k4 branch (:1173-1262) takes every k term; so the fp64 result
+// equals the oracle's restatement of that arithmetic bit for bit (for
+// finite values: unstored entries are zero, and a zero term leaves an FMA
+// chain unchanged).  The fp32 / fp16 / bf16 forms use separate fp32
+// multiply and add.  C rows of up to 32
 // blocks accumulate in shared memory, longer rows in place.  FP64
 // arithmetic on the CUDA cores: the 4x4 products are too small for tcgen05
 // (M >= 64), and on B200 the fp64 MMA rate equals the fp64 FMA rate.  The
@@ -459,6 +463,11 @@ struct NumT<AMGT_DOUBLE> {
     __device__ static double ld(const double *p, long long i) { return p[i]; }
     __device__ static double mul(double a, double b) { return __dmul_rn(a, b); }
     __device__ static double add(double a, double b) { return __dadd_rn(a, b); }
+    // product entry step: the reference's contracted `temp += a * b`
+    __device__ static double madd(double a, double b, double t, bool first)
+    {
+        return __fma_rn(a, b, first ? 0.0 : t);
+    }
 };
 template <>
 struct NumT<AMGT_FLOAT> {
@@ -467,6 +476,10 @@ struct NumT<AMGT_FLOAT> {
     __device__ static float ld(const float *p, long long i) { return p[i]; }
     __device__ static float mul(float a, float b) { return __fmul_rn(a, b); }
     __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
+    __device__ static float madd(float a, float b, float t, bool first)
+    {
+        return first ? mul(a, b) : add(t, mul(a, b));
+    }
 };
 template <>
 struct NumT<AMGT_HALF> {
@@ -475,6 +488,10 @@ struct NumT<AMGT_HALF> {
     __device__ static float ld(const __half *p, long long i) { return __half2float(p[i]); }
     __device__ static float mul(float a, float b) { return __fmul_rn(a, b); }
     __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
+    __device__ static float madd(float a, float b, float t, bool first)
+    {
+        return first ? mul(a, b) : add(t, mul(a, b));
+    }
 };
 template <>
 struct NumT<AMGT_BF16> {
@@ -483,6 +500,10 @@ struct NumT<AMGT_BF16> {
     __device__ static float ld(const __nv_bfloat16 *p, long long i) { return __bfloat162float(p[i]); }
     __device__ static float mul(float a, float b) { return __fmul_rn(a, b); }
     __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
+    __device__ static float madd(float a, float b, float t, bool first)
+    {
+        return first ? mul(a, b) : add(t, mul(a, b));
+    }
 };
 
 template <int PREC>
@@ -714,7 +735,7 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                             row4_smem<PREC>(bp + kk * AR, bk);
 #pragma unroll
                             for (int c = 0; c < 4; ++c)
-                                s[c] = kk == 0 ? T::mul(ar[0], bk[c]) : T::add(s[c], T::mul(ar[kk], bk[c]));
+                                s[c] = T::madd(ar[kk], bk[c], s[c], kk == 0);
                         }
                     }
                     // ordered accumulation: same C block row -> rounds in lane order

@@ -332,10 +332,15 @@ static const void *value_array(const amgt_bsr *A, int prec)
     }
 }
 
-// Storage read by an fp64 product: the shadow that holds every value
-// exactly when amgt_bsr_make_exact found one (same results, fewer bytes).
+// Storage a product reads: for fp64, the shadow that holds every value
+// exactly when amgt_bsr_make_exact found one (same results, fewer bytes);
+// for fp32, the fp16 shadow when it holds every value exactly (the same
+// fp32 inputs and the same fp32 sums at half the bytes), so that a reduced
+// precision never reads more value bytes than the fp64 form of the same
+// operator.  bf16 keeps its own rounding.
 static int storage_mode(const amgt_bsr *A, int prec)
 {
+    if (prec == AMGT_FLOAT && A->exact_prec == AMGT_HALF && A->blcVal_fp16) return AMGT_HALF;
     if (prec != AMGT_DOUBLE) return prec;
     if (A->exact_prec == AMGT_HALF && A->blcVal_fp16) return kExact16;
     if (A->exact_prec == AMGT_FLOAT && A->blcVal_fp32) return kExact32;
@@ -680,7 +685,7 @@ int amgt_bsr_residual(int prec, const amgt_bsr *A, const double *f, const double
 {
     if (!A || prec < AMGT_DOUBLE || prec > AMGT_BF16) return AMGT_ERR_INVALID;
     if (A->row == 0) return AMGT_OK;
-    if (!f || !u || !r || !A->blcPtr || !value_array(A, prec)) return AMGT_ERR_INVALID;
+    if (!f || !u || !r || !A->blcPtr || !value_array(A, storage_mode(A, prec))) return AMGT_ERR_INVALID;
     DeviceState *st;
     AMGT_TRY(device_state(&st));
     return spmv_residual(prec, A, f, u, r, (cudaStream_t)stream, st->sm_count);
@@ -691,7 +696,8 @@ int amgt_bsr_jacobi(int prec, const amgt_bsr *A, const double *inv_l1, double we
 {
     if (!A || prec < AMGT_DOUBLE || prec > AMGT_BF16 || A->row != A->col) return AMGT_ERR_INVALID;
     if (A->row == 0) return AMGT_OK;
-    if (!inv_l1 || !f || !u || !u_out || u == u_out || !A->blcPtr || !value_array(A, prec)) return AMGT_ERR_INVALID;
+    if (!inv_l1 || !f || !u || !u_out || u == u_out || !A->blcPtr || !value_array(A, storage_mode(A, prec)))
+        return AMGT_ERR_INVALID;
     DeviceState *st;
     AMGT_TRY(device_state(&st));
     return spmv_jacobi(prec, A, inv_l1, weight, f, u, u_out, (cudaStream_t)stream, st->sm_count);

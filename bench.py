@@ -262,9 +262,14 @@ def geometric_interps(problems, dims, coarse_rows=64):
 
 
 MIXED_POLICY = [0, 1, 1, 2]  # level 0 fp64, 1-2 fp32, >= 3 fp16 (values); fp32 accumulation
+FGMRES_IR = {"solver": 1, "restart": 30, "inner_prec0": 1, "inner_tol": 1e-4}
+FGMRES_IR_DESC = ("FGMRES(30) with iterative refinement: fp64 residual and update per refinement step; inner "
+                  "FGMRES with level 0 in fp32 (exact fp16 storage where it holds), levels 1-2 fp32, >=3 fp16, "
+                  "fp32 Krylov basis, fp64 inner products; Galerkin products at each level's precision")
 
 
-def amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, policy, smooth0, flexible, reps=3, exact=1, galerkin=0):
+def amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, policy, smooth0, flexible, reps=3, exact=1, galerkin=0,
+                    **extra):
     """Setup + solve to ||b - A x|| / ||b|| <= 1e-8 through the library;
     device-resident inputs.  Returns timings, iterations and the residual
     recomputed in fp64 from the returned x."""
@@ -274,7 +279,8 @@ def amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, policy, smooth0, flexi
     dev = lambda M: (M[0], M[1]) + tuple(torch.from_numpy(v).cuda() for v in M[2:])  # noqa: E731
     dA, dPs = dev(A_host), [dev(P) for P in Ps_host]
     b = torch.from_numpy(b_host).cuda()
-    prm = default_params(flexible=flexible, smooth_prec0=smooth0, exact_storage=exact, galerkin_by_level=galerkin)
+    prm = default_params(flexible=flexible, smooth_prec0=smooth0, exact_storage=exact, galerkin_by_level=galerkin,
+                         **extra)
     S = AmgSolver(dA, dPs, prm)  # warm-up: module loads, pools
     S.solve(b)
     S.free()
@@ -496,9 +502,12 @@ def run_amgt(args):
         f64 = amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, [0], 0, 0)
         f64_8 = amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, [0], 0, 0, exact=0)
         mix = amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, MIXED_POLICY, 1, 1, galerkin=1)
+        gir = amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, MIXED_POLICY, 1, 0, galerkin=1,
+                              **FGMRES_IR)
         err = float(torch.linalg.vector_norm(mix["x"] - f64["x"]) / torch.linalg.vector_norm(f64["x"]))
         setup_solve = {}
-        for name, rres in (("fp64", f64), ("fp64_8byte_values", f64_8), ("mixed", mix)):
+        for name, rres in (("fp64", f64), ("fp64_8byte_values", f64_8), ("mixed", mix),
+                           ("mixed_fgmres_ir", gir)):
             setup_solve[name] = {k: (float(f"{v:.5g}") if isinstance(v, float) else v) for k, v in rres.items()
                                  if k not in ("x", "levels", "setup_ms")}
             setup_solve[name]["total_s"] = round(rres["setup_s"] + rres["solve_s"], 5)
@@ -513,6 +522,11 @@ def run_amgt(args):
                                           "products at each level's precision; flexible CG")
         setup_solve["mixed"]["rel_err_vs_fp64_solution"] = err
         setup_solve["mixed"]["speedup_vs_fp64"] = round(setup_solve["fp64"]["total_s"] / setup_solve["mixed"]["total_s"], 3)
+        setup_solve["mixed_fgmres_ir"]["policy"] = FGMRES_IR_DESC
+        setup_solve["mixed_fgmres_ir"]["rel_err_vs_fp64_solution"] = float(
+            torch.linalg.vector_norm(gir["x"] - f64["x"]) / torch.linalg.vector_norm(f64["x"]))
+        setup_solve["mixed_fgmres_ir"]["speedup_vs_fp64"] = round(
+            setup_solve["fp64"]["total_s"] / setup_solve["mixed_fgmres_ir"]["total_s"], 3)
         setup_solve["e2e_fp64"] = amg_e2e(amgt, torch, A_host, Ps_host, b_host, [0], 0, 0)
         setup_solve["problem"] = (f"3D 7-point Poisson {GRID[0]}^3, b uniform[-1,1] seed 0, linear-interpolation "
                                   f"hierarchy ({len(Ps_host) + 1} levels), PCG + V(1,1) l1-Jacobi, tol 1e-8")
@@ -525,13 +539,19 @@ def run_amgt(args):
         vb_host = problems.rand_uniform(0, V_host[0])
         vf64 = amg_setup_solve(amgt, torch, V_host, VPs_host, vb_host, [0], 0, 0)
         vmix = amg_setup_solve(amgt, torch, V_host, VPs_host, vb_host, MIXED_POLICY, 1, 1, galerkin=1)
+        vgir = amg_setup_solve(amgt, torch, V_host, VPs_host, vb_host, MIXED_POLICY, 1, 0, galerkin=1, **FGMRES_IR)
         vc = {"problem": "3D 27-point variable-coefficient diffusion 96^3 (884,736 rows, 23.4 M nonzeros), "
                          "b uniform[-1,1] seed 0, linear-interpolation hierarchy, PCG + V(1,1) l1-Jacobi, tol 1e-8"}
-        for name, rres in (("fp64", vf64), ("mixed", vmix)):
+        for name, rres in (("fp64", vf64), ("mixed", vmix), ("mixed_fgmres_ir", vgir)):
             vc[name] = {k: float(f"{rres[k]:.5g}") if isinstance(rres[k], float) else rres[k]
                         for k in ("setup_s", "solve_s", "iters", "relres_fp64_verified")}
             vc[name]["total_s"] = round(rres["setup_s"] + rres["solve_s"], 5)
-        vc["mixed"]["speedup_vs_fp64"] = round(vc["fp64"]["total_s"] / vc["mixed"]["total_s"], 3)
+            vc[name]["setup_ms"] = {k: round(v, 3) for k, v in rres["setup_ms"].items()}
+        for name, rres in (("mixed", vmix), ("mixed_fgmres_ir", vgir)):
+            vc[name]["speedup_vs_fp64"] = round(vc["fp64"]["total_s"] / vc[name]["total_s"], 3)
+            vc[name]["rel_err_vs_fp64_solution"] = float(
+                torch.linalg.vector_norm(rres["x"] - vf64["x"]) / torch.linalg.vector_norm(vf64["x"]))
+        vc["mixed_fgmres_ir"]["policy"] = FGMRES_IR_DESC
         setup_solve["varcoef27_96"] = vc
         if world == 1 and rank == 0 and not args.no_cpu:
             setup_solve["cpu_oracle"], xo = cpu_amg(GRID, b_host)

@@ -74,7 +74,7 @@ AMGT_API int amgt_kernel_arch(int *binary_version);
  * with hypre_TAlloc, R/seq_mv/csr_spgemm_device.c:1808-1839).  Exceptions,
  * all small and all pinned HOST memory from cudaMallocHost: each host
  * thread's 512-byte read-back staging per device (freed when the thread
- * exits), and an AMG handle's read-back slots (32 bytes plus
+ * exits), and an AMG handle's read-back slots (64 bytes plus
  * 8 * (max_iter + 2) bytes, freed by amgt_amg_destroy); the per-device
  * error word (16 bytes, cudaMalloc, held until exit); and the fixed array of
  * amgt_spmv_segmented_noalloc.
@@ -339,7 +339,26 @@ typedef struct {
     int exact_storage;     /* fp64 operators whose values fp16 / fp32 hold
                               exactly are read from that shadow
                               (amgt_bsr_make_exact; same results), default 1 */
+    int solver;            /* AMGT_SOLVER_PCG (default) or AMGT_SOLVER_FGMRES_IR */
+    int restart;           /* FGMRES basis size m (default 30, 1 .. 32)      */
+    double inner_tol;      /* an inner FGMRES solve stops when its residual
+                              estimate is <= inner_tol times the outer
+                              residual it started from (default 1e-4)      */
+    int inner_prec0;       /* level-0 precision inside the inner solve: its
+                              matvec and the cycle's level-0 residual
+                              (default AMGT_FLOAT)                          */
+    int max_outer;         /* refinement steps at most (default 20)        */
 } amgt_amg_params;
+
+/* FGMRES with iterative refinement (the reference's R/krylov/flexgmres.c
+ * as the outer solver, refined in fp64): each refinement step computes the
+ * fp64 residual r = b - A x (level 0 in fp64), solves A d = r with FGMRES(m)
+ * preconditioned by the V-cycle, the inner matvec and the cycle's level-0
+ * residual at inner_prec0 and the Krylov basis stored in fp32 (inner
+ * products and the update of x in fp64), and adds d to x.  The inner loop is
+ * one CUDA graph launch per refinement step. */
+#define AMGT_SOLVER_PCG 0
+#define AMGT_SOLVER_FGMRES_IR 1
 
 typedef struct amgt_amg amgt_amg;
 
@@ -351,8 +370,11 @@ AMGT_API void amgt_amg_default_params(amgt_amg_params *p);
 AMGT_API int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P,
                             const amgt_amg_params *params, amgt_amg **out,
                             amgt_stream_t stream);
-/* x: initial guess in, solution out (device).  Reads ||r||^2 (8 bytes) once
- * per iteration; each iteration after the first is one CUDA graph launch. */
+/* x: initial guess in, solution out (device).  PCG: the iteration loop is
+ * one CUDA graph launch and one read-back (one launch and an 8-byte read
+ * per iteration where the runtime lacks conditional graph nodes).
+ * FGMRES-IR: one read-back per refinement step; *iterations counts inner
+ * FGMRES iterations, *rel_res is the last fp64 residual ||b - A x|| / ||b||. */
 AMGT_API int amgt_amg_solve(amgt_amg *amg, const double *b, double *x,
                             int *iterations, double *rel_res, amgt_stream_t stream);
 AMGT_API int amgt_amg_num_levels(const amgt_amg *amg);
@@ -363,7 +385,9 @@ AMGT_API int amgt_amg_level(const amgt_amg *amg, int level, amgt_bsr *A_view, in
  * overlapping the other phases), Galerkin SpGEMMs, smoother data + exact
  * and reduced-precision shadows + coarse inverse + vectors. */
 AMGT_API int amgt_amg_setup_times(const amgt_amg *amg, double *ms);
-/* Relative residual per iteration (entry 0 = initial); returns the count. */
+/* Relative residual per iteration (entry 0 = initial); returns the count.
+ * FGMRES-IR: the inner solves' residual estimates relative to ||b||, and at
+ * each refinement step the fp64 residual. */
 AMGT_API int amgt_amg_residual_history(const amgt_amg *amg, double *hist, int cap);
 AMGT_API int amgt_amg_destroy(amgt_amg *amg, amgt_stream_t stream);
 

@@ -640,12 +640,26 @@ static int orc_int_cmp(const void *a, const void *b)
  * added to C(r, c) only where the product bitmap has the bit.  DOUBLE in
  * fp64; FLOAT / HALF / BF16 with values rounded to the format and fp32
  * products, sums and C accumulators, C values returned as fp64 (exact) and
- * as the format's shadow (cshadow, may be NULL).  No fused multiply-add. */
-ORC_EXPORT void orc_spgemm_fill(int prec, int brA, const int *aptr, const int *aidx,
-                                const uint16_t *amap, const double *aval, int bcB,
-                                const int *bptr, const int *bidx, const uint16_t *bmap,
-                                const double *bval, const int *cptr, int *cidx,
-                                uint16_t *cmap, double *cval, void *cshadow)
+ * as the format's shadow (cshadow, may be NULL).
+ *
+ * contract (DOUBLE only): each product entry is the fused multiply-add
+ * chain t = fma(a[r][k], b[k][c], t) over k ascending, started from zero.
+ * That is the reference's own fp64 arithmetic: its scalar branch writes
+ * `temp_valC[ii*4+kk] += a * b` (:1317), which nvcc contracts into an FMA
+ * (its build passes no --fmad=false), and its tensor-core branch for A
+ * blocks of >= 10 stored entries (:1173-1262, mma.m8n8k4.f64) takes every
+ * k term, stored or not; a term whose A or B value is an unstored zero
+ * leaves an FMA chain unchanged for finite values, so both branches give
+ * this chain as long as the m8n8k4 product rounds like a k-ordered chain
+ * (the PTX description of the f64 mma fixes no order; the tests that use
+ * this variant against the tensor-core branch's blocks allow 1e-12
+ * relative).  contract = 0: separate multiply and add (the arithmetic the
+ * fp32 form keeps). */
+static void orc_spgemm_fill_impl(int prec, int contract, int brA, const int *aptr, const int *aidx,
+                                 const uint16_t *amap, const double *aval, int bcB,
+                                 const int *bptr, const int *bidx, const uint16_t *bmap,
+                                 const double *bval, const int *cptr, int *cidx,
+                                 uint16_t *cmap, double *cval, void *cshadow)
 {
 #pragma omp parallel
     {
@@ -700,8 +714,10 @@ ORC_EXPORT void orc_spgemm_fill(int prec, int brA, const int *aptr, const int *a
                                 if (!(mc & (1u << (4 * r + c)))) continue;
                                 double s = 0.0;
                                 for (int kk = 0; kk < 4; ++kk)
-                                    if ((ma & (1u << (4 * r + kk))) && (mb & (1u << (4 * kk + c))))
-                                        s = s + av[4 * r + kk] * bv[4 * kk + c];
+                                    if ((ma & (1u << (4 * r + kk))) && (mb & (1u << (4 * kk + c)))) {
+                                        if (contract) s = fma(av[4 * r + kk], bv[4 * kk + c], s);
+                                        else s = s + av[4 * r + kk] * bv[4 * kk + c];
+                                    }
                                 accd[16 * t + 4 * r + c] += s;
                             }
                     } else {
@@ -737,6 +753,27 @@ ORC_EXPORT void orc_spgemm_fill(int prec, int brA, const int *aptr, const int *a
         }
         free(pos); free(mark); free(accd); free(accf);
     }
+}
+
+ORC_EXPORT void orc_spgemm_fill(int prec, int brA, const int *aptr, const int *aidx,
+                                const uint16_t *amap, const double *aval, int bcB,
+                                const int *bptr, const int *bidx, const uint16_t *bmap,
+                                const double *bval, const int *cptr, int *cidx,
+                                uint16_t *cmap, double *cval, void *cshadow)
+{
+    orc_spgemm_fill_impl(prec, 0, brA, aptr, aidx, amap, aval, bcB, bptr, bidx, bmap, bval, cptr, cidx, cmap, cval,
+                         cshadow);
+}
+
+/* The same with the reference's fp64 contraction (contract = 1 above). */
+ORC_EXPORT void orc_spgemm_fill_fma(int prec, int brA, const int *aptr, const int *aidx,
+                                    const uint16_t *amap, const double *aval, int bcB,
+                                    const int *bptr, const int *bidx, const uint16_t *bmap,
+                                    const double *bval, const int *cptr, int *cidx,
+                                    uint16_t *cmap, double *cval, void *cshadow)
+{
+    orc_spgemm_fill_impl(prec, 1, brA, aptr, aidx, amap, aval, bcB, bptr, bidx, bmap, bval, cptr, cidx, cmap, cval,
+                         cshadow);
 }
 
 /* ------------------------------------------------------------ transpose */
@@ -889,7 +926,7 @@ ORC_EXPORT void *orc_amg_setup(int n, const int *ia, const int *ja, const double
         int *apidx = (int *)malloc(sizeof(int) * (size_t)(apn ? apn : 1));
         uint16_t *apmap = (uint16_t *)malloc(sizeof(uint16_t) * (size_t)(apn ? apn : 1));
         double *apval = (double *)malloc(sizeof(double) * 16 * (size_t)(apn ? apn : 1));
-        orc_spgemm_fill(ORC_DOUBLE, abr, v->bptr, v->bidx, v->bmap, v->bval, pbc, v->pptr, v->pidx, v->pmap, v->pval,
+        orc_spgemm_fill_fma(ORC_DOUBLE, abr, v->bptr, v->bidx, v->bmap, v->bval, pbc, v->pptr, v->pidx, v->pmap, v->pval,
                         apptr, apidx, apmap, apval, NULL);
         /* RAP = R AP */
         c->n = pn[l];
@@ -899,7 +936,7 @@ ORC_EXPORT void *orc_amg_setup(int n, const int *ia, const int *ja, const double
         c->bidx = (int *)malloc(sizeof(int) * (size_t)(cn ? cn : 1));
         c->bmap = (uint16_t *)malloc(sizeof(uint16_t) * (size_t)(cn ? cn : 1));
         c->bval = (double *)malloc(sizeof(double) * 16 * (size_t)(cn ? cn : 1));
-        orc_spgemm_fill(ORC_DOUBLE, pbc, v->rptr, v->ridx, v->rmap, v->rval, pbc, apptr, apidx, apmap, apval, c->bptr,
+        orc_spgemm_fill_fma(ORC_DOUBLE, pbc, v->rptr, v->ridx, v->rmap, v->rval, pbc, apptr, apidx, apmap, apval, c->bptr,
                         c->bidx, c->bmap, c->bval, NULL);
         free(apptr); free(apidx); free(apmap); free(apval);
     }

@@ -74,6 +74,8 @@ def lib():
                                        ctypes.POINTER(_i64)]
         L.orc_spgemm_fill.argtypes = [c_int, c_int, _i32p, _i32p, _u16p, _f64p, c_int, _i32p, _i32p, _u16p,
                                       _f64p, _i32p, _i32p, _u16p, _f64p, _vp]
+        L.orc_spgemm_fill_fma.argtypes = [c_int, c_int, _i32p, _i32p, _u16p, _f64p, c_int, _i32p, _i32p, _u16p,
+                                      _f64p, _i32p, _i32p, _u16p, _f64p, _vp]
         L.orc_amg_setup.restype = _vp
         L.orc_amg_setup.argtypes = [c_int, _i32p, _i32p, _f64p, c_int, _vp, _vp, _vp, _vp, _vp, c_double]
         L.orc_amg_solve.restype = c_int
@@ -262,8 +264,10 @@ def spgemm_count(A: BSR, B: BSR):
     return int(nb), int(bits.value)
 
 
-def spgemm(A: BSR, B: BSR, prec=DOUBLE):
-    """C = A*B in mBSR; returns (C, shadow or None)."""
+def spgemm(A: BSR, B: BSR, prec=DOUBLE, contract=True):
+    """C = A*B in mBSR; returns (C, shadow or None).  contract (fp64): each
+    4x4 product entry is the k-ordered fused multiply-add chain of the
+    reference's fp64 kernel; False: separate multiply and add."""
     L = lib()
     cptr = np.zeros(A.brow + 1, np.int32)
     bits = _i64()
@@ -275,8 +279,9 @@ def spgemm(A: BSR, B: BSR, prec=DOUBLE):
     sh = None
     if prec != DOUBLE:
         sh = np.zeros(max(nb, 1) * 16, np.float32 if prec == FLOAT else np.uint16)
-    L.orc_spgemm_fill(prec, A.brow, A.bptr, A.bidx, A.bmap, A.bval, B.bcol, B.bptr, B.bidx, B.bmap, B.bval,
-                      cptr, cidx, cmap, cval, None if sh is None else sh.ctypes.data)
+    fill = L.orc_spgemm_fill_fma if contract else L.orc_spgemm_fill
+    fill(prec, A.brow, A.bptr, A.bidx, A.bmap, A.bval, B.bcol, B.bptr, B.bidx, B.bmap, B.bval,
+         cptr, cidx, cmap, cval, None if sh is None else sh.ctypes.data)
     C = BSR(A.m, B.n, cptr, cidx[:nb], cmap[:nb], cval[: nb * 16])
     return C, (None if sh is None else sh[: nb * 16])
 

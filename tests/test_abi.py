@@ -51,9 +51,11 @@ def test_amg_setup_rejects_bad_params_without_a_device():
     A = _lib.AmgtCsr(8, 8, 0, None, None, None)
     h = ctypes.c_void_p()
     for field, bad in (("max_iter", 0), ("max_iter", -3), ("tol", -1.0), ("tol", float("nan")),
-                       ("max_coarse_rows", 0)):
+                       ("max_coarse_rows", 0), ("solver", 2), ("restart", 0), ("restart", 33),
+                       ("inner_prec0", 4), ("inner_tol", -1.0), ("max_outer", 0)):
         p = _lib.AmgtAmgParams()
         L.amgt_amg_default_params(ctypes.byref(p))
+        p.solver = _lib.SOLVER_FGMRES_IR
         setattr(p, field, bad)
         assert L.amgt_amg_setup(ctypes.byref(A), 0, None, ctypes.byref(p), ctypes.byref(h), None) == 1, field
         assert not h.value

@@ -296,3 +296,70 @@ def test_amg_singular_coarsest_is_reported(amgt, orc):
         assert ei.value.status == 1
     finally:
         amgt.set_level_policy([])
+
+
+@pytest.mark.parametrize("kind", ["7pt_40", "varcoef27_28"])
+@pytest.mark.parametrize("mixed", [0, 1])
+def test_fgmres_ir_converges_and_matches_fp64_oracle(amgt, orc, kind, mixed):
+    """FGMRES(30) with iterative refinement: the fp64 residual reaches 1e-8
+    (checked again by the oracle in fp64), and x agrees with the oracle's
+    fp64 AMG-PCG solution of the same system to 1e-6 relative (both stop at
+    a relative residual of 1e-8).  mixed: levels 1-2 fp32, >= 3 fp16, level
+    0 inside the inner solve in fp32 (exact fp16 storage where it holds)."""
+    from amgt_b200 import _lib
+
+    dims = (40, 36, 32) if kind == "7pt_40" else (28, 26, 24)
+    A = orc.laplacian(*dims) if kind == "7pt_40" else orc.varcoef27(*dims, seed=1)
+    Ps = orc.geometric_hierarchy(*dims)
+    b = orc.rand_uniform(0, A.n)
+    xo, it_o, _, _ = orc.Amg(A, Ps).solve(b)
+    amgt.set_level_policy([0, 1, 1, 2] if mixed else [0])
+    try:
+        kw = dict(solver=_lib.SOLVER_FGMRES_IR, inner_prec0=1 if mixed else 0, smooth_prec0=1 if mixed else 0,
+                  galerkin_by_level=mixed)
+        S = _gpu_solver(amgt, A, Ps, **kw)
+        x, it, rel = S.solve(torch.from_numpy(b).cuda())
+        hist = S.history()
+        S.free()
+    finally:
+        amgt.set_level_policy([])
+    assert rel <= 1e-8 and 0 < it <= 40
+    assert hist[-1] == pytest.approx(rel)
+    xg = x.cpu().numpy()
+    assert np.linalg.norm(b - A.to_scipy() @ xg) <= 1.0000001e-8 * np.linalg.norm(b)
+    assert np.linalg.norm(xg - xo) <= 1e-6 * np.linalg.norm(xo)
+
+
+def test_fgmres_ir_graph_and_direct_launches_agree_bit_for_bit(amgt, orc):
+    from amgt_b200 import _lib
+
+    dims = (24, 22, 20)
+    A = orc.varcoef27(*dims, seed=2)
+    Ps = orc.geometric_hierarchy(*dims)
+    b = torch.from_numpy(orc.rand_uniform(3, A.n)).cuda()
+    amgt.set_level_policy([0, 1, 2])
+    try:
+        out = []
+        for g in (1, 0):
+            S = _gpu_solver(amgt, A, Ps, solver=_lib.SOLVER_FGMRES_IR, use_graph=g, inner_prec0=1)
+            for _ in range(2):  # a second solve reuses the built graph
+                x, it, rel = S.solve(b)
+                out.append((x.clone(), it, rel, S.history()))
+            S.free()
+    finally:
+        amgt.set_level_policy([])
+    for x, it, rel, h in out[1:]:
+        assert torch.equal(x, out[0][0]) and it == out[0][1] and rel == out[0][2] and h == out[0][3]
+
+
+def test_fgmres_ir_stops_at_max_iter(amgt, orc):
+    from amgt_b200 import _lib
+
+    dims = (32, 32, 32)
+    A = orc.laplacian(*dims)
+    Ps = orc.geometric_hierarchy(*dims)
+    b = torch.from_numpy(orc.rand_uniform(0, A.n)).cuda()
+    S = _gpu_solver(amgt, A, Ps, solver=_lib.SOLVER_FGMRES_IR, max_iter=3, inner_tol=1e-12)
+    x, it, rel = S.solve(b)
+    S.free()
+    assert it == 3 and rel > 1e-8

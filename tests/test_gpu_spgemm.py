@@ -1,8 +1,10 @@
 """GPU parity: mBSR SpGEMM through the C ABI.
 
 C's block pattern and bitmaps equal the oracle bit for bit; values too, in
-every precision (both sides use the same product order and no fused
-multiply-add); the fused CSR output equals the oracle's mBSR -> CSR.  The
+every precision: fp64 with the reference's arithmetic (each 4x4 product
+entry a k-ordered fused multiply-add chain, products added in A block
+order), fp32 / fp16 / bf16 with separate fp32 multiply and add in the same
+order; the fused CSR output equals the oracle's mBSR -> CSR.  The
 structural nnz of A*A on HYPRE's generators equals the reference's recorded
 known answers."""
 import json
@@ -35,6 +37,11 @@ def _pair(orc, kind):
         S.sort_indices()
         R = orc.CSR(S.shape[0], S.shape[1], S.indptr.astype(np.int32), S.indices.astype(np.int32), S.data.copy())
         return R, AP
+    if kind == "AA_varcoef27":
+        # random coefficients on both sides: the fp64 products round, so
+        # the fused multiply-add chain is visible in the last bits
+        A = orc.varcoef27(14, 12, 11, seed=5)
+        return A, A
     if kind == "AA_5pt":
         A = orc.laplacian(70, 66, 1)
         return A, A
@@ -47,7 +54,7 @@ def _pair(orc, kind):
     raise KeyError(kind)
 
 
-KINDS = ["AP_7pt", "AP_varcoef27", "RAP_varcoef27", "AA_5pt", "AAA_27pt"]
+KINDS = ["AP_7pt", "AP_varcoef27", "RAP_varcoef27", "AA_varcoef27", "AA_5pt", "AAA_27pt"]
 
 
 @pytest.mark.parametrize("kind", KINDS)

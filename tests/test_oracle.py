@@ -189,6 +189,57 @@ def test_spgemm_oracle_matches_scipy(orc):
     np.testing.assert_allclose(Cc.a, S.data, rtol=1e-12, atol=1e-14)
 
 
+def test_spgemm_fma_contraction_follows_the_reference_arithmetic(orc):
+    """The contracted fp64 product (the reference's `temp += a * b`, which
+    nvcc turns into fma) against a hand-written fma chain on a few blocks,
+    and against the uncontracted restatement within 1e-12 of |A| |B|.
+    The 27-point operator's blocks hold 10 or more entries, the ones the
+    reference multiplies with mma.m8n8k4.f64 (csr_spgemm_device.c:1173)."""
+    from fractions import Fraction
+
+    def fma(a, b, c):  # a * b + c exactly, rounded once (Fraction -> float rounds to nearest even)
+        return float(Fraction(a) * Fraction(b) + Fraction(c))
+
+    A = orc.varcoef27(9, 8, 7, seed=4)
+    BA = orc.csr2bsr(A)
+    BP = BA  # A * A: random coefficients, so the products round
+    assert max(bin(int(m)).count("1") for m in BA.bmap) >= 10
+    C1, _ = orc.spgemm(BA, BP)                  # contracted (default)
+    C0, _ = orc.spgemm(BA, BP, contract=False)  # separate multiply and add
+    np.testing.assert_array_equal(C1.bidx, C0.bidx)
+    np.testing.assert_array_equal(C1.bmap, C0.bmap)
+    aa = orc.BSR(BA.m, BA.n, BA.bptr, BA.bidx, BA.bmap, np.abs(BA.bval))
+    ap = orc.BSR(BP.m, BP.n, BP.bptr, BP.bidx, BP.bmap, np.abs(BP.bval))
+    bound, _ = orc.spgemm(aa, ap)
+    assert np.all(np.abs(C1.bval - C0.bval) <= 1e-12 * bound.bval)
+    assert np.any(C1.bval != C0.bval)  # the contraction is visible in the last bits
+    # block row 0 by hand: C(0, J) = sum over A blocks in stored order of
+    # the fma-chained 4x4 products
+    pos = {int(j): t for t, j in enumerate(C1.bidx[C1.bptr[0]:C1.bptr[1]])}
+    acc = np.zeros((len(pos), 16))
+    for p in range(BA.bptr[0], BA.bptr[1]):
+        k, ma = int(BA.bidx[p]), int(BA.bmap[p])
+        a = BA.bval[16 * p:16 * p + 16]
+        for q in range(BP.bptr[k], BP.bptr[k + 1]):
+            mb = int(BP.bmap[q])
+            mc = orc.bitmatmul(ma, mb)
+            if not mc:
+                continue
+            b = BP.bval[16 * q:16 * q + 16]
+            t = pos[int(BP.bidx[q])]
+            for r in range(4):
+                for c in range(4):
+                    if not (mc >> (4 * r + c)) & 1:
+                        continue
+                    s = 0.0
+                    for kk in range(4):
+                        if (ma >> (4 * r + kk)) & 1 and (mb >> (4 * kk + c)) & 1:
+                            s = fma(a[4 * r + kk], b[4 * kk + c], s)
+                    acc[t, 4 * r + c] += s
+    got = C1.bval[:16 * len(pos)].reshape(-1, 16)
+    np.testing.assert_array_equal(got.view(np.uint64), acc.view(np.uint64))
+
+
 def test_transpose_oracle(orc):
     P, _ = orc.interp(9, 7, 6)
     B = orc.csr2bsr(P)
