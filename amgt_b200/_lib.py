@@ -60,6 +60,12 @@ class AmgtPbsr(ctypes.Structure):
                 ("rowVoff", c_void_p), ("val", c_void_p), ("max_blc_per_row", c_int)]
 
 
+class AmgtTuneResult(ctypes.Structure):
+    _fields_ = [("count", c_int), ("candidate", c_int * 8), ("ms", ctypes.c_float * 8), ("choice", c_int)]
+
+
+ENGINE_AUTO, ENGINE_CUDA_CORE, ENGINE_TENSOR_CORE = 0, 1, 2
+
 # name -> (restype, argtypes); every symbol include/amgt_b200.h declares
 SIGNATURES = {
     "amgt_status_string": (ctypes.c_char_p, [c_int]),
@@ -80,6 +86,9 @@ SIGNATURES = {
     "amgt_csr_free": (c_int, [P(AmgtCsr), c_void_p]),
     "amgt_spmv": (c_int, [c_int, c_double, P(AmgtBsr), c_void_p, c_double, c_void_p, c_void_p]),
     "amgt_spmm": (c_int, [c_int, c_double, P(AmgtBsr), c_int, c_void_p, c_int, c_double, c_void_p, c_int, c_void_p]),
+    "amgt_spmm_rm": (c_int, [c_int, c_int, c_double, P(AmgtBsr), c_int, c_void_p, c_double, c_void_p, c_void_p]),
+    "amgt_autotune": (c_int, [P(AmgtBsr), c_int, c_int, P(AmgtTuneResult), c_void_p]),
+    "amgt_autotune_clear": (c_int, []),
     "amgt_bsr_l1_norms": (c_int, [P(AmgtBsr), c_void_p, c_void_p]),
     "amgt_bsr_residual": (c_int, [c_int, P(AmgtBsr), c_void_p, c_void_p, c_void_p, c_void_p]),
     "amgt_bsr_jacobi": (c_int, [c_int, P(AmgtBsr), c_void_p, c_double, c_void_p, c_void_p, c_void_p, c_void_p]),

@@ -119,6 +119,11 @@ int block_row_stats(amgt_bsr *A, cudaStream_t s);
 int spmv_segmented_with_scratch(int prec, double alpha, const amgt_bsr *A, const double *x, double beta, double *y,
                                 double *part, int sm_count, cudaStream_t s);
 
+// Autotuner table (autotune.cu): the SpMV lanes per block row chosen for
+// A (0: none), and dropping A's entries when it is freed.
+int tuned_lpr(const amgt_bsr *A);
+void tune_forget(const amgt_bsr *A);
+
 // y = beta * y (y = 0 when beta == 0) over n entries (spmv.cu).
 int scale_vector(long long n, double beta, double *y, int sm_count, cudaStream_t s);
 

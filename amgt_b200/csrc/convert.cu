@@ -900,6 +900,7 @@ int amgt_bsr_free(amgt_bsr *A, amgt_stream_t stream)
 {
     if (!A) return AMGT_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
+    tune_forget(A);
     free_ptr(A->blcPtr, s);
     free_ptr(A->blcIdx, s);
     free_ptr(A->blcVal, s);

@@ -348,8 +348,8 @@ static int storage_mode(const amgt_bsr *A, int prec)
 }
 
 
-// Lanes per block row from the mean block-row length (overridable with
-// AMGT_SPMV_LPR for tuning runs).
+// Lanes per block row: amgt_autotune's choice for this matrix when it has
+// one, else from the mean block-row length (AMGT_SPMV_LPR overrides both).
 static int pick_lpr(const amgt_bsr *A, int mode)
 {
     // the choice depends on the structure only: with the same segment length
@@ -361,6 +361,8 @@ static int pick_lpr(const amgt_bsr *A, int mode)
         env = e ? atoi(e) : 0;
     }
     if (env == 4 || env == 8 || env == 16 || env == 32) return env;
+    const int tuned = tuned_lpr(A);  // amgt_autotune's measured choice for this matrix
+    if (tuned) return tuned;
     const double avg = A->blc_row ? (double)A->blc_num / A->blc_row : 0.0;
     if (avg <= 4.0) return 4;    // interpolation 128^3 (3.3): 4 beat 8 for 8- and 2-byte values
     if (avg <= 10.0) return 8;   // 7-point 128^3 (6.9): 8 beat 4 and 16 for 8-byte values

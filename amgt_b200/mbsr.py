@@ -175,6 +175,31 @@ class Bsr:
         return Y
 
 
+    def spmm_rm(self, X: torch.Tensor, Y: torch.Tensor | None = None, alpha: float = 1.0, beta: float = 0.0,
+                prec: int = DOUBLE, engine: int = 0, stream=None) -> torch.Tensor:
+        """Row-major multivectors: X (ncols, nvec), Y (nrows, nvec), float64
+        contiguous, nvec <= 32 (amgt_spmm_rm; engine 0 auto, 1 CUDA cores,
+        2 tensor cores)."""
+        nvec = X.shape[1]
+        if Y is None:
+            Y = torch.zeros(self.s.row, nvec, dtype=torch.float64, device="cuda")
+            beta = 0.0
+        for T, rows in ((X, self.s.col), (Y, self.s.row)):
+            if not (T.is_cuda and T.dtype == torch.float64 and T.is_contiguous() and T.shape == (rows, nvec)):
+                raise TypeError("X, Y must be contiguous (rows, nvec) float64 CUDA tensors")
+        check(L.lib().amgt_spmm_rm(prec, engine, alpha, ctypes.byref(self.s), nvec, X.data_ptr(), beta,
+                                   Y.data_ptr(), _stream(stream)), "amgt_spmm_rm")
+        return Y
+
+    def autotune(self, prec: int = DOUBLE, nvec: int = 1, stream=None) -> dict:
+        """amgt_autotune: times the launch shapes on this matrix and keeps
+        the fastest; returns {candidate code: ms} and the choice."""
+        r = L.AmgtTuneResult()
+        check(L.lib().amgt_autotune(ctypes.byref(self.s), prec, nvec, ctypes.byref(r), _stream(stream)),
+              "amgt_autotune")
+        return {"choice": r.choice, "ms": {int(r.candidate[i]): float(r.ms[i]) for i in range(r.count)}}
+
+
 class PackedBsr:
     """amgt_pbsr: mBSR with only the set bits' values stored."""
 

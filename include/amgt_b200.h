@@ -222,6 +222,48 @@ AMGT_API int amgt_spmm(int prec, double alpha, const amgt_bsr *A, int nvec,
               const double *x, int ldx, double beta, double *y, int ldy,
               amgt_stream_t stream);
 
+/* Row-major multivector SpMM for the batching form (many right-hand sides
+ * at once): Y[i*nvec + v] <- alpha * (A X)[i][v] + beta * Y[i*nvec + v],
+ * X[j*nvec + v], 1 <= nvec <= 32, X and Y fp64.  The reference's matvec
+ * hook ignores num_vectors (R/seq_mv/csr_matvec_device.c:2409-2437); its
+ * multivector storage is column-wise (:139-170), this one interleaves the
+ * vectors so that a block column's x rows are contiguous.
+ * prec FLOAT / HALF / BF16 on the tensor cores (engine TENSOR_CORE): two
+ * block rows per mma.m16n8k8 (tf32 in, fp32 accumulate), values and x split
+ * into tf32 high and low parts so that the products carry fp32 accuracy;
+ * the result is combined with beta * Y in fp64 (so Y = B, alpha = -1,
+ * beta = 1 gives an fp64 residual of products computed on the tensor
+ * cores).  prec DOUBLE: fp64 on the CUDA cores.  engine CUDA_CORE: a warp
+ * per block row, a lane per right-hand side.  engine AUTO: amgt_autotune's
+ * choice for (A, prec, nvec), else the tensor cores with 8 warps per CTA.
+ * An fp32 request on a matrix whose exact fp16 shadow holds every value
+ * reads that shadow.  Never blocks the host. */
+#define AMGT_ENGINE_AUTO 0
+#define AMGT_ENGINE_CUDA_CORE 1
+#define AMGT_ENGINE_TENSOR_CORE 2
+AMGT_API int amgt_spmm_rm(int prec, int engine, double alpha, const amgt_bsr *A, int nvec, const double *X,
+                          double beta, double *Y, amgt_stream_t stream);
+
+/* Autotuner (no reference counterpart: the reference's launch shape is
+ * fixed, WARP_NUM_SPMV = 4, R/seq_mv/seq_mv.h:84-99).  Times every
+ * candidate launch shape on A (3 warm-up + 10 timed launches each, CUDA
+ * events on `stream`; blocks the host) and keeps the fastest for A:
+ *   nvec == 1: lanes per block row of amgt_spmv and the fused forms,
+ *              candidates 4, 8, 16, 32 (the choice changes the order of a
+ *              row's sums, not its terms);
+ *   nvec > 1:  amgt_spmm_rm's engine and warps per CTA, candidate code
+ *              10 * engine + warps (engine 0 CUDA cores, 1 tensor cores).
+ * The choice is dropped when A is freed (amgt_bsr_free) or by
+ * amgt_autotune_clear. */
+typedef struct {
+    int count;          /* candidates timed                 */
+    int candidate[8];   /* their codes                       */
+    float ms[8];        /* mean time per launch              */
+    int choice;         /* the fastest code, now in use      */
+} amgt_tune_result;
+AMGT_API int amgt_autotune(const amgt_bsr *A, int prec, int nvec, amgt_tune_result *out, amgt_stream_t stream);
+AMGT_API int amgt_autotune_clear(void);
+
 /* ------------------------------------------------ smoother / residual */
 /* l1 row norms l1[i] = sum_j |a_ij| of the fp64 values: the norms HYPRE's
  * l1-Jacobi (relax 18) divides by, hypre_ParCSRComputeL1Norms option 1
