@@ -102,6 +102,10 @@ SIGNATURES = {
     "amgt_amg_default_params": (None, [P(AmgtAmgParams)]),
     "amgt_amg_setup": (c_int, [P(AmgtCsr), c_int, P(AmgtCsr), P(AmgtAmgParams), P(c_void_p), c_void_p]),
     "amgt_amg_solve": (c_int, [c_void_p, c_void_p, c_void_p, P(c_int), P(c_double), c_void_p]),
+    "amgt_amg_solve_multi": (c_int, [c_void_p, c_int, c_void_p, c_void_p, P(c_int), P(c_double), c_void_p]),
+    "amgt_batch_setup": (c_int, [c_int, P(AmgtCsr), P(c_int), P(AmgtCsr), P(AmgtAmgParams), P(c_void_p), c_void_p]),
+    "amgt_amg_solve_batch": (c_int, [c_void_p, c_void_p, c_void_p, P(c_int), P(c_double), P(c_int), c_void_p]),
+    "amgt_batch_offsets": (c_int, [c_void_p, P(c_int), c_int]),
     "amgt_amg_num_levels": (c_int, [c_void_p]),
     "amgt_amg_level": (c_int, [c_void_p, c_int, P(AmgtBsr), P(c_int)]),
     "amgt_amg_setup_times": (c_int, [c_void_p, P(c_double)]),

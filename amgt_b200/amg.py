@@ -56,6 +56,22 @@ class AmgSolver:
                                      _stream(stream)), "amgt_amg_solve")
         return x, it.value, rel.value
 
+    def solve_multi(self, B: torch.Tensor, X: torch.Tensor | None = None, stream=None):
+        """Solves A X = B for the columns of B, (n, nrhs) row-major float64,
+        nrhs <= 32, all at once (amgt_amg_solve_multi); returns (X,
+        iterations per column, relative residual per column)."""
+        n, nv = B.shape
+        if X is None:
+            X = torch.zeros_like(B)
+        for T in (B, X):
+            if not (T.is_cuda and T.dtype == torch.float64 and T.is_contiguous() and T.shape == (self.n, nv)):
+                raise TypeError("B and X must be contiguous (n, nrhs) float64 CUDA tensors")
+        its = (ctypes.c_int * nv)()
+        rel = (ctypes.c_double * nv)()
+        check(L.lib().amgt_amg_solve_multi(self.h, nv, B.data_ptr(), X.data_ptr(), its, rel, _stream(stream)),
+              "amgt_amg_solve_multi")
+        return X, list(its), list(rel)
+
     def num_levels(self) -> int:
         return L.lib().amgt_amg_num_levels(self.h)
 
@@ -87,3 +103,45 @@ class AmgSolver:
             self.free()
         except Exception:
             pass
+
+
+class BatchSolver(AmgSolver):
+    """Independent systems of uneven size, solved at once: systems = [(A,
+    [P_0, ...]), ...] with device CSR tuples (amgt_batch_setup)."""
+
+    def __init__(self, systems, params: AmgtAmgParams | None = None, stream=None):
+        self._keep = [A for A, _ in systems] + [P for _, Ps in systems for P in Ps]
+        ns = len(systems)
+        A_arr = (L.AmgtCsr * ns)()
+        nlev = (ctypes.c_int * ns)()
+        flat = [P for _, Ps in systems for P in Ps]
+        P_arr = (L.AmgtCsr * max(1, len(flat)))()
+        for i, (A, Ps) in enumerate(systems):
+            A_arr[i] = csr_struct(*A)
+            nlev[i] = len(Ps)
+        for i, P in enumerate(flat):
+            P_arr[i] = csr_struct(*P)
+        self.params = params if params is not None else default_params()
+        self.h = ctypes.c_void_p()
+        check(L.lib().amgt_batch_setup(ns, A_arr, nlev, P_arr, ctypes.byref(self.params), ctypes.byref(self.h),
+                                       _stream(stream)), "amgt_batch_setup")
+        offs = (ctypes.c_int * (ns + 1))()
+        L.lib().amgt_batch_offsets(self.h, offs, ns + 1)
+        self.offsets = list(offs)
+        self.nsys = ns
+        self.n = self.offsets[-1]
+
+    def solve_batch(self, b: torch.Tensor, x: torch.Tensor | None = None, stream=None):
+        """b, x: concatenated float64 CUDA vectors; returns (x, iterations
+        per system, relative residual per system, loop iterations)."""
+        if x is None:
+            x = torch.zeros_like(b)
+        for v in (b, x):
+            if not (v.is_cuda and v.dtype == torch.float64 and v.is_contiguous() and v.numel() == self.n):
+                raise TypeError("b and x must be contiguous float64 CUDA vectors of the batch's size")
+        its = (ctypes.c_int * self.nsys)()
+        rel = (ctypes.c_double * self.nsys)()
+        bit = ctypes.c_int()
+        check(L.lib().amgt_amg_solve_batch(self.h, b.data_ptr(), x.data_ptr(), its, rel, ctypes.byref(bit),
+                                           _stream(stream)), "amgt_amg_solve_batch")
+        return x, list(its), list(rel), bit.value

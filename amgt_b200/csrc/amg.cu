@@ -29,12 +29,9 @@
 #include <cstring>
 #include <vector>
 
-#include "amgt_internal.cuh"
+#include "amg_handle.cuh"
 
 namespace amgt {
-
-constexpr int kDotGrid = 1184;  // 8 x 148 SMs
-constexpr int kDotThreads = 256;
 
 enum { S_BB = 0, S_RR = 1, S_RZ = 2, S_PQ = 3, S_ALPHA = 4, S_BETA = 5, S_ZRPREV = 6, S_NSCAL = 8 };
 enum { OP_STORE = 0, OP_ALPHA = 1, OP_BETA = 2, OP_BETA_FLEX = 3 };
@@ -133,31 +130,42 @@ __global__ void jacobi_zero_kernel(long long n, const double *__restrict__ f, co
         u[i] = w * f[i] * inv_l1[i];
 }
 
-// u = M f with M dense (row-major, nc x nc), one warp per row
-__global__ void dense_mv_kernel(int nc, const double *__restrict__ M, const double *__restrict__ f,
-                                double *__restrict__ u)
+// u = M f with M the coarsest inverse: dense diagonal blocks, block b
+// rows cb_off[b] .. cb_off[b+1]-1, row-major at M + cb_doff[b] (one block
+// for a single system); one warp per row
+__global__ void dense_mv_kernel(int nc, const int *__restrict__ row_blk, const int *__restrict__ cb_off,
+                                const long long *__restrict__ cb_doff, const double *__restrict__ M,
+                                const double *__restrict__ f, double *__restrict__ u)
 {
     grid_dependency_wait();
     const int lane = threadIdx.x & 31;
     for (int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < nc; row += (gridDim.x * blockDim.x) >> 5) {
+        const int b = row_blk[row], o = cb_off[b], nb = cb_off[b + 1] - o;
+        const double *Mr = M + cb_doff[b] + (long long)(row - o) * nb;
         double s = 0.0;
-        for (int j = lane; j < nc; j += 32) s += M[(long long)row * nc + j] * f[j];
+        for (int j = lane; j < nb; j += 32) s += Mr[j] * f[o + j];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(FULL, s, o);
+        for (int o2 = 16; o2 > 0; o2 >>= 1) s += __shfl_xor_sync(FULL, s, o2);
         if (lane == 0) u[row] = s;
     }
 }
 
-// mBSR -> dense (row-major), for the coarsest operator
+// mBSR -> dense diagonal blocks (row-major per block, as dense_mv_kernel
+// reads them); entries outside a row's block are not stored (the
+// operator is block-diagonal when there are several blocks)
 __global__ void bsr_to_dense_kernel(int m, int n, const int *__restrict__ ptr, const int *__restrict__ idx,
-                                    const double *__restrict__ val, double *__restrict__ D)
+                                    const double *__restrict__ val, const int *__restrict__ row_blk,
+                                    const int *__restrict__ cb_off, const long long *__restrict__ cb_doff,
+                                    double *__restrict__ D)
 {
     for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < m; row += gridDim.x * blockDim.x) {
         const int b = row >> 2, q = row & 3;
+        const int rb = row_blk[row], o = cb_off[rb], nb = cb_off[rb + 1] - o;
+        double *Dr = D + cb_doff[rb] + (long long)(row - o) * nb;
         for (int k = ptr[b]; k < ptr[b + 1]; ++k)
             for (int c = 0; c < 4; ++c) {
                 const int col = 4 * idx[k] + c;
-                if (col < n) D[(long long)row * n + col] = val[16LL * k + 4 * q + c];
+                if (col < n && col >= o && col < o + nb) Dr[col - o] = val[16LL * k + 4 * q + c];
             }
     }
 }
@@ -294,6 +302,39 @@ __global__ void gj_gather_kernel(int nc, const double *__restrict__ T, const int
          e += (long long)gridDim.x * blockDim.x) {
         const int c = (int)(e / nc), k = (int)(e % nc);
         inv[(long long)c * nc + piv[k]] = T[(long long)piv[c] * nc + k];
+    }
+}
+
+// Several diagonal blocks (a batch of systems): one CTA inverts each block
+// in place with the same steps as gj_small_kernel, then gathers it.
+__global__ void __launch_bounds__(1024) gj_blocks_kernel(const int *__restrict__ cb_off,
+                                                        const long long *__restrict__ cb_doff, double *__restrict__ T,
+                                                        double *__restrict__ inv, int *__restrict__ used,
+                                                        int *__restrict__ piv, double *__restrict__ rowp,
+                                                        double *__restrict__ colc, int *__restrict__ bad)
+{
+    __shared__ double sval[1024];
+    __shared__ int sidx[1024];
+    const int o = cb_off[blockIdx.x], nb = cb_off[blockIdx.x + 1] - o;
+    double *Tb = T + cb_doff[blockIdx.x], *Ib = inv + cb_doff[blockIdx.x];
+    int *ub = used + o, *pb = piv + o;
+    double *rb = rowp + o, *cb = colc + o;
+    for (int r = threadIdx.x; r < nb; r += blockDim.x) ub[r] = 0;
+    __syncthreads();
+    for (int c = 0; c < nb; ++c) {
+        gj_pivot_phase(nb, c, Tb, ub, pb, rb, cb, bad, sval, sidx);
+        __syncthreads();
+        const int p = pb[c];
+        const double a = gj_pivot_value(c, rb);
+        for (long long e = threadIdx.x; e < (long long)nb * nb; e += blockDim.x) {
+            const int r = (int)(e / nb), k = (int)(e % nb);
+            Tb[e] = gj_update(Tb[e], r, k, p, c, a, rb, cb);
+        }
+        __syncthreads();
+    }
+    for (long long e = threadIdx.x; e < (long long)nb * nb; e += blockDim.x) {
+        const int c = (int)(e / nb), k = (int)(e % nb);
+        Ib[(long long)c * nb + pb[k]] = Tb[(long long)pb[c] * nb + k];
     }
 }
 
@@ -580,54 +621,7 @@ __global__ void gm_update_kernel(long long n, const float *__restrict__ Z, const
     }
 }
 
-struct Level {
-    amgt_bsr A{}, P{}, R{};
-    amgt_pbsr pA{}, pAs{}, pP{}, pR{};  // packed: cycle operator, level-0 smoother, transfers
-    double *inv_l1 = nullptr;
-    double *f = nullptr, *u = nullptr, *t = nullptr, *s = nullptr;
-    int n = 0;
-    int prec = AMGT_DOUBLE;           // smoother SpMVs on A_l
-    int prec_transfer = AMGT_DOUBLE;  // R_l / P_l SpMVs
-};
-
 }  // namespace amgt
-
-// Opaque handle of the C ABI.
-struct amgt_amg {
-    std::vector<amgt::Level> lv;
-    amgt_amg_params prm;
-    double *coarse_inv = nullptr;
-    int nc = 0;
-    long long n0 = 0;
-    double *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
-    double *scal = nullptr, *part = nullptr;
-    double *pinned = nullptr;  // host: ||r||^2 read-back
-    int sm_count = 0, grid0 = 0;
-    cudaGraphExec_t graph = nullptr;
-    cudaStream_t graph_stream = nullptr;
-    const double *graph_b = nullptr;
-    double *graph_xout = nullptr;
-    // the whole iteration loop as one graph (a conditional while node); the
-    // loop's iteration count and ||r||^2 per iteration stay on the device
-    cudaGraphExec_t loop = nullptr;
-    double *loop_xout = nullptr;
-    bool loop_failed = false;
-    int *loop_it = nullptr;     // device: iterations done
-    double *loop_rr = nullptr;  // device: ||r||^2 after iteration k, k = 1 .. max_iter
-    double *loop_pinned = nullptr;
-    uint64_t graph_launches = 0, loop_launches = 0;  // our kernels per iteration in each graph
-    double setup_ms[5] = {0, 0, 0, 0, 0};
-    std::vector<double> hist;
-    // FGMRES with iterative refinement (solver = AMGT_SOLVER_FGMRES_IR)
-    int resid_prec0 = AMGT_DOUBLE;  // the cycle's level-0 residual precision
-    float *gmV = nullptr, *gmZ = nullptr;  // basis (m + 1 vectors), preconditioned vectors (m)
-    double *gm = nullptr;                  // Hessenberg, rotations, g, y, slots (GmLayout)
-    double *gm_vin = nullptr, *gm_zout = nullptr, *gm_w = nullptr, *gm_part = nullptr;
-    int *gm_j = nullptr;                   // device: inner iteration index
-    cudaGraphExec_t gm_loop = nullptr;
-    bool gm_loop_failed = false;
-    uint64_t gm_loop_launches = 0;
-};
 
 using namespace amgt;
 
@@ -663,12 +657,17 @@ void destroy_handle(amgt_amg *h, cudaStream_t s)
     free_ptr(h->gm_w, s);
     free_ptr(h->gm_part, s);
     free_ptr(h->gm_j, s);
+    if (h->mr) free_multi_rhs(h->mr, s);
+    if (h->batch) free_batch(h->batch, s);
     if (h->graph_stream) cudaStreamDestroy(h->graph_stream);
     free_ptr(h->loop_it, s);
     free_ptr(h->loop_rr, s);
     if (h->loop_pinned) cudaFreeHost(h->loop_pinned);
     for (auto &v : h->lv) free_level(v, s);
     free_ptr(h->coarse_inv, s);
+    free_ptr(h->cb_off, s);
+    free_ptr(h->cb_doff, s);
+    free_ptr(h->row_blk, s);
     free_ptr(h->r, s);
     free_ptr(h->z, s);
     free_ptr(h->p, s);
@@ -802,7 +801,8 @@ int cycle(amgt_amg *h, const double *rhs0, double *out0, cudaStream_t s)
     Level &c = lv[L - 1];
     const double *fc = (L == 1) ? rhs0 : c.f;
     double *uc = (L == 1) ? out0 : c.s;
-    AMGT_LAUNCH_PDL(dense_mv_kernel, grid_for(8, c.n, h->sm_count, 8), 256, 0, s, c.n, h->coarse_inv, fc, uc);
+    AMGT_LAUNCH_PDL(dense_mv_kernel, grid_for(8, c.n, h->sm_count, 8), 256, 0, s, c.n, (const int *)h->row_blk,
+                    (const int *)h->cb_off, (const long long *)h->cb_doff, (const double *)h->coarse_inv, fc, uc);
     for (int l = L - 2; l >= 0; --l) {
         Level &v = lv[l];
         const double *f = (l == 0) ? rhs0 : v.f;
@@ -1082,6 +1082,8 @@ int fgmres_ir_solve(amgt_amg *h, const double *b, double *x, int *iterations, do
 
 }  // namespace
 
+int amgt::amg_cycle(amgt_amg *h, const double *rhs0, double *out0, cudaStream_t s) { return cycle(h, rhs0, out0, s); }
+
 extern "C" {
 
 void amgt_amg_default_params(amgt_amg_params *p)
@@ -1108,6 +1110,14 @@ void amgt_amg_default_params(amgt_amg_params *p)
 
 int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const amgt_amg_params *params,
                    amgt_amg **out, amgt_stream_t stream)
+{
+    return amgt::amg_setup_blocks(A, num_interp, P, params, out, stream, nullptr);
+}
+
+}  // extern "C"
+
+int amgt::amg_setup_blocks(const amgt_csr *A, int num_interp, const amgt_csr *P, const amgt_amg_params *params,
+                           amgt_amg **out, amgt_stream_t stream, const std::vector<std::vector<int>> *sys_rows)
 {
     if (!A || !out || num_interp < 0 || (num_interp > 0 && !P) || A->num_rows != A->num_cols || A->num_rows <= 0)
         return AMGT_ERR_INVALID;
@@ -1239,28 +1249,73 @@ int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const a
         pm.mark(2, s);
     }
     h->lv[L - 1].prec = amgt_precision_for_level(L - 1);
-    // coarsest: dense form and its inverse, on the GPU (Gauss-Jordan); the
-    // singularity flag is read back with the exactness bits below
+    // coarsest: dense diagonal blocks (one, or one per system of a batch)
+    // and their inverses, on the GPU (Gauss-Jordan); the singularity flag is
+    // read back with the exactness bits below
     h->nc = h->lv[L - 1].n;
     if (h->nc > h->prm.max_coarse_rows) {
         rc = AMGT_ERR_TOO_LARGE;
         goto fail;
     }
     {
-        const size_t nn = (size_t)h->nc * h->nc;
-        if ((rc = alloc_n(&dense, nn, s)) || (rc = alloc_n(&h->coarse_inv, nn, s))) goto fail;
-        if (cudaMemsetAsync(dense, 0, sizeof(double) * nn, s) != cudaSuccess ||
+        std::vector<int> boff{0};
+        if (sys_rows)
+            for (const auto &r : *sys_rows) boff.push_back(boff.back() + r[L - 1]);
+        else
+            boff.push_back(h->nc);
+        if (boff.back() != h->nc) {
+            rc = AMGT_ERR_INVALID;
+            goto fail;
+        }
+        const int nb = (int)boff.size() - 1;
+        std::vector<long long> doff{0};
+        std::vector<int> rblk(h->nc);
+        for (int b = 0; b < nb; ++b) {
+            const long long w = boff[b + 1] - boff[b];
+            doff.push_back(doff.back() + w * w);
+            for (int r = boff[b]; r < boff[b + 1]; ++r) rblk[r] = b;
+        }
+        const size_t nn = (size_t)doff.back();
+        int *bad = reinterpret_cast<int *>(xflags + 3 * num_interp + 2);
+        h->ncb = nb;
+        if ((rc = alloc_n(&dense, nn, s)) || (rc = alloc_n(&h->coarse_inv, nn, s)) ||
+            (rc = alloc_n(&h->cb_off, (size_t)nb + 1, s)) || (rc = alloc_n(&h->cb_doff, (size_t)nb + 1, s)) ||
+            (rc = alloc_n(&h->row_blk, (size_t)h->nc, s)))
+            goto fail;
+        if (cudaMemcpyAsync(h->cb_off, boff.data(), sizeof(int) * boff.size(), cudaMemcpyHostToDevice, s) !=
+                cudaSuccess ||
+            cudaMemcpyAsync(h->cb_doff, doff.data(), sizeof(long long) * doff.size(), cudaMemcpyHostToDevice, s) !=
+                cudaSuccess ||
+            cudaMemcpyAsync(h->row_blk, rblk.data(), sizeof(int) * rblk.size(), cudaMemcpyHostToDevice, s) !=
+                cudaSuccess ||
+            cudaMemsetAsync(dense, 0, sizeof(double) * nn, s) != cudaSuccess ||
             cudaMemsetAsync(xflags + 3 * num_interp + 2, 0, sizeof(int64_t), s) != cudaSuccess) {
             rc = AMGT_ERR_CUDA;
             goto fail;
         }
         AMGT_LAUNCH(bsr_to_dense_kernel, grid_for(256, h->nc, h->sm_count, 8), 256, 0, s, h->nc, h->nc,
-                    h->lv[L - 1].A.blcPtr, h->lv[L - 1].A.blcIdx, h->lv[L - 1].A.blcVal, dense);
+                    h->lv[L - 1].A.blcPtr, h->lv[L - 1].A.blcIdx, h->lv[L - 1].A.blcVal, (const int *)h->row_blk,
+                    (const int *)h->cb_off, (const long long *)h->cb_doff, dense);
         // the flag slot after the last operator's (never a P or R slot: the
         // coarsest level has none) holds the singular mark
-        if ((rc = dense_invert(h->nc, dense, h->coarse_inv, reinterpret_cast<int *>(xflags + 3 * num_interp + 2),
-                               h->sm_count, s)))
-            goto fail;
+        if (nb == 1) {
+            if ((rc = dense_invert(h->nc, dense, h->coarse_inv, bad, h->sm_count, s))) goto fail;
+        } else {
+            int *used = nullptr, *piv = nullptr;
+            double *rowp = nullptr, *colc = nullptr;
+            if (!(rc = alloc_n(&used, h->nc, s)) && !(rc = alloc_n(&piv, h->nc, s)) &&
+                !(rc = alloc_n(&rowp, h->nc, s)) && !(rc = alloc_n(&colc, h->nc, s))) {
+                count_launch();
+                gj_blocks_kernel<<<nb, 1024, 0, s>>>(h->cb_off, h->cb_doff, dense, h->coarse_inv, used, piv, rowp,
+                                                     colc, bad);
+                if (cudaGetLastError() != cudaSuccess) rc = AMGT_ERR_CUDA;
+            }
+            free_ptr(used, s);
+            free_ptr(piv, s);
+            free_ptr(rowp, s);
+            free_ptr(colc, s);
+            if (rc) goto fail;
+        }
         free_ptr(dense, s);
     }
     // exact narrow storage of the operators used in fp64 (level 0, fp64
@@ -1386,6 +1441,8 @@ fail:
     destroy_handle(h, s);
     return rc;
 }
+
+extern "C" {
 
 int amgt_amg_solve(amgt_amg *h, const double *b, double *x, int *iterations, double *rel_res, amgt_stream_t stream)
 {

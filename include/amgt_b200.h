@@ -419,6 +419,43 @@ AMGT_API int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P
  * FGMRES iterations, *rel_res is the last fp64 residual ||b - A x|| / ||b||. */
 AMGT_API int amgt_amg_solve(amgt_amg *amg, const double *b, double *x,
                             int *iterations, double *rel_res, amgt_stream_t stream);
+/* Many right-hand sides at once on the same hierarchy (the batching form):
+ * B and X row-major n x nrhs (x_i of right-hand side v at X[i*nrhs + v]),
+ * 1 <= nrhs <= 32; X holds the initial guesses and receives the solutions.
+ * Refinement in fp64 (R = B - A X with fp64 values; X += D) around a
+ * correction A D = R solved by PCG in lockstep over the columns, each with
+ * its own scalars and its own stop (inner_tol * ||R_v||), preconditioned by
+ * one V(1,1) cycle whose every operator is one amgt_spmm_rm over all
+ * columns at its level's precision (reduced-precision levels on the tensor
+ * cores; level 0 inside the correction at inner_prec0).  Each correction is
+ * one CUDA graph launch.  Stops when every column reaches tol, or after
+ * max_iter correction iterations in total, or max_outer refinements.
+ * iterations[v]: correction iterations column v took; rel_res[v]: its
+ * final ||B_v - A X_v|| / ||B_v|| in fp64 (both arrays may be NULL). */
+AMGT_API int amgt_amg_solve_multi(amgt_amg *amg, int nrhs, const double *B, double *X, int *iterations,
+                                  double *rel_res, amgt_stream_t stream);
+/* A batch of independent systems of uneven size solved at once (the
+ * batching form; no reference counterpart: HYPRE solves one system per
+ * call).  A[s] (square, device CSR) and its interpolations P[s][0 ..
+ * nlev[s] - 1], given flattened system after system in P, are concatenated
+ * block-diagonally level by level (a system with fewer levels continues
+ * with identity blocks, which leave its coarse operator unchanged), and
+ * one hierarchy is set up for the concatenation (as amgt_amg_setup, with
+ * its params).  Systems are rows offsets[s] .. offsets[s + 1] - 1 of the
+ * concatenated vectors (amgt_batch_offsets). */
+AMGT_API int amgt_batch_setup(int nsys, const amgt_csr *A, const int *nlev, const amgt_csr *P,
+                              const amgt_amg_params *params, amgt_amg **out, amgt_stream_t stream);
+/* One PCG per system in lockstep (each its own scalars; a system stops at
+ * ||b_s - A_s x_s|| / ||b_s|| <= tol), preconditioned by one V(1,1) cycle
+ * of the block-diagonal hierarchy, the whole iteration loop one CUDA graph
+ * launch.  b, x: concatenated device vectors (x: initial guess in, solution
+ * out).  iterations[s], rel_res[s] (fp64 residual of the returned x_s):
+ * arrays of nsys, or NULL; *batch_iterations: the loop's iterations. */
+AMGT_API int amgt_amg_solve_batch(amgt_amg *amg, const double *b, double *x, int *iterations, double *rel_res,
+                                  int *batch_iterations, amgt_stream_t stream);
+/* offsets[0 .. nsys] (cap entries at most); returns nsys, or -1 when amg
+ * was not built by amgt_batch_setup. */
+AMGT_API int amgt_batch_offsets(const amgt_amg *amg, int *offsets, int cap);
 AMGT_API int amgt_amg_num_levels(const amgt_amg *amg);
 /* Borrowed view of level `level`'s operator and its cycle precision. */
 AMGT_API int amgt_amg_level(const amgt_amg *amg, int level, amgt_bsr *A_view, int *prec);
