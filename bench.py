@@ -339,6 +339,135 @@ def amg_e2e(amgt, torch, A_host, Ps_host, b_host, policy, smooth0, flexible):
             "d2h_bytes": int(xh.numel() * 8)}
 
 
+def spmm_bytes(nblk: int, brow: int, m: int, n: int, nvec: int, val_bytes: int, beta: bool = False) -> int:
+    """Algorithmic bytes of one row-major SpMM: block values + block columns
+    + block-row pointers + X once + Y written (+ Y read when beta != 0)."""
+    return nblk * (16 * val_bytes + 4) + 4 * (brow + 1) + 8 * n * nvec + 8 * m * nvec * (2 if beta else 1)
+
+
+def batching_report(amgt, torch, problems, stream):
+    """The batching form: (a) 7-point 64^3 with 32 right-hand sides
+    (amgt_amg_solve_multi: every cycle operator one SpMM over all columns;
+    the 32-vector SpMM timed alone, with the autotuner's choice) against 32
+    single-right-hand-side solves; (b) 64 2D 5-point systems with sides
+    uniform in [32, 512] (seed 0) in one graph launch (amgt_batch_setup +
+    amgt_amg_solve_batch) against 64 solves one after another."""
+    from amgt_b200.amg import AmgSolver, BatchSolver, default_params
+
+    out = {}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dims = (64, 64, 64)
+    m, n, ia, ja, a = problems.laplacian(*dims)
+    dA = (m, n) + tuple(torch.from_numpy(v).cuda() for v in (ia, ja, a))
+    Ps = geometric_interps(problems, dims)
+    dPs = [(P[0], P[1]) + tuple(torch.from_numpy(v).cuda() for v in P[2:]) for P in Ps]
+    nv = 32
+    B = torch.from_numpy(np.ascontiguousarray(np.stack([problems.rand_uniform(v, n) for v in range(nv)], axis=1))).cuda()
+    # the SpMM alone: fp32-requested values (the exact fp16 shadow) on the tensor cores vs CUDA cores
+    G = amgt.Bsr.from_csr(*dA)
+    G.make_exact()
+    tune = G.autotune(prec=1, nvec=nv)
+    X = torch.rand(n, nv, dtype=torch.float64, device="cuda")
+    Y = torch.zeros(m, nv, dtype=torch.float64, device="cuda")
+    vb = 2 if G.s.exact_prec == 2 else 4
+    nbytes = spmm_bytes(G.nblk, G.s.blc_row, m, n, nv, vb)
+    spmm = {"workload": f"7-point {dims[0]}^3, {nv} right-hand sides, fp32 values read from the exact fp16 shadow",
+            "bytes_per_call": nbytes, "autotune_ms": {str(k): round(v, 5) for k, v in tune["ms"].items()},
+            "autotune_choice": tune["choice"], "choice_code": "10 * engine (0 CUDA cores, 1 tensor cores) + warps/CTA"}
+    for name, eng in (("tensor_cores", 2), ("cuda_cores", 1), ("autotuned", 0)):
+        for _ in range(3):
+            G.spmm_rm(X, Y, prec=1, engine=eng)
+        ev0.record(stream)
+        for _ in range(20):
+            G.spmm_rm(X, Y, prec=1, engine=eng)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / 20
+        spmm[name] = {"ms": round(ms, 5), "gbs": round(nbytes / (ms * 1e-3) / 1e9, 1)}
+    peak, _ = read_peaks()
+    spmm["roofline"] = {"bound": "hbm", "achieved": spmm["autotuned"]["gbs"], "peak": peak, "unit": "GB/s",
+                        "frac": round(spmm["autotuned"]["gbs"] / peak, 4)}
+    out["spmm_64cubed_32rhs"] = spmm
+    del G, X, Y
+    # (a) the multi-right-hand-side solve, mixed: levels 1-2 fp32, >= 3 fp16,
+    # level 0 in the correction fp32; fp64 refinement
+    amgt.set_level_policy(MIXED_POLICY)
+    prm = default_params(inner_prec0=1, galerkin_by_level=1)
+    S = AmgSolver(dA, dPs, prm)
+    S.solve_multi(B)  # warm-up (builds the vectors and the loop graph)
+    S.free()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    S = AmgSolver(dA, dPs, prm)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    Xs, its, rel = S.solve_multi(B)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    S.free()
+    amgt.set_level_policy([])
+    multi = {"setup_s": round(t1 - t0, 5), "solve_s": round(t2 - t1, 5), "iters_per_column": [min(its), max(its)],
+             "max_rel_res": max(rel)}
+    # the same 32 right-hand sides one at a time (plain fp64 PCG, one graph launch each)
+    amgt.set_level_policy([0])
+    S = AmgSolver(dA, dPs, default_params())
+    b0 = B[:, 0].contiguous()
+    S.solve(b0)
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
+    for v in range(nv):
+        S.solve(B[:, v].contiguous())
+    torch.cuda.synchronize()
+    t4 = time.perf_counter()
+    S.free()
+    amgt.set_level_policy([])
+    multi["one_at_a_time_fp64_solve_s"] = round(t4 - t3, 5)
+    multi["speedup_solve"] = round((t4 - t3) / multi["solve_s"], 2)
+    out["multi_rhs_64cubed_32"] = multi
+    # (b) 64 uneven systems in one launch
+    sides = np.random.default_rng(0).integers(32, 513, size=64)
+    systems = []
+    for side in sides:
+        sm, sn, sia, sja, sa = problems.laplacian(int(side), int(side), 1)
+        sA = (sm, sn) + tuple(torch.from_numpy(v).cuda() for v in (sia, sja, sa))
+        sPs = [(P[0], P[1]) + tuple(torch.from_numpy(v).cuda() for v in P[2:])
+               for P in geometric_interps(problems, (int(side), int(side), 1))]
+        systems.append((sA, sPs))
+    rows = sum(int(s_) ** 2 for s_ in sides)
+    bb = torch.from_numpy(np.concatenate([problems.rand_uniform(i, int(s_) ** 2) for i, s_ in enumerate(sides)])).cuda()
+    amgt.set_level_policy([0])
+    Bs = BatchSolver(systems)
+    Bs.solve_batch(bb)  # warm-up
+    Bs.free()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Bs = BatchSolver(systems)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    launches0 = amgt.kernel_launch_count()
+    xb, its, rel, loop_it = Bs.solve_batch(bb)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    off = Bs.offsets
+    Bs.free()
+    # one system at a time
+    t3 = time.perf_counter()
+    for i, (sA, sPs) in enumerate(systems):
+        S = AmgSolver(sA, sPs)
+        S.solve(bb[off[i]:off[i + 1]].contiguous())
+        S.free()
+    torch.cuda.synchronize()
+    t4 = time.perf_counter()
+    amgt.set_level_policy([])
+    out["batch_64_systems"] = {
+        "systems": 64, "sides": [int(min(sides)), int(max(sides))], "rows": rows, "setup_s": round(t1 - t0, 5),
+        "solve_s": round(t2 - t1, 5), "total_s": round(t2 - t0, 5), "loop_iterations": loop_it,
+        "iters_per_system": [min(its), max(its)], "max_rel_res": max(rel),
+        "one_system_at_a_time_total_s": round(t4 - t3, 5), "speedup_total": round((t4 - t3) / (t2 - t0), 2),
+        "solve_launches": "one CUDA graph launch (a conditional while node) for every iteration of every system"}
+    return out
+
+
 def cpu_amg(grid, b_host):
     """The oracle's AMG-PCG (C, OpenMP, all host threads) on the same problem."""
     from oracle import oracle as orc
@@ -558,6 +687,10 @@ def run_amgt(args):
             setup_solve["fp64"]["rel_err_vs_cpu_oracle"] = float(
                 np.linalg.norm(f64["x"].cpu().numpy() - xo) / np.linalg.norm(xo))
 
+    batching = None
+    if not args.no_batch:
+        batching = batching_report(amgt, torch, problems, stream)
+
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -592,6 +725,7 @@ def run_amgt(args):
         "clocks": clocks,
         "levels": levels,
         "setup_solve": setup_solve,
+        "batching": batching,
     }
     print(json.dumps(line), flush=True)
 
@@ -606,6 +740,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-levels", action="store_true", help="skip the hierarchy / per-level report")
     ap.add_argument("--no-solve", action="store_true", help="skip the AMG setup + solve report")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batching-form report")
     ap.add_argument("--grid", type=int, default=128, help="cube side (profiling captures only)")
     args = ap.parse_args()
     global GRID
