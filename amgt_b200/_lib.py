@@ -111,6 +111,14 @@ SIGNATURES = {
     "amgt_amg_setup_times": (c_int, [c_void_p, P(c_double)]),
     "amgt_amg_residual_history": (c_int, [c_void_p, P(c_double), c_int]),
     "amgt_amg_destroy": (c_int, [c_void_p, c_void_p]),
+    "amgt_amg_setup_adaptive": (c_int, [P(AmgtCsr), c_void_p, c_void_p, P(AmgtAmgParams), P(c_void_p), c_void_p]),
+    "amgt_level_features": (c_int, [P(AmgtBsr), c_int, P(c_int), P(ctypes.c_float), c_void_p]),
+    "amgt_structured_interp": (c_int, [P(c_int), P(c_int), P(AmgtCsr), P(c_int), c_void_p]),
+    "amgt_aniso_problem": (c_int, [P(c_int), c_double, c_double, P(AmgtCsr), c_void_p]),
+    "amgt_mlp_forward": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "amgt_mlp_grad": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "amgt_mlp_train": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int, c_int, ctypes.c_float, ctypes.c_uint,
+                               P(ctypes.c_float), c_void_p]),
     "amgt_CSRMatrixCreate": (P(AmgtCSRMatrix), [c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int]),
     "amgt_CSRMatrixDestroy": (c_int, [P(AmgtCSRMatrix)]),
     "amgt_set_stream": (c_int, [c_void_p]),

@@ -1111,14 +1111,31 @@ void amgt_amg_default_params(amgt_amg_params *p)
 int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P, const amgt_amg_params *params,
                    amgt_amg **out, amgt_stream_t stream)
 {
-    return amgt::amg_setup_blocks(A, num_interp, P, params, out, stream, nullptr);
+    return amgt::amg_setup_blocks(A, num_interp, P, params, out, stream, nullptr, nullptr, nullptr);
+}
+
+int amgt_amg_setup_adaptive(const amgt_csr *A, amgt_coarsen_fn fn, void *ctx, const amgt_amg_params *params,
+                            amgt_amg **out, amgt_stream_t stream)
+{
+    if (!fn) return AMGT_ERR_INVALID;
+    return amgt::amg_setup_blocks(A, 0, nullptr, params, out, stream, nullptr, fn, ctx);
 }
 
 }  // extern "C"
 
 int amgt::amg_setup_blocks(const amgt_csr *A, int num_interp, const amgt_csr *P, const amgt_amg_params *params,
-                           amgt_amg **out, amgt_stream_t stream, const std::vector<std::vector<int>> *sys_rows)
+                           amgt_amg **out, amgt_stream_t stream, const std::vector<std::vector<int>> *sys_rows,
+                           amgt_coarsen_fn cb, void *cb_ctx)
 {
+    // with a coarsening callback, P_l and level l's precision come from it,
+    // level by level, once A_l exists (num_interp: the most it may give)
+    std::vector<amgt_csr> Pcb;
+    if (cb) {
+        num_interp = (params ? params->max_levels : 25) - 1;
+        if (num_interp < 0) num_interp = 0;
+        Pcb.resize(num_interp + 1);
+        P = Pcb.data();
+    }
     if (!A || !out || num_interp < 0 || (num_interp > 0 && !P) || A->num_rows != A->num_cols || A->num_rows <= 0)
         return AMGT_ERR_INVALID;
     *out = nullptr;
@@ -1174,12 +1191,13 @@ int amgt::amg_setup_blocks(const amgt_csr *A, int num_interp, const amgt_csr *P,
         goto fail;
     }
     h->lv.resize(L);
-    nx.exact = h->prm.exact_storage != 0;
+    nx.exact = h->prm.exact_storage != 0 && !cb;  // fused checks follow the policy table
     nx.xflags = xflags;
     nx.fused16 = &fused16;
     // hierarchy: P_0 converted while A's conversion runs, R_l transposed
-    // and P_{l+1} converted while level l's A P runs
-    if (L > 1) {
+    // and P_{l+1} converted while level l's A P runs (with a callback, P_l
+    // exists only once A_l does: each is converted when it arrives)
+    if (L > 1 && !cb) {
         nx.P = &P[0];
         nx.Pb = &h->lv[0].P;
         nx.PRb = &h->lv[0].R;
@@ -1203,9 +1221,39 @@ int amgt::amg_setup_blocks(const amgt_csr *A, int num_interp, const amgt_csr *P,
     pm.mark(0, s);
     for (int l = 0; l < L - 1; ++l) {
         Level &v = h->lv[l];
+        if (cb) {
+            int prec_l = AMGT_DOUBLE;
+            amgt_csr Pl{};
+            const int r = cb(l, &v.A, &Pl, &prec_l, cb_ctx);
+            if (r < 0 || prec_l < AMGT_DOUBLE || prec_l > AMGT_BF16) {
+                rc = AMGT_ERR_INVALID;
+                goto fail;
+            }
+            v.prec = prec_l;
+            if (r == 1) {  // A_l is the coarsest level
+                L = l + 1;
+                h->lv.resize(L);
+                break;
+            }
+            Pcb[l] = Pl;
+            // P_l's arrays may still be arriving on the caller's stream:
+            // the second stream converts it after them
+            if (cudaEventRecord(nx.p_ready[l % 2], s) != cudaSuccess ||
+                cudaStreamWaitEvent(nx.s2, nx.p_ready[l % 2], 0) != cudaSuccess) {
+                rc = AMGT_ERR_CUDA;
+                goto fail;
+            }
+            nx.P = &Pcb[l];
+            nx.Pb = &v.P;
+            nx.PRb = &v.R;
+            nx.pslot = l % 2;
+            nx.plevel = l;
+        }
         if (P[l].num_rows != v.n || P[l].num_cols <= 0) { rc = AMGT_ERR_INVALID; goto fail; }
-        v.prec = amgt_precision_for_level(l);
-        v.prec_transfer = amgt_precision_for_level(l + 1);
+        if (!cb) {
+            v.prec = amgt_precision_for_level(l);
+            v.prec_transfer = amgt_precision_for_level(l + 1);
+        }
         // A P waits for P_l only (converted now if no call issued it),
         // R (A P) for R_l (transposed now if A P's call did not)
         if (nx.P && (rc = prepare_interp(&nx))) goto fail;
@@ -1216,7 +1264,7 @@ int amgt::amg_setup_blocks(const amgt_csr *A, int num_interp, const amgt_csr *P,
         pm.mark(1, s);
         const int gp = h->prm.galerkin_by_level ? v.prec : AMGT_DOUBLE;
         amgt_bsr AP{};
-        if (l + 1 < L - 1) {
+        if (l + 1 < L - 1 && !cb) {
             nx.P = &P[l + 1];
             nx.Pb = &h->lv[l + 1].P;
             nx.PRb = &h->lv[l + 1].R;
@@ -1236,7 +1284,7 @@ int amgt::amg_setup_blocks(const amgt_csr *A, int num_interp, const amgt_csr *P,
         {
             // A_{l+1} in fp64 is checked for exact storage by the numeric pass
             CvtFuse fz;
-            fz.want16 = h->prm.exact_storage && gp == AMGT_DOUBLE &&
+            fz.want16 = h->prm.exact_storage && gp == AMGT_DOUBLE && !cb &&
                         amgt_precision_for_level(l + 1) == AMGT_DOUBLE;
             fz.flags = xflags + 3 * (l + 1);
             rc = spgemm_impl(gp, &v.R, &AP, &h->lv[l + 1].A, nullptr, stream, nullptr, nullptr,
@@ -1248,7 +1296,23 @@ int amgt::amg_setup_blocks(const amgt_csr *A, int num_interp, const amgt_csr *P,
         h->lv[l + 1].n = h->lv[l + 1].A.row;
         pm.mark(2, s);
     }
-    h->lv[L - 1].prec = amgt_precision_for_level(L - 1);
+    if (cb) {
+        // the coarsest level's precision when the level cap ended the loop,
+        // and each transfer at its coarse level's precision
+        if (L == num_interp + 1 || (h->prm.max_levels > 0 && L == h->prm.max_levels)) {
+            int prec_l = AMGT_DOUBLE;
+            amgt_csr unused{};
+            if (cb(L - 1, &h->lv[L - 1].A, &unused, &prec_l, cb_ctx) < 0 || prec_l < AMGT_DOUBLE ||
+                prec_l > AMGT_BF16) {
+                rc = AMGT_ERR_INVALID;
+                goto fail;
+            }
+            h->lv[L - 1].prec = prec_l;
+        }
+        for (int l = 0; l + 1 < L; ++l) h->lv[l].prec_transfer = h->lv[l + 1].prec;
+    } else {
+        h->lv[L - 1].prec = amgt_precision_for_level(L - 1);
+    }
     // coarsest: dense diagonal blocks (one, or one per system of a batch)
     // and their inverses, on the GPU (Gauss-Jordan); the singularity flag is
     // read back with the exactness bits below

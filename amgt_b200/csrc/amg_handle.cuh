@@ -76,9 +76,12 @@ namespace amgt {
 int amg_cycle(amgt_amg *h, const double *rhs0, double *out0, cudaStream_t s);
 // amgt_amg_setup with the coarsest operator inverted per diagonal block:
 // block s has sys_rows[s][L - 1] rows, L the levels set up (nullptr: one
-// block)
+// block).
+// With cb: P_l and level l's precision from the callback, once A_l exists
+// (amgt_amg_setup_adaptive).
 int amg_setup_blocks(const amgt_csr *A, int num_interp, const amgt_csr *P, const amgt_amg_params *params,
-                     amgt_amg **out, amgt_stream_t stream, const std::vector<std::vector<int>> *sys_rows);
+                     amgt_amg **out, amgt_stream_t stream, const std::vector<std::vector<int>> *sys_rows,
+                     amgt_coarsen_fn cb, void *cb_ctx);
 }  // namespace amgt
 
 

@@ -367,7 +367,8 @@ int amgt_batch_setup(int nsys, const amgt_csr *A, const int *nlev, const amgt_cs
         if (cudaGetLastError() != cudaSuccess) rc = AMGT_ERR_CUDA;
         if (!rc && cudaStreamSynchronize(s) != cudaSuccess) rc = AMGT_ERR_CUDA;  // ddesc is reused next level
     }
-    if (!rc) rc = amg_setup_blocks(&cat[0], Lmax, Lmax > 0 ? &cat[1] : nullptr, params, &h, stream, &rows);
+    if (!rc) rc = amg_setup_blocks(&cat[0], Lmax, Lmax > 0 ? &cat[1] : nullptr, params, &h, stream, &rows, nullptr,
+                                  nullptr);
     for (auto &C : cat) {
         free_ptr(C.i, s);
         free_ptr(C.j, s);

@@ -412,6 +412,22 @@ AMGT_API void amgt_amg_default_params(amgt_amg_params *p);
 AMGT_API int amgt_amg_setup(const amgt_csr *A, int num_interp, const amgt_csr *P,
                             const amgt_amg_params *params, amgt_amg **out,
                             amgt_stream_t stream);
+/* Level-by-level setup with the coarsening decided by the caller, once
+ * each level's operator exists (the place of BoomerAMG's coarsening and
+ * interpolation, R/parcsr_ls/par_amg_setup.c, which HYPRE runs per level on
+ * A_l).  fn(level, A_l, P, prec, ctx) is called on the setup's host thread
+ * for level = 0, 1, ...: it sets *prec to level l's precision (its
+ * smoother and cycle SpMVs; the transfers of level l - 1 use it too) and
+ * either returns 0 with *P the interpolation from level l + 1 to level l
+ * (device CSR, A_l->row rows; the caller keeps its arrays alive until the
+ * setup returns), or returns 1 to make A_l the coarsest level; a negative
+ * return aborts the setup (AMGT_ERR_INVALID).  A_l is a borrowed view,
+ * valid during the call; fn may run library calls on the same stream.
+ * When params->max_levels ends the hierarchy, fn is called once more for
+ * the coarsest level's precision.  The rest is amgt_amg_setup's. */
+typedef int (*amgt_coarsen_fn)(int level, const amgt_bsr *A, amgt_csr *P, int *prec, void *ctx);
+AMGT_API int amgt_amg_setup_adaptive(const amgt_csr *A, amgt_coarsen_fn fn, void *ctx, const amgt_amg_params *params,
+                                     amgt_amg **out, amgt_stream_t stream);
 /* x: initial guess in, solution out (device).  PCG: the iteration loop is
  * one CUDA graph launch and one read-back (one launch and an 8-byte read
  * per iteration where the runtime lacks conditional graph nodes).
@@ -469,6 +485,59 @@ AMGT_API int amgt_amg_setup_times(const amgt_amg *amg, double *ms);
  * each refinement step the fp64 residual. */
 AMGT_API int amgt_amg_residual_history(const amgt_amg *amg, double *hist, int cap);
 AMGT_API int amgt_amg_destroy(amgt_amg *amg, amgt_stream_t stream);
+
+/* --------------------------------- learned precision / theta policy */
+/* No reference counterpart: AmgT's precision per level is a fixed table
+ * (get_calculationPrecison, R/seq_mv/csr_spgemm_device.c:1847-1862) and
+ * BoomerAMG's strength threshold a fixed parameter
+ * (HYPRE_BoomerAMGSetStrongThreshold).  These are the pieces of a policy
+ * that picks both per level from cheap features of the level's operator. */
+#define AMGT_MLP_IN 16
+#define AMGT_MLP_HIDDEN 64
+#define AMGT_MLP_OUT 4
+#define AMGT_MLP_NPARAM 5508 /* W1 64x16, b1 64, W2 64x64, b2 64, W3 4x64, b3 4 */
+
+/* 16 features of level `level`'s operator A (fp64 values), on an nx x ny x
+ * nz grid dims[0..2] (the grid decodes a column offset into grid axes):
+ * log10 rows, CSR nonzeros per row / 10, block fill, mean and minimum
+ * diagonal dominance |a_ii| / sum_j!=i |a_ij| (capped at 10), mean and
+ * spread of row sum / |a_ii|, share of positive off-diagonals, the shares
+ * of coupling |a_ij| / |a_ii| along x, y, z and across axes, mean largest
+ * off-diagonal / |a_ii|, level / 10, 3D flag, 1.  out: 16 host floats.
+ * One host read-back. */
+AMGT_API int amgt_level_features(const amgt_bsr *A, int level, const int *dims, float *out, amgt_stream_t stream);
+
+/* Linear interpolation between vertex-centred structured grids along the
+ * axes with coarsen[d] != 0 (coarse point j on fine point 2j), identity
+ * along the others: P (device CSR from the allocator, free with
+ * amgt_csr_free), cdims = the coarse grid.  One host read-back. */
+AMGT_API int amgt_structured_interp(const int *dims, const int *coarsen, amgt_csr *P, int *cdims,
+                                    amgt_stream_t stream);
+
+/* Test and training problem (the learned policy's matrices): rotated
+ * anisotropic diffusion -div(K grad u) on dims[0] x dims[1] x dims[2],
+ * K = R(angle) diag(1, eps) R^T in the x-y plane and 1 along z, Dirichlet
+ * boundary, unit spacing; 9-point x-y stencil (the mixed derivative by
+ * central differences) plus the z neighbours.  Rows: diagonal first, then
+ * ascending columns, as HYPRE's generators store them.  A: device CSR from
+ * the allocator (free with amgt_csr_free).  One host read-back. */
+AMGT_API int amgt_aniso_problem(const int *dims, double eps, double angle, amgt_csr *A, amgt_stream_t stream);
+
+/* The 16 -> 64 -> 64 -> 4 MLP (fp32, ReLU; params: AMGT_MLP_NPARAM device
+ * floats).  Output 0: logit of theta; 1 .. 3: logits of the level's
+ * precision (fp64, fp32, fp16).  X: n x 16, out: n x 4 (device).
+ * amgt_mlp_grad: the mean over the n samples of the gradient of
+ * (sigmoid(o0) - T[2i])^2 + cross-entropy(softmax(o1..o3), class T[2i+1])
+ * into grad (AMGT_MLP_NPARAM device floats) and the mean loss into *loss
+ * (device, may be NULL).  amgt_mlp_train: Adam (beta 0.9, 0.999) over
+ * `epochs` passes of seeded shuffles in minibatches of `batch`, params
+ * updated in place; loss_hist (host, may be NULL): mean loss of each
+ * epoch's last minibatch. */
+AMGT_API int amgt_mlp_forward(const float *params, int n, const float *X, float *out, amgt_stream_t stream);
+AMGT_API int amgt_mlp_grad(const float *params, int n, const float *X, const float *T, float *grad, float *loss,
+                           amgt_stream_t stream);
+AMGT_API int amgt_mlp_train(float *params, int n, const float *X, const float *T, int epochs, int batch, float lr,
+                            unsigned seed, float *loss_hist, amgt_stream_t stream);
 
 /* ------------------------------------------ HYPRE-facing mirror layer */
 /* The fields of hypre_CSRMatrix that the AmgT path reads and writes

@@ -1,0 +1,144 @@
+"""GPU tests of the learned policy's kernels against the oracle
+(oracle/mlp_oracle.py) and of the level-by-level setup.
+
+MLP (fp32 kernels vs the float64 restatement): outputs within 1e-4 of the
+output scale; the mean gradient within 1e-3 of the largest gradient entry;
+training reduces the loss.  Features within 1e-5 relative (fp32 output of
+fp64 sums).  Structured interpolation and the problem generator: bit for
+bit.  Setup through the coarsening callback: theta = 0 reproduces the
+geometric hierarchy (same levels and iterations as amgt_amg_setup with
+linear interpolation); theta picks only the strong axis on an aligned
+anisotropic operator."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from gpu_util import to_dev
+from oracle import mlp_oracle as mo
+
+pytestmark = pytest.mark.gpu
+
+
+def _dense(m, n, ia, ja, a):
+    D = np.zeros((m, n))
+    for r in range(m):
+        D[r, ja[ia[r]:ia[r + 1]]] = a[ia[r]:ia[r + 1]]
+    return D
+
+
+@pytest.mark.parametrize("dims,eps,angle", [((9, 7, 1), 1e-2, 0.4), ((6, 5, 4), 0.3, 2.0), ((8, 8, 1), 1.0, 0.0)])
+def test_aniso_problem_matches_oracle(amgt, dims, eps, angle):
+    from amgt_b200 import policy
+
+    m, n, ia, ja, a = policy.aniso_problem(dims, eps, angle)
+    om, on, oia, oja, oa = mo.aniso_problem(dims, eps, angle)
+    assert (m, n) == (om, on)
+    np.testing.assert_array_equal(ia.cpu().numpy(), oia)
+    np.testing.assert_array_equal(ja.cpu().numpy(), oja)
+    np.testing.assert_array_equal(a.cpu().numpy().view(np.uint64), oa.view(np.uint64))
+
+
+@pytest.mark.parametrize("dims,axes", [((9, 7, 5), (1, 1, 1)), ((8, 6, 1), (0, 1, 0)), ((9, 6, 4), (1, 0, 1)),
+                                       ((5, 1, 1), (1, 1, 1))])
+def test_structured_interp_matches_oracle(amgt, dims, axes):
+    L = amgt.lib()
+    P = amgt._lib.AmgtCsr()
+    cd = (ctypes.c_int * 3)()
+    assert L.amgt_structured_interp((ctypes.c_int * 3)(*dims), (ctypes.c_int * 3)(*axes), ctypes.byref(P), cd,
+                                    None) == 0
+    from amgt_b200.mbsr import view
+
+    ia = view(P.i, P.num_rows + 1, torch.int32).cpu().numpy()
+    ja = view(P.j, P.num_nonzeros, torch.int32).cpu().numpy()
+    a = view(P.data, P.num_nonzeros, torch.float64).cpu().numpy()
+    D = mo.structured_interp(dims, axes)
+    np.testing.assert_array_equal(_dense(P.num_rows, P.num_cols, ia, ja, a), D)
+    for r in range(P.num_rows):  # columns ascend within a row
+        assert np.all(np.diff(ja[ia[r]:ia[r + 1]]) > 0)
+    L.amgt_csr_free(ctypes.byref(P), None)
+
+
+@pytest.mark.parametrize("dims,eps,angle,level", [((11, 9, 1), 1e-2, 0.3, 0), ((6, 6, 5), 0.2, 1.1, 2)])
+def test_level_features_match_oracle(amgt, orc, dims, eps, angle, level):
+    from amgt_b200 import policy
+
+    A = policy.aniso_problem(dims, eps, angle)
+    G = amgt.Bsr.from_csr(*A)
+    f = policy.level_features(G.s, level, dims)
+    Ah = (A[0], A[1], A[2].cpu().numpy(), A[3].cpu().numpy(), A[4].cpu().numpy())
+    want = mo.features(_dense(*Ah), level, dims)
+    want[2] = G.s.csr_nnz / (16.0 * G.nblk)
+    np.testing.assert_allclose(f, want, rtol=1e-5, atol=1e-6)
+
+
+def test_mlp_forward_and_gradient_match_oracle(amgt):
+    L = amgt.lib()
+    rng = np.random.default_rng(3)
+    p = rng.normal(0, 0.3, mo.NPARAM).astype(np.float32)
+    X = rng.normal(0, 1, (300, 16)).astype(np.float32)
+    T = np.stack([rng.uniform(0, 1, 300), rng.integers(0, 3, 300)], axis=1).astype(np.float32)
+    P, Xd, Td = (torch.from_numpy(v).cuda() for v in (p, X, T))
+    out = torch.zeros(300, 4, dtype=torch.float32, device="cuda")
+    assert L.amgt_mlp_forward(P.data_ptr(), 300, Xd.data_ptr(), out.data_ptr(), None) == 0
+    _, _, o = mo.forward(p, X)
+    np.testing.assert_allclose(out.cpu().numpy(), o, rtol=1e-4, atol=1e-4 * np.abs(o).max())
+    g = torch.zeros(mo.NPARAM, dtype=torch.float32, device="cuda")
+    ls = torch.zeros(1, dtype=torch.float32, device="cuda")
+    assert L.amgt_mlp_grad(P.data_ptr(), 300, Xd.data_ptr(), Td.data_ptr(), g.data_ptr(), ls.data_ptr(), None) == 0
+    gw = mo.grad(p, X, T)
+    assert np.max(np.abs(g.cpu().numpy() - gw)) <= 1e-3 * np.abs(gw).max()
+    assert abs(float(ls.item()) - mo.loss(p, X, T)) <= 1e-4 * abs(mo.loss(p, X, T))
+
+
+def test_mlp_training_fits_a_separable_task(amgt):
+    from amgt_b200 import policy
+
+    rng = np.random.default_rng(4)
+    X = rng.normal(0, 1, (2000, 16)).astype(np.float32)
+    X[:, 15] = 1.0
+    th = 1.0 / (1.0 + np.exp(-(X[:, 0] - 0.5 * X[:, 1])))
+    cls = (X[:, 2] > 0.3).astype(np.float32) + (X[:, 2] > 1.0)
+    T = np.stack([th, cls], axis=1).astype(np.float32)
+    params, hist = policy.train(X, T, epochs=60, batch=128, lr=3e-3, seed=1)
+    assert hist[-1] < 0.25 * hist[0]
+    _, _, o = mo.forward(params, X)
+    acc = np.mean(np.argmax(o[:, 1:4], axis=1) == cls)
+    assert acc > 0.9
+
+
+def test_adaptive_setup_theta0_is_the_geometric_hierarchy(amgt, orc):
+    from amgt_b200 import policy
+    from amgt_b200.amg import AmgSolver, default_params
+
+    dims = (24, 20, 18)
+    A = orc.laplacian(*dims)
+    b = torch.from_numpy(orc.rand_uniform(0, A.n)).cuda()
+    amgt.set_level_policy([0])
+    try:
+        G = AmgSolver(to_dev(A), [to_dev(P) for P in orc.geometric_hierarchy(*dims)], default_params())
+        _, itg, relg = G.solve(b)
+        levels_g = [G.level(l)["rows"] for l in range(G.num_levels())]
+        G.free()
+    finally:
+        amgt.set_level_policy([])
+    S = policy.AdaptiveSolver(to_dev(A), dims, policy.FixedPolicy(0.0))
+    _, its, rels = S.solve(b)
+    assert [S.level(l)["rows"] for l in range(S.num_levels())] == levels_g
+    assert its == itg and rels <= 1e-8
+    assert all(t["axes"] in (None, [1, 1, 1]) for t in S.trace)
+    S.free()
+
+
+def test_adaptive_setup_semicoarsens_the_strong_axis(amgt):
+    from amgt_b200 import policy
+
+    dims = (40, 40, 1)
+    A = policy.aniso_problem(dims, 1e-3, 0.0)  # strong coupling along x only
+    S = policy.AdaptiveSolver(A, dims, policy.FixedPolicy(0.25))
+    assert S.trace[0]["axes"] == [1, 0, 0]
+    b = torch.ones(A[0], dtype=torch.float64, device="cuda")
+    _, it, rel = S.solve(b)
+    assert rel <= 1e-8 and it < 40
+    S.free()
