@@ -47,3 +47,31 @@ def test_aniso_problem_is_symmetric_and_anisotropic():
         D[r, ja[ia[r]:ia[r + 1]]] = a[ia[r]:ia[r + 1]]
     np.testing.assert_allclose(D, D.T, atol=1e-15)
     assert np.all(np.linalg.eigvalsh(D) > 0)
+
+
+def test_committed_network_fits_its_training_set():
+    """The trained weights (amgt_b200/data/policy_mlp.npy, trained on the
+    GPU by amgt_mlp_train) against the committed dataset, evaluated by the
+    oracle's forward pass: the loss is far below the initial network's, and
+    the theta it predicts tracks the labels."""
+    import os
+
+    import amgt_b200.policy as pol
+
+    d = np.load(os.path.join(os.path.dirname(pol.WEIGHTS), "policy_dataset.npz"))
+    X, T = d["X"], d["T"]
+    assert X.shape[1] == 16 and T.shape == (X.shape[0], 2) and X.shape[0] > 20000
+    assert set(np.unique(T[:, 1])) <= {0.0, 1.0, 2.0}
+    w = np.load(pol.WEIGHTS)
+    rng = np.random.default_rng(0)
+    w0 = np.zeros(mo.NPARAM, np.float32)
+    o = 0
+    for fan_in, fan_out in ((16, 64), (64, 64), (64, 4)):  # the initialisation train() uses
+        n = fan_out * fan_in
+        w0[o:o + n] = rng.normal(0.0, np.sqrt(2.0 / fan_in), size=n)
+        o += n + fan_out
+    trained, initial = mo.loss(w, X, T), mo.loss(w0, X, T)
+    assert trained < 0.2 * initial
+    _, _, out = mo.forward(w, X)
+    theta = 1.0 / (1.0 + np.exp(-out[:, 0]))
+    assert np.corrcoef(theta, T[:, 0])[0, 1] > 0.8
