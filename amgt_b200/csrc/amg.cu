@@ -662,7 +662,7 @@ void destroy_handle(amgt_amg *h, cudaStream_t s)
     if (h->graph_stream) cudaStreamDestroy(h->graph_stream);
     free_ptr(h->loop_it, s);
     free_ptr(h->loop_rr, s);
-    if (h->loop_pinned) cudaFreeHost(h->loop_pinned);
+    // loop_pinned and mr_pinned live inside the one pinned block h->pinned
     for (auto &v : h->lv) free_level(v, s);
     free_ptr(h->coarse_inv, s);
     free_ptr(h->cb_off, s);
@@ -868,7 +868,7 @@ int build_loop_graph(amgt_amg *h, double *x)
     }
     if (!h->graph_stream) AMGT_CUDA_TRY(cudaStreamCreateWithFlags(&h->graph_stream, cudaStreamNonBlocking));
     if (!h->loop_it || !h->loop_rr) return AMGT_ERR_INVALID;  // allocated by the setup
-    if (!h->loop_pinned) AMGT_CUDA_TRY(cudaMallocHost(&h->loop_pinned, sizeof(double) * (h->prm.max_iter + 2)));
+    if (!h->loop_pinned) return AMGT_ERR_INVALID;  // allocated by the setup
     cudaGraph_t g = nullptr;
     AMGT_CUDA_TRY(cudaGraphCreate(&g, 0));
     cudaGraphConditionalHandle cond;
@@ -1014,7 +1014,7 @@ int fgmres_ir_solve(amgt_amg *h, const double *b, double *x, int *iterations, do
     const int m = h->prm.restart;
     const long long n = h->n0;
     const int max_iter = h->prm.max_iter;
-    if (!h->loop_pinned) AMGT_CUDA_TRY(cudaMallocHost(&h->loop_pinned, sizeof(double) * (max_iter + 2)));
+    if (!h->loop_pinned) return AMGT_ERR_INVALID;  // allocated by the setup
     h->hist.clear();
     AMGT_CUDA_TRY(cudaMemsetAsync(h->loop_it, 0, sizeof(int), s));
     AMGT_TRY(dot(h, b, b, S_BB, OP_STORE, s));
@@ -1478,7 +1478,12 @@ int amgt::amg_setup_blocks(const amgt_csr *A, int num_interp, const amgt_csr *P,
         }
     }
     AMGT_CUDA_TRY(cudaMemsetAsync(h->scal, 0, sizeof(double) * S_NSCAL, s));
-    AMGT_CUDA_TRY(cudaMallocHost(&h->pinned, sizeof(double) * 8));
+    // every host read-back slot of the solvers in one pinned block, so that
+    // no solve allocates: 8 scalars, the multi-right-hand-side solve's 160,
+    // and the loop's iteration count and max_iter + 1 residual norms
+    AMGT_CUDA_TRY(cudaMallocHost(&h->pinned, sizeof(double) * (8 + 160 + (size_t)h->prm.max_iter + 2)));
+    h->mr_pinned = h->pinned + 8;
+    h->loop_pinned = h->pinned + 168;
     free_ptr(xflags, s);
     pm.mark(3, s);
     pm.accumulate(h->setup_ms);  // waits for the setup's last work

@@ -41,7 +41,7 @@ struct amgt_amg {
     long long n0 = 0;
     double *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
     double *scal = nullptr, *part = nullptr;
-    double *pinned = nullptr;  // host: ||r||^2 read-back
+    double *pinned = nullptr;  // host: one pinned block of every read-back slot (setup allocates it)
     int sm_count = 0, grid0 = 0;
     cudaGraphExec_t graph = nullptr;
     cudaStream_t graph_stream = nullptr;
@@ -54,7 +54,8 @@ struct amgt_amg {
     bool loop_failed = false;
     int *loop_it = nullptr;     // device: iterations done
     double *loop_rr = nullptr;  // device: ||r||^2 after iteration k, k = 1 .. max_iter
-    double *loop_pinned = nullptr;
+    double *loop_pinned = nullptr;  // host, inside the pinned block (below)
+    double *mr_pinned = nullptr;    // host, 160 slots of the multi-right-hand-side solve
     uint64_t graph_launches = 0, loop_launches = 0;  // our kernels per iteration in each graph
     double setup_ms[5] = {0, 0, 0, 0, 0};
     std::vector<double> hist;

@@ -43,7 +43,7 @@ struct MultiRhs {
     double *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *d = nullptr, *res = nullptr;
     double *scal = nullptr, *part = nullptr;
     int *cnt = nullptr;   // device: [32] iterations per column, [32] total inner iterations
-    double *pinned = nullptr;  // host: 2 * 32 norms + counts
+    double *pinned = nullptr;  // host, the handle's: 2 * 32 norms, counts, the loop flag
     cudaGraphExec_t loop = nullptr;
     bool loop_failed = false;
     uint64_t loop_launches = 0;
@@ -68,7 +68,6 @@ void free_multi_rhs(MultiRhs *mr, cudaStream_t s)
     free_ptr(mr->scal, s);
     free_ptr(mr->part, s);
     free_ptr(mr->cnt, s);
-    if (mr->pinned) cudaFreeHost(mr->pinned);
     delete mr;
 }
 
@@ -405,7 +404,7 @@ int make_multi_rhs(amgt_amg *h, int nv, cudaStream_t s, MultiRhs **out)
                 (rc = alloc_n(&mr->scal, (size_t)MS_NSLOT * 32, s)) ||
                 (rc = alloc_n(&mr->part, (size_t)kMvGrid * 32, s)) || (rc = alloc_n(&mr->cnt, 40, s))))
         rc = rc ? rc : AMGT_ERR_ALLOC;
-    if (!rc && cudaMallocHost(&mr->pinned, sizeof(double) * 128) != cudaSuccess) rc = AMGT_ERR_CUDA;
+    mr->pinned = h->mr_pinned;  // the handle's pinned block (no allocation here)
     if (!rc && cudaMemsetAsync(mr->scal, 0, sizeof(double) * MS_NSLOT * 32, s) != cudaSuccess) rc = AMGT_ERR_CUDA;
     if (rc) {
         cudaGetLastError();
