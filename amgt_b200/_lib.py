@@ -66,6 +66,10 @@ class AmgtTuneResult(ctypes.Structure):
 
 ENGINE_AUTO, ENGINE_CUDA_CORE, ENGINE_TENSOR_CORE = 0, 1, 2
 
+
+class AmgtBoomerParams(ctypes.Structure):
+    _fields_ = [("theta", c_double), ("max_row_sum", c_double), ("p_max", c_int), ("coarsen_type", c_int)]
+
 # name -> (restype, argtypes); every symbol include/amgt_b200.h declares
 SIGNATURES = {
     "amgt_status_string": (ctypes.c_char_p, [c_int]),
@@ -112,6 +116,16 @@ SIGNATURES = {
     "amgt_amg_residual_history": (c_int, [c_void_p, P(c_double), c_int]),
     "amgt_amg_destroy": (c_int, [c_void_p, c_void_p]),
     "amgt_amg_setup_adaptive": (c_int, [P(AmgtCsr), c_void_p, c_void_p, P(AmgtAmgParams), P(c_void_p), c_void_p]),
+    "amgt_boomer_default_params": (None, [P(AmgtBoomerParams)]),
+    "amgt_boomer_coarsen_host": (c_int, [c_int, c_void_p, c_void_p, c_void_p, P(AmgtBoomerParams), c_void_p,
+                                         P(AmgtCsr)]),
+    "amgt_boomer_free_host": (c_int, [P(AmgtCsr)]),
+    "amgt_boomer_interp": (c_int, [P(AmgtBsr), P(AmgtBoomerParams), P(AmgtCsr), c_void_p, c_void_p]),
+    "amgt_boomer_hierarchy_host": (c_int, [c_int, c_void_p, c_void_p, c_void_p, P(AmgtBoomerParams), c_int, c_int,
+                                           P(c_void_p)]),
+    "amgt_boomer_hierarchy_levels": (c_int, [c_void_p]),
+    "amgt_boomer_hierarchy_level": (c_int, [c_void_p, c_int, P(AmgtCsr), P(AmgtCsr)]),
+    "amgt_boomer_hierarchy_free": (None, [c_void_p]),
     "amgt_level_features": (c_int, [P(AmgtBsr), c_int, P(c_int), P(ctypes.c_float), c_void_p]),
     "amgt_structured_interp": (c_int, [P(c_int), P(c_int), P(AmgtCsr), P(c_int), c_void_p]),
     "amgt_aniso_problem": (c_int, [P(c_int), c_double, c_double, P(AmgtCsr), c_void_p]),

@@ -14,10 +14,10 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libamgt_b200.so")
 SOURCES = ["runtime.cu", "convert.cu", "spmv.cu", "spgemm.cu", "hypre_mirror.cu", "noalloc.cu", "amg.cu", "packed.cu",
-           "spmm_tc.cu", "autotune.cu", "multirhs.cu", "batch.cu", "policy.cu"]
+           "spmm_tc.cu", "autotune.cu", "multirhs.cu", "batch.cu", "policy.cu", "boomer.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden", "-cudart", "static",
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off", "-cudart", "static",
          "--expt-relaxed-constexpr"]
 
 

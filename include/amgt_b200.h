@@ -487,6 +487,64 @@ AMGT_API int amgt_amg_setup_times(const amgt_amg *amg, double *ms);
 AMGT_API int amgt_amg_residual_history(const amgt_amg *amg, double *hist, int cap);
 AMGT_API int amgt_amg_destroy(amgt_amg *amg, amgt_stream_t stream);
 
+/* --------------------------------------- BoomerAMG coarsening (host) */
+/* One level of BoomerAMG's coarsening and interpolation with the settings
+ * the headline configurations name: HMIS (Ruge-Stueben first pass, then
+ * PMIS; hypre_BoomerAMGCoarsenHMIS, R/parcsr_ls/par_coarsen.c:2845),
+ * classical strength with threshold theta and max_row_sum
+ * (hypre_BoomerAMGCreateS, par_strength.c), extended+i interpolation
+ * (hypre_BoomerAMGBuildExtPIInterp, par_lr_interp.c:1025) truncated to p_max
+ * entries per row with rescaling (hypre_ParCSRMatrixTruncate), one process.
+ * Host code, as HYPRE 2.31's HMIS is.  No reference counterpart inside the
+ * AmgT path: this is the caller's side of the SpGEMM hook (what produces
+ * the P of the Galerkin products). */
+typedef struct {
+    double theta;        /* strength threshold (default 0.25)               */
+    double max_row_sum;  /* rows with |sum| > max_row_sum |a_ii|: all weak;
+                            1.0 turns the test off (default 1.0, the ij
+                            driver's value, R/test/ij.c:290)               */
+    int p_max;           /* interpolation entries per row (default 4, the ij
+                            driver's, R/test/ij.c:244; 0: all)             */
+    int coarsen_type;    /* 10: HMIS (default, the ij driver's,
+                            R/test/ij.c:247); 8: PMIS (BoomerAMG's GPU
+                            default, R/parcsr_ls/par_amg.c:304-316)        */
+} amgt_boomer_params;
+AMGT_API void amgt_boomer_default_params(amgt_boomer_params *p);
+/* Host CSR in (rows with the diagonal first, as HYPRE stores them); P out in
+ * HOST memory from malloc (free with amgt_boomer_free_host); cf_marker (host,
+ * n, may be NULL): 1 for C points, -1 for F points. */
+AMGT_API int amgt_boomer_coarsen_host(int n, const int *ia, const int *ja, const double *a,
+                                      const amgt_boomer_params *prm, int *cf_marker, amgt_csr *P);
+AMGT_API int amgt_boomer_free_host(amgt_csr *P);
+/* The same for a device mBSR operator (copied to the host with its rows
+ * reordered diagonal first); P in DEVICE memory from the allocator (free
+ * with amgt_csr_free).  Blocks the host.  Usable as the coarsening of
+ * amgt_amg_setup_adaptive. */
+AMGT_API int amgt_boomer_interp(const amgt_bsr *A, const amgt_boomer_params *prm, amgt_csr *P, int *cf_marker,
+                                amgt_stream_t stream);
+/* The whole hierarchy on the host as HYPRE's CPU BoomerAMG builds it on one
+ * process (hypre_BoomerAMGSetup, R/parcsr_ls/par_amg_setup.c): each level
+ * as amgt_boomer_coarsen_host, then A_{l+1} = P^T (A_l P) in the order and
+ * arithmetic of hypre_ParCSRMatrixRAPKTHost (R/parcsr_mv/
+ * par_csr_triplemat.c:877-880; hypre_CSRMatrixMultiplyHost, R/seq_mv/
+ * csr_matop.c:665), so the next level sees HYPRE's column order and its
+ * truncation breaks ties as HYPRE's does.  A (host, n rows, each row's
+ * diagonal first: HYPRE's storage).  Stops at a level of at most max_coarse
+ * rows (HYPRE's default 9), at max_levels levels (default 25), or when a
+ * level does not coarsen.  AMGT_ERR_UNSUPPORTED where HYPRE would switch to
+ * CLJP coarsening (a coarse level of at least 3/4 of its fine level,
+ * par_amg_setup.c:3166). */
+typedef struct amgt_boomer_hier amgt_boomer_hier;
+AMGT_API int amgt_boomer_hierarchy_host(int n, const int *ia, const int *ja, const double *a,
+                                        const amgt_boomer_params *prm, int max_levels, int max_coarse,
+                                        amgt_boomer_hier **out);
+AMGT_API int amgt_boomer_hierarchy_levels(const amgt_boomer_hier *h);
+/* Host views owned by h of level l's operator A_l (l < levels) and
+ * interpolation P_l (l < levels - 1; zeroed on the coarsest level); either
+ * output may be NULL. */
+AMGT_API int amgt_boomer_hierarchy_level(const amgt_boomer_hier *h, int l, amgt_csr *A, amgt_csr *P);
+AMGT_API void amgt_boomer_hierarchy_free(amgt_boomer_hier *h);
+
 /* --------------------------------- learned precision / theta policy */
 /* No reference counterpart: AmgT's precision per level is a fixed table
  * (get_calculationPrecison, R/seq_mv/csr_spgemm_device.c:1847-1862) and
