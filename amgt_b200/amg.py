@@ -94,13 +94,14 @@ class AmgSolver:
         check(L.lib().amgt_amg_level(self.h, l, ctypes.byref(b), ctypes.byref(prec)), "amgt_amg_level")
         c = L.AmgtCsr()
         check(L.lib().amgt_bsr_to_csr(ctypes.byref(b), ctypes.byref(c), None), "amgt_bsr_to_csr")
+        shape = (c.num_rows, c.num_cols)
         try:
             ia = view(c.i, c.num_rows + 1, torch.int32).cpu().numpy()
             ja = view(c.j, c.num_nonzeros, torch.int32).cpu().numpy()
             a = view(c.data, c.num_nonzeros, torch.float64).cpu().numpy()
         finally:
             L.lib().amgt_csr_free(ctypes.byref(c), None)
-        return sp.csr_matrix((a, ja, ia), shape=(c.num_rows, c.num_cols))
+        return sp.csr_matrix((a, ja, ia), shape=shape)
 
     def setup_times(self):
         ms = (ctypes.c_double * 4)()

@@ -33,7 +33,11 @@ def test_matches_the_recorded_hypre_run(amgt, orc, dims, its, rel, levels, oc):
     from amgt_b200 import boomer
 
     A = orc.laplacian(*dims)
-    S = boomer.BoomerSolver(to_dev(A))
+    amgt.set_level_policy([0])  # every level fp64 (the library's default table is AmgT's mixed one)
+    try:
+        S = boomer.BoomerSolver(to_dev(A))
+    finally:
+        amgt.set_level_policy([])
     try:
         assert S.num_levels() == levels
         if oc is not None:
@@ -75,7 +79,7 @@ def test_device_levels_follow_the_sorted_restatement(amgt, orc):
 
     A = orc.laplacian(96, 80, 1)
     _, As = boomer.host_hierarchy(A.to_scipy(), boomer.params())
-    S = boomer.BoomerSolver(to_dev(A), levels="device")
+    S = boomer.BoomerSolver(to_dev(A), levels="device", precs=(amgt.DOUBLE,))
     try:
         assert [S.level(l)["rows"] for l in range(S.num_levels())] == [a.shape[0] for a in As]
         b = torch.from_numpy(boomer.ij_random_rhs(A.m)).cuda()
