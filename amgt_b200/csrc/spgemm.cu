@@ -822,6 +822,285 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
     }
 }
 
+// ------------------------------------------------------- gathered numeric
+// The numeric phase by C block: every C block gathers its own ordered list
+// of (A block, B block) pairs, so that the work spreads over all C blocks
+// of the product whatever the row lengths (a few long rows of a coarse
+// level no longer serialise on a few warps), and no two lanes ever add to
+// the same C value (no ordering rounds).  Two kernels:
+//   order   one warp per A block row moves the row's sorted pattern into C
+//           and sorts the row's pairs by C block, stably (pair order = A
+//           block order), into the row's scratch slice: glist[gbeg[c] ..
+//           gbeg[c] + gnum[c]) lists C block c's pairs in the order the
+//           sequential product adds them.  Rows of at most kSymCap C
+//           blocks: a flattened pass over 32 pairs at a time with
+//           shared-memory counters, equal C blocks of a step ranked in lane
+//           order; each pair's C block is the symbolic pass's pair slot
+//           (rows of at most kSymCap pairs) or a search of the row's sorted
+//           pattern copied to shared memory.  Rows of more C blocks go one A
+//           block at a time (the B blocks of one A block hit distinct C
+//           blocks), with the counters in gnum.
+//   Used for products of fewer than 64 A block rows per SM (the coarse
+//   levels, whose few long rows leave the staged kernel's warps idle); the
+//   staged kernel keeps the others.
+//   gather  four lanes per C block (lane r: row r), each pair's A row and
+//           B block read from global memory (L1 / L2), the product entry the
+//           same fused chain as the staged kernel, the products added in
+//           list order: C equals the staged kernel's result bit for bit.
+// Writes C's values (+ shadow, + the fused exactness bits); the CSR form,
+// when wanted, comes from spgemm_csr_kernel.
+__global__ void __launch_bounds__(32 * kNumWarps)
+spgemm_order_kernel(int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
+                    const int *__restrict__ bptr, const int *__restrict__ bidx, const int *__restrict__ cptr,
+                    int *__restrict__ cidx, uint16_t *__restrict__ cmap, const int64_t *__restrict__ ub_off,
+                    const int *__restrict__ skey, const uint16_t *__restrict__ smap,
+                    const uint16_t *__restrict__ pslot, int2 *__restrict__ glist, long long *__restrict__ gbeg,
+                    int *__restrict__ gnum)
+{
+    __shared__ int cnt_s[kNumWarps][kSymCap];
+    __shared__ int key_s[kNumWarps][kSymCap];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int *cnt = cnt_s[warp], *keys = key_s[warp];
+    for (int b = blockIdx.x * kNumWarps + warp; b < brA; b += gridDim.x * kNumWarps) {
+        const int c0 = cptr[b], cn = cptr[b + 1] - c0;
+        const long long sbase = ub_off[b], npairs = ub_off[b + 1] - sbase;
+        for (int t = lane; t < cn; t += 32) {
+            cidx[c0 + t] = skey[sbase + t];
+            cmap[c0 + t] = smap[sbase + t];
+        }
+        const int a0 = aptr[b], a1 = aptr[b + 1];
+        const bool direct = npairs <= kSymCap;  // pair slots from the symbolic pass
+        if (cn <= kSymCap) {
+            for (int t = lane; t < cn; t += 32) {
+                cnt[t] = 0;
+                if (!direct) keys[t] = skey[sbase + t];
+            }
+            __syncwarp();
+            // pass 0 counts, pass 1 places; pairs enumerated in row order
+            for (int pass = 0; pass < 2; ++pass) {
+                long long qbase = sbase;
+                for (int ib = a0; ib < a1; ib += 32) {
+                    int j0 = 0, len = 0;
+                    if (ib + lane < a1) {
+                        const int k = aidx[ib + lane];
+                        j0 = bptr[k];
+                        len = bptr[k + 1] - j0;
+                    }
+                    int total;
+                    const int excl = warp_excl_scan(len, lane, &total);
+                    for (int q0 = 0; q0 < total; q0 += 32) {
+                        const int q = q0 + lane;
+                        // the A block of pair q: the last lane whose first pair is <= q
+                        // (every lane searches, so that the shuffles are uniform)
+                        int src = 0;
+#pragma unroll
+                        for (int st = 16; st > 0; st >>= 1) {
+                            const int e = __shfl_sync(FULL, excl, src + st);
+                            if (e <= q) src += st;
+                        }
+                        const int sj0 = __shfl_sync(FULL, j0, src), sex = __shfl_sync(FULL, excl, src);
+                        int t = -1;
+                        if (q < total) {
+                            if (direct) {
+                                const unsigned short ps = pslot[qbase + q];
+                                t = ps < cn ? (int)ps : -1;
+                            } else {  // the pair's C block from the row's sorted pattern
+                                const int key = bidx[sj0 + (q - sex)];
+                                int lo = 0, hi = cn - 1;
+                                while (lo < hi) {
+                                    const int mid = (lo + hi) >> 1;
+                                    if (keys[mid] < key) lo = mid + 1;
+                                    else hi = mid;
+                                }
+                                t = (cn > 0 && keys[lo] == key) ? lo : -1;
+                            }
+                        }
+                        if (pass == 0) {
+                            if (t >= 0) atomicAdd(&cnt[t], 1);
+                        } else {
+                            const unsigned peers = __match_any_sync(FULL, t >= 0 ? t : -1 - lane);
+                            if (t >= 0) {
+                                const int rank = __popc(peers & lanemask_lt(lane));
+                                glist[sbase + cnt[t] + rank] = make_int2(ib + src, sj0 + (q - sex));
+                            }
+                            __syncwarp();
+                            if (t >= 0 && (peers & lanemask_lt(lane)) == 0) cnt[t] += __popc(peers);
+                        }
+                        __syncwarp();
+                    }
+                    qbase += total;
+                }
+                __syncwarp();
+                if (pass == 0) {  // counts -> list starts (cnt then runs from the start)
+                    int carry = 0;
+                    for (int t0 = 0; t0 < cn; t0 += 32) {
+                        const int t = t0 + lane;
+                        const int c = t < cn ? cnt[t] : 0;
+                        int tot;
+                        const int off = warp_excl_scan(c, lane, &tot) + carry;
+                        if (t < cn) {
+                            gbeg[c0 + t] = sbase + off;
+                            gnum[c0 + t] = c;
+                            cnt[t] = off;
+                        }
+                        carry += tot;
+                    }
+                    __syncwarp();
+                }
+            }
+        } else {
+            // a row of more than kSymCap C blocks: one A block at a time,
+            // counters in gnum (cleared by the caller)
+            for (int pass = 0; pass < 2; ++pass) {
+                for (int i = a0; i < a1; ++i) {
+                    const int k = aidx[i];
+                    for (int j = bptr[k] + lane; j < bptr[k + 1]; j += 32) {
+                        const int key = bidx[j];
+                        const int tt = search_sorted(skey + sbase, cn, key);
+                        if (tt < cn && skey[sbase + tt] == key) {
+                            if (pass == 0) {
+                                atomicAdd(&gnum[c0 + tt], 1);
+                            } else {
+                                glist[gbeg[c0 + tt] + gnum[c0 + tt]] = make_int2(i, j);
+                                gnum[c0 + tt] += 1;  // the B blocks of one A block hit distinct C blocks
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+                __syncwarp();
+                if (pass == 0) {
+                    long long carry = sbase;
+                    for (int t0 = 0; t0 < cn; t0 += 32) {
+                        const int t = t0 + lane;
+                        const int c = t < cn ? gnum[c0 + t] : 0;
+                        int tot;
+                        const int off = warp_excl_scan(c, lane, &tot);
+                        if (t < cn) {
+                            gbeg[c0 + t] = carry + off;
+                            gnum[c0 + t] = 0;
+                        }
+                        carry += tot;
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+    }
+}
+
+// One block row (four values) of a stored block, widened to the
+// accumulator type, through the read-only path.
+template <int PREC>
+__device__ __forceinline__ void row4_ldg(const typename NumT<PREC>::val_t *p, typename NumT<PREC>::acc_t out[4])
+{
+    if constexpr (PREC == AMGT_DOUBLE) {
+        const double2 u = __ldg(reinterpret_cast<const double2 *>(p)), w = __ldg(reinterpret_cast<const double2 *>(p) + 1);
+        out[0] = u.x; out[1] = u.y; out[2] = w.x; out[3] = w.y;
+    } else if constexpr (PREC == AMGT_FLOAT) {
+        const float4 u = __ldg(reinterpret_cast<const float4 *>(p));
+        out[0] = u.x; out[1] = u.y; out[2] = u.z; out[3] = u.w;
+    } else {
+        const uint2 u = __ldg(reinterpret_cast<const uint2 *>(p));
+        const typename NumT<PREC>::val_t *v = reinterpret_cast<const typename NumT<PREC>::val_t *>(&u);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) out[q] = NumT<PREC>::ld(v, q);
+    }
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(256)
+spgemm_gather_kernel(int nbC, const typename NumT<PREC>::val_t *__restrict__ aval,
+                     const typename NumT<PREC>::val_t *__restrict__ bval, const int2 *__restrict__ glist,
+                     const long long *__restrict__ gbeg, const int *__restrict__ gnum, double *__restrict__ cval,
+                     void *__restrict__ cshadow, unsigned long long *__restrict__ cflags)
+{
+    using T = NumT<PREC>;
+    using acc_t = typename T::acc_t;
+    const int r = threadIdx.x & 3;
+    bool not32 = false, not16 = false;
+    const long long g0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 2;
+    const long long gstride = ((long long)gridDim.x * blockDim.x) >> 2;
+    for (long long g = g0; g < nbC; g += gstride) {
+        const long long beg = gbeg[g];
+        const int n = gnum[g];
+        acc_t acc[4] = {(acc_t)0, (acc_t)0, (acc_t)0, (acc_t)0};
+        for (int k = 0; k < n; ++k) {
+            const int2 pr = __ldg(glist + beg + k);
+            acc_t ar[4], s[4];
+            row4_ldg<PREC>(aval + 16LL * pr.x + 4 * r, ar);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                acc_t bk[4];
+                row4_ldg<PREC>(bval + 16LL * pr.y + 4 * kk, bk);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) s[c] = T::madd(ar[kk], bk[c], s[c], kk == 0);
+            }
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[c] = T::add(acc[c], s[c]);
+        }
+        double *d = cval + 16 * g + 4 * r;
+        reinterpret_cast<double2 *>(d)[0] = make_double2((double)acc[0], (double)acc[1]);
+        reinterpret_cast<double2 *>(d)[1] = make_double2((double)acc[2], (double)acc[3]);
+        if constexpr (PREC == AMGT_DOUBLE) {
+            if (cshadow) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const __half hv = __double2half(acc[c]);
+                    static_cast<__half *>(cshadow)[16 * g + 4 * r + c] = hv;
+                    if ((double)__double2float_rn(acc[c]) != acc[c]) not32 = true;
+                    if ((double)__half2float(hv) != acc[c]) not16 = true;
+                }
+            }
+        } else if (cshadow) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) store_shadow<PREC>(cshadow, 16 * g + 4 * r + c, acc[c]);
+        }
+    }
+    if (PREC == AMGT_DOUBLE && cshadow) {
+        const unsigned b32 = __ballot_sync(FULL, not32), b16 = __ballot_sync(FULL, not16);
+        if ((threadIdx.x & 31) == 0 && (b32 | b16)) atomicOr(cflags, (b32 ? 1ull : 0ull) | (b16 ? 2ull : 0ull));
+    }
+}
+
+// CSR form of C from its blocks: one warp per block row, scalar row by
+// scalar row, entries in ascending column order.
+__global__ void __launch_bounds__(32 * kNumWarps)
+spgemm_csr_kernel(int m, int brA, const int *__restrict__ cptr, const int *__restrict__ cidx,
+                  const uint16_t *__restrict__ cmap, const double *__restrict__ cval, const int *__restrict__ csr_i,
+                  int *__restrict__ csr_j, double *__restrict__ csr_a)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int b = blockIdx.x * kNumWarps + warp; b < brA; b += gridDim.x * kNumWarps) {
+        const int c0 = cptr[b], cn = cptr[b + 1] - c0;
+        for (int qr = 0; qr < 4 && 4 * b + qr < m; ++qr) {
+            int out = csr_i[4 * b + qr];
+            for (int tt = 0; tt < cn; tt += 32) {
+                const int t = tt + lane;
+                uint32_t nib = 0;
+                int col0 = 0;
+                if (t < cn) {
+                    nib = (cmap[c0 + t] >> (4 * qr)) & 0xFu;
+                    col0 = 4 * cidx[c0 + t];
+                }
+                int tot;
+                const int off = warp_excl_scan(__popc(nib), lane, &tot);
+                if (nib) {
+                    int o = out + off;
+#pragma unroll
+                    for (int cc = 0; cc < 4; ++cc)
+                        if (nib & (1u << cc)) {
+                            csr_j[o] = col0 + cc;
+                            csr_a[o] = cval[16LL * (c0 + t) + 4 * qr + cc];
+                            ++o;
+                        }
+                }
+                out += tot;
+            }
+        }
+    }
+}
+
 template <int PREC>
 static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B, const void *bval, amgt_bsr *C,
                           void *cshadow, amgt_csr *Ccsr, const int64_t *ub_off, const int *skey,
@@ -886,6 +1165,8 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     uint16_t *smap = nullptr, *pslot = nullptr;  // scratch: pattern, per-pair C block
     const int64_t *h = nullptr;
     int nbC = 0, nnzC = 0;
+    long long cap = 0;  // scratch capacity in pairs
+    unsigned char *arena3 = nullptr;  // gathered numeric: pair lists and their starts / lengths
     void *cshadow = nullptr;
     if (prec != AMGT_DOUBLE) {
         if (!shadow_of(A, prec)) {
@@ -922,7 +1203,7 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     {
         // scratch size: the host-side bound nblk(A) * longest B row when it is
         // modest, else the exact total (one read-back)
-        long long cap = (B->max_blc_per_row > 0 || B->blc_num == 0)
+        cap = (B->max_blc_per_row > 0 || B->blc_num == 0)
                             ? (long long)A->blc_num * (long long)B->max_blc_per_row
                             : -1;
         if (cap < 0 || cap > (256LL << 20)) {
@@ -1002,6 +1283,49 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
         Ccsr->num_nonzeros = nnzC;
         if ((rc = alloc_n(&Ccsr->j, nnzC, s)) || (rc = alloc_n(&Ccsr->data, nnzC, s))) goto fail;
     }
+    // products of few A block rows (coarse levels, long rows): the gathered
+    // numeric; others: the staged one, whose warp-per-row layout keeps every
+    // SM busy there and reads each A row once (both give the same C bit for bit)
+    if (brA < 64 * st->sm_count) {
+        const size_t o_beg = align256(8 * (size_t)cap), o_num = o_beg + align256(8 * (size_t)nbC + 8),
+                     o_end = o_num + align256(4 * (size_t)nbC + 4);
+        if ((rc = alloc_n(&arena3, o_end, s))) goto fail;
+        int2 *glist = reinterpret_cast<int2 *>(arena3);
+        long long *gbeg = reinterpret_cast<long long *>(arena3 + o_beg);
+        int *gnum = reinterpret_cast<int *>(arena3 + o_num);
+        if (brA > 0) {
+            AMGT_CUDA_TRY(cudaMemsetAsync(gnum, 0, 4 * (size_t)nbC + 4, s));
+            AMGT_LAUNCH(spgemm_order_kernel, grid_for(kNumWarps, brA, st->sm_count, 8), 32 * kNumWarps, 0, s, brA,
+                        A->blcPtr, A->blcIdx, B->blcPtr, B->blcIdx, C->blcPtr, C->blcIdx, C->blcMap, ub_off, skey,
+                        smap, pslot, glist, gbeg, gnum);
+        }
+        if (nbC > 0) {
+            const long long want = (4LL * nbC + 255) / 256;
+            const int grid = (int)std::min<long long>(want, 16LL * st->sm_count);
+            unsigned long long *flags = fuse ? reinterpret_cast<unsigned long long *>(fuse->flags) : nullptr;
+            switch (prec) {
+            case AMGT_DOUBLE:
+                AMGT_LAUNCH(spgemm_gather_kernel<AMGT_DOUBLE>, grid, 256, 0, s, nbC, A->blcVal, B->blcVal, glist,
+                            gbeg, gnum, C->blcVal, cshadow, flags);
+                break;
+            case AMGT_FLOAT:
+                AMGT_LAUNCH(spgemm_gather_kernel<AMGT_FLOAT>, grid, 256, 0, s, nbC, Atmp.blcVal_fp32,
+                            Btmp.blcVal_fp32, glist, gbeg, gnum, C->blcVal, cshadow, nullptr);
+                break;
+            case AMGT_HALF:
+                AMGT_LAUNCH(spgemm_gather_kernel<AMGT_HALF>, grid, 256, 0, s, nbC, (const __half *)Atmp.blcVal_fp16,
+                            (const __half *)Btmp.blcVal_fp16, glist, gbeg, gnum, C->blcVal, cshadow, nullptr);
+                break;
+            default:
+                AMGT_LAUNCH(spgemm_gather_kernel<AMGT_BF16>, grid, 256, 0, s, nbC,
+                            (const __nv_bfloat16 *)Atmp.blcVal_bf16, (const __nv_bfloat16 *)Btmp.blcVal_bf16, glist, gbeg, gnum, C->blcVal, cshadow, nullptr);
+                break;
+            }
+        }
+        if (Ccsr && brA > 0)
+            AMGT_LAUNCH(spgemm_csr_kernel, grid_for(kNumWarps, brA, st->sm_count, 8), 32 * kNumWarps, 0, s, m, brA,
+                        C->blcPtr, C->blcIdx, C->blcMap, C->blcVal, Ccsr->i, Ccsr->j, Ccsr->data);
+    } else
     switch (prec) {
     case AMGT_DOUBLE:
         rc = launch_numeric<AMGT_DOUBLE>(A, A->blcVal, B, B->blcVal, C, cshadow, Ccsr, ub_off, skey, smap, pslot, s,
@@ -1024,12 +1348,12 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     if (rc) goto fail;
     C->csr_nnz = nnzC;
     C->avg_nnz = nbC ? (double)nnzC / nbC : 0.0;
-    free_ptr(arena, s); free_ptr(arena2, s); free_ptr(csr_tmp, s);
+    free_ptr(arena, s); free_ptr(arena2, s); free_ptr(arena3, s); free_ptr(csr_tmp, s);
     if (ownA) { free_ptr(Atmp.blcVal_fp32, s); free_ptr(Atmp.blcVal_fp16, s); free_ptr(Atmp.blcVal_bf16, s); }
     if (ownB) { free_ptr(Btmp.blcVal_fp32, s); free_ptr(Btmp.blcVal_fp16, s); free_ptr(Btmp.blcVal_bf16, s); }
     return AMGT_OK;
 fail:
-    free_ptr(arena, s); free_ptr(arena2, s); free_ptr(csr_tmp, s);
+    free_ptr(arena, s); free_ptr(arena2, s); free_ptr(arena3, s); free_ptr(csr_tmp, s);
     if (ownA) { free_ptr(Atmp.blcVal_fp32, s); free_ptr(Atmp.blcVal_fp16, s); free_ptr(Atmp.blcVal_bf16, s); }
     if (ownB) { free_ptr(Btmp.blcVal_fp32, s); free_ptr(Btmp.blcVal_fp16, s); free_ptr(Btmp.blcVal_bf16, s); }
     amgt_bsr_free(C, stream);

@@ -51,10 +51,27 @@ def _pair(orc, kind):
         A = orc.box(13, 12, 11)
         A2 = orc.bsr2csr(orc.spgemm(orc.csr2bsr(A), orc.csr2bsr(A))[0])
         return A, A2
+    if kind == "AP_7pt_large":
+        # enough A block rows (> 64 per SM) for the staged warp-per-row numeric
+        A = orc.laplacian(48, 40, 40)
+        P, _ = orc.interp(48, 40, 40)
+        return A, P
+    if kind == "WIDE_row":
+        # a dense first row: > 1024 C blocks in one row (the gathered numeric's
+        # A-block-at-a-time ordering)
+        rng = np.random.default_rng(7)
+        n = 5000
+        rows = [np.arange(n)] + [np.unique(rng.integers(0, n, 5)) for _ in range(15)]
+        ia = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int32)
+        ja = np.concatenate(rows).astype(np.int32)
+        A = orc.CSR(16, n, ia, ja, rng.uniform(-1, 1, ja.size))
+        T = orc.laplacian(n, 1, 1)
+        B = orc.CSR(T.m, T.n, T.ia, T.ja, rng.uniform(-1, 1, T.ja.size))
+        return A, B
     raise KeyError(kind)
 
 
-KINDS = ["AP_7pt", "AP_varcoef27", "RAP_varcoef27", "AA_varcoef27", "AA_5pt", "AAA_27pt"]
+KINDS = ["AP_7pt", "AP_varcoef27", "RAP_varcoef27", "AA_varcoef27", "AA_5pt", "AAA_27pt", "AP_7pt_large", "WIDE_row"]
 
 
 @pytest.mark.parametrize("kind", KINDS)
