@@ -202,6 +202,8 @@ def _solver_class():
                                "coarse": int(As[l + 1].shape[0]) if l + 1 < len(As) else None}
                               for l in range(len(As))]
                 dev = a.device
+                for P in Ps:  # same operator; sorted rows take the conversion's merge path
+                    P.sort_indices()
                 Pd = [(P.shape[0], P.shape[1], torch.from_numpy(P.indptr.astype(np.int32)).to(dev),
                        torch.from_numpy(P.indices.astype(np.int32)).to(dev), torch.from_numpy(P.data).to(dev))
                       for P in Ps]

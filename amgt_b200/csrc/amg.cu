@@ -674,7 +674,7 @@ void destroy_handle(amgt_amg *h, cudaStream_t s)
     free_ptr(h->q, s);
     free_ptr(h->scal, s);
     free_ptr(h->part, s);
-    if (h->pinned) cudaFreeHost(h->pinned);
+    pinned_put(h->pinned);
     delete h;
 }
 
@@ -1481,7 +1481,11 @@ int amgt::amg_setup_blocks(const amgt_csr *A, int num_interp, const amgt_csr *P,
     // every host read-back slot of the solvers in one pinned block, so that
     // no solve allocates: 8 scalars, the multi-right-hand-side solve's 160,
     // and the loop's iteration count and max_iter + 1 residual norms
-    AMGT_CUDA_TRY(cudaMallocHost(&h->pinned, sizeof(double) * (8 + 160 + (size_t)h->prm.max_iter + 2)));
+    {
+        void *pb = nullptr;
+        if ((rc = pinned_get(sizeof(double) * (8 + 160 + (size_t)h->prm.max_iter + 2), &pb))) goto fail;
+        h->pinned = static_cast<double *>(pb);
+    }
     h->mr_pinned = h->pinned + 8;
     h->loop_pinned = h->pinned + 168;
     free_ptr(xflags, s);

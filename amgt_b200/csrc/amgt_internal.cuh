@@ -197,6 +197,11 @@ int exclusive_scan_i64(const int64_t *in, int64_t *out, int n, cudaStream_t s);
 // returns a pointer to the pinned slots (valid until the thread's next
 // read_back on the device).
 int read_back(const int64_t *dev, int count, cudaStream_t s, const int64_t **host);
+// Pinned host blocks for the handles' read-back slots, from a library cache
+// reused across handles (cudaMallocHost only on a miss); pinned_put returns
+// a block to the cache, amgt_trim_pool frees the cached ones.
+int pinned_get(size_t bytes, void **out);
+void pinned_put(void *p);
 
 // ----------------------------------------------------------------- bitmaps
 // Boolean 4x4 product of two block bitmaps (bit r*4+c = entry (r, c)): OR

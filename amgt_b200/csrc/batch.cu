@@ -198,7 +198,7 @@ void free_batch(Batch *b, cudaStream_t s)
     free_ptr(b->scal, s);
     free_ptr(b->part, s);
     free_ptr(b->cnt, s);
-    if (b->pinned) cudaFreeHost(b->pinned);
+    pinned_put(b->pinned);
     delete b;
 }
 
@@ -407,7 +407,7 @@ int amgt_batch_setup(int nsys, const amgt_csr *A, const int *nlev, const amgt_cs
         cudaMemcpyAsync(b->sys_tile, stile.data(), sizeof(int) * stile.size(), cudaMemcpyHostToDevice, s) !=
             cudaSuccess ||
         cudaMemsetAsync(b->scal, 0, sizeof(double) * BS_NSLOT * nsys, s) != cudaSuccess ||
-        cudaMallocHost(&b->pinned, sizeof(double) * (3 * (size_t)nsys + 4)) != cudaSuccess) {
+        pinned_get(sizeof(double) * (3 * (size_t)nsys + 4), reinterpret_cast<void **>(&b->pinned)) != AMGT_OK) {
         cudaGetLastError();
         free_batch(b, s);
         amgt_amg_destroy(h, stream);

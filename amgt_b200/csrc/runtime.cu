@@ -3,6 +3,7 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -252,6 +253,51 @@ static int staging(int64_t **out)
     return AMGT_OK;
 }
 
+// The handles' pinned read-back blocks.  cudaMallocHost can take
+// milliseconds in a process that already holds much pinned or device
+// memory -- longer than a whole setup's work on the coarse levels -- so
+// blocks are kept when a handle is destroyed and handed to the next one of
+// a fitting size; they stay until amgt_trim_pool or exit.
+static std::mutex g_pin_mu;
+static std::multimap<size_t, void *> g_pin_free;       // cached, by size
+static std::unordered_map<void *, size_t> g_pin_size;  // every block made here
+
+int pinned_get(size_t bytes, void **out)
+{
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    auto it = g_pin_free.lower_bound(bytes);
+    if (it != g_pin_free.end() && it->first <= 4 * bytes + 4096) {
+        *out = it->second;
+        g_pin_free.erase(it);
+        return AMGT_OK;
+    }
+    const size_t sz = (bytes + 4095) & ~(size_t)4095;
+    void *p = nullptr;
+    AMGT_CUDA_TRY(cudaMallocHost(&p, sz));
+    g_pin_size[p] = sz;
+    *out = p;
+    return AMGT_OK;
+}
+
+void pinned_put(void *p)
+{
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    auto s = g_pin_size.find(p);
+    if (s == g_pin_size.end()) return;  // not a block of this cache
+    g_pin_free.emplace(s->second, p);
+}
+
+static void pinned_trim()
+{
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    for (auto &kv : g_pin_free) {
+        g_pin_size.erase(kv.second);
+        cudaFreeHost(kv.second);
+    }
+    g_pin_free.clear();
+}
+
 int check_device_error(cudaStream_t s)
 {
     DeviceState *st;
@@ -424,6 +470,7 @@ int amgt_trim_pool(size_t keep_bytes)
     AMGT_CUDA_TRY(cudaGetDevice(&dev));
     flush_cache(dev);
     AMGT_CUDA_TRY(cudaDeviceSynchronize());
+    pinned_trim();
     AMGT_CUDA_TRY(cudaMemPoolTrimTo(pool, keep_bytes));
     return AMGT_OK;
 }

@@ -519,6 +519,8 @@ def boomer_report(amgt, torch, A_host, grid, cpu: bool):
     m, n, ia, ja, a = A_host
     t0 = time.perf_counter()
     Ps, As = boomer.hypre_hierarchy(sp.csr_matrix((a, ja, ia), shape=(m, n)))
+    for P in Ps:  # same operator; sorted rows take the conversion's merge path
+        P.sort_indices()
     host_s = time.perf_counter() - t0
     Ps_host = [(P.shape[0], P.shape[1], P.indptr.astype(np.int32), P.indices.astype(np.int32), P.data) for P in Ps]
     b_host = boomer.ij_random_rhs(m)

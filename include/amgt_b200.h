@@ -74,9 +74,10 @@ AMGT_API int amgt_kernel_arch(int *binary_version);
  * with hypre_TAlloc, R/seq_mv/csr_spgemm_device.c:1808-1839).  Exceptions,
  * all small and all pinned HOST memory from cudaMallocHost: each host
  * thread's 512-byte read-back staging per device (freed when the thread
- * exits), an AMG handle's read-back slots (8 * (max_iter + 170) bytes, one
- * block allocated by the setup and freed by amgt_amg_destroy) and a
- * batch's (8 * (3 * nsys + 4) bytes, amgt_batch_setup); the per-device
+ * exits), an AMG handle's read-back slots (8 * (max_iter + 170) bytes) and
+ * a batch's (8 * (3 * nsys + 4) bytes), each one block from a library cache
+ * of pinned blocks (taken by the setup, given back by amgt_amg_destroy,
+ * reused by later setups, freed by amgt_trim_pool); the per-device
  * error word (16 bytes, cudaMalloc, held until exit); and the fixed array of
  * amgt_spmv_segmented_noalloc.
  * Install or remove an allocator only while no other library call runs and
