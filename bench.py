@@ -572,6 +572,35 @@ def boomer_report(amgt, torch, A_host, grid, cpu: bool):
     return rep
 
 
+def boomer_setup_only(grid):
+    """Profiling captures: the BoomerAMG hierarchy of the 7-point operator
+    built on the host, then two fp64 setups on the GPU (the first loads
+    the modules); prints the second one's phase times."""
+    import scipy.sparse as sp
+    import torch
+
+    import amgt_b200 as amgt
+    from amgt_b200 import boomer, problems
+    from amgt_b200.amg import AmgSolver, default_params
+
+    m, n, ia, ja, a = problems.laplacian(*grid)
+    Ps, _ = boomer.hypre_hierarchy(sp.csr_matrix((a, ja, ia), shape=(m, n)))
+    dev = lambda *v: tuple(torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in v)  # noqa: E731
+    dPs = []
+    for P in Ps:
+        P.sort_indices()
+        dPs.append((P.shape[0], P.shape[1]) + dev(P.indptr.astype(np.int32), P.indices.astype(np.int32), P.data))
+    dA = (m, n) + dev(ia, ja, a)
+    amgt.set_level_policy([0])
+    for _ in range(2):
+        S = AmgSolver(dA, dPs, default_params())
+        torch.cuda.synchronize()
+        times = S.setup_times()
+        S.free()
+    amgt.set_level_policy([])
+    print(json.dumps({"boomer_setup_ms": {k: round(v, 3) for k, v in times.items()}}))
+
+
 def cpu_amg(grid, b_host):
     """The oracle's AMG-PCG (C, OpenMP, all host threads) on the same problem."""
     from oracle import oracle as orc
@@ -854,10 +883,15 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-policy report")
     ap.add_argument("--learned-seeds", type=int, default=20, help="held-out 128^3 problems in that report")
     ap.add_argument("--grid", type=int, default=128, help="cube side (profiling captures only)")
+    ap.add_argument("--boomer-setup-only", action="store_true",
+                    help="profiling captures only: one fp64 AMG setup on the BoomerAMG hierarchy of the --grid "
+                         "7-point operator (after one warm-up setup), no JSON line")
     args = ap.parse_args()
     global GRID
     GRID = (args.grid, args.grid, args.grid)
-    if args.impl == "reference":
+    if args.boomer_setup_only:
+        boomer_setup_only(GRID)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_amgt(args)
