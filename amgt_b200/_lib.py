@@ -103,6 +103,7 @@ SIGNATURES = {
     "amgt_pbsr_jacobi": (c_int, [P(AmgtPbsr), c_void_p, c_double, c_void_p, c_void_p, c_void_p, c_void_p]),
     "amgt_spmv_segmented_noalloc": (c_int, [c_int, c_double, P(AmgtBsr), c_void_p, c_double, c_void_p, c_void_p]),
     "amgt_spgemm": (c_int, [c_int, P(AmgtBsr), P(AmgtBsr), P(AmgtBsr), P(AmgtCsr), c_void_p]),
+    "amgt_spgemm_set_engine": (c_int, [c_int]),
     "amgt_amg_default_params": (None, [P(AmgtAmgParams)]),
     "amgt_amg_setup": (c_int, [P(AmgtCsr), c_int, P(AmgtCsr), P(AmgtAmgParams), P(c_void_p), c_void_p]),
     "amgt_amg_solve": (c_int, [c_void_p, c_void_p, c_void_p, P(c_int), P(c_double), c_void_p]),

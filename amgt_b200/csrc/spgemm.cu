@@ -35,6 +35,8 @@
 // arithmetic on the CUDA cores: the 4x4 products are too small for tcgen05
 // (M >= 64), and on B200 the fp64 MMA rate equals the fp64 FMA rate.  The
 // CSR form of C is written by the same kernel (no separate BSR2CSR pass).
+#include <atomic>
+
 #include "rowunion.cuh"
 
 namespace amgt {
@@ -1063,6 +1065,115 @@ spgemm_gather_kernel(int nbC, const typename NumT<PREC>::val_t *__restrict__ ava
     }
 }
 
+// Tensor-core form of the gathered numeric for fp16 / bf16 values
+// (amgt_spgemm_set_engine(AMGT_ENGINE_TENSOR_CORE)): one warp, four C
+// blocks, one mma.m16n8k16 per step with fp32 accumulation.  The four 4x4
+// products of a step (the k-th pair of each C block) sit block-diagonally
+// in the MMA: C block i's A block in rows 4i..4i+3, columns 4i..4i+3 of
+// the 16x16 A tile, its B block in rows 4i..4i+3, columns 0..3 of the 16x8
+// B tile, so rows 4i..4i+3, columns 0..3 of the accumulator are C block i
+// and the other products of the tile are zero terms (a quarter of the
+// tile's rows and half its columns carry data).  A C block with fewer pairs
+// takes zero blocks in the later steps.  Each entry is the tensor core's
+// sum of its products and the running fp32 value, in the tensor core's
+// order: not the sequential order of the CUDA-core form, so its parity is
+// a tolerance, not bit-exactness.
+template <int PREC>
+__device__ __forceinline__ uint32_t pack_pair_bits(uint16_t lo, uint16_t hi)
+{
+    return (uint32_t)lo | ((uint32_t)hi << 16);
+}
+
+template <int PREC>
+__device__ __forceinline__ void mma_16816(float d[4], const uint32_t a[4], const uint32_t b[2])
+{
+    if constexpr (PREC == AMGT_HALF) {
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+            "{%0,%1,%2,%3};\n"
+            : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+            : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+    } else {
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+            "{%0,%1,%2,%3};\n"
+            : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+            : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+    }
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(128)
+spgemm_gather_mma_kernel(int nbC, const uint16_t *__restrict__ aval, const uint16_t *__restrict__ bval,
+                         const int2 *__restrict__ glist, const long long *__restrict__ gbeg,
+                         const int *__restrict__ gnum, double *__restrict__ cval, void *__restrict__ cshadow)
+{
+    const int lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int ib = g >> 2, rr = g & 3, kk = (2 * t) & 3;
+    const bool aload = (t >> 1) == ib;  // this lane's A elements lie in the diagonal blocks
+    const int s0 = t >> 1, s1 = 2 + (t >> 1);
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; 4 * w < nbC; w += nwarps) {
+        const long long c0 = 4 * w;
+        // lane i < 4 holds C block c0 + i's list
+        long long beg = 0;
+        int n = 0;
+        if (lane < 4 && c0 + lane < nbC) {
+            beg = gbeg[c0 + lane];
+            n = gnum[c0 + lane];
+        }
+        int nmax = n;
+#pragma unroll
+        for (int o = 1; o < 4; o <<= 1) nmax = max(nmax, __shfl_xor_sync(FULL, nmax, o));
+        nmax = __shfl_sync(FULL, nmax, 0);
+        float d[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int k = 0; k < nmax; ++k) {
+            int2 p = make_int2(-1, -1);
+            if (lane < 4 && k < n) p = __ldg(glist + beg + k);
+            int px[4], py[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                px[i] = __shfl_sync(FULL, p.x, i);
+                py[i] = __shfl_sync(FULL, p.y, i);
+            }
+            uint32_t a[4] = {0u, 0u, 0u, 0u}, b[2] = {0u, 0u};
+            if (aload) {
+                if (px[ib] >= 0) a[0] = __ldg(reinterpret_cast<const uint32_t *>(aval + 16LL * px[ib] + 4 * rr + kk));
+                if (px[2 + ib] >= 0)
+                    a[3] = __ldg(reinterpret_cast<const uint32_t *>(aval + 16LL * px[2 + ib] + 4 * rr + kk));
+            }
+            if (g < 4) {
+                if (py[s0] >= 0) {
+                    const uint16_t *q = bval + 16LL * py[s0] + 4 * kk + g;
+                    b[0] = pack_pair_bits<PREC>(__ldg(q), __ldg(q + 4));
+                }
+                if (py[s1] >= 0) {
+                    const uint16_t *q = bval + 16LL * py[s1] + 4 * kk + g;
+                    b[1] = pack_pair_bits<PREC>(__ldg(q), __ldg(q + 4));
+                }
+            }
+            mma_16816<PREC>(d, a, b);
+        }
+        // rows g (C block ib) and g + 8 (C block 2 + ib), columns 2t, 2t + 1
+        if (t < 2) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const long long cb = c0 + (h ? 2 + ib : ib);
+                if (cb < nbC) {
+                    const long long o = 16 * cb + 4 * rr + 2 * t;
+                    cval[o] = (double)d[2 * h];
+                    cval[o + 1] = (double)d[2 * h + 1];
+                    if (cshadow) {
+                        store_shadow<PREC>(cshadow, o, d[2 * h]);
+                        store_shadow<PREC>(cshadow, o + 1, d[2 * h + 1]);
+                    }
+                }
+            }
+        }
+    }
+}
+
 // CSR form of C from its blocks: one warp per block row, scalar row by
 // scalar row, entries in ascending column order.
 __global__ void __launch_bounds__(32 * kNumWarps)
@@ -1134,6 +1245,9 @@ using namespace amgt;
 
 namespace amgt {
 
+// Engine of the fp16 / bf16 block products (amgt_spgemm_set_engine).
+static std::atomic<int> g_spgemm_engine{AMGT_ENGINE_AUTO};
+
 // amgt_spgemm with an optional host callback `between`, run after the
 // symbolic kernels are queued and before the host waits for C's size:
 // host work that can overlap them (the AMG setup converts the next
@@ -1166,6 +1280,8 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     const int64_t *h = nullptr;
     int nbC = 0, nnzC = 0;
     long long cap = 0;  // scratch capacity in pairs
+    const bool tensor =  // fp16 / bf16 block products on the tensor cores
+        g_spgemm_engine.load() == AMGT_ENGINE_TENSOR_CORE && (prec == AMGT_HALF || prec == AMGT_BF16);
     unsigned char *arena3 = nullptr;  // gathered numeric: pair lists and their starts / lengths
     void *cshadow = nullptr;
     if (prec != AMGT_DOUBLE) {
@@ -1285,8 +1401,10 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     }
     // products of few A block rows (coarse levels, long rows): the gathered
     // numeric; others: the staged one, whose warp-per-row layout keeps every
-    // SM busy there and reads each A row once (both give the same C bit for bit)
-    if (brA < 64 * st->sm_count) {
+    // SM busy there and reads each A row once (both give the same C bit for
+    // bit).  fp16 / bf16 products on the tensor-core engine: always the
+    // gathered form, its block products on the tensor cores.
+    if (brA < 64 * st->sm_count || tensor) {
         const size_t o_beg = align256(8 * (size_t)cap), o_num = o_beg + align256(8 * (size_t)nbC + 8),
                      o_end = o_num + align256(4 * (size_t)nbC + 4);
         if ((rc = alloc_n(&arena3, o_end, s))) goto fail;
@@ -1299,7 +1417,16 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
                         A->blcPtr, A->blcIdx, B->blcPtr, B->blcIdx, C->blcPtr, C->blcIdx, C->blcMap, ub_off, skey,
                         smap, pslot, glist, gbeg, gnum);
         }
-        if (nbC > 0) {
+        if (nbC > 0 && tensor) {
+            const long long want = (nbC + 15) / 16;  // 4 warps of 4 C blocks per CTA
+            const int grid = (int)std::min<long long>(want, 16LL * st->sm_count);
+            if (prec == AMGT_HALF)
+                AMGT_LAUNCH(spgemm_gather_mma_kernel<AMGT_HALF>, grid, 128, 0, s, nbC, Atmp.blcVal_fp16,
+                            Btmp.blcVal_fp16, glist, gbeg, gnum, C->blcVal, cshadow);
+            else
+                AMGT_LAUNCH(spgemm_gather_mma_kernel<AMGT_BF16>, grid, 128, 0, s, nbC, Atmp.blcVal_bf16,
+                            Btmp.blcVal_bf16, glist, gbeg, gnum, C->blcVal, cshadow);
+        } else if (nbC > 0) {
             const long long want = (4LL * nbC + 255) / 256;
             const int grid = (int)std::min<long long>(want, 16LL * st->sm_count);
             unsigned long long *flags = fuse ? reinterpret_cast<unsigned long long *>(fuse->flags) : nullptr;
@@ -1368,6 +1495,13 @@ extern "C" {
 int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amgt_csr *Ccsr, amgt_stream_t stream)
 {
     return amgt::spgemm_impl(prec, A, B, C, Ccsr, stream, nullptr, nullptr);
+}
+
+int amgt_spgemm_set_engine(int engine)
+{
+    if (engine < AMGT_ENGINE_AUTO || engine > AMGT_ENGINE_TENSOR_CORE) return AMGT_ERR_INVALID;
+    amgt::g_spgemm_engine.store(engine);
+    return AMGT_OK;
 }
 
 }  // extern "C"

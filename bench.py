@@ -527,6 +527,11 @@ def boomer_report(amgt, torch, A_host, grid, cpu: bool):
     f64 = amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, [0], 0, 0)
     mix = amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, MIXED_POLICY, 1, 1, galerkin=1)
     gir = amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, MIXED_POLICY, 1, 0, galerkin=1, **FGMRES_IR)
+    amgt.lib().amgt_spgemm_set_engine(2)  # fp16 Galerkin products of levels >= 3 on the tensor cores
+    try:
+        mtc = amg_setup_solve(amgt, torch, A_host, Ps_host, b_host, MIXED_POLICY, 1, 1, galerkin=1)
+    finally:
+        amgt.lib().amgt_spgemm_set_engine(0)
     nnz = [int(M.nnz) for M in As]
     rep = {"problem": f"3D 7-point Poisson {grid[0]}^3, b = ij -rhsrand (seed 22775, unit norm), BoomerAMG "
                       "settings: HMIS theta 0.25, ext+i P_max 4, l1-Jacobi V(1,1), tol 1e-8",
@@ -537,17 +542,19 @@ def boomer_report(amgt, torch, A_host, grid, cpu: bool):
                               "every form below",
            "reference_recorded": {"iters": 11, "relres": 2.411373e-09, "levels": 9, "operator_complexity": 3.27,
                                   "what": "HYPRE 2.31 CPU BoomerAMG from the AmgT tree, ij -rhsrand"}}
-    for name, rres in (("fp64", f64), ("mixed", mix), ("mixed_fgmres_ir", gir)):
+    for name, rres in (("fp64", f64), ("mixed", mix), ("mixed_fgmres_ir", gir), ("mixed_tensor_core_products", mtc)):
         rep[name] = {k: float(f"{rres[k]:.7g}") if isinstance(rres[k], float) else rres[k]
                      for k in ("setup_s", "solve_s", "iters", "relres", "relres_fp64_verified")}
         rep[name]["total_s"] = round(rres["setup_s"] + rres["solve_s"], 5)
         rep[name]["setup_ms"] = {k: round(v, 3) for k, v in rres["setup_ms"].items()}
-    for name, rres in (("mixed", mix), ("mixed_fgmres_ir", gir)):
+    for name, rres in (("mixed", mix), ("mixed_fgmres_ir", gir), ("mixed_tensor_core_products", mtc)):
         rep[name]["speedup_vs_fp64"] = round(rep["fp64"]["total_s"] / rep[name]["total_s"], 3)
         rep[name]["rel_err_vs_fp64_solution"] = float(
             torch.linalg.vector_norm(rres["x"] - f64["x"]) / torch.linalg.vector_norm(f64["x"]))
     rep["mixed"]["policy"] = "levels 0 fp64 (residual) / fp32 smoother, 1-2 fp32, >=3 fp16; flexible CG"
     rep["mixed_fgmres_ir"]["policy"] = FGMRES_IR_DESC
+    rep["mixed_tensor_core_products"]["policy"] = ("as mixed, with the fp16 Galerkin products (levels >= 3) on the "
+                                                   "tensor cores (amgt_spgemm_set_engine, mma.m16n8k16)")
     if cpu:
         from oracle import oracle as orc
 
@@ -572,10 +579,12 @@ def boomer_report(amgt, torch, A_host, grid, cpu: bool):
     return rep
 
 
-def boomer_setup_only(grid):
+def boomer_setup_only(grid, mixed: bool = False, engine: int = 0):
     """Profiling captures: the BoomerAMG hierarchy of the 7-point operator
-    built on the host, then two fp64 setups on the GPU (the first loads
-    the modules); prints the second one's phase times."""
+    built on the host, then two setups on the GPU (the first loads the
+    modules), fp64 or the mixed policy with Galerkin products at each
+    level's precision on the given SpGEMM engine; prints the second one's
+    phase times."""
     import scipy.sparse as sp
     import torch
 
@@ -591,12 +600,15 @@ def boomer_setup_only(grid):
         P.sort_indices()
         dPs.append((P.shape[0], P.shape[1]) + dev(P.indptr.astype(np.int32), P.indices.astype(np.int32), P.data))
     dA = (m, n) + dev(ia, ja, a)
-    amgt.set_level_policy([0])
+    amgt.set_level_policy(MIXED_POLICY if mixed else [0])
+    amgt.lib().amgt_spgemm_set_engine(engine)
+    prm = default_params(flexible=1, smooth_prec0=1, galerkin_by_level=1) if mixed else default_params()
     for _ in range(2):
-        S = AmgSolver(dA, dPs, default_params())
+        S = AmgSolver(dA, dPs, prm)
         torch.cuda.synchronize()
         times = S.setup_times()
         S.free()
+    amgt.lib().amgt_spgemm_set_engine(0)
     amgt.set_level_policy([])
     print(json.dumps({"boomer_setup_ms": {k: round(v, 3) for k, v in times.items()}}))
 
@@ -886,11 +898,15 @@ def main():
     ap.add_argument("--boomer-setup-only", action="store_true",
                     help="profiling captures only: one fp64 AMG setup on the BoomerAMG hierarchy of the --grid "
                          "7-point operator (after one warm-up setup), no JSON line")
+    ap.add_argument("--setup-mixed", action="store_true", help="with --boomer-setup-only: the mixed policy")
+    ap.add_argument("--spgemm-engine", type=int, default=0,
+                    help="with --boomer-setup-only: amgt_spgemm_set_engine (2: fp16 / bf16 products on the tensor "
+                         "cores)")
     args = ap.parse_args()
     global GRID
     GRID = (args.grid, args.grid, args.grid)
     if args.boomer_setup_only:
-        boomer_setup_only(GRID)
+        boomer_setup_only(GRID, args.setup_mixed, args.spgemm_engine)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -356,6 +356,16 @@ AMGT_API int amgt_spmv_segmented_noalloc(int prec, double alpha, const amgt_bsr 
  * Host-blocking twice (upper bound and C size). */
 AMGT_API int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C,
                 amgt_csr *Ccsr, amgt_stream_t stream);
+/* Engine of the HALF / BF16 block products of later amgt_spgemm calls (all
+ * threads; the reference multiplies dense A blocks on the tensor cores,
+ * numeric_spgemm_hybrid_f16, R/seq_mv/csr_spgemm_device.c:753-937):
+ * AMGT_ENGINE_AUTO / AMGT_ENGINE_CUDA_CORE (default): fp32 multiply and add
+ * in the sequential order, the same C bit for bit as the oracle;
+ * AMGT_ENGINE_TENSOR_CORE: mma.m16n8k16 with fp32 accumulation, four C
+ * blocks' 4x4 products per MMA (block-diagonal in the tile), sums in the
+ * tensor core's order (within about 1e-6 of |A||B| of the sequential
+ * result).  DOUBLE and FLOAT products are not affected. */
+AMGT_API int amgt_spgemm_set_engine(int engine);
 
 /* ------------------------------------------------ AMG setup + solve */
 /* Galerkin hierarchy on mBSR and a PCG solve preconditioned by one V(1,1)

@@ -85,6 +85,9 @@ def test_precision_policy_defaults_and_override():
     assert L.amgt_set_level_policy(bad, 1) == 1
     assert L.amgt_set_level_policy(None, 0) == 0
     assert [L.amgt_precision_for_level(l) for l in range(3)] == [0, 1, 2]
+    # the SpGEMM engine switch: AUTO / CUDA_CORE / TENSOR_CORE only
+    assert L.amgt_spgemm_set_engine(3) == 1 and L.amgt_spgemm_set_engine(-1) == 1
+    assert L.amgt_spgemm_set_engine(2) == 0 and L.amgt_spgemm_set_engine(0) == 0
 
 
 def test_invalid_arguments_are_rejected_without_a_device():

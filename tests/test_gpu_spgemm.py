@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 import torch
 
-from gpu_util import assert_bsr_equal, to_dev
+from gpu_util import assert_bsr_equal, bsr_host, to_dev
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
@@ -97,6 +97,36 @@ def test_spgemm_bit_exact(amgt, orc, kind, prec):
     assert GC.s.csr_nnz == Rc.nnz
     lens = np.diff(RC.bptr)
     assert GC.s.max_blc_per_row == lens.max()
+
+
+@pytest.mark.parametrize("kind", ["AP_7pt", "RAP_varcoef27", "AA_varcoef27", "AAA_27pt", "AP_7pt_large", "WIDE_row"])
+@pytest.mark.parametrize("prec", [2, 3])
+def test_spgemm_tensor_core_engine(amgt, orc, kind, prec):
+    """fp16 / bf16 block products on the tensor cores (mma.m16n8k16, fp32
+    accumulation, four C blocks per MMA): the pattern and bitmaps equal the
+    oracle's bit for bit; every value is within 1e-5 of (|A||B|) of the
+    oracle's sequential fp32 result on the same rounded values (the tensor
+    core sums in its own order); the CSR form carries the same values."""
+    A, B = _pair(orc, kind)
+    RA, RB = orc.csr2bsr(A), orc.csr2bsr(B)
+    RC, _ = orc.spgemm(RA, RB, prec=prec)
+    absA = orc.CSR(A.m, A.n, A.ia, A.ja, np.abs(A.a))
+    absB = orc.CSR(B.m, B.n, B.ia, B.ja, np.abs(B.a))
+    bound, _ = orc.spgemm(orc.csr2bsr(absA), orc.csr2bsr(absB), prec=0)
+    GA, GB = amgt.Bsr.from_csr(*to_dev(A)), amgt.Bsr.from_csr(*to_dev(B))
+    assert amgt.lib().amgt_spgemm_set_engine(2) == 0
+    try:
+        GC, csr = amgt.spgemm(GA, GB, prec=prec)
+    finally:
+        amgt.lib().amgt_spgemm_set_engine(0)
+    assert_bsr_equal(GC, RC, values=False)
+    got = bsr_host(GC)[3]
+    tol = 1e-5 * bound.bval + 1e-30
+    assert np.all(np.abs(got - RC.bval) <= tol), np.max(np.abs(got - RC.bval) / (bound.bval + 1e-300))
+    Rc = orc.bsr2csr(RC)
+    np.testing.assert_array_equal(csr.ja.cpu().numpy(), Rc.ja)
+    Gc = orc.bsr2csr(orc.BSR(GC.s.row, GC.s.col, *bsr_host(GC)))
+    np.testing.assert_array_equal(csr.a.cpu().numpy(), Gc.a)
 
 
 def test_spgemm_fp64_matches_scipy(amgt, orc):
