@@ -505,7 +505,7 @@ def learned_report(n_seeds: int):
     return out
 
 
-def boomer_report(amgt, torch, A_host, grid, cpu: bool):
+def boomer_report(amgt, torch, A_host, grid, cpu: bool, problem: str | None = None, recorded: bool = True):
     """The metric's setup + solve on its stated settings: BoomerAMG's HMIS
     (theta 0.25) + ext+i (P_max 4) hierarchy, built on the host as HYPRE's
     CPU setup builds it (amgt_boomer_hierarchy_host), then the GPU's
@@ -533,15 +533,17 @@ def boomer_report(amgt, torch, A_host, grid, cpu: bool):
     finally:
         amgt.lib().amgt_spgemm_set_engine(0)
     nnz = [int(M.nnz) for M in As]
-    rep = {"problem": f"3D 7-point Poisson {grid[0]}^3, b = ij -rhsrand (seed 22775, unit norm), BoomerAMG "
-                      "settings: HMIS theta 0.25, ext+i P_max 4, l1-Jacobi V(1,1), tol 1e-8",
+    rep = {"problem": (problem or f"3D 7-point Poisson {grid[0]}^3") + ", b = ij -rhsrand (seed 22775, unit norm), "
+                      "BoomerAMG settings: HMIS theta 0.25, ext+i P_max 4, l1-Jacobi V(1,1), tol 1e-8",
            "levels": [int(M.shape[0]) for M in As], "operator_complexity": round(sum(nnz) / nnz[0], 4),
            "host_coarsening_s": round(host_s, 3),
            "host_coarsening": "HMIS + ext+i + truncation + HYPRE-order Galerkin products on the host, one "
                               "thread (HYPRE 2.31 runs HMIS on the host in GPU builds too); the same P for "
                               "every form below",
-           "reference_recorded": {"iters": 11, "relres": 2.411373e-09, "levels": 9, "operator_complexity": 3.27,
-                                  "what": "HYPRE 2.31 CPU BoomerAMG from the AmgT tree, ij -rhsrand"}}
+           }
+    if recorded:
+        rep["reference_recorded"] = {"iters": 11, "relres": 2.411373e-09, "levels": 9, "operator_complexity": 3.27,
+                                     "what": "HYPRE 2.31 CPU BoomerAMG from the AmgT tree, ij -rhsrand"}
     for name, rres in (("fp64", f64), ("mixed", mix), ("mixed_fgmres_ir", gir), ("mixed_tensor_core_products", mtc)):
         rep[name] = {k: float(f"{rres[k]:.7g}") if isinstance(rres[k], float) else rres[k]
                      for k in ("setup_s", "solve_s", "iters", "relres", "relres_fp64_verified")}
@@ -829,6 +831,10 @@ def run_amgt(args):
         setup_solve["varcoef27_96"] = vc
         setup_solve["boomeramg_128"] = boomer_report(amgt, torch, A_host, GRID,
                                                      cpu=world == 1 and rank == 0 and not args.no_cpu)
+        # config 3's operator with the same settings (no recorded reference run)
+        setup_solve["boomeramg_varcoef27_96"] = boomer_report(
+            amgt, torch, V_host, vdims, cpu=False, recorded=False,
+            problem="3D 27-point variable-coefficient diffusion 96^3 (884,736 rows, 23.4 M nonzeros)")
         if world == 1 and rank == 0 and not args.no_cpu:
             setup_solve["cpu_oracle"], xo = cpu_amg(GRID, b_host)
             setup_solve["fp64"]["rel_err_vs_cpu_oracle"] = float(

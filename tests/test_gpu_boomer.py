@@ -88,3 +88,43 @@ def test_device_levels_follow_the_sorted_restatement(amgt, orc):
         assert _fp64_relres(A, x.cpu().numpy(), b.cpu().numpy()) <= 1e-8
     finally:
         S.free()
+
+
+def test_varcoef27_boomer_hierarchy_fp64_and_mixed(amgt, orc):
+    """Config 3's operator (27-point, log-normal coefficients) on BoomerAMG's
+    hierarchy: the GPU's fp64 PCG takes the oracle AMG-PCG's iterations on
+    the same interpolation operators with x within 1e-9; the mixed
+    FGMRES(30)-IR form reaches 1e-8 checked in fp64, x within 1e-6 of the
+    fp64 solution."""
+    from amgt_b200 import boomer
+    from amgt_b200.amg import AmgSolver, default_params
+
+    A = orc.varcoef27(26, 24, 22, seed=1)
+    Ps, _ = boomer.hypre_hierarchy(A.to_scipy())
+    Pc = []
+    for P in Ps:
+        P.sort_indices()
+        Pc.append(orc.CSR(P.shape[0], P.shape[1], P.indptr.astype(np.int32), P.indices.astype(np.int32), P.data))
+    bh = boomer.ij_random_rhs(A.m)
+    xo, ito, relo, _ = orc.Amg(A, Pc).solve(bh)
+    b = torch.from_numpy(bh).cuda()
+    amgt.set_level_policy([0])
+    try:
+        S = AmgSolver(to_dev(A), [to_dev(P) for P in Pc], default_params())
+        x, it, rel = S.solve(b)
+        S.free()
+    finally:
+        amgt.set_level_policy([])
+    assert it == ito and rel <= 1e-8
+    assert np.linalg.norm(x.cpu().numpy() - xo) <= 1e-9 * np.linalg.norm(xo)
+    amgt.set_level_policy([0, 1, 1, 2])
+    try:
+        prm = default_params(smooth_prec0=1, galerkin_by_level=1, solver=1, restart=30, inner_prec0=1,
+                             inner_tol=1e-4)
+        S = AmgSolver(to_dev(A), [to_dev(P) for P in Pc], prm)
+        xm, itm, relm = S.solve(b)
+        S.free()
+    finally:
+        amgt.set_level_policy([])
+    assert _fp64_relres(A, xm.cpu().numpy(), bh) <= 1e-8
+    assert np.linalg.norm(xm.cpu().numpy() - xo) <= 1e-6 * np.linalg.norm(xo)
