@@ -581,7 +581,7 @@ def boomer_report(amgt, torch, A_host, grid, cpu: bool, problem: str | None = No
     return rep
 
 
-def boomer_setup_only(grid, mixed: bool = False, engine: int = 0):
+def boomer_setup_only(grid, mixed: bool = False, engine: int = 0, operator: str = "7pt"):
     """Profiling captures: the BoomerAMG hierarchy of the 7-point operator
     built on the host, then two setups on the GPU (the first loads the
     modules), fp64 or the mixed policy with Galerkin products at each
@@ -594,7 +594,7 @@ def boomer_setup_only(grid, mixed: bool = False, engine: int = 0):
     from amgt_b200 import boomer, problems
     from amgt_b200.amg import AmgSolver, default_params
 
-    m, n, ia, ja, a = problems.laplacian(*grid)
+    m, n, ia, ja, a = problems.laplacian(*grid) if operator == "7pt" else problems.varcoef27(*grid, seed=1)
     Ps, _ = boomer.hypre_hierarchy(sp.csr_matrix((a, ja, ia), shape=(m, n)))
     dev = lambda *v: tuple(torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in v)  # noqa: E731
     dPs = []
@@ -905,6 +905,8 @@ def main():
                     help="profiling captures only: one fp64 AMG setup on the BoomerAMG hierarchy of the --grid "
                          "7-point operator (after one warm-up setup), no JSON line")
     ap.add_argument("--setup-mixed", action="store_true", help="with --boomer-setup-only: the mixed policy")
+    ap.add_argument("--operator", choices=["7pt", "27pt-varcoef"], default="7pt",
+                    help="with --boomer-setup-only: the 7-point operator or the 27-point variable-coefficient one")
     ap.add_argument("--spgemm-engine", type=int, default=0,
                     help="with --boomer-setup-only: amgt_spgemm_set_engine (2: fp16 / bf16 products on the tensor "
                          "cores)")
@@ -912,7 +914,7 @@ def main():
     global GRID
     GRID = (args.grid, args.grid, args.grid)
     if args.boomer_setup_only:
-        boomer_setup_only(GRID, args.setup_mixed, args.spgemm_engine)
+        boomer_setup_only(GRID, args.setup_mixed, args.spgemm_engine, args.operator)
     elif args.impl == "reference":
         run_reference(args)
     else:
