@@ -1280,6 +1280,8 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     const int64_t *h = nullptr;
     int nbC = 0, nnzC = 0;
     long long cap = 0;  // scratch capacity in pairs
+    int nlarge = 0;     // rows of more than kSymCap pairs
+    long long npairs = 0;  // (A block, B block) pairs of the product
     const bool tensor =  // fp16 / bf16 block products on the tensor cores
         g_spgemm_engine.load() == AMGT_ENGINE_TENSOR_CORE && (prec == AMGT_HALF || prec == AMGT_BF16);
     unsigned char *arena3 = nullptr;  // gathered numeric: pair lists and their starts / lengths
@@ -1318,11 +1320,13 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     if ((rc = exclusive_scan_i64(ub, ub_off, brA + 1, s))) goto fail;
     {
         // scratch size: the host-side bound nblk(A) * longest B row when it is
-        // modest, else the exact total (one read-back)
+        // modest (<= 32 Mi pairs, 256 MB of scratch), else the exact total
+        // (one read-back): a bound of gigabytes made the pool map and unmap
+        // memory inside the product
         cap = (B->max_blc_per_row > 0 || B->blc_num == 0)
                             ? (long long)A->blc_num * (long long)B->max_blc_per_row
                             : -1;
-        if (cap < 0 || cap > (256LL << 20)) {
+        if (cap < 0 || cap > (32LL << 20)) {
             AMGT_CUDA_TRY(cudaMemcpyAsync(&stats[2], ub_off + brA, sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
             if ((rc = read_back(stats, 4, s, &h))) goto fail;
             cap = h[2];
@@ -1346,7 +1350,7 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
         AMGT_LAUNCH((spgemm_symbolic_kernel<kSymCap, 2>), 6 * st->sm_count, 64, 0, s, m, brA, A->blcPtr,
                     A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, ccnt, csrcnt, large, stats, ub_off, skey,
                     smap, medium, nmedium, large, (int *)&stats[3], pslot, st->err);
-        AMGT_LAUNCH(spgemm_symbolic_large_kernel, 2 * st->sm_count, kSymLargeThreads, 0, s, m, A->blcPtr, A->blcIdx,
+        AMGT_LAUNCH(spgemm_symbolic_large_kernel, 6 * st->sm_count, kSymLargeThreads, 0, s, m, A->blcPtr, A->blcIdx,
                     A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, large, stats, ccnt, csrcnt, ub_off, skey, smap);
     }
     if ((rc = exclusive_scan_int(ccnt, C->blcPtr, brA + 1, s))) goto fail;
@@ -1366,8 +1370,12 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     if ((rc = exclusive_scan_int(csrcnt, csr_i, m + 1, s))) goto fail;
     AMGT_CUDA_TRY(cudaMemcpyAsync((int *)&stats[2] + 1, csr_i + m, sizeof(int), cudaMemcpyDeviceToDevice, s));
     if (between && (rc = between(ctx))) goto fail;
-    if ((rc = read_back(stats, 4, s, &h))) goto fail;
+    // the exact pair count rides along (it sizes the gathered numeric's lists)
+    AMGT_CUDA_TRY(cudaMemcpyAsync(&stats[4], ub_off + brA, sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
+    if ((rc = read_back(stats, 5, s, &h))) goto fail;
+    npairs = h[4];
     nbC = (int)(h[2] & 0xFFFFFFFF);
+    nlarge = (int)(h[3] & 0xFFFFFFFF);
     nnzC = (int)(h[2] >> 32);
     C->max_blc_per_row = (int)h[0];
     {
@@ -1399,13 +1407,14 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
         Ccsr->num_nonzeros = nnzC;
         if ((rc = alloc_n(&Ccsr->j, nnzC, s)) || (rc = alloc_n(&Ccsr->data, nnzC, s))) goto fail;
     }
-    // products of few A block rows (coarse levels, long rows): the gathered
-    // numeric; others: the staged one, whose warp-per-row layout keeps every
-    // SM busy there and reads each A row once (both give the same C bit for
-    // bit).  fp16 / bf16 products on the tensor-core engine: always the
+    // products of few A block rows (coarse levels), of more C blocks per
+    // row on average than the staged kernel accumulates in shared memory,
+    // or with many rows beyond kSymCap pairs: the gathered numeric; others:
+    // the staged one, whose warp-per-row layout keeps every SM busy on short
+    // rows and reads each A row once (both give the same C bit for bit).  fp16 / bf16 products on the tensor-core engine: always the
     // gathered form, its block products on the tensor cores.
-    if (brA < 64 * st->sm_count || tensor) {
-        const size_t o_beg = align256(8 * (size_t)cap), o_num = o_beg + align256(8 * (size_t)nbC + 8),
+    if (brA < 64 * st->sm_count || tensor || nbC > (long long)kNumCap * brA || 8LL * nlarge > brA) {
+        const size_t o_beg = align256(8 * (size_t)npairs), o_num = o_beg + align256(8 * (size_t)nbC + 8),
                      o_end = o_num + align256(4 * (size_t)nbC + 4);
         if ((rc = alloc_n(&arena3, o_end, s))) goto fail;
         int2 *glist = reinterpret_cast<int2 *>(arena3);
