@@ -843,8 +843,9 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
 //           block at a time (the B blocks of one A block hit distinct C
 //           blocks), with the counters in gnum.
 //   Used for products of fewer than 64 A block rows per SM (the coarse
-//   levels, whose few long rows leave the staged kernel's warps idle); the
-//   staged kernel keeps the others.
+//   levels, whose few long rows leave the staged kernel's warps idle), of
+//   more than 32 C blocks per row on average, or with more than an eighth
+//   of their rows beyond kSymCap pairs; the staged kernel keeps the others.
 //   gather  four lanes per C block (lane r: row r), each pair's A row and
 //           B block read from global memory (L1 / L2), the product entry the
 //           same fused chain as the staged kernel, the products added in
