@@ -352,7 +352,8 @@ AMGT_API int amgt_spmv_segmented_noalloc(int prec, double alpha, const amgt_bsr 
  * and added to C in A-row order.  FLOAT / HALF / BF16: A and B shadows
  * (built on demand), fp32 arithmetic, C values rounded to fp64 and a C
  * shadow of the same precision.  If Ccsr != NULL the CSR form of C
- * (BSR2CSR) is also written, fused into the numeric pass.
+ * (BSR2CSR) is also written, by the numeric pass itself (rows of few C
+ * blocks) or by a pass right after it.
  * Host-blocking twice (upper bound and C size). */
 AMGT_API int amgt_spgemm(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C,
                 amgt_csr *Ccsr, amgt_stream_t stream);
