@@ -211,3 +211,43 @@ def test_bad_arguments_are_rejected():
     assert lib.amgt_boomer_hierarchy_host(A.m, ia.ctypes.data, ja.ctypes.data, a.ctypes.data, ctypes.byref(bad), 25,
                                           9, ctypes.byref(h)) == 1
     assert not h.value
+
+
+def test_edge_cases():
+    """A 1-row matrix and a diagonal one have no strong couplings: no coarse
+    point, the hierarchy is the matrix alone; a matrix with positive
+    off-diagonal entries (weak by definition) coarsens by its negative ones
+    only; rows of P still sum as ext+i distributes them."""
+    lib = L.lib()
+    one = sp.csr_matrix(np.array([[2.0]]))
+    Ps, As = boomer.hypre_hierarchy(one)
+    assert Ps == [] and len(As) == 1
+    D = sp.diags(np.arange(1.0, 21.0)).tocsr()
+    Ps, As = boomer.hypre_hierarchy(D, max_coarse=2)
+    assert Ps == [] and len(As) == 1
+    P, cf = _level(D)
+    assert P.shape[1] == 0 and np.all(cf < 0)
+    # 1D Laplacian plus a positive long-range coupling in every row
+    n = 40
+    M = sp.diags([-np.ones(n - 1), 2.5 * np.ones(n), -np.ones(n - 1)], [-1, 0, 1]).tolil()
+    for i in range(n):
+        M[i, (i + 7) % n] = 0.1
+    M = M.tocsr()
+    M = (M + M.T) * 0.5
+    S = _strength(M)
+    for i in range(n):
+        assert all(M[i, j] < 0 for j in S[i])
+    P, cf = _level(M)
+    assert 0 < P.shape[1] < n
+    Ps, As = boomer.hypre_hierarchy(M, max_coarse=3)
+    assert [x.shape[0] for x in As] == [40, 20, 10, 5]  # 5 rows: every point C, coarsening stops
+    # bad sizes through the C ABI
+    h = ctypes.c_void_p()
+    ia = np.array([0, 1], np.int32)
+    ja = np.array([0], np.int32)
+    a = np.array([1.0])
+    assert lib.amgt_boomer_hierarchy_host(0, ia.ctypes.data, ja.ctypes.data, a.ctypes.data, None, 25, 9,
+                                          ctypes.byref(h)) == 1
+    bad_ja = np.array([3], np.int32)
+    assert lib.amgt_boomer_hierarchy_host(1, ia.ctypes.data, bad_ja.ctypes.data, a.ctypes.data, None, 25, 9,
+                                          ctypes.byref(h)) == 1
