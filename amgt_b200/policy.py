@@ -14,7 +14,7 @@ full coarsening does).  This is the place BoomerAMG's strength threshold
 
 Policies:
   FixedPolicy  theta and a precision table: the plain FP64 configuration
-               (theta 0.25, every level fp64) is the fallback and the judge;
+               (theta 0.25, every level fp64) is the fallback and the yardstick;
   MLPPolicy    the 16 -> 64 -> 64 -> 4 MLP (amgt_mlp_forward) on the level's
                features: theta = sigmoid(output 0), precision = argmax of
                outputs 1..3 (fp64 / fp32 / fp16); level 0 stays fp64 (its

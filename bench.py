@@ -491,7 +491,7 @@ def learned_report(n_seeds: int):
     against the plain FP64 configuration (theta 0.25, every level fp64) on
     held-out rotated anisotropic 128^3 problems (seeds 1,000,000 + k): setup
     (level by level through the coarsening callback) + solve to 1e-8, the
-    convergence factor as the judge; a learned solve that misses 1e-8 falls
+    convergence factor as the yardstick; a learned solve that misses 1e-8 falls
     back to fp64 and is charged both runs."""
     from amgt_b200 import policy
     from amgt_b200.train_policy import evaluate, summarize

@@ -147,7 +147,7 @@ def test_adaptive_setup_semicoarsens_the_strong_axis(amgt):
 def test_learned_policy_gains_over_the_plain_fp64_configuration(amgt):
     """The trained network (amgt_b200/data/policy_mlp.npy) against the method
     without it -- the plain FP64 configuration (theta 0.25, every level
-    fp64), which is also its fallback and its judge -- on held-out seeds
+    fp64), which is also its fallback and its yardstick -- on held-out seeds
     (40^3 here to keep the test short): every learned solve reaches 1e-8 in
     fp64 (checked again from x), its x agrees with the fp64 solution to
     1e-6, and the mean work (iterations x operator complexity) and mean
