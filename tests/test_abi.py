@@ -111,6 +111,15 @@ def test_mirror_matrix_create_destroy_host_only():
     assert h.contents.coasen_level == 3 and ord(h.contents.bsr_tag) == 0
     assert L.amgt_CSRMatrixDestroy(h) == 0
     assert not L.amgt_CSRMatrixCreate(-1, 8, 0, None, None, None, 0)
+    # BoomerAMG entry points: argument checks before any device work
+    A = _lib.AmgtBsr()
+    A.row, A.col = 8, 4  # not square
+    P = _lib.AmgtCsr()
+    assert L.amgt_boomer_interp(ctypes.byref(A), None, ctypes.byref(P), None, None) == 1
+    assert L.amgt_boomer_interp(None, None, ctypes.byref(P), None, None) == 1
+    assert L.amgt_boomer_hierarchy_levels(None) == 0
+    assert L.amgt_boomer_hierarchy_level(None, 0, None, None) == 1
+    assert L.amgt_boomer_free_host(None) == 1
 
 
 @pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES", None) == "", reason="explicitly hidden GPU")
