@@ -32,14 +32,28 @@ def params(theta: float = 0.25, max_row_sum: float = 1.0, p_max: int = 4, coarse
 
 def diag_first(n, ia, ja, a):
     """Rows reordered: the diagonal first, the rest ascending (HYPRE's
-    storage)."""
+    storage).  Rows must hold ascending columns; a row without a diagonal
+    entry keeps its order."""
     ia = np.asarray(ia, np.int32)
-    ja2 = np.array(ja, np.int32, copy=True)
-    a2 = np.array(a, np.float64, copy=True)
-    rows = np.repeat(np.arange(n), np.diff(ia))
-    key = np.where(ja2 == rows, -1, ja2)
-    order = np.lexsort((key, rows))
-    return ia, np.ascontiguousarray(ja2[order]), np.ascontiguousarray(a2[order])
+    ja = np.asarray(ja, np.int32)
+    a = np.asarray(a, np.float64)
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(ia))
+    is_diag = ja == rows
+    # an entry before its row's diagonal moves one place right; the diagonal
+    # moves to the row's start
+    before = np.zeros(ja.size, bool)
+    dpos = np.full(n, -1, np.int64)
+    dpos[rows[is_diag]] = np.flatnonzero(is_diag)
+    has = dpos[rows] >= 0
+    idx = np.arange(ja.size, dtype=np.int64)
+    before[has] = idx[has] < dpos[rows[has]]
+    dest = idx + before
+    dest[is_diag] = ia[rows[is_diag]]
+    ja2 = np.empty_like(ja)
+    a2 = np.empty_like(a)
+    ja2[dest] = ja
+    a2[dest] = a
+    return ia, ja2, a2
 
 
 def coarsen_host(n, ia, ja, a, prm: AmgtBoomerParams | None = None):

@@ -19,6 +19,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden,-ffp-contract=off", "-cudart", "static",
          "--expt-relaxed-constexpr"]
+# host code parallelised with OpenMP (BoomerAMG's coarsening on the host)
+OPENMP = {"boomer.cu": ["-Xcompiler", "-fopenmp"]}
 
 
 def _stale(target: str, deps: list[str]) -> bool:
@@ -38,14 +40,14 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         o = os.path.join(OBJ, src.replace(".cu", ".o"))
         objs.append(o)
         if _stale(o, [s] + headers) or ptxas_info:
-            cmd = [NVCC, *ARCH, *FLAGS, "-c", s, "-o", o]
+            cmd = [NVCC, *ARCH, *FLAGS, *OPENMP.get(src, []), "-c", s, "-o", o]
             if ptxas_info:
                 cmd.insert(1, "-Xptxas=-v")
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
     if _stale(LIB, objs):
-        cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]
+        cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-Xcompiler", "-fopenmp", "-o", LIB, *objs]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -63,30 +63,42 @@ struct Strength {
     std::vector<int> si, sj;  // strong off-diagonal couplings, A's row order
 };
 
-// Rows must hold their diagonal first.
+// Rows must hold their diagonal first.  Rows in parallel (OpenMP): a count
+// pass, then each row's strong columns in its own place, in row order.
+static int strong_row(int i, const int *ia, const int *ja, const double *a, double theta, double max_row_sum,
+                      int *out)
+{
+    const int b = ia[i], e = ia[i + 1];
+    if (!(b < e && ja[b] == i)) return 0;
+    const double diag = a[b];
+    double scale = 0.0, rsum = diag;
+    for (int k = b + 1; k < e; ++k) {
+        scale = diag < 0 ? std::max(scale, a[k]) : std::min(scale, a[k]);
+        rsum += a[k];
+    }
+    const bool all_weak = std::fabs(rsum) > std::fabs(diag) * max_row_sum && max_row_sum < 1.0;
+    if (all_weak) return 0;
+    int cnt = 0;
+    for (int k = b + 1; k < e; ++k) {
+        const bool strong = diag < 0 ? !(a[k] <= theta * scale) : !(a[k] >= theta * scale);
+        if (strong) {
+            if (out) out[cnt] = ja[k];
+            ++cnt;
+        }
+    }
+    return cnt;
+}
+
 Strength strength(int n, const int *ia, const int *ja, const double *a, double theta, double max_row_sum)
 {
     Strength S;
     S.si.assign(n + 1, 0);
-    S.sj.reserve(ia[n]);
-    for (int i = 0; i < n; ++i) {
-        const int b = ia[i], e = ia[i + 1];
-        if (b < e && ja[b] == i) {
-            const double diag = a[b];
-            double scale = 0.0, rsum = diag;
-            for (int k = b + 1; k < e; ++k) {
-                scale = diag < 0 ? std::max(scale, a[k]) : std::min(scale, a[k]);
-                rsum += a[k];
-            }
-            const bool all_weak = std::fabs(rsum) > std::fabs(diag) * max_row_sum && max_row_sum < 1.0;
-            if (!all_weak)
-                for (int k = b + 1; k < e; ++k) {
-                    const bool strong = diag < 0 ? !(a[k] <= theta * scale) : !(a[k] >= theta * scale);
-                    if (strong) S.sj.push_back(ja[k]);
-                }
-        }
-        S.si[i + 1] = (int)S.sj.size();
-    }
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) S.si[i + 1] = strong_row(i, ia, ja, a, theta, max_row_sum, nullptr);
+    for (int i = 0; i < n; ++i) S.si[i + 1] += S.si[i];
+    S.sj.resize(S.si[n]);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) strong_row(i, ia, ja, a, theta, max_row_sum, S.sj.data() + S.si[i]);
     return S;
 }
 
@@ -261,12 +273,23 @@ void pmis(int n, const Strength &S, std::vector<int> &cf, bool cf_init)
             graph.push_back(i);
         }
     }
+    // The loops over the graph run in parallel (OpenMP), as HYPRE's do: the
+    // independent-set pass only clears marks (every writer writes 0), and the
+    // C/F pass reads marks that stay > 0 for the set's points and <= 0 for
+    // the others whichever thread writes first, so the result is the
+    // sequential one.
     int iter = 0;
     while (!graph.empty()) {
+        const int gn = (int)graph.size();
         if (!cf_init || iter > 0) {
-            for (int i : graph)
+#pragma omp parallel for schedule(static)
+            for (int g = 0; g < gn; ++g) {
+                const int i = graph[g];
                 if (meas[i] > 1.0) cf[i] = 1;
-            for (int i : graph) {
+            }
+#pragma omp parallel for schedule(static)
+            for (int g = 0; g < gn; ++g) {
+                const int i = graph[g];
                 if (!(meas[i] > 1.0)) continue;
                 for (int k = S.si[i]; k < S.si[i + 1]; ++k) {
                     const int j = S.sj[k];
@@ -277,7 +300,9 @@ void pmis(int n, const Strength &S, std::vector<int> &cf, bool cf_init)
             }
         }
         ++iter;
-        for (int i : graph) {
+#pragma omp parallel for schedule(static)
+        for (int g = 0; g < gn; ++g) {
+            const int i = graph[g];
             if (meas[i] < 1.0) cf[i] = F_PT;
             if (cf[i] > 0) {
                 cf[i] = C_PT;
@@ -314,6 +339,109 @@ void qsort_abs_desc(int *v, double *w, int left, int right)
     qsort_abs_desc(v, w, last + 1, right);
 }
 
+struct ExtI {
+    const int *ia, *ja;
+    const double *a;
+    const Strength *S;
+    const int *cf, *f2c;
+};
+
+// Row i of ext+i (hypre_BoomerAMGBuildExtPIInterpHost, par_lr_interp.c:
+// 1520-1760): C_i-hat in discovery order at positions row0, row0 + 1, ...
+// of (pj, pa) and, when pj is given, the weights; returns the row's length.
+// marker and strong_f are the calling thread's (marker >= row0: position of
+// a C_i-hat point; strong_f: this row's mark of its strong F neighbours,
+// unique per row).
+int ext_i_row(const ExtI &E, int i, int *marker, int &strong_f, int row0, int *pj, double *pa)
+{
+    const int *ia = E.ia, *ja = E.ja, *cf = E.cf, *f2c = E.f2c;
+    const double *a = E.a;
+    const Strength &S = *E.S;
+    int len = 0;
+    if (cf[i] >= 0) {
+        if (pj) {
+            pj[row0] = f2c[i];
+            pa[row0] = 1.0;
+        }
+        return 1;
+    }
+    if (cf[i] == SF_PT) return 0;
+    --strong_f;
+    auto add = [&](int c) {
+        if (marker[c] < row0) {
+            marker[c] = row0 + len;
+            if (pj) {
+                pj[row0 + len] = f2c[c];
+                pa[row0 + len] = 0.0;
+            }
+            ++len;
+        }
+    };
+    for (int k = S.si[i]; k < S.si[i + 1]; ++k) {
+        const int i1 = S.sj[k];
+        if (cf[i1] >= 0) {
+            add(i1);
+        } else if (cf[i1] != SF_PT) {
+            marker[i1] = strong_f;
+            for (int kk = S.si[i1]; kk < S.si[i1 + 1]; ++kk) {
+                const int k1 = S.sj[kk];
+                if (cf[k1] >= 0) add(k1);
+            }
+        }
+    }
+    if (pj) {
+        double diag = a[ia[i]];
+        for (int k = ia[i] + 1; k < ia[i + 1]; ++k) {
+            const int i1 = ja[k];
+            if (marker[i1] >= row0) {
+                pa[marker[i1]] += a[k];
+            } else if (marker[i1] == strong_f) {
+                double sum = 0.0;
+                const int sgn = a[ia[i1]] < 0 ? -1 : 1;
+                for (int k2 = ia[i1] + 1; k2 < ia[i1 + 1]; ++k2) {
+                    const int i2 = ja[k2];
+                    if ((marker[i2] >= row0 || i2 == i) && sgn * a[k2] < 0) sum += a[k2];
+                }
+                if (sum != 0.0) {
+                    const double dist = a[k] / sum;
+                    for (int k2 = ia[i1] + 1; k2 < ia[i1 + 1]; ++k2) {
+                        const int i2 = ja[k2];
+                        if (marker[i2] >= row0 && sgn * a[k2] < 0) pa[marker[i2]] += dist * a[k2];
+                        if (i2 == i && sgn * a[k2] < 0) diag += dist * a[k2];
+                    }
+                } else {
+                    diag += a[k];
+                }
+            } else if (cf[i1] != SF_PT) {
+                diag += a[k];
+            }
+        }
+        if (diag != 0.0)
+            for (int k = row0; k < row0 + len; ++k) pa[k] /= -diag;
+    }
+    --strong_f;
+    return len;
+}
+
+// P_max truncation of one row (hypre_ParCSRMatrixTruncate's max_elmts
+// branch, par_csr_matrix.c:3100-3215): rows longer than p_max sorted by
+// |w| descending, the first p_max kept and rescaled to the former row sum;
+// returns the kept length.
+int truncate_row(int *pj, double *pa, int len, int p_max)
+{
+    if (p_max <= 0 || len <= p_max) return len;
+    double rsum = 0.0;
+    for (int k = 0; k < len; ++k) rsum += pa[k];
+    qsort_abs_desc(pj, pa, 0, len - 1);
+    double scale = 0.0;
+    for (int k = 0; k < p_max; ++k) scale += pa[k];
+    if (scale != 0.0 && scale != rsum) {
+        const double f = rsum / scale;
+        for (int k = 0; k < p_max; ++k) pa[k] *= f;
+    }
+    return p_max;
+}
+
 }  // namespace
 
 // Coarsening and ext+i interpolation of one level (host arrays; rows with
@@ -330,101 +458,49 @@ int boomer_level(int n, const int *ia, const int *ja, const double *a, const amg
     int nc = 0;
     for (int i = 0; i < n; ++i)
         if (cf[i] >= 0) f2c[i] = nc++;
+    // ext+i row by row, rows in parallel (OpenMP, contiguous row ranges per
+    // thread, so that a thread's row starts increase): a count pass sizes
+    // every row, then each row is built and truncated in its own place and
+    // the rows are compacted
     pi.assign(n + 1, 0);
-    pj.clear();
-    pa.clear();
-    std::vector<int> marker(n, -1);  // >= row start: position in P of a C_i-hat point
-    int strong_f = -2;
-    for (int i = 0; i < n; ++i) {
-        const int row0 = (int)pj.size();
-        if (cf[i] >= 0) {
-            pj.push_back(f2c[i]);
-            pa.push_back(1.0);
-        } else if (cf[i] != SF_PT) {
-            --strong_f;
-            for (int k = S.si[i]; k < S.si[i + 1]; ++k) {
-                const int i1 = S.sj[k];
-                if (cf[i1] >= 0) {
-                    if (marker[i1] < row0) {
-                        marker[i1] = (int)pj.size();
-                        pj.push_back(f2c[i1]);
-                        pa.push_back(0.0);
-                    }
-                } else if (cf[i1] != SF_PT) {
-                    marker[i1] = strong_f;
-                    for (int kk = S.si[i1]; kk < S.si[i1 + 1]; ++kk) {
-                        const int k1 = S.sj[kk];
-                        if (cf[k1] >= 0 && marker[k1] < row0) {
-                            marker[k1] = (int)pj.size();
-                            pj.push_back(f2c[k1]);
-                            pa.push_back(0.0);
-                        }
-                    }
-                }
-            }
-            double diag = a[ia[i]];
-            for (int k = ia[i] + 1; k < ia[i + 1]; ++k) {
-                const int i1 = ja[k];
-                if (marker[i1] >= row0) {
-                    pa[marker[i1]] += a[k];
-                } else if (marker[i1] == strong_f) {
-                    double sum = 0.0;
-                    const int sgn = a[ia[i1]] < 0 ? -1 : 1;
-                    for (int k2 = ia[i1] + 1; k2 < ia[i1 + 1]; ++k2) {
-                        const int i2 = ja[k2];
-                        if ((marker[i2] >= row0 || i2 == i) && sgn * a[k2] < 0) sum += a[k2];
-                    }
-                    if (sum != 0.0) {
-                        const double dist = a[k] / sum;
-                        for (int k2 = ia[i1] + 1; k2 < ia[i1 + 1]; ++k2) {
-                            const int i2 = ja[k2];
-                            if (marker[i2] >= row0 && sgn * a[k2] < 0) pa[marker[i2]] += dist * a[k2];
-                            if (i2 == i && sgn * a[k2] < 0) diag += dist * a[k2];
-                        }
-                    } else {
-                        diag += a[k];
-                    }
-                } else if (cf[i1] != SF_PT) {
-                    diag += a[k];
-                }
-            }
-            if (diag != 0.0)
-                for (int k = row0; k < (int)pj.size(); ++k) pa[k] /= -diag;
-            --strong_f;
-        }
-        pi[i + 1] = (int)pj.size();
-    }
-    // P_max truncation with rescaling, after the whole P is built (the
-    // markers above hold positions in pj, which must not move while rows
-    // are still being built), rows compacted in place
-    if (p_max > 0) {
-        int out = 0;
+    std::vector<int> keep(n, 0);
+    const ExtI E{ia, ja, a, &S, cf.data(), f2c.data()};
+#pragma omp parallel
+    {
+        std::vector<int> marker(n, -1);
+        int strong_f = -2, vpos = 0;  // vpos: the thread's running row start, so that markers stay below it
+#pragma omp for schedule(static)
         for (int i = 0; i < n; ++i) {
-            const int b = pi[i], len = pi[i + 1] - b;
-            pi[i] = out;
-            int keep = len;
-            if (len > p_max) {
-                double rsum = 0.0;
-                for (int k = b; k < b + len; ++k) rsum += pa[k];
-                qsort_abs_desc(pj.data() + b, pa.data() + b, 0, len - 1);
-                keep = p_max;
-                double scale = 0.0;
-                for (int k = b; k < b + keep; ++k) scale += pa[k];
-                if (scale != 0.0 && scale != rsum) {
-                    const double f = rsum / scale;
-                    for (int k = b; k < b + keep; ++k) pa[k] *= f;
-                }
-            }
-            for (int k = 0; k < keep; ++k) {
-                pj[out + k] = pj[b + k];
-                pa[out + k] = pa[b + k];
-            }
-            out += keep;
+            pi[i + 1] = ext_i_row(E, i, marker.data(), strong_f, vpos, nullptr, nullptr);
+            vpos += pi[i + 1];
         }
-        pi[n] = out;
-        pj.resize(out);
-        pa.resize(out);
     }
+    for (int i = 0; i < n; ++i) pi[i + 1] += pi[i];
+    std::vector<int> tj(pi[n]);
+    std::vector<double> ta(pi[n]);
+#pragma omp parallel
+    {
+        std::vector<int> marker(n, -1);
+        int strong_f = -2;
+#pragma omp for schedule(static)
+        for (int i = 0; i < n; ++i) {
+            const int row0 = pi[i];
+            const int len = ext_i_row(E, i, marker.data(), strong_f, row0, tj.data(), ta.data());
+            keep[i] = truncate_row(tj.data() + row0, ta.data() + row0, len, p_max);
+        }
+    }
+    // compaction: the kept entries of each row, in place order
+    std::vector<int> out(n + 1, 0);
+    for (int i = 0; i < n; ++i) out[i + 1] = out[i] + keep[i];
+    pj.resize(out[n]);
+    pa.resize(out[n]);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < keep[i]; ++k) {
+            pj[out[i] + k] = tj[pi[i] + k];
+            pa[out[i] + k] = ta[pi[i] + k];
+        }
+    pi.swap(out);
     return nc;
 }
 
@@ -470,6 +546,55 @@ HostCsr transpose(const HostCsr &A)
 // row ic of (R A) P (for each entry of that RA row in the order met, for
 // each entry of P's row; the diagonal stored first).  Plain multiply, then
 // add (par_rap.c:1700-1880).
+// Row ic of (R A) P into (cj, ca) at row0 (count only when cj is null);
+// returns its length.  a_stamp/a_pos/p_mark/ra_* are the calling thread's.
+static int rap_row(const HostCsr &R, const HostCsr &A, const HostCsr &P, int ic, int row0, int *a_stamp,
+                   int *a_pos, int *p_mark, std::vector<int> &ra_j, std::vector<double> &ra_a, int *cj, double *ca)
+{
+    int len = 1;  // the diagonal first
+    p_mark[ic] = row0;
+    if (cj) {
+        cj[row0] = ic;
+        ca[row0] = 0.0;
+    }
+    ra_j.clear();
+    ra_a.clear();
+    for (int kr = R.i[ic]; kr < R.i[ic + 1]; ++kr) {
+        const int i1 = R.j[kr];
+        const double r = R.a[kr];
+        for (int ka = A.i[i1]; ka < A.i[i1 + 1]; ++ka) {
+            const int i2 = A.j[ka];
+            const double ra = r * A.a[ka];
+            if (a_stamp[i2] != ic) {
+                a_stamp[i2] = ic;
+                a_pos[i2] = (int)ra_j.size();
+                ra_j.push_back(i2);
+                ra_a.push_back(ra);
+            } else {
+                ra_a[a_pos[i2]] += ra;
+            }
+        }
+    }
+    for (size_t t = 0; t < ra_j.size(); ++t) {
+        const int i1 = ra_j[t];
+        const double ra = ra_a[t];
+        for (int kp = P.i[i1]; kp < P.i[i1 + 1]; ++kp) {
+            const int i3 = P.j[kp];
+            if (p_mark[i3] < row0) {
+                p_mark[i3] = row0 + len;
+                if (cj) {
+                    cj[row0 + len] = i3;
+                    ca[row0 + len] = ra * P.a[kp];
+                }
+                ++len;
+            } else if (cj) {
+                ca[p_mark[i3]] += ra * P.a[kp];
+            }
+        }
+    }
+    return len;
+}
+
 HostCsr rap_kt(const HostCsr &A, const HostCsr &P)
 {
     const HostCsr R = transpose(P);
@@ -477,50 +602,34 @@ HostCsr rap_kt(const HostCsr &A, const HostCsr &P)
     HostCsr C;
     C.rows = C.cols = nc;
     C.i.assign(nc + 1, 0);
-    std::vector<int> a_stamp(A.cols, -1), a_pos(A.cols, 0), p_mark(nc, -1);
-    std::vector<int> ra_j;
-    std::vector<double> ra_a;
-    for (int ic = 0; ic < nc; ++ic) {
-        const int row0 = (int)C.j.size();
-        C.i[ic] = row0;
-        p_mark[ic] = row0;
-        C.j.push_back(ic);
-        C.a.push_back(0.0);
-        ra_j.clear();
-        ra_a.clear();
-        for (int kr = R.i[ic]; kr < R.i[ic + 1]; ++kr) {
-            const int i1 = R.j[kr];
-            const double r = R.a[kr];
-            for (int ka = A.i[i1]; ka < A.i[i1 + 1]; ++ka) {
-                const int i2 = A.j[ka];
-                const double ra = r * A.a[ka];
-                if (a_stamp[i2] != ic) {
-                    a_stamp[i2] = ic;
-                    a_pos[i2] = (int)ra_j.size();
-                    ra_j.push_back(i2);
-                    ra_a.push_back(ra);
+    // rows in parallel (OpenMP, contiguous ranges per thread): a count
+    // pass, then every row in its own place
+    for (int pass = 0; pass < 2; ++pass) {
+#pragma omp parallel
+        {
+            std::vector<int> a_stamp(A.cols, -1), a_pos(A.cols, 0), p_mark(nc, -1);
+            std::vector<int> ra_j;
+            std::vector<double> ra_a;
+            int vpos = 0;  // count pass: the thread's running row start
+#pragma omp for schedule(static)
+            for (int ic = 0; ic < nc; ++ic) {
+                if (pass == 0) {
+                    const int len = rap_row(R, A, P, ic, vpos, a_stamp.data(), a_pos.data(), p_mark.data(), ra_j,
+                                            ra_a, nullptr, nullptr);
+                    C.i[ic + 1] = len;
+                    vpos += len;
                 } else {
-                    ra_a[a_pos[i2]] += ra;
+                    rap_row(R, A, P, ic, C.i[ic], a_stamp.data(), a_pos.data(), p_mark.data(), ra_j, ra_a,
+                            C.j.data(), C.a.data());
                 }
             }
         }
-        for (size_t t = 0; t < ra_j.size(); ++t) {
-            const int i1 = ra_j[t];
-            const double ra = ra_a[t];
-            for (int kp = P.i[i1]; kp < P.i[i1 + 1]; ++kp) {
-                const int i3 = P.j[kp];
-                const double v = ra * P.a[kp];
-                if (p_mark[i3] < row0) {
-                    p_mark[i3] = (int)C.j.size();
-                    C.j.push_back(i3);
-                    C.a.push_back(v);
-                } else {
-                    C.a[p_mark[i3]] += v;
-                }
-            }
+        if (pass == 0) {
+            for (int ic = 0; ic < nc; ++ic) C.i[ic + 1] += C.i[ic];
+            C.j.resize(C.i[nc]);
+            C.a.resize(C.i[nc]);
         }
     }
-    C.i[nc] = (int)C.j.size();
     return C;
 }
 
