@@ -843,9 +843,9 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
 //           block at a time (the B blocks of one A block hit distinct C
 //           blocks), with the counters in gnum.
 //   Used for products of fewer than 64 A block rows per SM (the coarse
-//   levels, whose few long rows leave the staged kernel's warps idle), of
-//   more than 32 C blocks per row on average, or with more than an eighth
-//   of their rows beyond kSymCap pairs; the staged kernel keeps the others.
+//   levels, whose few long rows leave the staged kernel's warps idle) or
+//   with more than an eighth of their rows beyond kSymCap pairs; the staged
+//   kernel keeps the others.
 //   gather  four lanes per C block (lane r: row r), each pair's A row and
 //           B block read from global memory (L1 / L2), the product entry the
 //           same fused chain as the staged kernel, the products added in
@@ -1408,13 +1408,12 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
         Ccsr->num_nonzeros = nnzC;
         if ((rc = alloc_n(&Ccsr->j, nnzC, s)) || (rc = alloc_n(&Ccsr->data, nnzC, s))) goto fail;
     }
-    // products of few A block rows (coarse levels), of more C blocks per
-    // row on average than the staged kernel accumulates in shared memory,
-    // or with many rows beyond kSymCap pairs: the gathered numeric; others:
+    // products of few A block rows (coarse levels) or with many rows beyond
+    // kSymCap pairs: the gathered numeric; others:
     // the staged one, whose warp-per-row layout keeps every SM busy on short
     // rows and reads each A row once (both give the same C bit for bit).  fp16 / bf16 products on the tensor-core engine: always the
     // gathered form, its block products on the tensor cores.
-    if (brA < 64 * st->sm_count || tensor || nbC > (long long)kNumCap * brA || 8LL * nlarge > brA) {
+    if (brA < 64 * st->sm_count || tensor || 8LL * nlarge > brA) {
         const size_t o_beg = align256(8 * (size_t)npairs), o_num = o_beg + align256(8 * (size_t)nbC + 8),
                      o_end = o_num + align256(4 * (size_t)nbC + 4);
         if ((rc = alloc_n(&arena3, o_end, s))) goto fail;
