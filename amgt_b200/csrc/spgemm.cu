@@ -857,7 +857,7 @@ spgemm_order_kernel(int brA, const int *__restrict__ aptr, const int *__restrict
                     const int *__restrict__ bptr, const int *__restrict__ bidx, const int *__restrict__ cptr,
                     int *__restrict__ cidx, uint16_t *__restrict__ cmap, const int64_t *__restrict__ ub_off,
                     const int *__restrict__ skey, const uint16_t *__restrict__ smap,
-                    const uint16_t *__restrict__ pslot, int2 *__restrict__ glist, long long *__restrict__ gbeg,
+                    uint16_t *__restrict__ pslot, int2 *__restrict__ glist, long long *__restrict__ gbeg,
                     int *__restrict__ gnum)
 {
     __shared__ int cnt_s[kNumWarps][kSymCap];
@@ -904,10 +904,10 @@ spgemm_order_kernel(int brA, const int *__restrict__ aptr, const int *__restrict
                         const int sj0 = __shfl_sync(FULL, j0, src), sex = __shfl_sync(FULL, excl, src);
                         int t = -1;
                         if (q < total) {
-                            if (direct) {
+                            if (direct || pass == 1) {
                                 const unsigned short ps = pslot[qbase + q];
                                 t = ps < cn ? (int)ps : -1;
-                            } else {  // the pair's C block from the row's sorted pattern
+                            } else {  // the pair's C block from the row's sorted pattern, kept for pass 1
                                 const int key = bidx[sj0 + (q - sex)];
                                 int lo = 0, hi = cn - 1;
                                 while (lo < hi) {
@@ -916,6 +916,7 @@ spgemm_order_kernel(int brA, const int *__restrict__ aptr, const int *__restrict
                                     else hi = mid;
                                 }
                                 t = (cn > 0 && keys[lo] == key) ? lo : -1;
+                                pslot[qbase + q] = t >= 0 ? (unsigned short)t : (unsigned short)0xFFFF;
                             }
                         }
                         if (pass == 0) {
