@@ -1013,7 +1013,7 @@ __device__ __forceinline__ void row4_ldg(const typename NumT<PREC>::val_t *p, ty
 }
 
 template <int PREC>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 5)
 spgemm_gather_kernel(int nbC, const typename NumT<PREC>::val_t *__restrict__ aval,
                      const typename NumT<PREC>::val_t *__restrict__ bval, const int2 *__restrict__ glist,
                      const long long *__restrict__ gbeg, const int *__restrict__ gnum, double *__restrict__ cval,
