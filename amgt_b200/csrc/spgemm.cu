@@ -48,6 +48,7 @@ constexpr int kSymLargeThreads = 256;
 constexpr int kNumWarps = 4;
 constexpr int kNumCap = 32;       // C blocks a warp accumulates in shared memory
 constexpr int kNumWin = 256;      // pairs per window of the numeric pair -> A block table
+constexpr int kOrdCap = 512;      // C blocks of a row the order kernel counts in shared memory
 
 __device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
 
@@ -834,7 +835,7 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
 //           and sorts the row's pairs by C block, stably (pair order = A
 //           block order), into the row's scratch slice: glist[gbeg[c] ..
 //           gbeg[c] + gnum[c]) lists C block c's pairs in the order the
-//           sequential product adds them.  Rows of at most kSymCap C
+//           sequential product adds them.  Rows of at most kOrdCap C
 //           blocks: a flattened pass over 32 pairs at a time with
 //           shared-memory counters, equal C blocks of a step ranked in lane
 //           order; each pair's C block is the symbolic pass's pair slot
@@ -860,8 +861,8 @@ spgemm_order_kernel(int brA, const int *__restrict__ aptr, const int *__restrict
                     uint16_t *__restrict__ pslot, int2 *__restrict__ glist, long long *__restrict__ gbeg,
                     int *__restrict__ gnum)
 {
-    __shared__ int cnt_s[kNumWarps][kSymCap];
-    __shared__ int key_s[kNumWarps][kSymCap];
+    __shared__ int cnt_s[kNumWarps][kOrdCap];
+    __shared__ int key_s[kNumWarps][kOrdCap];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int *cnt = cnt_s[warp], *keys = key_s[warp];
     for (int b = blockIdx.x * kNumWarps + warp; b < brA; b += gridDim.x * kNumWarps) {
@@ -873,7 +874,7 @@ spgemm_order_kernel(int brA, const int *__restrict__ aptr, const int *__restrict
         }
         const int a0 = aptr[b], a1 = aptr[b + 1];
         const bool direct = npairs <= kSymCap;  // pair slots from the symbolic pass
-        if (cn <= kSymCap) {
+        if (cn <= kOrdCap) {
             for (int t = lane; t < cn; t += 32) {
                 cnt[t] = 0;
                 if (!direct) keys[t] = skey[sbase + t];
@@ -953,7 +954,7 @@ spgemm_order_kernel(int brA, const int *__restrict__ aptr, const int *__restrict
                 }
             }
         } else {
-            // a row of more than kSymCap C blocks: one A block at a time,
+            // a row of more than kOrdCap C blocks: one A block at a time,
             // counters in gnum (cleared by the caller)
             for (int pass = 0; pass < 2; ++pass) {
                 for (int i = a0; i < a1; ++i) {
