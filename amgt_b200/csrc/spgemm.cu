@@ -46,8 +46,9 @@ constexpr int kSymCap = 1024;     // pairs a warp sorts in shared memory
 constexpr int kSymWin = 8192;     // key window of the large-row path
 constexpr int kSymLargeThreads = 256;
 constexpr int kNumWarps = 4;
-constexpr int kNumCap = 32;       // C blocks a warp accumulates in shared memory
-constexpr int kNumWin = 256;      // pairs per window of the numeric pair -> A block table
+constexpr int kNumCap = 32;       // C blocks a warp accumulates in shared memory (products of short C rows)
+constexpr int kNumCapWide = 64;   // the same for products whose C rows mostly exceed kNumCap blocks
+constexpr int kNumWin = 128;      // pairs per window of the numeric's pair list
 constexpr int kOrdCap = 512;      // C blocks of a row the order kernel counts in shared memory
 
 __device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) - 1u; }
@@ -570,27 +571,52 @@ __device__ __forceinline__ void row4_smem(const unsigned char *p, typename NumT<
     }
 }
 
-// Shared memory of the numeric kernel per warp: C accumulators, two stages
-// of 8 staged B blocks (16 values + 16-byte pad) and 8 x 4 A rows, and the
-// pair -> A block table.
-template <int PREC>
+// Four accumulators of one C block row (16-byte aligned: the stride of a
+// block and the offset of a row are multiples of 16 bytes) as two double2
+// or one float4 access.
+template <typename acc_t>
+__device__ __forceinline__ void acc4_load(const acc_t *p, acc_t v[4])
+{
+    if constexpr (sizeof(acc_t) == 8) {
+        const double2 u = reinterpret_cast<const double2 *>(p)[0], w = reinterpret_cast<const double2 *>(p)[1];
+        v[0] = u.x; v[1] = u.y; v[2] = w.x; v[3] = w.y;
+    } else {
+        const float4 u = *reinterpret_cast<const float4 *>(p);
+        v[0] = u.x; v[1] = u.y; v[2] = u.z; v[3] = u.w;
+    }
+}
+template <typename acc_t>
+__device__ __forceinline__ void acc4_store(acc_t *p, const acc_t v[4])
+{
+    if constexpr (sizeof(acc_t) == 8) {
+        reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+    } else {
+        *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+}
+
+// Shared memory of the numeric kernel per warp: C accumulators (CAP C
+// blocks), two stages of 8 staged B blocks (16 values + 16-byte pad) and
+// 8 x 4 A rows, and the pair -> A block table.
+template <int PREC, int CAP>
 struct NumSmem {
     using V = typename NumT<PREC>::val_t;
     using acc_t = typename NumT<PREC>::acc_t;
     static constexpr int BB = 16 * (int)sizeof(V) + 16;  // staged B block bytes
     static constexpr int AR = 4 * (int)sizeof(V);        // staged A row bytes
-    static constexpr int b_off = kNumCap * NumStride<acc_t>::v * (int)sizeof(acc_t);
+    static constexpr int b_off = CAP * NumStride<acc_t>::v * (int)sizeof(acc_t);
     static constexpr int a_off = b_off + 2 * 8 * BB;
     static constexpr int p_off = a_off + 2 * 32 * AR;
-    static constexpr int per_warp = (p_off + kNumWin + 15) / 16 * 16;
+    static constexpr int per_warp = (p_off + 2 * kNumWin + 15) / 16 * 16;
 };
 
 // Numeric phase.  One warp per A block row; the row's (A block, B block)
 // pairs are flattened (up to 32 A blocks at a time: lane i holds A block
 // i's B row range, a warp scan of the lengths numbers the pairs, and a
-// shared table maps each pair of a 256-pair window to its A block) and
-// taken 8 at a time, 4 lanes per pair, lane r computing row r of the 4x4
-// product.  Steps are double-buffered: while step k is computed from
+// shared list holds, for a window of 128 pairs, those whose bitmap product
+// is non-zero, in order, with their A block) and taken 8 at a time, 4
+// lanes per pair, lane r computing row r of the 4x4 product.  Steps are double-buffered: while step k is computed from
 // shared memory, the asynchronous copies of step k+1's B blocks and A rows
 // (each lane copies its own rows of its own pair) and its pairs' C slots
 // are in flight.  A pair's C block comes from the symbolic pass (pslot, by
@@ -603,12 +629,13 @@ struct NumSmem {
 // are added to their C block in pair order (= A block order): pairs of one
 // step that hit the same C block row are applied in rounds, lowest lane
 // first (match_any), so the accumulation order is the sequential one.  Rows
-// of up to 32 C blocks accumulate in shared memory, longer rows in place in
+// of up to CAP C blocks (32; 64 for products of long C rows, at two thirds
+// of the warps per SM) accumulate in shared memory, longer rows in place in
 // C.  For fp64 with cshadow given, the final store also writes the fp16
 // rounding of every C value and the exactness bits of exact_check_kernel
 // into *cflags (bit 0: some value not an fp32 value, bit 1: not fp16).
-template <int PREC>
-__global__ void __launch_bounds__(32 * kNumWarps, 6)
+template <int PREC, int CAP>
+__global__ void __launch_bounds__(32 * kNumWarps, CAP == kNumCap ? 6 : 4)
 spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
                       const typename NumT<PREC>::val_t *__restrict__ aval, const int *__restrict__ bptr,
                       const int *__restrict__ bidx, const typename NumT<PREC>::val_t *__restrict__ bval,
@@ -622,7 +649,7 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
     using T = NumT<PREC>;
     using V = typename T::val_t;
     using acc_t = typename T::acc_t;
-    using SM = NumSmem<PREC>;
+    using SM = NumSmem<PREC, CAP>;
     constexpr int SS = NumStride<acc_t>::v;
     constexpr int CH = (int)sizeof(V);  // 16-byte chunks per block (16 values)
     constexpr int CPL = (CH + 3) / 4;   // B chunks copied per lane
@@ -632,7 +659,8 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
     const int ps = lane >> 2, r = lane & 3;
     unsigned char *wbase = num_smem + warp * SM::per_warp;
     acc_t *sa = reinterpret_cast<acc_t *>(wbase);
-    unsigned char *sB = wbase + SM::b_off, *sA = wbase + SM::a_off, *sp = wbase + SM::p_off;
+    unsigned char *sB = wbase + SM::b_off, *sA = wbase + SM::a_off;
+    uint16_t *sp = reinterpret_cast<uint16_t *>(wbase + SM::p_off);
     for (int b = blockIdx.x * kNumWarps + warp; b < brA; b += gridDim.x * kNumWarps) {
         const int c0 = cptr[b], cn = cptr[b + 1] - c0;
         // the row's pattern, sorted by the symbolic pass, moves from scratch to C
@@ -646,12 +674,18 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
             pkey = skey[sbase + lane];
             pmap = smap[sbase + lane];
         }
-        const bool small = cn <= kNumCap;
+        const bool small = cn <= CAP;
         double *ga = cval + 16LL * c0;
+        // zeroed one block row (4 values) per lane and iteration
         if (small) {
-            for (int t = lane; t < 16 * cn; t += 32) sa[(t >> 4) * SS + (t & 15)] = (acc_t)0;
+            const acc_t z[4] = {(acc_t)0, (acc_t)0, (acc_t)0, (acc_t)0};
+            for (int t = lane; t < 4 * cn; t += 32) acc4_store(sa + (t >> 2) * SS + 4 * (t & 3), z);
         } else {
-            for (int t = lane; t < 16 * cn; t += 32) ga[t] = 0.0;
+            for (int t = lane; t < 4 * cn; t += 32) {
+                double2 *d = reinterpret_cast<double2 *>(ga + 4LL * t);
+                d[0] = make_double2(0.0, 0.0);
+                d[1] = make_double2(0.0, 0.0);
+            }
         }
         __syncwarp();
         const int a0 = aptr[b], a1 = aptr[b + 1];
@@ -673,15 +707,32 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
             const int excl = incl - len;
             const int jd = j0 - excl;  // B block of pair q of A block i: q + jd[i]
             for (int w0 = 0; w0 < total; w0 += kNumWin) {
-                const int wend = min(total, w0 + kNumWin);
-                for (int q = max(excl, w0); q < min(incl, wend); ++q) sp[q - w0] = (unsigned char)lane;
+                const int wlen = min(total - w0, kNumWin);
+                for (int q = max(excl, w0); q < min(incl, w0 + wlen); ++q) sp[q - w0] = (uint16_t)lane;
                 __syncwarp();
+                // the window's pairs with a non-zero bitmap product, in pair
+                // order, compacted in place: (ordinal in the window << 8) |
+                // lane of the A block (rows beyond kSymCap pairs keep all)
+                int nq = 0;
+                for (int i0 = 0; i0 < wlen; i0 += 32) {
+                    const int i = i0 + lane;
+                    const bool in = i < wlen;
+                    const int src = in ? sp[i] : 0;
+                    const bool nz = in && (!direct || pslot[qbase + w0 + i] != 0xFFFF);
+                    const unsigned bal = __ballot_sync(FULL, nz);
+                    __syncwarp();  // every read of this chunk precedes the writes
+                    if (nz) sp[nq + __popc(bal & lanemask_lt(lane))] = (uint16_t)((i << 8) | src);
+                    nq += __popc(bal);
+                }
+                __syncwarp();
+                if (nq == 0) continue;  // warp-uniform
                 // issue of one step into stage `st`: copies of the lane's B
                 // rows and A row, and the pair's C slot (-1: no product)
-                auto issue = [&](int q0, int st) -> int {
-                    const int q = q0 + ps;
-                    const bool valid = q < wend;
-                    const int src = valid ? sp[q - w0] : 0;
+                auto issue = [&](int k0, int st) -> int {
+                    const int k = k0 + ps;
+                    const bool valid = k < nq;
+                    const int e = valid ? sp[k] : 0;
+                    const int src = e & 0xFF, q = w0 + (e >> 8);
                     const int j = q + __shfl_sync(FULL, jd, src);
                     int t = -1;
                     if (valid) {
@@ -714,12 +765,12 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                     cp_async_commit();
                     return t;
                 };
-                int tcur = issue(w0, 0);
+                int tcur = issue(0, 0);
                 int st = 0;
-                for (int q0 = w0; q0 < wend; q0 += 8, st ^= 1) {
+                for (int k0 = 0; k0 < nq; k0 += 8, st ^= 1) {
                     int tnext = -1;
-                    if (q0 + 8 < wend) {
-                        tnext = issue(q0 + 8, st ^ 1);
+                    if (k0 + 8 < nq) {
+                        tnext = issue(k0 + 8, st ^ 1);
                         cp_async_wait<1>();
                     } else {
                         cp_async_wait<0>();
@@ -749,9 +800,11 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                     for (int rd = 0; rd <= rounds; ++rd) {
                         if (found && rank == rd) {
                             if (small) {
-                                acc_t *d = sa + t * SS + 4 * r;
+                                acc_t *d = sa + t * SS + 4 * r, v[4];
+                                acc4_load(d, v);
 #pragma unroll
-                                for (int c = 0; c < 4; ++c) d[c] = T::add(d[c], s[c]);
+                                for (int c = 0; c < 4; ++c) v[c] = T::add(v[c], s[c]);
+                                acc4_store(d, v);
                             } else {
                                 double *d = ga + 16LL * t + 4 * r;
 #pragma unroll
@@ -774,18 +827,34 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
             cidx[c0 + t] = skey[sbase + t];
             cmap[c0 + t] = smap[sbase + t];
         }
-        for (int t = lane; t < 16 * cn; t += 32) {
-            const acc_t v = small ? sa[(t >> 4) * SS + (t & 15)] : (acc_t)ga[t];
-            ga[t] = (double)v;
+        // C values (+ shadow), one block row (4 values) per lane and iteration
+        for (int t = lane; t < 4 * cn; t += 32) {
+            acc_t v[4];
+            if (small) {
+                acc4_load(sa + (t >> 2) * SS + 4 * (t & 3), v);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) v[c] = (acc_t)ga[4LL * t + c];
+            }
+            double2 *g = reinterpret_cast<double2 *>(ga + 4LL * t);
+            g[0] = make_double2((double)v[0], (double)v[1]);
+            g[1] = make_double2((double)v[2], (double)v[3]);
             if constexpr (PREC == AMGT_DOUBLE) {
                 if (cshadow) {
-                    const __half hv = __double2half(v);
-                    static_cast<__half *>(cshadow)[16LL * c0 + t] = hv;
-                    if ((double)__double2float_rn(v) != v) not32 = true;
-                    if ((double)__half2float(hv) != v) not16 = true;
+                    __half hv[4];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        hv[c] = __double2half(v[c]);
+                        if ((double)__double2float_rn(v[c]) != v[c]) not32 = true;
+                        if ((double)__half2float(hv[c]) != v[c]) not16 = true;
+                    }
+                    __half2 *hs = reinterpret_cast<__half2 *>(static_cast<__half *>(cshadow) + 16LL * c0 + 4LL * t);
+                    hs[0] = __halves2half2(hv[0], hv[1]);
+                    hs[1] = __halves2half2(hv[2], hv[3]);
                 }
             } else if (cshadow) {
-                store_shadow<PREC>(cshadow, 16LL * c0 + t, v);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) store_shadow<PREC>(cshadow, 16LL * c0 + 4LL * t + c, v[c]);
             }
         }
         __syncwarp();
@@ -1215,21 +1284,39 @@ spgemm_csr_kernel(int m, int brA, const int *__restrict__ cptr, const int *__res
     }
 }
 
+template <int PREC, int CAP>
+static int launch_numeric_cap(const amgt_bsr *A, const void *aval, const amgt_bsr *B, const void *bval, amgt_bsr *C,
+                              void *cshadow, amgt_csr *Ccsr, const int64_t *ub_off, const int *skey,
+                              const uint16_t *smap, const uint16_t *pslot, cudaStream_t s, int sm_count,
+                              unsigned long long *cflags)
+{
+    using V = typename NumT<PREC>::val_t;
+    constexpr int smem = kNumWarps * NumSmem<PREC, CAP>::per_warp;
+    constexpr int per_sm = CAP == kNumCap ? 6 : 4;
+    AMGT_CUDA_TRY(cudaFuncSetAttribute(spgemm_numeric_kernel<PREC, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       smem));
+    AMGT_LAUNCH((spgemm_numeric_kernel<PREC, CAP>), grid_for(kNumWarps, A->blc_row, sm_count, per_sm),
+                32 * kNumWarps, smem, s, A->row, A->blc_row, A->blcPtr, A->blcIdx, (const V *)aval, B->blcPtr, B->blcIdx, (const V *)bval,
+                C->blcPtr, C->blcIdx, C->blcMap, C->blcVal, cshadow, Ccsr ? Ccsr->i : nullptr,
+                Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr, ub_off, skey, smap, pslot, cflags);
+    return AMGT_OK;
+}
+
+// The staged numeric with the accumulator capacity for C's row lengths:
+// 64 C blocks when the average C row exceeds 24 blocks (most rows would
+// otherwise accumulate in global memory), else 32 at more warps per SM.
 template <int PREC>
 static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B, const void *bval, amgt_bsr *C,
                           void *cshadow, amgt_csr *Ccsr, const int64_t *ub_off, const int *skey,
                           const uint16_t *smap, const uint16_t *pslot, cudaStream_t s, int sm_count,
                           unsigned long long *cflags = nullptr)
 {
-    using V = typename NumT<PREC>::val_t;
     if (A->blc_row == 0) return AMGT_OK;
-    constexpr int smem = kNumWarps * NumSmem<PREC>::per_warp;
-    AMGT_CUDA_TRY(cudaFuncSetAttribute(spgemm_numeric_kernel<PREC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    AMGT_LAUNCH(spgemm_numeric_kernel<PREC>, grid_for(kNumWarps, A->blc_row, sm_count, 6), 32 * kNumWarps, smem, s,
-                A->row, A->blc_row, A->blcPtr, A->blcIdx, (const V *)aval, B->blcPtr, B->blcIdx, (const V *)bval,
-                C->blcPtr, C->blcIdx, C->blcMap, C->blcVal, cshadow, Ccsr ? Ccsr->i : nullptr,
-                Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr, ub_off, skey, smap, pslot, cflags);
-    return AMGT_OK;
+    if (C->max_blc_per_row > kNumCap && 24LL * A->blc_row < (long long)C->blc_num)
+        return launch_numeric_cap<PREC, kNumCapWide>(A, aval, B, bval, C, cshadow, Ccsr, ub_off, skey, smap, pslot, s,
+                                                     sm_count, cflags);
+    return launch_numeric_cap<PREC, kNumCap>(A, aval, B, bval, C, cshadow, Ccsr, ub_off, skey, smap, pslot, s,
+                                             sm_count, cflags);
 }
 
 static void *shadow_of(const amgt_bsr *A, int prec)

@@ -56,6 +56,37 @@ def _pair(orc, kind):
         A = orc.laplacian(48, 40, 40)
         P, _ = orc.interp(48, 40, 40)
         return A, P
+    if kind == "AAA_7pt_wide":
+        # A * A^2 of the 7-point operator: every C row holds 33-64 blocks,
+        # enough block rows for the staged numeric, which then accumulates
+        # in 64-block shared-memory rows (random values: every rounding of
+        # the accumulation order shows)
+        T = orc.laplacian(48, 40, 40)
+        A = orc.CSR(T.m, T.n, T.ia, T.ja, np.random.default_rng(11).uniform(-1, 1, T.ja.size))
+        A2 = orc.bsr2csr(orc.spgemm(orc.csr2bsr(A), orc.csr2bsr(A))[0])
+        return A, A2
+    if kind == "AA_27pt_wide":
+        # A * A of the 27-point pattern: C rows of 50-75 blocks (64-block
+        # shared accumulators, the longer rows in global memory)
+        T = orc.box(40, 40, 24)
+        A = orc.CSR(T.m, T.n, T.ia, T.ja, np.random.default_rng(12).uniform(-1, 1, T.ja.size))
+        return A, A
+    if kind == "LONG_row_staged":
+        # the 7-point operator with its first four rows made long (every
+        # second column of the first 4,000): one block row of > 1024 pairs
+        # and > 64 C blocks among 19,200 short ones, so the staged numeric
+        # takes it (pairs found by searching the row's pattern, values
+        # accumulated in global memory)
+        T = orc.laplacian(48, 40, 40)
+        rng = np.random.default_rng(13)
+        ia, ja = T.ia.astype(np.int64), T.ja
+        long_cols = np.arange(0, 4000, 2, dtype=np.int32)
+        rows = [long_cols] * 4 + [ja[ia[i]:ia[i + 1]] for i in range(4, T.m)]
+        nia = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.int32)
+        nja = np.concatenate(rows).astype(np.int32)
+        A = orc.CSR(T.m, T.n, nia, nja, rng.uniform(-1, 1, nja.size))
+        B = orc.CSR(T.m, T.n, T.ia, T.ja, rng.uniform(-1, 1, T.ja.size))
+        return A, B
     if kind == "WIDE_row":
         # a dense first row: > 1024 C blocks in one row (the gathered numeric's
         # A-block-at-a-time ordering)
@@ -71,7 +102,8 @@ def _pair(orc, kind):
     raise KeyError(kind)
 
 
-KINDS = ["AP_7pt", "AP_varcoef27", "RAP_varcoef27", "AA_varcoef27", "AA_5pt", "AAA_27pt", "AP_7pt_large", "WIDE_row"]
+KINDS = ["AP_7pt", "AP_varcoef27", "RAP_varcoef27", "AA_varcoef27", "AA_5pt", "AAA_27pt", "AP_7pt_large",
+         "AAA_7pt_wide", "AA_27pt_wide", "LONG_row_staged", "WIDE_row"]
 
 
 @pytest.mark.parametrize("kind", KINDS)
