@@ -244,12 +244,8 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int *total)
     return x - v;
 }
 
-__device__ __forceinline__ int warp_sum(int v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-    return v;
-}
+// Sum over the full warp (one redux.sync; two's complement wraps alike).
+__device__ __forceinline__ int warp_sum(int v) { return (int)__reduce_add_sync(FULL, (unsigned)v); }
 
 // Grid sizes: a multiple of the SM count, capped by the work.
 inline int grid_for(int units_per_cta, long long units, int sm_count, int ctas_per_sm = 8)

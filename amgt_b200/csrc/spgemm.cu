@@ -55,26 +55,82 @@ __device__ __forceinline__ unsigned lanemask_lt(int lane) { return (1u << lane) 
 
 inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// A row of the symbolic pass: its block row, A block range and scratch
+// slice (offset, capacity = the pair bound, saturated).
+struct SymRow {
+    int b, a0, a1, ub;
+    long long base;
+};
+
+// The row of work item t (b = -1 past the end), read ahead of its use.
+__device__ __forceinline__ SymRow sym_row(int t, int nr, const int *__restrict__ rows, const int *__restrict__ aptr,
+                                          const int64_t *__restrict__ ub_off)
+{
+    SymRow h{-1, 0, 0, 0, 0};
+    if (t < nr) {
+        h.b = rows ? rows[t] : t;
+        h.a0 = aptr[h.b];
+        h.a1 = aptr[h.b + 1];
+        h.base = ub_off[h.b];
+        const long long u = ub_off[h.b + 1] - h.base;
+        h.ub = u > 0x7FFFFFFF ? 0x7FFFFFFF : (int)u;
+    }
+    return h;
+}
+
+// This lane's A block of a row's first 32 (column k, bitmap) and the range
+// of the B row it selects, read in two steps a row ahead of their use.
+struct SymLane {
+    int k, j0, len;
+    uint32_t ma;
+};
+template <int CAP>
+__device__ __forceinline__ void sym_lane_a(const SymRow &h, int lane, const int *__restrict__ aidx,
+                                           const uint16_t *__restrict__ amap, SymLane &l)
+{
+    l.k = -1;
+    l.ma = 0;
+    if (h.b >= 0 && h.ub <= CAP && h.a0 + lane < h.a1) {
+        l.k = aidx[h.a0 + lane];
+        l.ma = amap[h.a0 + lane];
+    }
+}
+__device__ __forceinline__ void sym_lane_b(SymLane &l, const int *__restrict__ bptr)
+{
+    l.j0 = 0;
+    l.len = 0;
+    if (l.k >= 0) {
+        l.j0 = bptr[l.k];
+        l.len = bptr[l.k + 1] - l.j0;
+    }
+}
+
 // Appends the row's non-zero-product pairs to the warp's list s[]; returns
 // the count (the caller bounds it via the upper bound).  Up to 32 A blocks
-// at a time: lane i fetches A block i's B row range, a warp scan of the
-// range lengths flattens the (A block, B block) pairs, and lane t takes
-// pair t, finding its A block by a five-step shuffle search; so every load
-// of a chunk is in flight at once.  Pairs come out in (A block, B block)
+// at a time: lane i fetches A block i's B row range (for the first 32,
+// `pre`, read ahead by the caller), a warp scan of the range lengths
+// flattens the (A block, B block) pairs, and lane t takes pair t, finding
+// its A block by a five-step shuffle search; so every load of a chunk is in
+// flight at once.  Pairs come out in (A block, B block)
 // order, tagged with their ordinal in the row (< 65536: rows here have at
 // most kSymCap pairs); pslot[ordinal] = 0xFFFF marks the pairs whose
 // bitmap product is zero (they add nothing to C).
-__device__ __forceinline__ int sym_collect(int lane, int a0, int a1, const int *__restrict__ aidx,
-                                           const uint16_t *__restrict__ amap, const int *__restrict__ bptr,
-                                           const int *__restrict__ bidx, const uint16_t *__restrict__ bmap,
-                                           unsigned long long *s, uint16_t *__restrict__ pslot)
+__device__ __forceinline__ int sym_collect(int lane, int a0, int a1, const SymLane &pre,
+                                           const int *__restrict__ aidx, const uint16_t *__restrict__ amap,
+                                           const int *__restrict__ bptr, const int *__restrict__ bidx,
+                                           const uint16_t *__restrict__ bmap, unsigned long long *s,
+                                           uint16_t *__restrict__ pslot)
 {
     int cnt = 0, qbase = 0;
     for (int ib = a0; ib < a1; ib += 32) {
         const int i = ib + lane;
         int j0 = 0, len = 0;
         uint32_t ma = 0;
-        if (i < a1) {
+        if (ib == a0) {
+            j0 = pre.j0;
+            len = pre.len;
+            ma = pre.ma;
+        } else if (i < a1) {
             const int k = aidx[i];
             ma = amap[i];
             j0 = bptr[k];
@@ -319,28 +375,43 @@ spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *
     unsigned long long *s = sbuf[warp];
     unsigned long long wmax = 0, wsq = 0;  // per-warp statistics, one atomic each at the end
     const int nr = rows ? *nrows : brA;
-    for (int t = blockIdx.x * WARPS + warp; t < nr; t += gridDim.x * WARPS) {
-        const int b = rows ? rows[t] : t;
-        const int a0 = aptr[b], a1 = aptr[b + 1];
-        const long long ub = ub_off[b + 1] - ub_off[b];
-        if (ub > CAP) {
+    // rows are read ahead so that a row's chain of dependent loads (row
+    // pointers -> A blocks -> B row ranges) overlaps the previous rows'
+    // work: the row pointers two rows ahead, the A blocks and B ranges one
+    const int stride = gridDim.x * WARPS;
+    int t = blockIdx.x * WARPS + warp;
+    SymRow cur = sym_row(t, nr, rows, aptr, ub_off), nxt = sym_row(t + stride, nr, rows, aptr, ub_off);
+    SymLane cl;
+    sym_lane_a<CAP>(cur, lane, aidx, amap, cl);
+    sym_lane_b(cl, bptr);
+    for (; t < nr; t += stride) {
+        SymLane nl;
+        sym_lane_a<CAP>(nxt, lane, aidx, amap, nl);
+        const SymRow nxt2 = sym_row(t + 2 * stride, nr, rows, aptr, ub_off);
+        const int b = cur.b;
+        if (cur.ub > CAP) {
             if (lane == 0) over[atomicAdd(nover, 1)] = b;
-            continue;
-        }
-        const long long base = ub_off[b];
-        const int cnt = sym_collect(lane, a0, a1, aidx, amap, bptr, bidx, bmap, s, pslot + base);
-        int csr[4];
-        const int u = cnt <= 32 ? sym_reduce32(lane, cnt, s, skey + base, smap + base, csr, pslot + base)
-                                : sym_reduce_hashed<CAP>(lane, cnt, s, stkey[warp], stval[warp], skey + base,
-                                                         smap + base, csr, pslot + base, (int)ub, err);
-        if (lane == 0) {
-            ccnt[b] = u;
+            sym_lane_b(nl, bptr);
+        } else {
+            const long long base = cur.base;
+            const int cnt = sym_collect(lane, cur.a0, cur.a1, cl, aidx, amap, bptr, bidx, bmap, s, pslot + base);
+            sym_lane_b(nl, bptr);
+            int csr[4];
+            const int u = cnt <= 32 ? sym_reduce32(lane, cnt, s, skey + base, smap + base, csr, pslot + base)
+                                    : sym_reduce_hashed<CAP>(lane, cnt, s, stkey[warp], stval[warp], skey + base,
+                                                             smap + base, csr, pslot + base, cur.ub, err);
+            if (lane == 0) {
+                ccnt[b] = u;
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (4 * b + q < m) csrcnt[4 * b + q] = csr[q];
-            wmax = wmax > (unsigned long long)u ? wmax : (unsigned long long)u;
-            wsq += (unsigned long long)u * (unsigned long long)u;
+                for (int q = 0; q < 4; ++q)
+                    if (4 * b + q < m) csrcnt[4 * b + q] = csr[q];
+                wmax = wmax > (unsigned long long)u ? wmax : (unsigned long long)u;
+                wsq += (unsigned long long)u * (unsigned long long)u;
+            }
         }
+        cur = nxt;
+        nxt = nxt2;
+        cl = nl;
     }
     if (lane == 0 && wsq) {
         atomicMax((unsigned long long *)&stats[0], wmax);
