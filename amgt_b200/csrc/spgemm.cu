@@ -48,6 +48,10 @@ constexpr int kSymLargeThreads = 256;
 constexpr int kNumWarps = 4;
 constexpr int kNumCap = 32;       // C blocks a warp accumulates in shared memory (products of short C rows)
 constexpr int kNumCapWide = 64;   // the same for products whose C rows mostly exceed kNumCap blocks
+constexpr int kNumCapNarrow = 16; // the same for products of at most 16 C blocks per row
+// CTAs per SM of the numeric kernel for an accumulator capacity: shared
+// memory and registers (64 / 80 / 128 per thread) both allow that many
+__host__ __device__ constexpr int num_ctas_per_sm(int cap) { return cap <= 16 ? 8 : cap <= 32 ? 6 : 4; }
 constexpr int kNumWin = 128;      // pairs per window of the numeric's pair list
 constexpr int kOrdCap = 512;      // C blocks of a row the order kernel counts in shared memory
 
@@ -353,11 +357,12 @@ __global__ void spgemm_ub_kernel(int m, int brA, const int *__restrict__ aptr, c
 
 // One pass: per A block row, the sorted C block columns and bitmaps go to
 // the row's scratch slice (offset ub_off[b], capacity ub[b]); C blocks per
-// row -> ccnt[b], CSR nonzeros per scalar row -> csrcnt[4b+q].  Two
-// instances: CAP = 256 over all rows (small shared buffer, high occupancy),
-// passing rows with more pairs to the CAP = 1024 instance through a list
-// (rows[], count in *nrows), which passes rows beyond that to the window
-// kernel's list.
+// row -> ccnt[b], CSR nonzeros per scalar row -> csrcnt[4b+q].  Launched
+// with CAP = 256 over all rows (small shared buffer, high occupancy),
+// passing rows with more pairs to spgemm_symbolic_hashed_kernel (up to
+// 1024 pairs) through a list (rows[], count in *nrows), which passes rows
+// beyond that to the window kernel's list.  (Given rows[], the kernel takes
+// a list the same way.)
 template <int CAP, int WARPS>
 __global__ void __launch_bounds__(32 * WARPS)
 spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
@@ -412,6 +417,193 @@ spgemm_symbolic_kernel(int m, int brA, const int *__restrict__ aptr, const int *
         cur = nxt;
         nxt = nxt2;
         cl = nl;
+    }
+    if (lane == 0 && wsq) {
+        atomicMax((unsigned long long *)&stats[0], wmax);
+        atomicAdd((unsigned long long *)&stats[1], wsq);
+    }
+}
+
+// Bitonic sort of n ints (a power of two) in shared memory by one warp.
+__device__ __forceinline__ void warp_sort_smem_int(int *s, int n, int lane)
+{
+    for (int k = 2; k <= n; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < n; i += 32) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const int a = s[i], b = s[ixj];
+                    if ((a > b) == ((i & k) == 0)) {
+                        s[i] = b;
+                        s[ixj] = a;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Home slot of `key` in a shared hash table of H slots (linear probing
+// from there).
+template <int H>
+__device__ __forceinline__ int hash_slot(int key)
+{
+    return (int)(((unsigned)key * 0x9E3779B1u) >> (32 - __builtin_ctz(H)));
+}
+
+// Rows of 257 .. H pairs (the 256-pair instance's list): every pair with a
+// non-zero bitmap product goes straight into a shared hash table of the
+// row's C blocks (atomicCAS on the column, atomicOr on the bitmap, the
+// pair's table slot into pslot) as it is formed, with no list of the
+// row's pairs; the distinct columns are then sorted (a bitonic sort of
+// the keys, each key's slot found again by probing), and a second pass
+// over the row's pairs turns slots into ranks.  Same output as the
+// 256-pair instance (C's columns ascending with OR-ed bitmaps, each pair's
+// C block), in 12 KB of shared memory per warp, so that 18 warps per SM
+// hold rows.  Rows beyond H pairs go on to the window kernel's list.
+template <int H, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS)
+spgemm_symbolic_hashed_kernel(int m, const int *__restrict__ aptr, const int *__restrict__ aidx,
+                              const uint16_t *__restrict__ amap, const int *__restrict__ bptr,
+                              const int *__restrict__ bidx, const uint16_t *__restrict__ bmap,
+                              int *__restrict__ ccnt, int *__restrict__ csrcnt, int64_t *__restrict__ stats,
+                              const int64_t *__restrict__ ub_off, int *__restrict__ skey,
+                              uint16_t *__restrict__ smap, const int *__restrict__ rows,
+                              const int *__restrict__ nrows, int *__restrict__ over, int *__restrict__ nover,
+                              uint16_t *__restrict__ pslot, int *__restrict__ err)
+{
+    __shared__ int tkey_s[WARPS][H];
+    __shared__ unsigned tval_s[WARPS][H];
+    __shared__ int kbuf_s[WARPS][H];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int *tkey = tkey_s[warp], *kbuf = kbuf_s[warp];
+    unsigned *tval = tval_s[warp];
+    unsigned long long wmax = 0, wsq = 0;
+    const int nr = *nrows;
+    for (int t = blockIdx.x * WARPS + warp; t < nr; t += gridDim.x * WARPS) {
+        const int b = rows[t];
+        const int a0 = aptr[b], a1 = aptr[b + 1];
+        const long long base = ub_off[b], ub = ub_off[b + 1] - base;
+        if (ub > H) {
+            if (lane == 0) over[atomicAdd(nover, 1)] = b;
+            continue;
+        }
+        for (int i = lane; i < H; i += 32) {
+            tkey[i] = -1;
+            tval[i] = 0;
+        }
+        __syncwarp();
+        // pairs, 32 at a time (flattened as in sym_collect), into the table
+        int qbase = 0;
+        for (int ib = a0; ib < a1; ib += 32) {
+            const int i = ib + lane;
+            int j0 = 0, len = 0;
+            uint32_t ma = 0;
+            if (i < a1) {
+                const int k = aidx[i];
+                ma = amap[i];
+                j0 = bptr[k];
+                len = bptr[k + 1] - j0;
+            }
+            int incl = len;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int total = __shfl_sync(FULL, incl, 31);
+            const int excl = incl - len;
+            for (int t0 = 0; t0 < total; t0 += 32) {
+                const int tq = t0 + lane;
+                int src = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int v = __shfl_sync(FULL, incl, min(src + step - 1, 31));
+                    if (v <= tq) src += step;
+                }
+                src = min(src, 31);
+                const int sj0 = __shfl_sync(FULL, j0, src), sex = __shfl_sync(FULL, excl, src);
+                const uint32_t sma = __shfl_sync(FULL, ma, src);
+                if (tq < total) {
+                    const int j = sj0 + (tq - sex);
+                    const uint32_t mc = bitmap_mul(sma, bmap[j]);
+                    uint16_t slot = 0xFFFF;
+                    if (mc) {
+                        const int key = bidx[j];
+                        int h = hash_slot<H>(key), probe = 0;
+                        for (; probe < H; ++probe) {
+                            const int prev = atomicCAS(&tkey[h], -1, key);
+                            if (prev == -1 || prev == key) break;
+                            h = (h + 1) & (H - 1);
+                        }
+                        if (probe == H) {  // cannot happen (at most H pairs); kept as a bound
+                            raise_error(err, DEV_ERR_PROBE);
+                        } else {
+                            atomicOr(&tval[h], mc);
+                            slot = (uint16_t)h;
+                        }
+                    }
+                    pslot[base + qbase + tq] = slot;
+                }
+            }
+            qbase += total;
+        }
+        __syncwarp();
+        // distinct columns -> kbuf[0 .. u), then ascending
+        int u = 0;
+        for (int i0 = 0; i0 < H; i0 += 32) {
+            const int key = tkey[i0 + lane];
+            const unsigned bal = __ballot_sync(FULL, key >= 0);
+            if (key >= 0) kbuf[u + __popc(bal & lanemask_lt(lane))] = key;
+            u += __popc(bal);
+        }
+        __syncwarp();
+        if (u > 32) {
+            int n = 64;
+            while (n < u) n <<= 1;
+            for (int i = u + lane; i < n; i += 32) kbuf[i] = 0x7FFFFFFF;
+            __syncwarp();
+            warp_sort_smem_int(kbuf, n, lane);
+        } else {  // rank among at most 32 keys by comparing with all
+            const int key = lane < u ? kbuf[lane] : 0x7FFFFFFF;
+            int rank = 0;
+            for (int l = 0; l < u; ++l) rank += __shfl_sync(FULL, key, l) < key;
+            __syncwarp();
+            if (lane < u) kbuf[rank] = key;
+            __syncwarp();
+        }
+        // C block p: its column, OR-ed bitmap and CSR counts; its table slot
+        // then holds its rank
+        int c01 = 0, c23 = 0;  // CSR counts of scalar rows 0 / 1 and 2 / 3, 16 bits each
+        for (int p = lane; p < u; p += 32) {
+            const int key = kbuf[p];
+            int h = hash_slot<H>(key);
+            for (int probe = 0; probe < H && tkey[h] != key; ++probe) h = (h + 1) & (H - 1);
+            const uint32_t mp = tval[h];
+            skey[base + p] = key;
+            smap[base + p] = (uint16_t)mp;
+            c01 += __popc(mp & 0xFu) | (__popc((mp >> 4) & 0xFu) << 16);
+            c23 += __popc((mp >> 8) & 0xFu) | (__popc((mp >> 12) & 0xFu) << 16);
+            tval[h] = (unsigned)p;
+        }
+        __syncwarp();
+        for (int q = lane; q < ub; q += 32) {
+            const uint16_t h = pslot[base + q];
+            if (h != 0xFFFF) pslot[base + q] = (uint16_t)tval[h];
+        }
+        c01 = warp_sum(c01);
+        c23 = warp_sum(c23);
+        if (lane == 0) {
+            ccnt[b] = u;
+            const int csr[4] = {c01 & 0xFFFF, c01 >> 16, c23 & 0xFFFF, c23 >> 16};
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (4 * b + q < m) csrcnt[4 * b + q] = csr[q];
+            wmax = wmax > (unsigned long long)u ? wmax : (unsigned long long)u;
+            wsq += (unsigned long long)u * (unsigned long long)u;
+        }
+        __syncwarp();
     }
     if (lane == 0 && wsq) {
         atomicMax((unsigned long long *)&stats[0], wmax);
@@ -700,13 +892,12 @@ struct NumSmem {
 // are added to their C block in pair order (= A block order): pairs of one
 // step that hit the same C block row are applied in rounds, lowest lane
 // first (match_any), so the accumulation order is the sequential one.  Rows
-// of up to CAP C blocks (32; 64 for products of long C rows, at two thirds
-// of the warps per SM) accumulate in shared memory, longer rows in place in
-// C.  For fp64 with cshadow given, the final store also writes the fp16
+// of up to CAP C blocks (16, 32 or 64 by C's row lengths, at 32, 24 or 16
+// warps per SM) accumulate in shared memory, longer rows in place in C.  For fp64 with cshadow given, the final store also writes the fp16
 // rounding of every C value and the exactness bits of exact_check_kernel
 // into *cflags (bit 0: some value not an fp32 value, bit 1: not fp16).
 template <int PREC, int CAP>
-__global__ void __launch_bounds__(32 * kNumWarps, CAP == kNumCap ? 6 : 4)
+__global__ void __launch_bounds__(32 * kNumWarps, num_ctas_per_sm(CAP))
 spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *__restrict__ aidx,
                       const typename NumT<PREC>::val_t *__restrict__ aval, const int *__restrict__ bptr,
                       const int *__restrict__ bidx, const typename NumT<PREC>::val_t *__restrict__ bval,
@@ -1363,7 +1554,7 @@ static int launch_numeric_cap(const amgt_bsr *A, const void *aval, const amgt_bs
 {
     using V = typename NumT<PREC>::val_t;
     constexpr int smem = kNumWarps * NumSmem<PREC, CAP>::per_warp;
-    constexpr int per_sm = CAP == kNumCap ? 6 : 4;
+    constexpr int per_sm = num_ctas_per_sm(CAP);
     AMGT_CUDA_TRY(cudaFuncSetAttribute(spgemm_numeric_kernel<PREC, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        smem));
     AMGT_LAUNCH((spgemm_numeric_kernel<PREC, CAP>), grid_for(kNumWarps, A->blc_row, sm_count, per_sm),
@@ -1374,8 +1565,9 @@ static int launch_numeric_cap(const amgt_bsr *A, const void *aval, const amgt_bs
 }
 
 // The staged numeric with the accumulator capacity for C's row lengths:
-// 64 C blocks when the average C row exceeds 24 blocks (most rows would
-// otherwise accumulate in global memory), else 32 at more warps per SM.
+// 16 C blocks when no C row is longer (32 warps per SM), 64 when the
+// average C row exceeds 24 blocks (most rows would otherwise accumulate in
+// global memory; 16 warps per SM), else 32 (24 warps per SM).
 template <int PREC>
 static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B, const void *bval, amgt_bsr *C,
                           void *cshadow, amgt_csr *Ccsr, const int64_t *ub_off, const int *skey,
@@ -1383,6 +1575,9 @@ static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B
                           unsigned long long *cflags = nullptr)
 {
     if (A->blc_row == 0) return AMGT_OK;
+    if (C->max_blc_per_row <= kNumCapNarrow)
+        return launch_numeric_cap<PREC, kNumCapNarrow>(A, aval, B, bval, C, cshadow, Ccsr, ub_off, skey, smap, pslot,
+                                                       s, sm_count, cflags);
     if (C->max_blc_per_row > kNumCap && 24LL * A->blc_row < (long long)C->blc_num)
         return launch_numeric_cap<PREC, kNumCapWide>(A, aval, B, bval, C, cshadow, Ccsr, ub_off, skey, smap, pslot, s,
                                                      sm_count, cflags);
@@ -1508,9 +1703,9 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
                     32 * kSymWarps, 0, s, m, brA, A->blcPtr, A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap,
                     ccnt, csrcnt, large, stats, ub_off, skey, smap, nullptr, nullptr, medium, nmedium, pslot,
                     st->err);
-        AMGT_LAUNCH((spgemm_symbolic_kernel<kSymCap, 2>), 6 * st->sm_count, 64, 0, s, m, brA, A->blcPtr,
-                    A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, ccnt, csrcnt, large, stats, ub_off, skey,
-                    smap, medium, nmedium, large, (int *)&stats[3], pslot, st->err);
+        AMGT_LAUNCH((spgemm_symbolic_hashed_kernel<kSymCap, 2>), 9 * st->sm_count, 64, 0, s, m, A->blcPtr,
+                    A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, ccnt, csrcnt, stats, ub_off, skey, smap,
+                    medium, nmedium, large, (int *)&stats[3], pslot, st->err);
         AMGT_LAUNCH(spgemm_symbolic_large_kernel, 6 * st->sm_count, kSymLargeThreads, 0, s, m, A->blcPtr, A->blcIdx,
                     A->blcMap, B->blcPtr, B->blcIdx, B->blcMap, large, stats, ccnt, csrcnt, ub_off, skey, smap);
     }
