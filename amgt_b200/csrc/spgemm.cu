@@ -49,9 +49,13 @@ constexpr int kNumWarps = 4;
 constexpr int kNumCap = 32;       // C blocks a warp accumulates in shared memory (products of short C rows)
 constexpr int kNumCapWide = 64;   // the same for products whose C rows mostly exceed kNumCap blocks
 constexpr int kNumCapNarrow = 16; // the same for products of at most 16 C blocks per row
+constexpr int kNumCapMid = 24;    // ... and of at most 24
 // CTAs per SM of the numeric kernel for an accumulator capacity: shared
-// memory and registers (64 / 80 / 128 per thread) both allow that many
-__host__ __device__ constexpr int num_ctas_per_sm(int cap) { return cap <= 16 ? 8 : cap <= 32 ? 6 : 4; }
+// memory and registers (64 / 72 / 80 / 128 per thread) both allow that many
+__host__ __device__ constexpr int num_ctas_per_sm(int cap)
+{
+    return cap <= 16 ? 8 : cap <= 24 ? 7 : cap <= 32 ? 6 : 4;
+}
 constexpr int kNumWin = 128;      // pairs per window of the numeric's pair list
 constexpr int kOrdCap = 512;      // C blocks of a row the order kernel counts in shared memory
 
@@ -892,8 +896,9 @@ struct NumSmem {
 // are added to their C block in pair order (= A block order): pairs of one
 // step that hit the same C block row are applied in rounds, lowest lane
 // first (match_any), so the accumulation order is the sequential one.  Rows
-// of up to CAP C blocks (16, 32 or 64 by C's row lengths, at 32, 24 or 16
-// warps per SM) accumulate in shared memory, longer rows in place in C.  For fp64 with cshadow given, the final store also writes the fp16
+// of up to CAP C blocks (16, 24, 32 or 64 by C's row lengths, at 32, 28,
+// 24 or 16 warps per SM) accumulate in shared memory, longer rows in place
+// in C.  For fp64 with cshadow given, the final store also writes the fp16
 // rounding of every C value and the exactness bits of exact_check_kernel
 // into *cflags (bit 0: some value not an fp32 value, bit 1: not fp16).
 template <int PREC, int CAP>
@@ -1565,9 +1570,9 @@ static int launch_numeric_cap(const amgt_bsr *A, const void *aval, const amgt_bs
 }
 
 // The staged numeric with the accumulator capacity for C's row lengths:
-// 16 C blocks when no C row is longer (32 warps per SM), 64 when the
-// average C row exceeds 24 blocks (most rows would otherwise accumulate in
-// global memory; 16 warps per SM), else 32 (24 warps per SM).
+// 16 or 24 C blocks when no C row is longer (32 / 28 warps per SM), 64 when
+// the average C row exceeds 24 blocks (most rows would otherwise accumulate
+// in global memory; 16 warps per SM), else 32 (24 warps per SM).
 template <int PREC>
 static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B, const void *bval, amgt_bsr *C,
                           void *cshadow, amgt_csr *Ccsr, const int64_t *ub_off, const int *skey,
@@ -1578,6 +1583,9 @@ static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B
     if (C->max_blc_per_row <= kNumCapNarrow)
         return launch_numeric_cap<PREC, kNumCapNarrow>(A, aval, B, bval, C, cshadow, Ccsr, ub_off, skey, smap, pslot,
                                                        s, sm_count, cflags);
+    if (C->max_blc_per_row <= kNumCapMid)
+        return launch_numeric_cap<PREC, kNumCapMid>(A, aval, B, bval, C, cshadow, Ccsr, ub_off, skey, smap, pslot, s,
+                                                    sm_count, cflags);
     if (C->max_blc_per_row > kNumCap && 24LL * A->blc_row < (long long)C->blc_num)
         return launch_numeric_cap<PREC, kNumCapWide>(A, aval, B, bval, C, cshadow, Ccsr, ub_off, skey, smap, pslot, s,
                                                      sm_count, cflags);
@@ -1699,7 +1707,18 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     if (brA > 0) {
         // medium-row list and count live behind the large list (2 * brA + 1 ints)
         int *medium = large + brA, *nmedium = large + 2 * brA;  // *nmedium cleared by spgemm_ub_kernel
-        AMGT_LAUNCH((spgemm_symbolic_kernel<256, kSymWarps>), grid_for(kSymWarps, brA, st->sm_count, 16),
+        // as many CTAs as are resident at once: the rows are shared out
+        // evenly, and no CTA waits for a slot to take its share
+        static const int sym_resident = [] {
+            int n = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, spgemm_symbolic_kernel<256, kSymWarps>,
+                                                              32 * kSymWarps, 0) != cudaSuccess || n < 1) {
+                (void)cudaGetLastError();  // clear the error of the query; a default grid follows
+                n = 8;
+            }
+            return n;
+        }();
+        AMGT_LAUNCH((spgemm_symbolic_kernel<256, kSymWarps>), grid_for(kSymWarps, brA, st->sm_count, sym_resident),
                     32 * kSymWarps, 0, s, m, brA, A->blcPtr, A->blcIdx, A->blcMap, B->blcPtr, B->blcIdx, B->blcMap,
                     ccnt, csrcnt, large, stats, ub_off, skey, smap, nullptr, nullptr, medium, nmedium, pslot,
                     st->err);

@@ -56,6 +56,19 @@ def _pair(orc, kind):
         A = orc.laplacian(48, 40, 40)
         P, _ = orc.interp(48, 40, 40)
         return A, P
+    if kind == "AA_7pt_large":
+        # C rows of 17-23 blocks: the staged numeric with 24-block
+        # accumulators (random values: every rounding of the order shows)
+        T = orc.laplacian(48, 40, 40)
+        A = orc.CSR(T.m, T.n, T.ia, T.ja, np.random.default_rng(14).uniform(-1, 1, T.ja.size))
+        return A, A
+    if kind == "A2A2_9pt":
+        # A^2 * A^2 of the 9-point pattern: C rows of 25-27 blocks, the staged
+        # numeric with 32-block accumulators
+        T = orc.box(200, 200, 1)
+        A = orc.CSR(T.m, T.n, T.ia, T.ja, np.random.default_rng(15).uniform(-1, 1, T.ja.size))
+        A2 = orc.bsr2csr(orc.spgemm(orc.csr2bsr(A), orc.csr2bsr(A))[0])
+        return A2, A2
     if kind == "AAA_7pt_wide":
         # A * A^2 of the 7-point operator: every C row holds 33-64 blocks,
         # enough block rows for the staged numeric, which then accumulates
@@ -103,7 +116,7 @@ def _pair(orc, kind):
 
 
 KINDS = ["AP_7pt", "AP_varcoef27", "RAP_varcoef27", "AA_varcoef27", "AA_5pt", "AAA_27pt", "AP_7pt_large",
-         "AAA_7pt_wide", "AA_27pt_wide", "LONG_row_staged", "WIDE_row"]
+         "AA_7pt_large", "A2A2_9pt", "AAA_7pt_wide", "AA_27pt_wide", "LONG_row_staged", "WIDE_row"]
 
 
 @pytest.mark.parametrize("kind", KINDS)
