@@ -615,8 +615,58 @@ spgemm_symbolic_hashed_kernel(int m, const int *__restrict__ aptr, const int *__
     }
 }
 
+// The row's (A block, B block) pairs with a non-zero bitmap product, given
+// to f(column, product bitmap): warp `warp` of `nw` takes A blocks a0 +
+// warp + nw * l, 32 of them at a time (lane l fetches A block l's B row
+// range, a warp scan of the lengths flattens the pairs, lane t takes pair
+// t, finding its A block by a five-step shuffle search), so that every load
+// of a chunk is in flight at once.
+template <typename F>
+__device__ __forceinline__ void for_row_pairs(int a0, int a1, int warp, int nw, int lane,
+                                              const int *__restrict__ aidx, const uint16_t *__restrict__ amap,
+                                              const int *__restrict__ bptr, const int *__restrict__ bidx,
+                                              const uint16_t *__restrict__ bmap, F f)
+{
+    for (int c0 = a0 + warp; c0 < a1; c0 += 32 * nw) {
+        const int i = c0 + nw * lane;
+        int j0 = 0, len = 0;
+        uint32_t ma = 0;
+        if (i < a1) {
+            const int k = aidx[i];
+            ma = amap[i];
+            j0 = bptr[k];
+            len = bptr[k + 1] - j0;
+        }
+        int incl = len;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int total = __shfl_sync(FULL, incl, 31);
+        const int excl = incl - len;
+        for (int t0 = 0; t0 < total; t0 += 32) {
+            const int t = t0 + lane;
+            int src = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int v = __shfl_sync(FULL, incl, min(src + step - 1, 31));
+                if (v <= t) src += step;
+            }
+            src = min(src, 31);
+            const int sj0 = __shfl_sync(FULL, j0, src), sex = __shfl_sync(FULL, excl, src);
+            const uint32_t sma = __shfl_sync(FULL, ma, src);
+            if (t < total) {
+                const int j = sj0 + (t - sex);
+                const uint32_t mc = bitmap_mul(sma, bmap[j]);
+                if (mc) f(bidx[j], mc);
+            }
+        }
+    }
+}
+
 // Rows with more than kSymCap pairs: window sweep over the reachable block
-// columns, 8 warps walking the A blocks, lanes the B rows.
+// columns, the row's pairs flattened over the CTA's warps (for_row_pairs).
 __global__ void __launch_bounds__(kSymLargeThreads)
 spgemm_symbolic_large_kernel(int m, const int *__restrict__ aptr, const int *__restrict__ aidx,
                              const uint16_t *__restrict__ amap, const int *__restrict__ bptr,
@@ -640,15 +690,10 @@ spgemm_symbolic_large_kernel(int m, const int *__restrict__ aptr, const int *__r
         }
         __syncthreads();
         int lo = 0x7FFFFFFF, hi = -1;
-        for (int i = a0 + warp; i < a1; i += nw) {
-            const int k = aidx[i];
-            const uint32_t ma = amap[i];
-            for (int j = bptr[k] + lane; j < bptr[k + 1]; j += 32)
-                if (bitmap_mul(ma, bmap[j])) {
-                    lo = min(lo, bidx[j]);
-                    hi = max(hi, bidx[j]);
-                }
-        }
+        for_row_pairs(a0, a1, warp, nw, lane, aidx, amap, bptr, bidx, bmap, [&](int key, uint32_t) {
+            lo = min(lo, key);
+            hi = max(hi, key);
+        });
         atomicMin(&smin, lo);
         atomicMax(&smax, hi);
         __syncthreads();
@@ -659,16 +704,10 @@ spgemm_symbolic_large_kernel(int m, const int *__restrict__ aptr, const int *__r
         for (long long w0 = kmin; w0 <= kmax; w0 += kSymWin) {
             for (int i = tid; i < kSymWin; i += blockDim.x) maps[i] = 0;
             __syncthreads();
-            for (int i = a0 + warp; i < a1; i += nw) {
-                const int k = aidx[i];
-                const uint32_t ma = amap[i];
-                for (int j = bptr[k] + lane; j < bptr[k + 1]; j += 32) {
-                    const long long key = bidx[j] - w0;
-                    if (key < 0 || key >= kSymWin) continue;
-                    const uint32_t mc = bitmap_mul(ma, bmap[j]);
-                    if (mc) atomicOr(&maps[key], mc);
-                }
-            }
+            for_row_pairs(a0, a1, warp, nw, lane, aidx, amap, bptr, bidx, bmap, [&](int col, uint32_t mc) {
+                const long long key = col - w0;
+                if (key >= 0 && key < kSymWin) atomicOr(&maps[key], mc);
+            });
             __syncthreads();
             const int s0 = tid * (kSymWin / kSymLargeThreads);
             int c = 0;
@@ -1183,8 +1222,13 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
 //   levels, whose few long rows leave the staged kernel's warps idle) or
 //   with more than an eighth of their rows beyond kSymCap pairs; the staged
 //   kernel keeps the others.
-//   gather  four lanes per C block (lane r: row r), each pair's A row and
-//           B block read from global memory (L1 / L2), the product entry the
+//   gather  four lanes per C block (lane r: row r), the C block's pairs
+//           streamed through a ring of kGatherSlots shared-memory slots per
+//           C block (lane r copies row r of the pair's A block and of its B
+//           block with cp.async, kGatherSlots - 1 pairs ahead, the list
+//           entries four to eight ahead in registers, the next C block's
+//           bounds and first entries during this one), so that several
+//           pairs' loads of every C block are in flight; the product entry the
 //           same fused chain as the staged kernel, the products added in
 //           list order: C equals the staged kernel's result bit for bit.
 // Writes C's values (+ shadow, + the fused exactness bits); the CSR form,
@@ -1330,27 +1374,17 @@ spgemm_order_kernel(int brA, const int *__restrict__ aptr, const int *__restrict
     }
 }
 
-// One block row (four values) of a stored block, widened to the
-// accumulator type, through the read-only path.
+constexpr int kGatherSlots = 4;     // ring slots per C block: pairs in flight = kGatherSlots - 1
+constexpr int kGatherThreads = 128;  // 32 C blocks per CTA
 template <int PREC>
-__device__ __forceinline__ void row4_ldg(const typename NumT<PREC>::val_t *p, typename NumT<PREC>::acc_t out[4])
-{
-    if constexpr (PREC == AMGT_DOUBLE) {
-        const double2 u = __ldg(reinterpret_cast<const double2 *>(p)), w = __ldg(reinterpret_cast<const double2 *>(p) + 1);
-        out[0] = u.x; out[1] = u.y; out[2] = w.x; out[3] = w.y;
-    } else if constexpr (PREC == AMGT_FLOAT) {
-        const float4 u = __ldg(reinterpret_cast<const float4 *>(p));
-        out[0] = u.x; out[1] = u.y; out[2] = u.z; out[3] = u.w;
-    } else {
-        const uint2 u = __ldg(reinterpret_cast<const uint2 *>(p));
-        const typename NumT<PREC>::val_t *v = reinterpret_cast<const typename NumT<PREC>::val_t *>(&u);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) out[q] = NumT<PREC>::ld(v, q);
-    }
-}
+struct GatherSmem {
+    static constexpr int AR = 4 * (int)sizeof(typename NumT<PREC>::val_t);  // one block row
+    static constexpr int slot = 8 * AR;                                     // A block, then B block
+    static constexpr int per_cta = (kGatherThreads / 4) * kGatherSlots * slot;
+};
 
 template <int PREC>
-__global__ void __launch_bounds__(256, 5)
+__global__ void __launch_bounds__(kGatherThreads, 6)
 spgemm_gather_kernel(int nbC, const typename NumT<PREC>::val_t *__restrict__ aval,
                      const typename NumT<PREC>::val_t *__restrict__ bval, const int2 *__restrict__ glist,
                      const long long *__restrict__ gbeg, const int *__restrict__ gnum, double *__restrict__ cval,
@@ -1358,28 +1392,103 @@ spgemm_gather_kernel(int nbC, const typename NumT<PREC>::val_t *__restrict__ ava
 {
     using T = NumT<PREC>;
     using acc_t = typename T::acc_t;
+    using GS = GatherSmem<PREC>;
+    constexpr int AR = GS::AR, SLOT = GS::slot, S = kGatherSlots;
+    extern __shared__ __align__(16) unsigned char gather_smem[];
     const int r = threadIdx.x & 3;
+    const unsigned gmask = 0xFu << (threadIdx.x & 28);  // this C block's four lanes
+    unsigned char *ring = gather_smem + (threadIdx.x >> 2) * S * SLOT;
     bool not32 = false, not16 = false;
     const long long g0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 2;
     const long long gstride = ((long long)gridDim.x * blockDim.x) >> 2;
+    // copies of row r of pair pr's A block and B block into slot `sl`
+    auto issue = [&](int2 pr, int sl) {
+        const unsigned char *asrc = reinterpret_cast<const unsigned char *>(aval + 16LL * pr.x + 4 * r);
+        const unsigned char *bsrc = reinterpret_cast<const unsigned char *>(bval + 16LL * pr.y + 4 * r);
+        unsigned char *adst = ring + sl * SLOT + r * AR, *bdst = adst + 4 * AR;
+        if constexpr (AR == 32) {
+            cp_async16(adst, asrc);
+            cp_async16(adst + 16, asrc + 16);
+            cp_async16(bdst, bsrc);
+            cp_async16(bdst + 16, bsrc + 16);
+        } else if constexpr (AR == 16) {
+            cp_async16(adst, asrc);
+            cp_async16(bdst, bsrc);
+        } else {
+            cp_async8(adst, asrc);
+            cp_async8(bdst, bsrc);
+        }
+    };
+    // list entries travel in batches of four, lane r holding entry 4m + r of
+    // its C block's list and handing it to the group by a shuffle: the batch
+    // after the one being issued is already in flight, and the next C
+    // block's bounds and first batch are read while this one is computed
+    const int gl = threadIdx.x & 28;  // the group's first lane in the warp
+    auto entry = [&](long long beg, int n, int i) -> int2 {
+        return i < n ? __ldg(glist + beg + i) : make_int2(0, 0);
+    };
+    long long beg = 0, begN = 0;
+    int n = 0, nN = 0;
+    int2 ent = make_int2(0, 0);
+    if (g0 < nbC) {
+        beg = gbeg[g0];
+        n = gnum[g0];
+        ent = entry(beg, n, r);
+    }
+    if (g0 + gstride < nbC) {
+        begN = gbeg[g0 + gstride];
+        nN = gnum[g0 + gstride];
+    }
     for (long long g = g0; g < nbC; g += gstride) {
-        const long long beg = gbeg[g];
-        const int n = gnum[g];
+        // the C block after next: its bounds; the next one: its first batch
+        long long begNN = 0;
+        int nNN = 0;
+        if (g + 2 * gstride < nbC) {
+            begNN = gbeg[g + 2 * gstride];
+            nNN = gnum[g + 2 * gstride];
+        }
+        const int2 entNext = entry(begN, nN, r);
+        int2 entn = entry(beg, n, 4 + r);
+        int kb = 0;  // first entry of the batch in `ent`
+        auto take = [&](int i) -> int2 {  // entry i (kb <= i < kb + 4) from its lane
+            const int src = gl | (i - kb);
+            return make_int2(__shfl_sync(gmask, ent.x, src), __shfl_sync(gmask, ent.y, src));
+        };
+        // pairs 0 .. S-2 in flight
+#pragma unroll
+        for (int u = 0; u < S - 1; ++u) {
+            const int2 pr = take(u);
+            if (u < n) issue(pr, u);
+            cp_async_commit();
+        }
         acc_t acc[4] = {(acc_t)0, (acc_t)0, (acc_t)0, (acc_t)0};
         for (int k = 0; k < n; ++k) {
-            const int2 pr = __ldg(glist + beg + k);
+            const int ka = k + S - 1;  // the pair issued now
+            if (ka == kb + 4) {        // next batch; the one after it goes in flight
+                ent = entn;
+                kb += 4;
+                entn = entry(beg, n, kb + 4 + r);
+            }
+            const int2 pr = take(ka);
+            if (ka < n) issue(pr, ka % S);
+            cp_async_commit();
+            cp_async_wait<S - 1>();  // pair k's copies are complete
+            __syncwarp(gmask);
+            const unsigned char *sl = ring + (k % S) * SLOT;
             acc_t ar[4], s[4];
-            row4_ldg<PREC>(aval + 16LL * pr.x + 4 * r, ar);
+            row4_smem<PREC>(sl + r * AR, ar);
 #pragma unroll
             for (int kk = 0; kk < 4; ++kk) {
                 acc_t bk[4];
-                row4_ldg<PREC>(bval + 16LL * pr.y + 4 * kk, bk);
+                row4_smem<PREC>(sl + 4 * AR + kk * AR, bk);
 #pragma unroll
                 for (int c = 0; c < 4; ++c) s[c] = T::madd(ar[kk], bk[c], s[c], kk == 0);
             }
 #pragma unroll
             for (int c = 0; c < 4; ++c) acc[c] = T::add(acc[c], s[c]);
+            __syncwarp(gmask);  // slot k % S is refilled by the next iteration's issue
         }
+        cp_async_wait<0>();
         double *d = cval + 16 * g + 4 * r;
         reinterpret_cast<double2 *>(d)[0] = make_double2((double)acc[0], (double)acc[1]);
         reinterpret_cast<double2 *>(d)[1] = make_double2((double)acc[2], (double)acc[3]);
@@ -1397,6 +1506,11 @@ spgemm_gather_kernel(int nbC, const typename NumT<PREC>::val_t *__restrict__ ava
 #pragma unroll
             for (int c = 0; c < 4; ++c) store_shadow<PREC>(cshadow, 16 * g + 4 * r + c, acc[c]);
         }
+        beg = begN;
+        n = nN;
+        begN = begNN;
+        nN = nNN;
+        ent = entNext;
     }
     if (PREC == AMGT_DOUBLE && cshadow) {
         const unsigned b32 = __ballot_sync(FULL, not32), b16 = __ballot_sync(FULL, not16);
@@ -1796,7 +1910,18 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
         int *gnum = reinterpret_cast<int *>(arena3 + o_num);
         if (brA > 0) {
             AMGT_CUDA_TRY(cudaMemsetAsync(gnum, 0, 4 * (size_t)nbC + 4, s));
-            AMGT_LAUNCH(spgemm_order_kernel, grid_for(kNumWarps, brA, st->sm_count, 8), 32 * kNumWarps, 0, s, brA,
+            static const int ord_resident = [] {  // CTAs resident at once
+                int n = 0;
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, spgemm_order_kernel, 32 * kNumWarps, 0) !=
+                        cudaSuccess ||
+                    n < 1) {
+                    (void)cudaGetLastError();  // clear the error of the query; a default grid follows
+                    n = 8;
+                }
+                return n;
+            }();
+            AMGT_LAUNCH(spgemm_order_kernel, grid_for(kNumWarps, brA, st->sm_count, ord_resident), 32 * kNumWarps, 0,
+                        s, brA,
                         A->blcPtr, A->blcIdx, B->blcPtr, B->blcIdx, C->blcPtr, C->blcIdx, C->blcMap, ub_off, skey,
                         smap, pslot, glist, gbeg, gnum);
         }
@@ -1810,25 +1935,28 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
                 AMGT_LAUNCH(spgemm_gather_mma_kernel<AMGT_BF16>, grid, 128, 0, s, nbC, Atmp.blcVal_bf16,
                             Btmp.blcVal_bf16, glist, gbeg, gnum, C->blcVal, cshadow);
         } else if (nbC > 0) {
-            const long long want = (4LL * nbC + 255) / 256;
-            const int grid = (int)std::min<long long>(want, 16LL * st->sm_count);
+            // four lanes per C block; as many CTAs as are resident at once
+            const long long want = (4LL * nbC + kGatherThreads - 1) / kGatherThreads;
+            const int grid = (int)std::min<long long>(want, 6LL * st->sm_count);
             unsigned long long *flags = fuse ? reinterpret_cast<unsigned long long *>(fuse->flags) : nullptr;
             switch (prec) {
             case AMGT_DOUBLE:
-                AMGT_LAUNCH(spgemm_gather_kernel<AMGT_DOUBLE>, grid, 256, 0, s, nbC, A->blcVal, B->blcVal, glist,
-                            gbeg, gnum, C->blcVal, cshadow, flags);
+                AMGT_LAUNCH(spgemm_gather_kernel<AMGT_DOUBLE>, grid, kGatherThreads, GatherSmem<AMGT_DOUBLE>::per_cta,
+                            s, nbC, A->blcVal, B->blcVal, glist, gbeg, gnum, C->blcVal, cshadow, flags);
                 break;
             case AMGT_FLOAT:
-                AMGT_LAUNCH(spgemm_gather_kernel<AMGT_FLOAT>, grid, 256, 0, s, nbC, Atmp.blcVal_fp32,
-                            Btmp.blcVal_fp32, glist, gbeg, gnum, C->blcVal, cshadow, nullptr);
+                AMGT_LAUNCH(spgemm_gather_kernel<AMGT_FLOAT>, grid, kGatherThreads, GatherSmem<AMGT_FLOAT>::per_cta, s,
+                            nbC, Atmp.blcVal_fp32, Btmp.blcVal_fp32, glist, gbeg, gnum, C->blcVal, cshadow, nullptr);
                 break;
             case AMGT_HALF:
-                AMGT_LAUNCH(spgemm_gather_kernel<AMGT_HALF>, grid, 256, 0, s, nbC, (const __half *)Atmp.blcVal_fp16,
-                            (const __half *)Btmp.blcVal_fp16, glist, gbeg, gnum, C->blcVal, cshadow, nullptr);
+                AMGT_LAUNCH(spgemm_gather_kernel<AMGT_HALF>, grid, kGatherThreads, GatherSmem<AMGT_HALF>::per_cta, s,
+                            nbC, (const __half *)Atmp.blcVal_fp16, (const __half *)Btmp.blcVal_fp16, glist, gbeg, gnum,
+                            C->blcVal, cshadow, nullptr);
                 break;
             default:
-                AMGT_LAUNCH(spgemm_gather_kernel<AMGT_BF16>, grid, 256, 0, s, nbC,
-                            (const __nv_bfloat16 *)Atmp.blcVal_bf16, (const __nv_bfloat16 *)Btmp.blcVal_bf16, glist, gbeg, gnum, C->blcVal, cshadow, nullptr);
+                AMGT_LAUNCH(spgemm_gather_kernel<AMGT_BF16>, grid, kGatherThreads, GatherSmem<AMGT_BF16>::per_cta, s,
+                            nbC, (const __nv_bfloat16 *)Atmp.blcVal_bf16, (const __nv_bfloat16 *)Btmp.blcVal_bf16,
+                            glist, gbeg, gnum, C->blcVal, cshadow, nullptr);
                 break;
             }
         }
