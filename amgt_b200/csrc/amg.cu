@@ -786,16 +786,26 @@ int cycle(amgt_amg *h, const double *rhs0, double *out0, cudaStream_t s)
     const int L = (int)lv.size();
     const double w = h->prm.relax_weight;
     const bool pk = h->prm.packed != 0;
+    bool have_u = false;  // level l's sweep from a zero guess came with the restriction into it
     for (int l = 0; l < L - 1; ++l) {
         Level &v = lv[l];
         const double *f = (l == 0) ? rhs0 : v.f;
-        AMGT_LAUNCH_PDL(jacobi_zero_kernel, grid_n(h, v.n), 256, 0, s, (long long)v.n, f, v.inv_l1, w, v.u);
+        if (!have_u)
+            AMGT_LAUNCH_PDL(jacobi_zero_kernel, grid_n(h, v.n), 256, 0, s, (long long)v.n, f, v.inv_l1, w, v.u);
+        have_u = false;
         if (pk) {
             AMGT_TRY(pbsr_residual(&v.pA, f, v.u, v.t, s, h->sm_count));
             AMGT_TRY(pbsr_spmv(&v.pR, 1.0, v.t, 0.0, lv[l + 1].f, s, h->sm_count));
         } else {
             AMGT_TRY(spmv_residual(l == 0 ? h->resid_prec0 : v.prec, &v.A, f, v.u, v.t, s, h->sm_count));
-            AMGT_TRY(amgt_spmv(v.prec_transfer, 1.0, &v.R, v.t, 0.0, lv[l + 1].f, (amgt_stream_t)s));
+            Level &nx = lv[l + 1];
+            if (l + 1 < L - 1 && restrict_fusable(&v.R)) {  // the next level smooths: fuse its first sweep
+                AMGT_TRY(spmv_restrict_jacobi0(v.prec_transfer, &v.R, v.t, nx.f, nx.inv_l1, w, nx.u, s,
+                                               h->sm_count));
+                have_u = true;
+            } else {
+                AMGT_TRY(amgt_spmv(v.prec_transfer, 1.0, &v.R, v.t, 0.0, nx.f, (amgt_stream_t)s));
+            }
         }
     }
     Level &c = lv[L - 1];

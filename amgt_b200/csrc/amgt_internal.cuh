@@ -136,6 +136,13 @@ int spmv_residual(int prec, const amgt_bsr *A, const double *f, const double *u,
 int spmv_jacobi(int prec, const amgt_bsr *A, const double *inv_l1, double w, const double *f, const double *u,
                 double *u_out, cudaStream_t s, int sm_count);
 int spmv_dot(int prec, const amgt_bsr *A, const double *u, double *out, double *partial, int grid, cudaStream_t s);
+// f = R t with amgt_spmv's arithmetic (alpha 1, beta 0) and, in the same
+// pass, u = w f ./ l1 (jacobi_zero_kernel's arithmetic): a restriction and
+// the coarser level's first l1-Jacobi sweep from a zero guess.  R must be
+// restrict_fusable (non-empty, not on the segmented path).
+bool restrict_fusable(const amgt_bsr *R);
+int spmv_restrict_jacobi0(int prec, const amgt_bsr *R, const double *t, double *f, const double *inv_l1, double w,
+                          double *u, cudaStream_t s, int sm_count);
 int bsr_l1_norms(const amgt_bsr *A, double *l1, int invert, cudaStream_t s, int sm_count);
 
 // Packed-value forms (packed.cu), same contracts as the dense ones.

@@ -45,7 +45,8 @@ __device__ __forceinline__ typename ValTraits<PREC>::acc_t block_row_dot(const v
 
 // A lane group's blocks k, k + G, k + 2G, ... of one block row, two per
 // step so that both loads are in flight before the FMAs; products are
-// added in block order.
+// added in block order.  (Four per step measured slower here: the 128^3
+// SpMV 77.7 -> 85.7 us, the interpolation 47.6 -> 77.7 us.)
 template <int PREC, int G, bool SAFE>
 __device__ __forceinline__ typename ValTraits<PREC>::acc_t row_dot(const void *__restrict__ val,
                                                                    const int *__restrict__ idx,
@@ -63,12 +64,22 @@ __device__ __forceinline__ typename ValTraits<PREC>::acc_t row_dot(const void *_
 
 // The same walk with the blocks dealt alternately to two sums (a lane group
 // standing for two of the row's segments: blocks k, k + 2G, ... and
-// k + G, k + 3G, ...), with the loads and the order of each sum unchanged.
+// k + G, k + 3G, ...), with the loads and the order of each sum unchanged;
+// four blocks per step (the level-0 passes over the exact fp16 shadow,
+// 44 -> 40.5 us at 128^3).
 template <int PREC, int G, bool SAFE>
 __device__ __forceinline__ void row_dot2(const void *__restrict__ val, const int *__restrict__ idx,
                                          const double *__restrict__ x, int n, int k, int end, int q,
                                          typename ValTraits<PREC>::acc_t &a0, typename ValTraits<PREC>::acc_t &a1)
 {
+    for (; k + 3 * G < end; k += 4 * G) {
+        const int c0 = __ldcs(idx + k), c1 = __ldcs(idx + k + G), c2 = __ldcs(idx + k + 2 * G),
+                  c3 = __ldcs(idx + k + 3 * G);
+        a0 = block_row_dot<PREC, SAFE>(val, x, n, k, q, c0, a0);
+        a1 = block_row_dot<PREC, SAFE>(val, x, n, k + G, q, c1, a1);
+        a0 = block_row_dot<PREC, SAFE>(val, x, n, k + 2 * G, q, c2, a0);
+        a1 = block_row_dot<PREC, SAFE>(val, x, n, k + 3 * G, q, c3, a1);
+    }
     for (; k + G < end; k += 2 * G) {
         const int c0 = __ldcs(idx + k), c1 = __ldcs(idx + k + G);
         a0 = block_row_dot<PREC, SAFE>(val, x, n, k, q, c0, a0);
@@ -233,15 +244,18 @@ spmm_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__re
 //   EPI_RESID : out = f - A u                          (residual, par_cycle.c:678)
 //   EPI_JACOBI: out = u + w (f - A u) / l1             (Relax 18, par_relax.c:1178-1260)
 //   EPI_DOT   : out = A u, and dot partials of u . out (PCG's p.q), one per CTA
+//   EPI_RESTRICT_JACOBI0: out = A u (a restriction) and out2 = w out ./ l1
+//               (the coarser level's l1-Jacobi sweep from a zero guess)
 // x is u.  Same load pattern and per-row summation order as spmv_kernel.
-enum { EPI_RESID = 0, EPI_JACOBI = 1, EPI_DOT = 2 };
+enum { EPI_RESID = 0, EPI_JACOBI = 1, EPI_DOT = 2, EPI_RESTRICT_JACOBI0 = 3 };
 
 struct EpiArgs {
     const double *f;       // RESID, JACOBI
-    const double *inv_l1;  // JACOBI
-    double w;              // JACOBI
+    const double *inv_l1;  // JACOBI, RESTRICT_JACOBI0
+    double w;              // JACOBI, RESTRICT_JACOBI0
     double *out;
     double *partial;       // DOT: [gridDim.x]
+    double *out2;          // RESTRICT_JACOBI0
 };
 
 template <int PREC, int LPR, bool SAFE, int EPI, int V = 1>
@@ -272,6 +286,9 @@ spmv_epi_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *
                     e.out[row] = e.f[row] - ax;
                 } else if constexpr (EPI == EPI_JACOBI) {
                     e.out[row] = x[row] + e.w * (e.f[row] - ax) * e.inv_l1[row];
+                } else if constexpr (EPI == EPI_RESTRICT_JACOBI0) {
+                    e.out[row] = ax;
+                    e.out2[row] = e.w * ax * e.inv_l1[row];
                 } else {
                     e.out[row] = ax;
                     dot += x[row] * ax;
@@ -575,6 +592,20 @@ int spmv_jacobi(int prec, const amgt_bsr *A, const double *inv_l1, double w, con
 {
     EpiArgs e{f, inv_l1, w, u_out, nullptr};
     return launch_epi_prec<EPI_JACOBI>(prec, A, u, e, epi_grid(A, sm_count), s, sm_count);
+}
+
+bool restrict_fusable(const amgt_bsr *R)
+{
+    const bool seg = R->rowPtrbyWarp && R->rowIdxbyWarp && R->warpnum > 0 && R->max_blc_per_row > 256;
+    return R->row > 0 && R->blc_num > 0 && R->col > 0 && !seg;
+}
+
+int spmv_restrict_jacobi0(int prec, const amgt_bsr *R, const double *t, double *f, const double *inv_l1, double w,
+                          double *u, cudaStream_t s, int sm_count)
+{
+    if (!restrict_fusable(R)) return AMGT_ERR_INVALID;
+    EpiArgs e{nullptr, inv_l1, w, f, nullptr, u};
+    return launch_epi_prec<EPI_RESTRICT_JACOBI0>(prec, R, t, e, epi_grid(R, sm_count), s, sm_count);
 }
 
 int spmv_dot(int prec, const amgt_bsr *A, const double *u, double *out, double *partial, int grid, cudaStream_t s)

@@ -612,12 +612,13 @@ def boomer_report(amgt, torch, A_host, grid, cpu: bool, problem: str | None = No
     return rep
 
 
-def boomer_setup_only(grid, mixed: bool = False, engine: int = 0, operator: str = "7pt"):
+def boomer_setup_only(grid, mixed: bool = False, engine: int = 0, operator: str = "7pt", solves: int = 0):
     """Profiling captures: the BoomerAMG hierarchy of the 7-point operator
     built on the host, then two setups on the GPU (the first loads the
     modules), fp64 or the mixed policy with Galerkin products at each
     level's precision on the given SpGEMM engine; prints the second one's
-    phase times."""
+    phase times, then (solves > 0) that many solves of the ij driver's
+    right-hand side on the second setup, with the last one's time."""
     import scipy.sparse as sp
     import torch
 
@@ -636,14 +637,25 @@ def boomer_setup_only(grid, mixed: bool = False, engine: int = 0, operator: str 
     amgt.set_level_policy(MIXED_POLICY if mixed else [0])
     amgt.lib().amgt_spgemm_set_engine(engine)
     prm = default_params(flexible=1, smooth_prec0=1, galerkin_by_level=1) if mixed else default_params()
-    for _ in range(2):
+    for rep in range(2):
         S = AmgSolver(dA, dPs, prm)
         torch.cuda.synchronize()
         times = S.setup_times()
-        S.free()
+        if rep == 0:
+            S.free()
     amgt.lib().amgt_spgemm_set_engine(0)
     amgt.set_level_policy([])
     print(json.dumps({"boomer_setup_ms": {k: round(v, 3) for k, v in times.items()}}))
+    if solves > 0:
+        b = torch.from_numpy(boomer.ij_random_rhs(m)).cuda()
+        for _ in range(solves):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            _, it, rel = S.solve(b)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+        print(json.dumps({"boomer_solve_ms": round(1e3 * (t1 - t0), 3), "iters": it, "relres": rel}))
+    S.free()
 
 
 def cpu_amg(grid, b_host):
@@ -938,6 +950,8 @@ def main():
     ap.add_argument("--setup-mixed", action="store_true", help="with --boomer-setup-only: the mixed policy")
     ap.add_argument("--operator", choices=["7pt", "27pt-varcoef"], default="7pt",
                     help="with --boomer-setup-only: the 7-point operator or the 27-point variable-coefficient one")
+    ap.add_argument("--boomer-solves", type=int, default=0,
+                    help="with --boomer-setup-only: that many solves after the setup (the last one timed)")
     ap.add_argument("--spgemm-engine", type=int, default=0,
                     help="with --boomer-setup-only: amgt_spgemm_set_engine (2: fp16 / bf16 products on the tensor "
                          "cores)")
@@ -945,7 +959,7 @@ def main():
     global GRID
     GRID = (args.grid, args.grid, args.grid)
     if args.boomer_setup_only:
-        boomer_setup_only(GRID, args.setup_mixed, args.spgemm_engine, args.operator)
+        boomer_setup_only(GRID, args.setup_mixed, args.spgemm_engine, args.operator, args.boomer_solves)
     elif args.impl == "reference":
         run_reference(args)
     else:
