@@ -612,7 +612,8 @@ def boomer_report(amgt, torch, A_host, grid, cpu: bool, problem: str | None = No
     return rep
 
 
-def boomer_setup_only(grid, mixed: bool = False, engine: int = 0, operator: str = "7pt", solves: int = 0):
+def boomer_setup_only(grid, mixed: bool = False, engine: int = 0, operator: str = "7pt", solves: int = 0,
+                      packed: int = 0):
     """Profiling captures: the BoomerAMG hierarchy of the 7-point operator
     built on the host, then two setups on the GPU (the first loads the
     modules), fp64 or the mixed policy with Galerkin products at each
@@ -637,6 +638,7 @@ def boomer_setup_only(grid, mixed: bool = False, engine: int = 0, operator: str 
     amgt.set_level_policy(MIXED_POLICY if mixed else [0])
     amgt.lib().amgt_spgemm_set_engine(engine)
     prm = default_params(flexible=1, smooth_prec0=1, galerkin_by_level=1) if mixed else default_params()
+    prm.packed = packed
     for rep in range(2):
         S = AmgSolver(dA, dPs, prm)
         torch.cuda.synchronize()
@@ -952,6 +954,8 @@ def main():
                     help="with --boomer-setup-only: the 7-point operator or the 27-point variable-coefficient one")
     ap.add_argument("--boomer-solves", type=int, default=0,
                     help="with --boomer-setup-only: that many solves after the setup (the last one timed)")
+    ap.add_argument("--packed", type=int, default=0,
+                    help="with --boomer-setup-only: amgt_amg_params.packed (1: bitmap-packed values in the cycle)")
     ap.add_argument("--spgemm-engine", type=int, default=0,
                     help="with --boomer-setup-only: amgt_spgemm_set_engine (2: fp16 / bf16 products on the tensor "
                          "cores)")
@@ -959,7 +963,8 @@ def main():
     global GRID
     GRID = (args.grid, args.grid, args.grid)
     if args.boomer_setup_only:
-        boomer_setup_only(GRID, args.setup_mixed, args.spgemm_engine, args.operator, args.boomer_solves)
+        boomer_setup_only(GRID, args.setup_mixed, args.spgemm_engine, args.operator, args.boomer_solves,
+                          args.packed)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -16,7 +16,10 @@ TOL = {0: 1e-12, 1: 1e-5, 2: 1e-5, 3: 1e-5}
 
 def _mats(orc):
     return {"7pt": orc.laplacian(30, 26, 22), "varcoef27": orc.varcoef27(17, 15, 13, seed=2),
-            "ragged": random_csr(orc, 1001, 1234, 20, seed=3), "interp": orc.interp(21, 17, 13)[0]}
+            "ragged": random_csr(orc, 1001, 1234, 20, seed=3), "interp": orc.interp(21, 17, 13)[0],
+            # block rows of more values than a segment stages at once (512):
+            # the chunk-by-chunk staging
+            "long": random_csr(orc, 203, 6000, 40, seed=4, dense_rows={5: 1500, 6: 900, 77: 2500})}
 
 
 @pytest.fixture(scope="module")
@@ -50,7 +53,7 @@ def test_pack_values_exact(amgt, orc, mats, prec):
         np.testing.assert_array_equal(got, orc.make_shadow(prec, want))
 
 
-@pytest.mark.parametrize("name", ["7pt", "varcoef27", "ragged", "interp"])
+@pytest.mark.parametrize("name", ["7pt", "varcoef27", "ragged", "interp", "long"])
 @pytest.mark.parametrize("prec", [0, 1, 2, 3])
 def test_packed_spmv_matches_oracle(amgt, orc, mats, name, prec):
     A = mats[name]
