@@ -9,11 +9,13 @@
 // order) the lanes walk the B row it selects; every B block whose bitmap
 // product with the A block is non-zero (bitMatrixMul, :189-205) becomes a
 // (B block column, product bitmap) pair, appended to the warp's shared
-// memory list.  The list is sorted (registers when <= 32 pairs, shared
-// memory bitonic sort when <= 1024) and equal columns are merged with an OR
-// of their bitmaps: that is C's block pattern and C's bitmap, bit for bit.
-// Rows with more than 1024 pairs go to a CTA that sweeps the column range
-// in windows of 8192 with a shared-memory bitmap table.  One pass: each
+// memory list.  Equal columns are merged with an OR of their bitmaps and
+// the distinct columns sorted (rows of <= 32 pairs in registers, <= 256
+// through a shared hash table and a sort of the distinct columns, <= 1024
+// pairs inserted straight into the hash table as they are formed): that is
+// C's block pattern and C's bitmap, bit for bit.  Rows with more than 1024
+// pairs go to a CTA that sweeps the column range in windows of 8192 with a
+// shared-memory bitmap table.  One pass: each
 // row's sorted pattern goes to its slice of a scratch array (offsets from a
 // scan of the per-row pair bounds) with its block and CSR counts; one host
 // read-back then sizes C, and the numeric kernel moves the pattern into C.
@@ -30,8 +32,8 @@
 // equals the oracle's restatement of that arithmetic bit for bit (for
 // finite values: unstored entries are zero, and a zero term leaves an FMA
 // chain unchanged).  The fp32 / fp16 / bf16 forms use separate fp32
-// multiply and add.  C rows of up to 32
-// blocks accumulate in shared memory, longer rows in place.  FP64
+// multiply and add.  C rows of up to 16, 24, 32 or 64 blocks (by the
+// product's row lengths) accumulate in shared memory, longer rows in place.  FP64
 // arithmetic on the CUDA cores: the 4x4 products are too small for tcgen05
 // (M >= 64), and on B200 the fp64 MMA rate equals the fp64 FMA rate.  The
 // CSR form of C is written by the same kernel (no separate BSR2CSR pass).
@@ -904,7 +906,7 @@ __device__ __forceinline__ void acc4_store(acc_t *p, const acc_t v[4])
 
 // Shared memory of the numeric kernel per warp: C accumulators (CAP C
 // blocks), two stages of 8 staged B blocks (16 values + 16-byte pad) and
-// 8 x 4 A rows, and the pair -> A block table.
+// 8 x 4 A rows, and the window's list of pairs with a product.
 template <int PREC, int CAP>
 struct NumSmem {
     using V = typename NumT<PREC>::val_t;
