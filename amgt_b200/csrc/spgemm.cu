@@ -1382,7 +1382,10 @@ template <int PREC>
 struct GatherSmem {
     static constexpr int AR = 4 * (int)sizeof(typename NumT<PREC>::val_t);  // one block row
     static constexpr int slot = 8 * AR;                                     // A block, then B block
-    static constexpr int per_cta = (kGatherThreads / 4) * kGatherSlots * slot;
+    // a C block's ring, padded by 16 bytes so that the eight C blocks of a
+    // warp, reading the same row of their B blocks, hit distinct banks
+    static constexpr int group = kGatherSlots * slot + 16;
+    static constexpr int per_cta = (kGatherThreads / 4) * group;
 };
 
 template <int PREC>
@@ -1399,7 +1402,7 @@ spgemm_gather_kernel(int nbC, const typename NumT<PREC>::val_t *__restrict__ ava
     extern __shared__ __align__(16) unsigned char gather_smem[];
     const int r = threadIdx.x & 3;
     const unsigned gmask = 0xFu << (threadIdx.x & 28);  // this C block's four lanes
-    unsigned char *ring = gather_smem + (threadIdx.x >> 2) * S * SLOT;
+    unsigned char *ring = gather_smem + (threadIdx.x >> 2) * GS::group;
     bool not32 = false, not16 = false;
     const long long g0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 2;
     const long long gstride = ((long long)gridDim.x * blockDim.x) >> 2;
