@@ -724,7 +724,10 @@ int prepare_interp(void *ctx)
     AMGT_TRY(transpose_pending(nx));
     if (!nx->P) return AMGT_OK;
     CvtFuse f;
-    f.want16 = nx->exact && amgt_precision_for_level(nx->plevel + 1) == AMGT_DOUBLE;
+    // transfers used in fp64 or fp32 are checked for exact fp16 storage by
+    // the conversion's fill pass (the transpose then carries the result)
+    const int tp = amgt_precision_for_level(nx->plevel + 1);
+    f.want16 = nx->exact && (tp == AMGT_DOUBLE || tp == AMGT_FLOAT);
     f.flags = nx->xflags + 3 * nx->plevel + 1;
     AMGT_TRY(csr_to_bsr_impl(nx->P, nx->Pb, (amgt_stream_t)nx->s2, nullptr, nullptr, f.want16 ? &f : nullptr));
     if (f.want16 && f.fused) (*nx->fused16)[3 * nx->plevel + 1] = 1;
