@@ -1295,10 +1295,15 @@ int amgt::amg_setup_blocks(const amgt_csr *A, int num_interp, const amgt_csr *P,
             goto fail;
         }
         {
-            // A_{l+1} in fp64 is checked for exact storage by the numeric pass
+            // A_{l+1} used in fp64 or fp32 is checked for exact fp16 storage
+            // by the numeric pass, which also writes the fp32 shadow of an
+            // fp64 product for a level used in fp32
             CvtFuse fz;
-            fz.want16 = h->prm.exact_storage && gp == AMGT_DOUBLE && !cb &&
-                        amgt_precision_for_level(l + 1) == AMGT_DOUBLE;
+            const int np = amgt_precision_for_level(l + 1);
+            fz.want16 = h->prm.exact_storage && !cb &&
+                        ((gp == AMGT_DOUBLE && (np == AMGT_DOUBLE || np == AMGT_FLOAT)) ||
+                         (gp == AMGT_FLOAT && np == AMGT_FLOAT));
+            fz.want32 = fz.want16 && gp == AMGT_DOUBLE && np == AMGT_FLOAT;
             fz.flags = xflags + 3 * (l + 1);
             rc = spgemm_impl(gp, &v.R, &AP, &h->lv[l + 1].A, nullptr, stream, nullptr, nullptr,
                              fz.want16 ? &fz : nullptr);

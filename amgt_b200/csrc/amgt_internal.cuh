@@ -171,6 +171,7 @@ int bsr_exact_apply(amgt_bsr *A, int64_t flag, bool own16, cudaStream_t s);
 // the same bits.
 struct CvtFuse {
     bool want16 = false;
+    bool want32 = false;  // fp64 Galerkin products: write the fp32 shadow as well (a level used in fp32)
     int64_t *flags = nullptr;
     double *l1 = nullptr;
     int invert = 0;

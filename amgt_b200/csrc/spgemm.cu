@@ -951,7 +951,8 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                       double *__restrict__ cval, void *__restrict__ cshadow, const int *__restrict__ csr_i,
                       int *__restrict__ csr_j, double *__restrict__ csr_a, const int64_t *__restrict__ ub_off,
                       const int *__restrict__ skey, const uint16_t *__restrict__ smap,
-                      const uint16_t *__restrict__ pslot, unsigned long long *__restrict__ cflags)
+                      const uint16_t *__restrict__ pslot, unsigned long long *__restrict__ cflags,
+                      void *__restrict__ cextra)
 {
     bool not32 = false, not16 = false;
     using T = NumT<PREC>;
@@ -1160,9 +1161,26 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
                     hs[0] = __halves2half2(hv[0], hv[1]);
                     hs[1] = __halves2half2(hv[2], hv[3]);
                 }
+                if (cextra)  // the fp32 shadow of a level used in fp32
+                    *reinterpret_cast<float4 *>(static_cast<float *>(cextra) + 16LL * c0 + 4LL * t) =
+                        make_float4(__double2float_rn(v[0]), __double2float_rn(v[1]), __double2float_rn(v[2]),
+                                    __double2float_rn(v[3]));
             } else if (cshadow) {
 #pragma unroll
                 for (int c = 0; c < 4; ++c) store_shadow<PREC>(cshadow, 16LL * c0 + 4LL * t + c, v[c]);
+                if constexpr (PREC == AMGT_FLOAT) {
+                    if (cextra) {  // fp16 candidate shadow and its exactness bit
+                        __half hv[4];
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            hv[c] = __float2half_rn(v[c]);
+                            if (__half2float(hv[c]) != v[c]) not16 = true;
+                        }
+                        __half2 *hs = reinterpret_cast<__half2 *>(static_cast<__half *>(cextra) + 16LL * c0 + 4LL * t);
+                        hs[0] = __halves2half2(hv[0], hv[1]);
+                        hs[1] = __halves2half2(hv[2], hv[3]);
+                    }
+                }
             }
         }
         __syncwarp();
@@ -1196,7 +1214,8 @@ spgemm_numeric_kernel(int m, int brA, const int *__restrict__ aptr, const int *_
         }
         __syncwarp();
     }
-    if (PREC == AMGT_DOUBLE && cshadow) {  // the row loop is warp-uniform: all lanes are here
+    // the row loop is warp-uniform: all lanes are here
+    if ((PREC == AMGT_DOUBLE && cshadow) || (PREC == AMGT_FLOAT && cextra)) {
         const unsigned b32 = __ballot_sync(FULL, not32), b16 = __ballot_sync(FULL, not16);
         if (lane == 0 && (b32 | b16)) atomicOr(cflags, (b32 ? 1ull : 0ull) | (b16 ? 2ull : 0ull));
     }
@@ -1393,7 +1412,7 @@ __global__ void __launch_bounds__(kGatherThreads, 6)
 spgemm_gather_kernel(int nbC, const typename NumT<PREC>::val_t *__restrict__ aval,
                      const typename NumT<PREC>::val_t *__restrict__ bval, const int2 *__restrict__ glist,
                      const long long *__restrict__ gbeg, const int *__restrict__ gnum, double *__restrict__ cval,
-                     void *__restrict__ cshadow, unsigned long long *__restrict__ cflags)
+                     void *__restrict__ cshadow, unsigned long long *__restrict__ cflags, void *__restrict__ cextra)
 {
     using T = NumT<PREC>;
     using acc_t = typename T::acc_t;
@@ -1507,9 +1526,22 @@ spgemm_gather_kernel(int nbC, const typename NumT<PREC>::val_t *__restrict__ ava
                     if ((double)__half2float(hv) != acc[c]) not16 = true;
                 }
             }
+            if (cextra)  // the fp32 shadow of a level used in fp32
+#pragma unroll
+                for (int c = 0; c < 4; ++c) static_cast<float *>(cextra)[16 * g + 4 * r + c] = __double2float_rn(acc[c]);
         } else if (cshadow) {
 #pragma unroll
             for (int c = 0; c < 4; ++c) store_shadow<PREC>(cshadow, 16 * g + 4 * r + c, acc[c]);
+            if constexpr (PREC == AMGT_FLOAT) {
+                if (cextra) {  // fp16 candidate shadow and its exactness bit
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const __half hv = __float2half_rn(acc[c]);
+                        static_cast<__half *>(cextra)[16 * g + 4 * r + c] = hv;
+                        if (__half2float(hv) != acc[c]) not16 = true;
+                    }
+                }
+            }
         }
         beg = begN;
         n = nN;
@@ -1517,7 +1549,7 @@ spgemm_gather_kernel(int nbC, const typename NumT<PREC>::val_t *__restrict__ ava
         nN = nNN;
         ent = entNext;
     }
-    if (PREC == AMGT_DOUBLE && cshadow) {
+    if ((PREC == AMGT_DOUBLE && cshadow) || (PREC == AMGT_FLOAT && cextra)) {
         const unsigned b32 = __ballot_sync(FULL, not32), b16 = __ballot_sync(FULL, not16);
         if ((threadIdx.x & 31) == 0 && (b32 | b16)) atomicOr(cflags, (b32 ? 1ull : 0ull) | (b16 ? 2ull : 0ull));
     }
@@ -1674,7 +1706,7 @@ template <int PREC, int CAP>
 static int launch_numeric_cap(const amgt_bsr *A, const void *aval, const amgt_bsr *B, const void *bval, amgt_bsr *C,
                               void *cshadow, amgt_csr *Ccsr, const int64_t *ub_off, const int *skey,
                               const uint16_t *smap, const uint16_t *pslot, cudaStream_t s, int sm_count,
-                              unsigned long long *cflags)
+                              unsigned long long *cflags, void *cextra)
 {
     using V = typename NumT<PREC>::val_t;
     constexpr int smem = kNumWarps * NumSmem<PREC, CAP>::per_warp;
@@ -1684,7 +1716,7 @@ static int launch_numeric_cap(const amgt_bsr *A, const void *aval, const amgt_bs
     AMGT_LAUNCH((spgemm_numeric_kernel<PREC, CAP>), grid_for(kNumWarps, A->blc_row, sm_count, per_sm),
                 32 * kNumWarps, smem, s, A->row, A->blc_row, A->blcPtr, A->blcIdx, (const V *)aval, B->blcPtr, B->blcIdx, (const V *)bval,
                 C->blcPtr, C->blcIdx, C->blcMap, C->blcVal, cshadow, Ccsr ? Ccsr->i : nullptr,
-                Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr, ub_off, skey, smap, pslot, cflags);
+                Ccsr ? Ccsr->j : nullptr, Ccsr ? Ccsr->data : nullptr, ub_off, skey, smap, pslot, cflags, cextra);
     return AMGT_OK;
 }
 
@@ -1696,20 +1728,20 @@ template <int PREC>
 static int launch_numeric(const amgt_bsr *A, const void *aval, const amgt_bsr *B, const void *bval, amgt_bsr *C,
                           void *cshadow, amgt_csr *Ccsr, const int64_t *ub_off, const int *skey,
                           const uint16_t *smap, const uint16_t *pslot, cudaStream_t s, int sm_count,
-                          unsigned long long *cflags = nullptr)
+                          unsigned long long *cflags = nullptr, void *cextra = nullptr)
 {
     if (A->blc_row == 0) return AMGT_OK;
     if (C->max_blc_per_row <= kNumCapNarrow)
         return launch_numeric_cap<PREC, kNumCapNarrow>(A, aval, B, bval, C, cshadow, Ccsr, ub_off, skey, smap, pslot,
-                                                       s, sm_count, cflags);
+                                                       s, sm_count, cflags, cextra);
     if (C->max_blc_per_row <= kNumCapMid)
         return launch_numeric_cap<PREC, kNumCapMid>(A, aval, B, bval, C, cshadow, Ccsr, ub_off, skey, smap, pslot, s,
-                                                    sm_count, cflags);
+                                                    sm_count, cflags, cextra);
     if (C->max_blc_per_row > kNumCap && 24LL * A->blc_row < (long long)C->blc_num)
         return launch_numeric_cap<PREC, kNumCapWide>(A, aval, B, bval, C, cshadow, Ccsr, ub_off, skey, smap, pslot, s,
-                                                     sm_count, cflags);
+                                                     sm_count, cflags, cextra);
     return launch_numeric_cap<PREC, kNumCap>(A, aval, B, bval, C, cshadow, Ccsr, ub_off, skey, smap, pslot, s,
-                                             sm_count, cflags);
+                                             sm_count, cflags, cextra);
 }
 
 static void *shadow_of(const amgt_bsr *A, int prec)
@@ -1769,6 +1801,7 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
         g_spgemm_engine.load() == AMGT_ENGINE_TENSOR_CORE && (prec == AMGT_HALF || prec == AMGT_BF16);
     unsigned char *arena3 = nullptr;  // gathered numeric: pair lists and their starts / lengths
     void *cshadow = nullptr;
+    void *cextra = nullptr;  // fp64 products: the fp32 shadow; fp32 products: the fp16 candidate (CvtFuse)
     if (prec != AMGT_DOUBLE) {
         if (!shadow_of(A, prec)) {
             Atmp.blcVal_fp32 = nullptr; Atmp.blcVal_fp16 = nullptr; Atmp.blcVal_bf16 = nullptr;
@@ -1886,6 +1919,11 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     if (prec == AMGT_FLOAT) {
         if ((rc = alloc_n(&C->blcVal_fp32, 16LL * nbC, s))) goto fail;
         cshadow = C->blcVal_fp32;
+        if (fuse && fuse->want16 && nbC > 0) {  // fp16 exactness of the fp32 values fused too
+            if ((rc = alloc_n(&C->blcVal_fp16, 16LL * nbC, s))) goto fail;
+            cextra = C->blcVal_fp16;
+            fuse->fused = true;
+        }
     } else if (prec == AMGT_HALF) {
         if ((rc = alloc_n(&C->blcVal_fp16, 16LL * nbC, s))) goto fail;
         cshadow = C->blcVal_fp16;
@@ -1896,6 +1934,10 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
         if ((rc = alloc_n(&C->blcVal_fp16, 16LL * nbC, s))) goto fail;
         cshadow = C->blcVal_fp16;
         fuse->fused = true;
+        if (fuse->want32) {  // and the fp32 shadow of a level used in fp32
+            if ((rc = alloc_n(&C->blcVal_fp32, 16LL * nbC, s))) goto fail;
+            cextra = C->blcVal_fp32;
+        }
     }
     if (Ccsr) {
         Ccsr->num_nonzeros = nnzC;
@@ -1947,21 +1989,22 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
             switch (prec) {
             case AMGT_DOUBLE:
                 AMGT_LAUNCH(spgemm_gather_kernel<AMGT_DOUBLE>, grid, kGatherThreads, GatherSmem<AMGT_DOUBLE>::per_cta,
-                            s, nbC, A->blcVal, B->blcVal, glist, gbeg, gnum, C->blcVal, cshadow, flags);
+                            s, nbC, A->blcVal, B->blcVal, glist, gbeg, gnum, C->blcVal, cshadow, flags, cextra);
                 break;
             case AMGT_FLOAT:
                 AMGT_LAUNCH(spgemm_gather_kernel<AMGT_FLOAT>, grid, kGatherThreads, GatherSmem<AMGT_FLOAT>::per_cta, s,
-                            nbC, Atmp.blcVal_fp32, Btmp.blcVal_fp32, glist, gbeg, gnum, C->blcVal, cshadow, nullptr);
+                            nbC, Atmp.blcVal_fp32, Btmp.blcVal_fp32, glist, gbeg, gnum, C->blcVal, cshadow, flags,
+                            cextra);
                 break;
             case AMGT_HALF:
                 AMGT_LAUNCH(spgemm_gather_kernel<AMGT_HALF>, grid, kGatherThreads, GatherSmem<AMGT_HALF>::per_cta, s,
                             nbC, (const __half *)Atmp.blcVal_fp16, (const __half *)Btmp.blcVal_fp16, glist, gbeg, gnum,
-                            C->blcVal, cshadow, nullptr);
+                            C->blcVal, cshadow, nullptr, nullptr);
                 break;
             default:
                 AMGT_LAUNCH(spgemm_gather_kernel<AMGT_BF16>, grid, kGatherThreads, GatherSmem<AMGT_BF16>::per_cta, s,
                             nbC, (const __nv_bfloat16 *)Atmp.blcVal_bf16, (const __nv_bfloat16 *)Btmp.blcVal_bf16,
-                            glist, gbeg, gnum, C->blcVal, cshadow, nullptr);
+                            glist, gbeg, gnum, C->blcVal, cshadow, nullptr, nullptr);
                 break;
             }
         }
@@ -1973,11 +2016,13 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
     case AMGT_DOUBLE:
         rc = launch_numeric<AMGT_DOUBLE>(A, A->blcVal, B, B->blcVal, C, cshadow, Ccsr, ub_off, skey, smap, pslot, s,
                                          st->sm_count, fuse ? reinterpret_cast<unsigned long long *>(fuse->flags)
-                                                            : nullptr);
+                                                            : nullptr,
+                                         cextra);
         break;
     case AMGT_FLOAT:
         rc = launch_numeric<AMGT_FLOAT>(A, Atmp.blcVal_fp32, B, Btmp.blcVal_fp32, C, cshadow, Ccsr, ub_off, skey,
-                                        smap, pslot, s, st->sm_count);
+                                        smap, pslot, s, st->sm_count,
+                                        fuse ? reinterpret_cast<unsigned long long *>(fuse->flags) : nullptr, cextra);
         break;
     case AMGT_HALF:
         rc = launch_numeric<AMGT_HALF>(A, Atmp.blcVal_fp16, B, Btmp.blcVal_fp16, C, cshadow, Ccsr, ub_off, skey,
