@@ -711,7 +711,9 @@ int transpose_pending(NextInterp *nx)
 {
     if (!nx->Tb) return AMGT_OK;
     const bool with16 = (*nx->fused16)[3 * nx->tlevel + 1] != 0;
-    AMGT_TRY(bsr_transpose_impl(nx->Tb, nx->TRb, (amgt_stream_t)nx->s2, with16));
+    // R = P^T carries P's fp16 candidate and, for a transfer used in fp32,
+    // P's fp32 shadow written by the conversion
+    AMGT_TRY(bsr_transpose_impl(nx->Tb, nx->TRb, (amgt_stream_t)nx->s2, with16, with16));
     if (with16) (*nx->fused16)[3 * nx->tlevel + 2] = 1;
     AMGT_CUDA_TRY(cudaEventRecord(nx->r_ready[nx->rslot], nx->s2));
     nx->Tb = nullptr;
@@ -728,6 +730,7 @@ int prepare_interp(void *ctx)
     // the conversion's fill pass (the transpose then carries the result)
     const int tp = amgt_precision_for_level(nx->plevel + 1);
     f.want16 = nx->exact && (tp == AMGT_DOUBLE || tp == AMGT_FLOAT);
+    f.want32 = f.want16 && tp == AMGT_FLOAT;
     f.flags = nx->xflags + 3 * nx->plevel + 1;
     AMGT_TRY(csr_to_bsr_impl(nx->P, nx->Pb, (amgt_stream_t)nx->s2, nullptr, nullptr, f.want16 ? &f : nullptr));
     if (f.want16 && f.fused) (*nx->fused16)[3 * nx->plevel + 1] = 1;

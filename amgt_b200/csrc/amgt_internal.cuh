@@ -171,7 +171,7 @@ int bsr_exact_apply(amgt_bsr *A, int64_t flag, bool own16, cudaStream_t s);
 // the same bits.
 struct CvtFuse {
     bool want16 = false;
-    bool want32 = false;  // fp64 Galerkin products: write the fp32 shadow as well (a level used in fp32)
+    bool want32 = false;  // with want16: write the fp32 shadow as well (an operator used in fp32)
     int64_t *flags = nullptr;
     double *l1 = nullptr;
     int invert = 0;
@@ -193,7 +193,7 @@ int spgemm_impl(int prec, const amgt_bsr *A, const amgt_bsr *B, amgt_bsr *C, amg
 
 // amgt_bsr_transpose; with16: A's fp16 shadow, when present, is
 // transposed with the values (convert.cu).
-int bsr_transpose_impl(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream, bool with16);
+int bsr_transpose_impl(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream, bool with16, bool with32 = false);
 
 // Exclusive scan of n ints (in may equal out), CUB with allocator scratch.
 int exclusive_scan_int(const int *in, int *out, int n, cudaStream_t s);

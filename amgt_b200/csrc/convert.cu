@@ -423,7 +423,8 @@ csr2bsr_large_kernel(int m, int n, const int *__restrict__ ia, const int *__rest
 // value, slot byte) into shared memory with coalesced loads.
 // With every block row on this path the pass can also write, from the
 // values it holds: the fp16 rounding of each stored value and the
-// exactness bits of exact_check_kernel (v16, flags), and each row's l1 norm
+// exactness bits of exact_check_kernel (v16, flags), the fp32 rounding
+// (v32, for an operator used in fp32), and each row's l1 norm
 // summed as l1_norm_kernel sums it (blocks in order, |v0| + |v1| + |v2| +
 // |v3| per block; 1 / norm with l1_invert).
 constexpr int kFsWarps = 4;
@@ -432,6 +433,7 @@ constexpr int kFsCap = 256;  // entries of a warp's 8 block rows held in shared 
 struct FillExtras {
     __half *v16;                // nullable
     unsigned long long *flags;  // with v16
+    float *v32;                 // nullable
     double *l1;                 // nullable
     int l1_invert;
 };
@@ -530,6 +532,10 @@ csr2bsr_fill_sorted_kernel(int m, const int *__restrict__ ia, const int *__restr
                     d16[0] = __halves2half2(hh[0], hh[1]);
                     d16[1] = __halves2half2(hh[2], hh[3]);
                 }
+                if (fx.v32)
+                    *reinterpret_cast<float4 *>(fx.v32 + 16LL * (base + sl) + 4 * q) =
+                        make_float4(__double2float_rn(v0), __double2float_rn(v1), __double2float_rn(v2),
+                                    __double2float_rn(v3));
                 l1s += fabs(v0) + fabs(v1) + fabs(v2) + fabs(v3);
                 unsigned mp = bits << (4 * q);
                 mp |= __shfl_xor_sync(gmask, mp, 1);
@@ -865,7 +871,8 @@ __global__ void transpose_gather_kernel(int nblk, const int *__restrict__ src, c
                                         const uint16_t *__restrict__ amap, const double *__restrict__ aval,
                                         int *__restrict__ tidx, uint16_t *__restrict__ tmap,
                                         double *__restrict__ tval, const __half *__restrict__ aval16,
-                                        __half *__restrict__ tval16)
+                                        __half *__restrict__ tval16, const float *__restrict__ aval32,
+                                        float *__restrict__ tval32)
 {
     // 16 threads per block: thread e writes entry e of the transposed block
     const long long total = (long long)nblk * 16;
@@ -875,6 +882,7 @@ __global__ void transpose_gather_kernel(int nblk, const int *__restrict__ src, c
         const int r = e >> 2, c = e & 3;  // entry (r, c) of the transpose = (c, r) of the source
         tval[t] = aval[(size_t)16 * sidx + 4 * c + r];
         if (aval16) tval16[t] = aval16[(size_t)16 * sidx + 4 * c + r];
+        if (aval32) tval32[t] = aval32[(size_t)16 * sidx + 4 * c + r];
         if (e == 0) {
             tidx[d] = rowid[sidx];
             tmap[d] = (uint16_t)bitmap_transpose(amap[sidx]);
@@ -956,7 +964,7 @@ int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int 
     int rc = AMGT_OK;
     const int64_t *h = nullptr;
     int nb = 0;
-    FillExtras fx{nullptr, nullptr, nullptr, 0};
+    FillExtras fx{nullptr, nullptr, nullptr, nullptr, 0};
     bool all_sorted = false;  // no block row left to the warp or large-row kernels
     static std::atomic<bool> smem_set[64];  // per device: the large-row kernels' shared-memory opt-in
     int dev = 0;
@@ -1017,6 +1025,10 @@ int csr_to_bsr_impl(const amgt_csr *A, amgt_bsr *out, amgt_stream_t stream, int 
                 if ((rc = alloc_n(&out->blcVal_fp16, (size_t)16 * nb, s))) goto fail;
                 fx.v16 = reinterpret_cast<__half *>(out->blcVal_fp16);
                 fx.flags = reinterpret_cast<unsigned long long *>(fuse->flags);
+                if (fuse->want32) {
+                    if ((rc = alloc_n(&out->blcVal_fp32, (size_t)16 * nb, s))) goto fail;
+                    fx.v32 = out->blcVal_fp32;
+                }
             }
             fuse->fused = true;
         }
@@ -1186,7 +1198,7 @@ int amgt_bsr_make_exact(amgt_bsr *A, amgt_stream_t stream)
 
 namespace amgt {
 
-int bsr_transpose_impl(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream, bool with16)
+int bsr_transpose_impl(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream, bool with16, bool with32)
 {
     if (!A || !out || (A->blc_row > 0 && !A->blcPtr)) return AMGT_ERR_INVALID;
     DeviceState *st;
@@ -1224,12 +1236,14 @@ int bsr_transpose_impl(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream, b
         if (!tmp) { rc = AMGT_ERR_ALLOC; goto fail; }
         count_launch();
         AMGT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys_in, keys_out, iota, src, nb, 0, bits, s));
-        const bool g16 = with16 && A->blcVal_fp16;
+        const bool g16 = with16 && A->blcVal_fp16, g32 = with32 && A->blcVal_fp32;
         if (g16 && (rc = alloc_n(&out->blcVal_fp16, (size_t)16 * nb, s))) goto fail;
+        if (g32 && (rc = alloc_n(&out->blcVal_fp32, (size_t)16 * nb, s))) goto fail;
         AMGT_LAUNCH(transpose_gather_kernel, grid_for(256, 16LL * nb, st->sm_count, 8), 256, 0, s, nb, src, rowid,
                     A->blcMap, A->blcVal, out->blcIdx, out->blcMap, out->blcVal,
                     g16 ? reinterpret_cast<const __half *>(A->blcVal_fp16) : nullptr,
-                    g16 ? reinterpret_cast<__half *>(out->blcVal_fp16) : nullptr);
+                    g16 ? reinterpret_cast<__half *>(out->blcVal_fp16) : nullptr, g32 ? A->blcVal_fp32 : nullptr,
+                    g32 ? out->blcVal_fp32 : nullptr);
     }
     if ((rc = exclusive_scan_int(hist, out->blcPtr, bcol + 1, s))) goto fail;
     free_ptr(rowid, s); free_ptr(iota, s); free_ptr(keys_out, s); free_ptr(src, s); free_ptr(hist, s);
@@ -1248,7 +1262,7 @@ extern "C" {
 
 int amgt_bsr_transpose(const amgt_bsr *A, amgt_bsr *out, amgt_stream_t stream)
 {
-    return amgt::bsr_transpose_impl(A, out, stream, false);
+    return amgt::bsr_transpose_impl(A, out, stream, false, false);
 }
 
 }  // extern "C"
