@@ -100,6 +100,14 @@ def _pair(orc, kind):
         A = orc.CSR(T.m, T.n, nia, nja, rng.uniform(-1, 1, nja.size))
         B = orc.CSR(T.m, T.n, T.ia, T.ja, rng.uniform(-1, 1, T.ja.size))
         return A, B
+    if kind == "A2A3_27pt_long":
+        # A^2 * A^3 of the 27-point pattern: rows of 4,000-9,800 pairs into at
+        # most 484 C blocks (the gathered numeric's order pass on long rows)
+        T = orc.box(16, 14, 13)
+        A = orc.CSR(T.m, T.n, T.ia, T.ja, np.random.default_rng(16).uniform(-1, 1, T.ja.size))
+        A2 = orc.bsr2csr(orc.spgemm(orc.csr2bsr(A), orc.csr2bsr(A))[0])
+        A3 = orc.bsr2csr(orc.spgemm(orc.csr2bsr(A2), orc.csr2bsr(A))[0])
+        return A2, A3
     if kind == "WIDE_row":
         # a dense first row: > 1024 C blocks in one row (the gathered numeric's
         # A-block-at-a-time ordering)
@@ -116,7 +124,7 @@ def _pair(orc, kind):
 
 
 KINDS = ["AP_7pt", "AP_varcoef27", "RAP_varcoef27", "AA_varcoef27", "AA_5pt", "AAA_27pt", "AP_7pt_large",
-         "AA_7pt_large", "A2A2_9pt", "AAA_7pt_wide", "AA_27pt_wide", "LONG_row_staged", "WIDE_row"]
+         "AA_7pt_large", "A2A2_9pt", "AAA_7pt_wide", "AA_27pt_wide", "LONG_row_staged", "A2A3_27pt_long", "WIDE_row"]
 
 
 @pytest.mark.parametrize("kind", KINDS)
