@@ -167,8 +167,11 @@ int bsr_exact_apply(amgt_bsr *A, int64_t flag, bool own16, cudaStream_t s);
 // every block row takes the sorted path (else `fused` stays false and the
 // caller runs the separate passes): with want16, the exactness check of
 // bsr_exact_check (the fp16 shadow, allocated here, and the flag bits in
-// *flags); with l1, the row norms of bsr_l1_norms (1 / norm when invert),
-// the same bits.
+// *flags), and with want32 the fp32 shadow as well; with l1, the row norms
+// of bsr_l1_norms (1 / norm when invert), the same bits.  spgemm_impl takes
+// the same request for its product: fp64 products write the fp16 shadow and
+// the bits (and with want32 the fp32 shadow), fp32 products the fp16
+// candidate beside their fp32 values and its bit.
 struct CvtFuse {
     bool want16 = false;
     bool want32 = false;  // with want16: write the fp32 shadow as well (an operator used in fp32)
