@@ -57,7 +57,7 @@ class AmgtAmgParams(ctypes.Structure):
 class AmgtPbsr(ctypes.Structure):
     _fields_ = [("row", c_int), ("col", c_int), ("blc_row", c_int), ("blc_col", c_int), ("blc_num", c_int),
                 ("nnz", c_int), ("prec", c_int), ("blcPtr", c_void_p), ("blcIdx", c_void_p), ("blcMap", c_void_p),
-                ("rowVoff", c_void_p), ("val", c_void_p), ("max_blc_per_row", c_int)]
+                ("rowVoff", c_void_p), ("val", c_void_p), ("max_blc_per_row", c_int), ("blcVoff", c_void_p)]
 
 
 class AmgtTuneResult(ctypes.Structure):

@@ -6,9 +6,8 @@
 // packed form keeps the block structure (block-row pointers, block columns
 // and bitmaps, borrowed from the mBSR matrix) and stores only the values of
 // set bits, block after block, in bitmap order (row-major inside the
-// block), plus each block row's offset into that array.
-// Bytes per block: 4 (column) + 2 (bitmap) + s * set bits, plus 4 per
-// block row.
+// block), plus each block's and each block row's offset into that array.
+// Bytes per block: 4 (column) + 2 (bitmap) + 4 (offset) + s * set bits.
 #include <cstdlib>
 
 #include "spmv_common.cuh"
@@ -25,20 +24,6 @@ struct PEpiArgs {
     double *out;           // y (AXPBY reads it when beta != 0)
     double *partial;       // DOT: [gridDim.x]
 };
-
-template <int PREC>
-__device__ __forceinline__ typename ValTraits<PREC>::acc_t packed_value(const void *__restrict__ val, long long i)
-{
-    if constexpr (PREC == AMGT_DOUBLE) return __ldcs(static_cast<const double *>(val) + i);
-    else if constexpr (PREC == AMGT_FLOAT) return __ldcs(static_cast<const float *>(val) + i);
-    else if constexpr (PREC == AMGT_HALF) {
-        const unsigned short h = __ldcs(static_cast<const unsigned short *>(val) + i);
-        return __half2float(__ushort_as_half(h));
-    } else {
-        const unsigned short h = __ldcs(static_cast<const unsigned short *>(val) + i);
-        return __bfloat162float(__ushort_as_bfloat16(h));
-    }
-}
 
 template <int PREC>
 struct PackedT {
@@ -65,95 +50,74 @@ __device__ __forceinline__ typename ValTraits<PREC>::acc_t widen(typename Packed
     else return v;
 }
 
-// One warp, 32 / LPR segments of LPR lanes, one block row per segment.
-// The row's packed values are contiguous (row offset rvoff[b]), so the
-// segment loads them into shared memory with consecutive loads in the same
-// round trip as the row's block columns and bitmaps (lane j of the segment
-// takes block j of a chunk of LPR blocks); a popcount scan over the chunk
-// gives each block's first value.  Then 4 lanes per block, lane q taking
-// block row q, multiply with x like the 16-value kernel (an FMA for every
-// column, zero where the bit is clear).  Segments step in lockstep so the
-// warp can synchronise; rows whose values do not fit the staging slice are
-// taken in chunks of LPR blocks.
+// SpMV on the packed values, each block's first value given (blcVoff):
+// laid out like the 16-value kernel — LPR lanes per block row, 4 lanes per block,
+// lane q taking block row q, the row's blocks dealt to the LPR/4 lane
+// groups two per step — with lane q reading only its row's stored values
+// (popc of its bitmap nibble, from voff[k] + the set bits before it) and an
+// FMA for every column, zero where the bit is clear: the sums of the
+// 16-value kernel at the same lanes per row, bit for bit, from a third of
+// the bytes at AMG fills.  A block's column, bitmap and value offset load
+// together, its values and x one trip later.
+template <int PREC, bool SAFE>
+__device__ __forceinline__ typename ValTraits<PREC>::acc_t pblock_dot(const typename PackedT<PREC>::val_t *__restrict__ val,
+                                                                      const double *__restrict__ x, int n, int vo,
+                                                                      uint32_t mp, int q, int col,
+                                                                      typename ValTraits<PREC>::acc_t acc)
+{
+    using acc_t = typename ValTraits<PREC>::acc_t;
+    const uint32_t nib = (mp >> (4 * q)) & 0xFu;
+    int o = vo + __popc(mp & ((1u << (4 * q)) - 1u));
+    double xv[4];
+    load_x4<SAFE>(x, col, n, xv);
+    acc_t w[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        w[c] = (acc_t)0;
+        if ((nib >> c) & 1u) w[c] = widen<PREC>(__ldcs(val + o++));
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc = fma(w[c], (acc_t)xv[c], acc);
+    return acc;
+}
+
 template <int PREC, int LPR, bool SAFE, int EPI>
 __global__ void __launch_bounds__(256)
-pspmv_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__restrict__ idx,
-             const uint16_t *__restrict__ map, const int *__restrict__ rvoff, const void *__restrict__ valv,
-             const double *__restrict__ x, PEpiArgs e)
+pspmv_off_kernel(int m, int n, int brow, const int *__restrict__ ptr, const int *__restrict__ idx,
+                 const uint16_t *__restrict__ map, const int *__restrict__ voff, const void *__restrict__ valv,
+                 const double *__restrict__ x, PEpiArgs e)
 {
+    grid_dependency_wait();  // launched with programmatic dependent launch
     using acc_t = typename ValTraits<PREC>::acc_t;
     using val_t = typename PackedT<PREC>::val_t;
     constexpr int RPW = 32 / LPR;
     constexpr int G = LPR / 4;
-    constexpr int CAP = 16 * LPR;  // staged values per segment (a chunk of LPR full blocks)
-    __shared__ val_t stage[8][RPW][CAP];
     __shared__ double sred[8];
     const val_t *__restrict__ val = static_cast<const val_t *>(valv);
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     const int sub = lane / LPR, l = lane % LPR, g = l >> 2, q = l & 3;
-    const int seg0 = sub * LPR;  // first lane of this segment
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    val_t *st = stage[wib][sub];
     double dot = 0.0;
     for (int b0 = warp * RPW; b0 < brow; b0 += nwarps * RPW) {
         const int b = b0 + sub;
-        int start = 0, end = 0, v0 = 0;
-        if (b < brow) {
-            start = ptr[b];
-            end = ptr[b + 1];
-            v0 = rvoff[b];
-        }
-        int chunks = (end - start + LPR - 1) / LPR;
-#pragma unroll
-        for (int o = LPR; o < 32; o <<= 1) chunks = max(chunks, __shfl_xor_sync(FULL, chunks, o));
+        const bool live = b < brow;
         acc_t acc = 0;
-        for (int ch = 0; ch < chunks; ++ch) {
-            const int cb = start + ch * LPR;
-            const int j = cb + l;  // this lane's block of the chunk
-            uint32_t mp = 0;
-            int col = 0;
-            if (j < end) {
-                mp = __ldcs(map + j);
-                col = __ldcs(idx + j);
+        if (live) {
+            int k = ptr[b] + g;
+            const int end = ptr[b + 1];
+            for (; k + G < end; k += 2 * G) {
+                const int c0 = __ldcs(idx + k), c1 = __ldcs(idx + k + G);
+                const uint32_t m0 = __ldcs(map + k), m1 = __ldcs(map + k + G);
+                const int o0 = __ldcs(voff + k), o1 = __ldcs(voff + k + G);
+                acc = pblock_dot<PREC, SAFE>(val, x, n, o0, m0, q, c0, acc);
+                acc = pblock_dot<PREC, SAFE>(val, x, n, o1, m1, q, c1, acc);
             }
-            const int cnt = __popc(mp);
-            // values of the chunk: [v0, v0 + chunk total); a single-chunk row
-            // knows its range from rvoff alone
-            int incl = cnt;
-#pragma unroll
-            for (int o = 1; o < LPR; o <<= 1) {
-                const int y = __shfl_up_sync(FULL, incl, o, LPR);
-                if (l >= o) incl += y;
-            }
-            const int total = __shfl_sync(FULL, incl, LPR - 1, LPR);
-            for (int v = l; v < total; v += LPR) st[v] = __ldcs(val + v0 + v);
-            const int excl = incl - cnt;
-            __syncwarp();
-            for (int it = 0; it < LPR / G; ++it) {
-                const int jj = it * G + g;  // block of the chunk this 4-lane group takes
-                const uint32_t bm = __shfl_sync(FULL, mp, seg0 + jj);
-                const int bc = __shfl_sync(FULL, col, seg0 + jj);
-                const int bo = __shfl_sync(FULL, excl, seg0 + jj);
-                if (cb + jj < end) {
-                    double xv[4];
-                    load_x4<SAFE>(x, bc, n, xv);
-                    const uint32_t nib = (bm >> (4 * q)) & 0xFu;
-                    int o = bo + __popc(bm & ((1u << (4 * q)) - 1u));
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        acc_t w = (acc_t)0;
-                        if ((nib >> c) & 1u) w = widen<PREC>(st[o++]);
-                        acc = fma(w, (acc_t)xv[c], acc);
-                    }
-                }
-            }
-            v0 += total;
-            __syncwarp();
+            if (k < end) acc = pblock_dot<PREC, SAFE>(val, x, n, __ldcs(voff + k), __ldcs(map + k), q, __ldcs(idx + k), acc);
         }
 #pragma unroll
         for (int o = 4; o < LPR; o <<= 1) acc += __shfl_xor_sync(FULL, acc, o);
-        if (b < brow && g == 0) {
+        if (live && g == 0) {
             const int row = 4 * b + q;
             if (row < m) {
                 const double ax = (double)acc;
@@ -225,10 +189,13 @@ static int packed_lpr(const amgt_pbsr *A)
         const char *ev = getenv("AMGT_PSPMV_LPR");
         env = ev ? atoi(ev) : 0;
     }
-    if (env == 8 || env == 16 || env == 32) return env;
+    if (env == 4 || env == 8 || env == 16 || env == 32) return env;
+    // the 16-value kernel's choice from the mean block-row length, so that
+    // the offset kernel's sums are that kernel's
     const double avg = A->blc_row ? (double)A->blc_num / A->blc_row : 0.0;
-    if (avg <= 3.0) return 8;
-    if (avg <= 12.0) return 16;
+    if (avg <= 4.0) return 4;
+    if (avg <= 10.0) return 8;
+    if (avg <= 20.0) return 16;
     return 32;
 }
 
@@ -245,13 +212,14 @@ static int launch_packed(const amgt_pbsr *A, const double *x, const PEpiArgs &e,
 #define AMGT_P_CASE(L)                                                                                       \
     if (lpr == L) {                                                                                          \
         if (safe)                                                                                            \
-            AMGT_LAUNCH((pspmv_kernel<PREC, L, true, EPI>), grid, 256, 0, s, A->row, A->col, A->blc_row,     \
-                        A->blcPtr, A->blcIdx, A->blcMap, A->rowVoff, A->val, x, e);                          \
+            AMGT_LAUNCH_PDL((pspmv_off_kernel<PREC, L, true, EPI>), grid, 256, 0, s, A->row, A->col,          \
+                            A->blc_row, A->blcPtr, A->blcIdx, A->blcMap, A->blcVoff, A->val, x, e);          \
         else                                                                                                 \
-            AMGT_LAUNCH((pspmv_kernel<PREC, L, false, EPI>), grid, 256, 0, s, A->row, A->col, A->blc_row,    \
-                        A->blcPtr, A->blcIdx, A->blcMap, A->rowVoff, A->val, x, e);                          \
+            AMGT_LAUNCH_PDL((pspmv_off_kernel<PREC, L, false, EPI>), grid, 256, 0, s, A->row, A->col,         \
+                            A->blc_row, A->blcPtr, A->blcIdx, A->blcMap, A->blcVoff, A->val, x, e);          \
         return AMGT_OK;                                                                                      \
     }
+    AMGT_P_CASE(4)
     AMGT_P_CASE(8)
     AMGT_P_CASE(16)
     AMGT_P_CASE(32)
@@ -308,6 +276,7 @@ int amgt_pbsr_free(amgt_pbsr *A, amgt_stream_t stream)
     if (!A) return AMGT_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;
     free_ptr(A->rowVoff, s);
+    free_ptr(A->blcVoff, s);
     free_ptr(A->val, s);
     memset(A, 0, sizeof(*A));
     return AMGT_OK;
@@ -368,7 +337,7 @@ int amgt_bsr_pack(const amgt_bsr *A, int prec, amgt_pbsr *out, amgt_stream_t str
     }
     free_ptr(cnt, s);
     free_ptr(tot, s);
-    free_ptr(voff, s);
+    out->blcVoff = voff;  // each block's first value (the offset kernel's index)
     return AMGT_OK;
 fail:
     free_ptr(cnt, s);

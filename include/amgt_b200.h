@@ -292,7 +292,8 @@ AMGT_API int amgt_bsr_jacobi(int prec, const amgt_bsr *A, const double *inv_l1,
  * packed from, which must outlive it.  At the fill of AMG operators (about
  * 4 of 16) an SpMV reads ~3x fewer bytes than on the 16-value blocks.  No
  * counterpart in the reference (it keeps 16 values per block).  Each block
- * row's values are contiguous, starting at rowVoff[b]. */
+ * row's values are contiguous, starting at rowVoff[b]; block k's start at
+ * blcVoff[k]. */
 typedef struct {
     int row, col, blc_row, blc_col, blc_num;
     int nnz;                  /* stored values (= set bits)            */
@@ -304,6 +305,8 @@ typedef struct {
                                  row's first value                      */
     void *val;                /* [nnz] double / float / half / bf16    */
     int max_blc_per_row;
+    int *blcVoff;             /* [blc_num + 1] offset of each block's
+                                 first value                            */
 } amgt_pbsr;
 
 AMGT_API int amgt_bsr_pack(const amgt_bsr *A, int prec, amgt_pbsr *out, amgt_stream_t stream);

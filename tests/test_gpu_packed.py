@@ -70,6 +70,22 @@ def test_packed_spmv_matches_oracle(amgt, orc, mats, name, prec):
 
 
 
+@pytest.mark.parametrize("name", ["7pt", "varcoef27", "ragged", "interp", "long"])
+def test_packed_fp64_spmv_equals_dense_bitwise(amgt, orc, mats, name):
+    """fp64 packed values: each lane sums its row of every block as the
+    16-value kernel does (same lanes per row, an FMA for every column, zero
+    where the bit is clear), so y is the dense SpMV's bit for bit."""
+    A = mats[name]
+    G = amgt.Bsr.from_csr(*to_dev(A))
+    Pk = G.pack(0)
+    x = torch.from_numpy(orc.rand_uniform(31, A.n)).cuda()
+    y0 = torch.from_numpy(orc.rand_uniform(32, A.m)).cuda()
+    yd, yp = y0.clone(), y0.clone()
+    G.spmv(x, yd, alpha=-0.75, beta=1.25)
+    Pk.spmv(x, yp, alpha=-0.75, beta=1.25)
+    assert torch.equal(yd.view(torch.int64), yp.view(torch.int64))
+
+
 def test_packed_residual_and_jacobi(amgt, orc, mats):
     A = mats["varcoef27"]
     R = orc.csr2bsr(A)
