@@ -742,33 +742,38 @@ def run_amgt(args):
     del Apk
 
     # e2e: host x in, host y out, through the C ABI, every step.  Serial:
-    # upload, product, download on one stream.  Pipelined: steps alternate
-    # between two streams with their own x / y, so one step's y download
-    # (device -> host) runs while the next step's x upload (host -> device)
-    # does; every step still moves its full x and y across PCIe.
+    # upload, product, download on one stream.  Pipelined: steps rotate over
+    # three streams with their own x / y, so one step's y download (device ->
+    # host) and the product run while the next step's x upload (host ->
+    # device) does, and an upload never waits for its stream's previous
+    # download; every step still moves its full x and y across PCIe.
+    NS = 3
     xh = torch.from_numpy(x_host).pin_memory()
-    yhs = [torch.empty(m, dtype=torch.float64).pin_memory() for _ in range(2)]
-    xs, ys = [x, torch.empty_like(x)], [y, torch.empty_like(y)]
-    streams = [stream, torch.cuda.Stream()]
+    yhs = [torch.empty(m, dtype=torch.float64).pin_memory() for _ in range(NS)]
+    xs = [x] + [torch.empty_like(x) for _ in range(NS - 1)]
+    ys = [y] + [torch.empty_like(y) for _ in range(NS - 1)]
+    streams = [stream] + [torch.cuda.Stream() for _ in range(NS - 1)]
 
     def e2e_step(i, pipelined):
-        j = i % 2 if pipelined else 0
+        j = i % NS if pipelined else 0
         with torch.cuda.stream(streams[j]):
             xs[j].copy_(xh, non_blocking=True)
             A.spmv(xs[j], ys[j])
             yhs[j].copy_(ys[j], non_blocking=True)
 
     def e2e_time(pipelined):
-        for i in range(2):
+        for i in range(NS):
             e2e_step(i, pipelined)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         ev0.record(stream)
-        streams[1].wait_event(ev0)
+        for sj in streams[1:]:
+            sj.wait_event(ev0)
         for i in range(args.steps):
             e2e_step(i, pipelined)
-        stream.wait_stream(streams[1])
+        for sj in streams[1:]:
+            stream.wait_stream(sj)
         ev1.record(stream)
         torch.cuda.synchronize()
         return max_over_ranks(ev0.elapsed_time(ev1) / args.steps, device="cuda")
@@ -777,7 +782,7 @@ def run_amgt(args):
     e2e_ms = e2e_time(True)
     e2e_value = whole_job_gbs(nbytes, e2e_ms, world)
     e2e_serial = whole_job_gbs(nbytes, e2e_serial_ms, world)
-    if not torch.equal(yhs[0], yhs[1]):
+    if not all(torch.equal(yhs[0], yh) for yh in yhs[1:]):
         raise RuntimeError("pipelined e2e steps disagree")
 
     # hierarchy: RAP per level and SpMV GB/s per level (not part of `value`);
@@ -920,8 +925,8 @@ def run_amgt(args):
                      else "fallback"},
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": 8 * n,
-                "d2h_bytes_per_step": 8 * m, "pipelined": "two streams: step k's y download overlaps step k+1's "
-                "x upload", "serial_value": round(e2e_serial, 2)},
+                "d2h_bytes_per_step": 8 * m, "pipelined": "three streams: step k's y download and product overlap "
+                "step k+1's x upload", "serial_value": round(e2e_serial, 2)},
         "gpu_launches": int(launches),
         "clocks": clocks,
         "levels": levels,
